@@ -1,0 +1,286 @@
+/* pmp_spray.h -- C ABI of the B200 Lagrangian spray particle update.
+ *
+ * Drop-in for PeleMP's SprayParticleContainer::updateParticles /
+ * calculateSpraySource path (Source/PP_Spray/SprayParticles.cpp:142-502,
+ * Source/PP_Spray/Drag.H:138-441).  Plain C types only: a host program (the
+ * C++ container shim in pelemp_b200/csrc/host, a ctypes binding, an AMReX
+ * build) calls these functions; the library owns the device copy of the
+ * droplets and launches the sm_100a kernels.
+ *
+ * Conventions
+ *  - 3D, AMReX index space; mesh arrays use the AMReX Array4 layout:
+ *    element (i,j,k,n) of a view sits at
+ *      p[(i-lo0) + (j-lo1)*jstride + (k-lo2)*kstride + n*nstride].
+ *  - Units follow the PeleLMeX coupling of the reference (MKS at the mesh
+ *    and droplet interface; PELELM_USE_SPRAY in Source/PP_Spray/SprayFuelData.H:44-54).
+ *  - Every function returns PMP_OK (0) or a PMP_ERR_* code; the library never
+ *    aborts the process (the reference calls amrex::Abort at
+ *    SprayParticles.cpp:350,422 and SprayInterpolation.H:122).
+ *  - One handle must not be used from two host threads at once; separate
+ *    handles are independent.  Kernels run on the stream passed in (NULL =
+ *    the legacy default stream) and the call returns once they completed.
+ */
+#ifndef PMP_SPRAY_H
+#define PMP_SPRAY_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PMP_MAX_FUEL 4
+#ifndef PMP_MAX_SPEC
+#define PMP_MAX_SPEC 8
+#endif
+#define PMP_NAME_LEN 32
+
+/* Particle real components of one droplet, SprayComps at
+ * Source/PP_Spray/SprayFuelData.H:10-19, for F fuels. */
+#define PMP_PSTATE_VEL 0
+#define PMP_PSTATE_T 3
+#define PMP_PSTATE_DIA 4
+#define PMP_PSTATE_Y 5
+#define PMP_PSTATE_NUMDENS(F) (5 + (F))
+#define PMP_PSTATE_N0(F) (6 + (F))
+#define PMP_PSTATE_BM1(F) (7 + (F))
+#define PMP_PSTATE_BM2(F) (8 + (F))
+#define PMP_PSTATE_FILMHGHT(F) (9 + (F))
+#define PMP_PSTATE_NUM(F) (10 + (F))
+#define PMP_MAX_RCOMP PMP_PSTATE_NUM(PMP_MAX_FUEL)
+
+enum pmp_status {
+  PMP_OK = 0,
+  PMP_ERR_LEFT_DOMAIN = 1,  /* droplet outside a non-periodic, non-reflective domain at entry */
+  PMP_ERR_STATE_BOX = 2,    /* interpolation stencil outside the grown state box */
+  PMP_ERR_SOURCE_BOX = 3,   /* deposit cell outside the grown source box */
+  PMP_ERR_UNSUPPORTED = 4,  /* breakup, splash, wall film or EB requested */
+  PMP_ERR_TIMEOUT = 5,      /* a bounded device wait gave up */
+  PMP_ERR_CUDA = 6,         /* a CUDA runtime call failed */
+  PMP_ERR_INVALID = 7,      /* bad argument */
+  PMP_ERR_NO_DEVICE = 8     /* no usable sm_100 device */
+};
+
+/* Precision / method forms of the update (pmp_spray_set_mode). */
+enum pmp_mode {
+  PMP_MODE_FP64 = 0,    /* plain method, FP64 throughout */
+  PMP_MODE_MIXED = 1,   /* FP32 bulk physics, FP64 near d->0 and for deposits */
+  PMP_MODE_LEARNED = 2  /* MLP surrogate for the evaporation sub-step + gate */
+};
+
+/* Boundary designation per face, as updateParticles computes it
+ * (SprayParticles.cpp:200-218): 0 periodic, 1 reflective, -1 outflow. */
+typedef struct pmp_geometry {
+  double plo[3];
+  double phi[3];
+  double dx[3];
+  int domain_lo[3];
+  int domain_hi[3];
+  int bndry_lo[3];
+  int bndry_hi[3];
+} pmp_geometry;
+
+/* Index box, inclusive bounds (amrex::Box, cell-centred). */
+typedef struct pmp_box {
+  int lo[3];
+  int hi[3];
+} pmp_box;
+
+/* View of one box of a multi-component mesh array (amrex::Array4). lo/hi are
+ * the bounds of the allocated (grown) box. */
+typedef struct pmp_box_view {
+  double* p;
+  int lo[3];
+  int hi[3];
+  long long jstride;
+  long long kstride;
+  long long nstride;
+  int ncomp;
+} pmp_box_view;
+
+/* Mirror of SprayComps' mesh component indices (SprayFuelData.H:20-28),
+ * assigned by the caller (SprayParticles.H:386). */
+typedef struct pmp_spray_comps {
+  int rhoIndx;
+  int momIndx;
+  int engIndx;
+  int utempIndx;
+  int specIndx;
+  int rhoSrcIndx;
+  int momSrcIndx;
+  int engSrcIndx;
+  int specSrcIndx;
+} pmp_spray_comps;
+
+/* Mirror of SprayData (SprayFuelData.H:115-143), F = nfuel entries used. */
+typedef struct pmp_spray_data {
+  int nfuel;
+  int mass_trans;
+  int mom_trans;
+  int fixed_parts;
+  int do_splash;
+  int do_breakup;
+  double min_eb_vfrac;
+  double ref_T;
+  double sigma;
+  double wall_T;
+  double theta_c;
+  double dtmod;
+  double body_force[3];
+  double critT[PMP_MAX_FUEL];
+  double boilT[PMP_MAX_FUEL];
+  double cp[PMP_MAX_FUEL];
+  double latent[PMP_MAX_FUEL];
+  double ref_latent[PMP_MAX_FUEL];
+  double psat_coef[4 * PMP_MAX_FUEL];
+  double rho_coef[4 * PMP_MAX_FUEL];
+  double lambda_coef[4 * PMP_MAX_FUEL];
+  double mu_coef[4 * PMP_MAX_FUEL];
+  int indx[PMP_MAX_FUEL];
+  int dep_indx[PMP_MAX_FUEL];
+} pmp_spray_data;
+
+/* The "particles.*" inputs readSprayParams parses
+ * (Source/PP_Spray/SpraySetup.cpp:73-253).  A coefficient array with
+ * ncoef_X[f] == 1 is a constant, == 4 a fit (getInpCoef, SpraySetup.cpp:22-58),
+ * == 0 absent. */
+typedef struct pmp_spray_inputs {
+  int nfuel;
+  char fuel_species[PMP_MAX_FUEL][PMP_NAME_LEN];
+  char dep_fuel_species[PMP_MAX_FUEL][PMP_NAME_LEN]; /* "" = same as fuel */
+  int mass_transfer;
+  int mom_transfer;
+  int fixed_parts;
+  int use_splash_model;
+  int use_breakup_model; /* 0 None, 1 TAB, 2 KHRT */
+  double cfl;            /* particles.cfl, <= 2 */
+  double fuel_ref_temp;
+  double crit_temp[PMP_MAX_FUEL];
+  double boil_temp[PMP_MAX_FUEL];
+  double cp[PMP_MAX_FUEL];
+  double latent[PMP_MAX_FUEL];
+  int ncoef_lambda[PMP_MAX_FUEL];
+  int ncoef_psat[PMP_MAX_FUEL];
+  int ncoef_rho[PMP_MAX_FUEL];
+  int ncoef_mu[PMP_MAX_FUEL];
+  double lambda[PMP_MAX_FUEL][4];
+  double psat[PMP_MAX_FUEL][4];
+  double rho[PMP_MAX_FUEL][4];
+  double mu[PMP_MAX_FUEL][4];
+  double body_force[3];
+} pmp_spray_inputs;
+
+/* Droplets of one box.  layout PMP_LAYOUT_AOS: aos points to n records of
+ *   { double pos[3]; double rdata[10+F]; int id; int cpu; }
+ * (amrex::Particle<NSR_SPR,0> with separate id/cpu words).
+ * layout PMP_LAYOUT_SOA: pos[d] and rdata[c] point to n doubles each, id to
+ * n ints.  id > 0 marks a live droplet (the reference kills with id = -1). */
+enum { PMP_LAYOUT_AOS = 0, PMP_LAYOUT_SOA = 1 };
+enum { PMP_WHERE_HOST = 0, PMP_WHERE_DEVICE = 1 };
+typedef struct pmp_particles {
+  int layout;
+  int where;
+  long long n;
+  void* aos;
+  double* pos[3];
+  double* rdata[PMP_MAX_RCOMP];
+  int* id;
+} pmp_particles;
+
+typedef struct pmp_spray_config {
+  int nfuel;                          /* SPRAY_FUEL_NUM */
+  int nspec;                          /* NUM_SPECIES */
+  char species[PMP_MAX_SPEC][PMP_NAME_LEN]; /* gas species, mechanism order */
+  int device;                         /* CUDA device ordinal */
+} pmp_spray_config;
+
+typedef struct pmp_error_info {
+  int code;
+  int box;
+  long long particle;   /* index within the box, caller order; -1 if none */
+  double pos[3];
+  char message[160];
+} pmp_error_info;
+
+/* Counters of the last update call. */
+typedef struct pmp_stats {
+  long long substeps;        /* droplet-substeps executed (live droplets x sub-cycles) */
+  long long killed;          /* droplets that evaporated or left the domain */
+  long long inner_steps;     /* sum over droplet-substeps of the inner nsub */
+  long long fallback;        /* learned form: droplet-substeps sent to the plain path */
+  double kernel_ms;          /* device time of the update kernels */
+} pmp_stats;
+
+typedef struct pmp_spray pmp_spray;
+
+/* Create a handle on cfg->device.  Replaces the static state of
+ * SprayParticleContainer (SprayParticles.H:388-405). */
+int pmp_spray_create(const pmp_spray_config* cfg, pmp_spray** out);
+int pmp_spray_destroy(pmp_spray* h);
+
+/* readSprayParams + spraySetup (SpraySetup.cpp:73-297): builds SprayData,
+ * maps fuel names to species indices, subtracts h_fuel(ref_T) from the
+ * latent heat (SpraySetup.cpp:284-290) and uploads it.  Rejects breakup and
+ * splash models with PMP_ERR_UNSUPPORTED. */
+int pmp_spray_setup(pmp_spray* h, const pmp_spray_inputs* in);
+/* Install an already built SprayData (the H2D copy at SpraySetup.cpp:294). */
+int pmp_spray_set_data(pmp_spray* h, const pmp_spray_data* data);
+int pmp_spray_get_data(const pmp_spray* h, pmp_spray_data* data);
+
+/* AssignSprayComps (SprayParticles.H:386). */
+int pmp_spray_set_comps(pmp_spray* h, const pmp_spray_comps* comps);
+/* Level geometry and boundary designation (SprayParticles.cpp:183-218). */
+int pmp_spray_set_geometry(pmp_spray* h, const pmp_geometry* geom);
+/* Valid boxes of the level's BoxArray, in ParIter order. */
+int pmp_spray_set_grids(pmp_spray* h, int nboxes, const pmp_box* boxes);
+
+/* Hand the droplets of box `box` to the library (copied; the library keeps
+ * them on the device, sorted by cell, and remembers the caller's order). */
+int pmp_spray_set_particles(pmp_spray* h, int box, const pmp_particles* p);
+/* Copy the droplets of box `box` back in the caller's order; out->n must be
+ * the count given to set_particles and out's arrays sized for it. */
+int pmp_spray_get_particles(pmp_spray* h, int box, pmp_particles* out);
+int pmp_spray_num_particles(const pmp_spray* h, int box, long long* n);
+
+/* SprayParticleContainer::updateParticles (SprayParticles.cpp:142-502) for
+ * all boxes in one call.  state[b] / source[b] are DEVICE views of box b's
+ * state and source fabs; deposits are added to source (callers zero it, as
+ * transferSource does at SprayParticles.H:294).  ltransparm is not needed:
+ * the transport model is built into the handle. */
+int pmp_spray_update(
+  pmp_spray* h, const pmp_box_view* state, const pmp_box_view* source,
+  int nboxes, double flow_dt, double time, int state_ghosts,
+  int source_ghosts, int is_virt, int is_ghost, int do_move,
+  double spray_cfl_lev, void* stream);
+
+/* Same call with HOST views: the state is copied to the device, the source
+ * deposits are added into the host source arrays after the update. */
+int pmp_spray_update_host(
+  pmp_spray* h, const pmp_box_view* state, const pmp_box_view* source,
+  int nboxes, double flow_dt, double time, int state_ghosts,
+  int source_ghosts, int is_virt, int is_ghost, int do_move,
+  double spray_cfl_lev, void* stream);
+
+/* moveKickDrift / moveKick (SprayParticles.cpp:37-87). */
+int pmp_spray_move_kick_drift(
+  pmp_spray* h, const pmp_box_view* state, const pmp_box_view* source,
+  int nboxes, double dt, double time, int is_virt, int is_ghost,
+  int state_ghosts, int source_ghosts, int do_move, double spray_cfl_lev,
+  void* stream);
+int pmp_spray_move_kick(
+  pmp_spray* h, const pmp_box_view* state, const pmp_box_view* source,
+  int nboxes, double dt, double time, int is_virt, int is_ghost,
+  int state_ghosts, int source_ghosts, double spray_cfl_lev, void* stream);
+
+/* Method form (enum pmp_mode), default PMP_MODE_FP64. */
+int pmp_spray_set_mode(pmp_spray* h, int mode);
+
+int pmp_spray_last_error(const pmp_spray* h, pmp_error_info* info);
+int pmp_spray_get_stats(const pmp_spray* h, pmp_stats* stats);
+
+/* Library version string. */
+const char* pmp_spray_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PMP_SPRAY_H */

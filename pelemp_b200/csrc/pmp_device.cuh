@@ -1,0 +1,116 @@
+// pmp_device.cuh -- device-side data structures of the spray update.
+//
+// KParams is the single __grid_constant__ argument of every update kernel:
+// the handle's mechanism (species reordered so that fuel f is species f),
+// the SprayData constants, the level geometry and the per-call settings.
+// BoxEntry describes one AMReX box: its state and source Array4 views and its
+// droplet range in the library's cell-sorted SoA.
+#pragma once
+
+#include <cstdint>
+
+#include "../../include/pmp_spray.h"
+
+namespace pmp {
+
+constexpr int kMaxSpec = PMP_MAX_SPEC;
+constexpr int kMaxFuel = PMP_MAX_FUEL;
+
+// SprayUnits, PeleLMeX branch (Source/PP_Spray/SprayFuelData.H:44-54,66)
+constexpr double kRuConv = 1.E-7;
+constexpr double kEngConv = 1.E-4;
+constexpr double kRhoConv = 1.E3;
+constexpr double kMassConv = 1.E-3;
+constexpr double kRhodConv = 0.1;
+constexpr double kMuConv = 0.1;
+constexpr double kLambdaConv = 1.E-5;
+constexpr double kPresConv = 0.1;
+constexpr double kRuCgs = 8.31446261815324e7;
+constexpr double kPatmCgs = 1013250.0;
+
+// Species in the caller's (mechanism) order.
+struct DevMech {
+  double mw_kg[kMaxSpec];            // kg/mol (gpv.mw after mass_conv)
+  double mw_g[kMaxSpec];             // g/mol (the transport model's W)
+  double ru_w[kMaxSpec];             // RU_cgs / W_gmol
+  double cp[kMaxSpec][5];            // cp/R polynomial
+  double hc[kMaxSpec][6];            // h/(RT) polynomial + a5
+  double mu[kMaxSpec][4];            // ln mu(lnT), CGS
+  double lam[kMaxSpec][4];           // ln lambda(lnT), CGS
+  double dbin[kMaxFuel][kMaxSpec][4];// ln(P D_{indx[f],j})(lnT), fuel rows
+};
+
+struct DevFuel {
+  double critT[kMaxFuel];
+  double boilT[kMaxFuel];
+  double cp[kMaxFuel];
+  double latent[kMaxFuel];
+  double ref_latent[kMaxFuel];
+  double psat_coef[4 * kMaxFuel];
+  double rho_coef[4 * kMaxFuel];
+  double hboil_ref[kMaxFuel];  // ref_latent * ((critT-ref_T)/(critT-boilT))^-0.38
+  int indx[kMaxFuel];          // gas species of fuel f
+  int dep[kMaxFuel];           // deposit species of fuel f
+  double ln10;                 // pmp_log(10.), as pmp_pow(10., y) uses it
+  double ref_T;
+  double dtmod;
+  double body_force[3];
+  int mass_trans;
+  int mom_trans;
+  int fixed_parts;
+};
+
+struct BoxEntry {
+  const double* st;          // state fab, component 0
+  double* sr;                // source fab, component 0
+  int st_lo[3];
+  int sr_lo[3];
+  long long st_js, st_ks, st_ns;
+  long long sr_js, sr_ks, sr_ns;
+  int state_lo[3], state_hi[3];   // tilebox grown by state_ghosts
+  int src_lo[3], src_hi[3];       // tilebox grown by source_ghosts
+  int sr_alo[3], sr_ahi[3];       // allocated bounds of the source view
+  int at_bounds;
+  int pad;
+  long long p_begin, p_end;       // droplet slots of this box
+};
+
+// Device status word block, zeroed before each update.
+struct DevStatus {
+  int code;
+  int box;
+  long long slot;
+  unsigned long long substeps;
+  unsigned long long killed;
+  unsigned long long inner;
+  unsigned long long fallback;
+};
+
+// SoA droplet store: ncomp double arrays of length cap, then ids.
+struct DevParts {
+  double* pos[3];
+  double* rd[PMP_MAX_RCOMP];
+  int* id;
+};
+
+struct KParams {
+  DevMech m;
+  DevFuel f;
+  DevParts parts;
+  // geometry
+  double plo[3], phi[3], dx[3], dxi[3];
+  double inv_vol;
+  int bndry_lo[3], bndry_hi[3];
+  // state / source component offsets (caller's mesh layout)
+  int c_rho, c_mom, c_T, c_spec;
+  int s_rho, s_mom, s_eng, s_spec;
+  // call settings
+  double flow_dt, sub_dt;
+  int num_iter, do_move, is_ghost, nboxes;
+  const BoxEntry* boxes;
+  const int* cta_box;
+  const long long* cta_start;
+  DevStatus* status;
+};
+
+}  // namespace pmp

@@ -1,0 +1,1158 @@
+// pmp_spray.cu -- implementation of the C ABI in include/pmp_spray.h.
+//
+// The handle replaces SprayParticleContainer's static state
+// (Source/PP_Spray/SprayParticles.H:388-405) and its particle tiles.  Droplets
+// handed in per box are copied to the device, sorted by the cell that holds
+// them, and packed into one structure-of-arrays; the permutation back to the
+// caller's order is kept.  pmp_spray_update is updateParticles
+// (SprayParticles.cpp:142-502) for all boxes in one launch.
+#include <cuda_runtime.h>
+
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "phys/pmp_thermo.h"
+#include "pmp_device.cuh"
+#include "spray_fp64.cuh"
+
+using pmp::BoxEntry;
+using pmp::DevStatus;
+using pmp::KParams;
+
+namespace {
+
+constexpr int kBlock = 128;
+constexpr int kSortPad = 8;  // cells of margin in the sort key around a box
+
+struct BoxStore {
+  long long n = 0;
+  double* d = nullptr;  // (3 + NR) * n doubles, sorted by cell
+  int* id = nullptr;
+  long long* perm = nullptr;  // sorted slot -> caller index
+};
+
+}  // namespace
+
+struct pmp_spray {
+  int device = 0;
+  int nfuel = 0;
+  int nspec = 0;
+  char species[PMP_MAX_SPEC][PMP_NAME_LEN];
+  pmp_mech mech;
+  pmp_spray_data data;
+  bool have_data = false;
+  pmp_spray_comps comps;
+  bool have_comps = false;
+  pmp_geometry geom;
+  bool have_geom = false;
+  std::vector<pmp_box> boxes;
+  int mode = PMP_MODE_FP64;
+  pmp::DevMech dmech;
+  pmp::DevFuel dfuel;
+  // per-box staged droplets (before packing)
+  std::vector<BoxStore> staged;
+  std::vector<bool> box_set;
+  // packed droplets
+  bool packed = false;
+  long long total = 0;
+  double* soa = nullptr;  // (3 + NR) arrays of length total
+  int* ids = nullptr;
+  long long* perm = nullptr;
+  std::vector<long long> box_begin;
+  int ncta = 0;
+  int* d_cta_box = nullptr;
+  long long* d_cta_start = nullptr;
+  BoxEntry* d_boxes = nullptr;
+  BoxEntry* h_boxes = nullptr;
+  int boxes_cap = 0;
+  DevStatus* d_status = nullptr;
+  DevStatus* h_status = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  pmp_error_info last_err;
+  pmp_stats stats;
+  // device mirrors of host views for pmp_spray_update_host
+  std::vector<double*> stage_state, stage_src;
+  std::vector<size_t> stage_state_n, stage_src_n;
+  int nr() const { return PMP_PSTATE_NUM(nfuel); }
+  int ncomp() const { return 3 + nr(); }
+};
+
+namespace {
+
+int set_err(pmp_spray* h, int code, const char* msg, int box = -1, long long particle = -1)
+{
+  if (h) {
+    memset(&h->last_err, 0, sizeof(h->last_err));
+    h->last_err.code = code;
+    h->last_err.box = box;
+    h->last_err.particle = particle;
+    snprintf(h->last_err.message, sizeof(h->last_err.message), "%s", msg);
+  }
+  return code;
+}
+
+#define PMP_CUDA(h, call)                                                   \
+  do {                                                                      \
+    cudaError_t e_ = (call);                                                \
+    if (e_ != cudaSuccess) {                                                \
+      char b_[160];                                                         \
+      snprintf(b_, sizeof(b_), "%s: %s", #call, cudaGetErrorString(e_));    \
+      return set_err((h), PMP_ERR_CUDA, b_);                                \
+    }                                                                       \
+  } while (0)
+
+// --------------------------------------------------------------------------
+// small data-movement kernels
+
+__global__ void k_aos_to_soa(const char* aos, long long n, int nr, double* soa, int* ids)
+{
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) {
+    return;
+  }
+  const size_t rec = sizeof(double) * (3 + nr) + 2 * sizeof(int);
+  const double* r = reinterpret_cast<const double*>(aos + i * rec);
+  for (int c = 0; c < 3 + nr; ++c) {
+    soa[c * n + i] = r[c];
+  }
+  ids[i] = *reinterpret_cast<const int*>(r + 3 + nr);
+}
+
+__global__ void k_soa_to_aos(const double* soa, const int* ids, long long n, int nr, char* aos)
+{
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) {
+    return;
+  }
+  const size_t rec = sizeof(double) * (3 + nr) + 2 * sizeof(int);
+  double* r = reinterpret_cast<double*>(aos + i * rec);
+  for (int c = 0; c < 3 + nr; ++c) {
+    r[c] = soa[c * n + i];
+  }
+  int* ip = reinterpret_cast<int*>(r + 3 + nr);
+  ip[0] = ids[i];
+  ip[1] = 0;
+}
+
+__global__ void k_cell_keys(
+  const double* x, const double* y, const double* z, long long n, double plo0, double plo1,
+  double plo2, double dxi0, double dxi1, double dxi2, int lo0, int lo1, int lo2, int nx, int ny,
+  int nz, unsigned* keys, long long* idx)
+{
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) {
+    return;
+  }
+  int c[3];
+  const double p[3] = {x[i], y[i], z[i]};
+  const double pl[3] = {plo0, plo1, plo2};
+  const double di[3] = {dxi0, dxi1, dxi2};
+  const int lo[3] = {lo0, lo1, lo2};
+  const int ext[3] = {nx, ny, nz};
+  for (int d = 0; d < 3; ++d) {
+    const double l = __dmul_rn(__dsub_rn(p[d], pl[d]), di[d]);
+    int v = static_cast<int>(floor(l)) - lo[d] + kSortPad;
+    v = v < 0 ? 0 : (v >= ext[d] ? ext[d] - 1 : v);
+    c[d] = v;
+  }
+  keys[i] = (unsigned)((c[2] * (long long)ext[1] + c[1]) * ext[0] + c[0]);
+  idx[i] = i;
+}
+
+// dst[c][s] = src[c][perm[s]] for every component; ids likewise
+__global__ void k_gather(
+  const double* src, const int* sid, const long long* perm, long long n, int ncomp, double* dst,
+  int* did)
+{
+  const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (s >= n) {
+    return;
+  }
+  const long long j = perm[s];
+  for (int c = 0; c < ncomp; ++c) {
+    dst[c * n + s] = src[c * n + j];
+  }
+  did[s] = sid[j];
+}
+
+// dst[c][perm[s]] = src[c * stride + s]: back to the caller's order
+__global__ void k_unsort(
+  const double* src, long long stride, const int* sid, const long long* perm, long long n, int ncomp,
+  double* dst, int* did)
+{
+  const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (s >= n) {
+    return;
+  }
+  const long long j = perm[s];
+  for (int c = 0; c < ncomp; ++c) {
+    dst[c * n + j] = src[c * stride + s];
+  }
+  did[j] = sid[s];
+}
+
+inline unsigned nblk(long long n, int b = 256) { return (unsigned)((n + b - 1) / b); }
+
+// --------------------------------------------------------------------------
+// handle helpers
+
+void free_store(BoxStore& s)
+{
+  cudaFree(s.d);
+  cudaFree(s.id);
+  cudaFree(s.perm);
+  s = BoxStore{};
+}
+
+void free_packed(pmp_spray* h)
+{
+  cudaFree(h->soa);
+  cudaFree(h->ids);
+  cudaFree(h->perm);
+  cudaFree(h->d_cta_box);
+  cudaFree(h->d_cta_start);
+  h->soa = nullptr;
+  h->ids = nullptr;
+  h->perm = nullptr;
+  h->d_cta_box = nullptr;
+  h->d_cta_start = nullptr;
+  h->packed = false;
+  h->ncta = 0;
+}
+
+// DevMech (species in mechanism order) and DevFuel from the mechanism and
+// SprayData.
+int build_device_tables(pmp_spray* h)
+{
+  const pmp_spray_data& d = h->data;
+  const int NF = h->nfuel;
+  const int NS = h->nspec;
+  for (int f = 0; f < NF; ++f) {
+    if (d.indx[f] < 0 || d.indx[f] >= NS || d.dep_indx[f] < 0 || d.dep_indx[f] >= NS) {
+      return set_err(h, PMP_ERR_INVALID, "fuel species index out of range");
+    }
+    for (int g = 0; g < f; ++g) {
+      if (d.indx[g] == d.indx[f]) {
+        return set_err(h, PMP_ERR_INVALID, "two fuels map to the same gas species");
+      }
+    }
+  }
+  pmp::DevMech& m = h->dmech;
+  memset(&m, 0, sizeof(m));
+  for (int k = 0; k < NS; ++k) {
+    m.mw_g[k] = h->mech.mw[k];
+    m.mw_kg[k] = h->mech.mw[k] * pmp::kMassConv;
+    m.ru_w[k] = PMP_RU_CGS / h->mech.mw[k];
+    for (int n = 0; n < 5; ++n) {
+      m.cp[k][n] = h->mech.cp[k][n];
+    }
+    for (int n = 0; n < 6; ++n) {
+      m.hc[k][n] = h->mech.hc[k][n];
+    }
+    for (int n = 0; n < 4; ++n) {
+      m.mu[k][n] = h->mech.mu[k][n];
+      m.lam[k][n] = h->mech.lam[k][n];
+    }
+  }
+  for (int f = 0; f < NF; ++f) {
+    for (int j = 0; j < NS; ++j) {
+      for (int n = 0; n < 4; ++n) {
+        m.dbin[f][j][n] = h->mech.dbin[d.indx[f]][j][n];
+      }
+    }
+  }
+  pmp::DevFuel& F = h->dfuel;
+  memset(&F, 0, sizeof(F));
+  for (int f = 0; f < NF; ++f) {
+    F.critT[f] = d.critT[f];
+    F.boilT[f] = d.boilT[f];
+    F.cp[f] = d.cp[f];
+    F.latent[f] = d.latent[f];
+    F.ref_latent[f] = d.ref_latent[f];
+    for (int c = 0; c < 4; ++c) {
+      F.psat_coef[4 * f + c] = d.psat_coef[4 * f + c];
+      F.rho_coef[4 * f + c] = d.rho_coef[4 * f + c];
+    }
+    // Hboil_ref of SprayData::calcBoilT (SprayFuelData.H:190-192): constant per fuel
+    F.hboil_ref[f] =
+      d.ref_latent[f] * pmp_pow((d.critT[f] - d.ref_T) / (d.critT[f] - d.boilT[f]), -0.38);
+    F.indx[f] = d.indx[f];
+    F.dep[f] = d.dep_indx[f];
+  }
+  F.ln10 = pmp_log(10.);
+  F.ref_T = d.ref_T;
+  F.dtmod = d.dtmod;
+  for (int i = 0; i < 3; ++i) {
+    F.body_force[i] = d.body_force[i];
+  }
+  F.mass_trans = d.mass_trans;
+  F.mom_trans = d.mom_trans;
+  F.fixed_parts = d.fixed_parts;
+  return PMP_OK;
+}
+
+int ensure_boxes_cap(pmp_spray* h, int n)
+{
+  if (n <= h->boxes_cap) {
+    return PMP_OK;
+  }
+  cudaFree(h->d_boxes);
+  cudaFreeHost(h->h_boxes);
+  h->d_boxes = nullptr;
+  h->h_boxes = nullptr;
+  PMP_CUDA(h, cudaMalloc(&h->d_boxes, sizeof(BoxEntry) * n));
+  PMP_CUDA(h, cudaMallocHost(&h->h_boxes, sizeof(BoxEntry) * n));
+  h->boxes_cap = n;
+  return PMP_OK;
+}
+
+int pack(pmp_spray* h)
+{
+  if (h->packed) {
+    return PMP_OK;
+  }
+  const int nb = (int)h->boxes.size();
+  for (int b = 0; b < nb; ++b) {
+    if (!h->box_set[b]) {
+      return set_err(h, PMP_ERR_INVALID, "set_particles was not called for every box", b);
+    }
+  }
+  free_packed(h);
+  const int nc = h->ncomp();
+  long long total = 0;
+  h->box_begin.assign(nb + 1, 0);
+  for (int b = 0; b < nb; ++b) {
+    h->box_begin[b] = total;
+    total += h->staged[b].n;
+  }
+  h->box_begin[nb] = total;
+  h->total = total;
+  const long long cap = total > 0 ? total : 1;
+  PMP_CUDA(h, cudaMalloc(&h->soa, sizeof(double) * nc * cap));
+  PMP_CUDA(h, cudaMalloc(&h->ids, sizeof(int) * cap));
+  PMP_CUDA(h, cudaMalloc(&h->perm, sizeof(long long) * cap));
+  for (int b = 0; b < nb; ++b) {
+    BoxStore& s = h->staged[b];
+    const long long o = h->box_begin[b];
+    if (s.n > 0) {
+      PMP_CUDA(h, cudaMemcpy2D(h->soa + o, sizeof(double) * cap, s.d, sizeof(double) * s.n,
+                               sizeof(double) * s.n, nc, cudaMemcpyDeviceToDevice));
+      PMP_CUDA(h, cudaMemcpy(h->ids + o, s.id, sizeof(int) * s.n, cudaMemcpyDeviceToDevice));
+      PMP_CUDA(h, cudaMemcpy(h->perm + o, s.perm, sizeof(long long) * s.n, cudaMemcpyDeviceToDevice));
+    }
+    free_store(s);
+  }
+  // CTA -> (box, first slot) map
+  std::vector<int> cb;
+  std::vector<long long> cs;
+  for (int b = 0; b < nb; ++b) {
+    for (long long o = h->box_begin[b]; o < h->box_begin[b + 1]; o += kBlock) {
+      cb.push_back(b);
+      cs.push_back(o);
+    }
+  }
+  h->ncta = (int)cb.size();
+  if (h->ncta > 0) {
+    PMP_CUDA(h, cudaMalloc(&h->d_cta_box, sizeof(int) * h->ncta));
+    PMP_CUDA(h, cudaMalloc(&h->d_cta_start, sizeof(long long) * h->ncta));
+    PMP_CUDA(h, cudaMemcpy(h->d_cta_box, cb.data(), sizeof(int) * h->ncta, cudaMemcpyHostToDevice));
+    PMP_CUDA(h, cudaMemcpy(h->d_cta_start, cs.data(), sizeof(long long) * h->ncta, cudaMemcpyHostToDevice));
+  }
+  h->packed = true;
+  return PMP_OK;
+}
+
+// Copy the droplets of box b (packed or staged) back into a device SoA of
+// caller order: out_d (nc * n doubles), out_id (n ints).
+int unsort_box(pmp_spray* h, int b, double* out_d, int* out_id, long long n)
+{
+  const int nc = h->ncomp();
+  if (n == 0) {
+    return PMP_OK;
+  }
+  if (h->packed) {
+    const long long o = h->box_begin[b];
+    k_unsort<<<nblk(n), 256>>>(h->soa + o, h->total, h->ids + o, h->perm + o, n, nc, out_d, out_id);
+  } else {
+    BoxStore& s = h->staged[b];
+    k_unsort<<<nblk(n), 256>>>(s.d, s.n, s.id, s.perm, n, nc, out_d, out_id);
+  }
+  PMP_CUDA(h, cudaGetLastError());
+  return PMP_OK;
+}
+
+bool view_covers(const pmp_box_view& v, const int* lo, const int* hi, int ncomp_needed)
+{
+  if (v.p == nullptr || v.ncomp < ncomp_needed) {
+    return false;
+  }
+  for (int d = 0; d < 3; ++d) {
+    if (lo[d] < v.lo[d] || hi[d] > v.hi[d]) {
+      return false;
+    }
+  }
+  return true;
+}
+
+size_t view_extent(const pmp_box_view& v)
+{
+  const long long nx = v.hi[0] - v.lo[0] + 1;
+  const long long ny = v.hi[1] - v.lo[1] + 1;
+  const long long nz = v.hi[2] - v.lo[2] + 1;
+  return (size_t)((v.ncomp - 1) * v.nstride + (nz - 1) * v.kstride + (ny - 1) * v.jstride + nx);
+}
+
+// tile_at_bndry (Source/PP_Spray/WallFunctions.H:8-35)
+int tile_at_bndry(const pmp_box& b, const pmp_geometry& g)
+{
+  bool inside = true;
+  for (int d = 0; d < 3; ++d) {
+    if (b.lo[d] - 1 < g.domain_lo[d] || b.hi[d] + 1 > g.domain_hi[d]) {
+      inside = false;
+    }
+  }
+  if (inside) {
+    return 0;
+  }
+  int at = 0;
+  for (int d = 0; d < 3; ++d) {
+    const bool lo_out = b.lo[d] - 1 < g.domain_lo[d];
+    const bool hi_out = b.hi[d] + 1 > g.domain_hi[d];
+    if ((lo_out && g.bndry_lo[d] != 0) || (hi_out && g.bndry_hi[d] != 0)) {
+      at = 1;
+    }
+  }
+  return at;
+}
+
+template <int NS, int NF>
+void launch_fp64(const KParams& P, int ncta, cudaStream_t st)
+{
+  pmp::spray_update_fp64<NS, NF, kBlock><<<ncta, kBlock, 0, st>>>(P);
+}
+
+int dispatch_fp64(int ns, int nf, const KParams& P, int ncta, cudaStream_t st)
+{
+#define PMP_CASE(S, F)          \
+  if (ns == S && nf == F) {     \
+    launch_fp64<S, F>(P, ncta, st); \
+    return PMP_OK;              \
+  }
+  PMP_CASE(3, 1)
+  PMP_CASE(5, 1)
+  PMP_CASE(5, 2)
+  PMP_CASE(4, 1)
+  PMP_CASE(4, 2)
+#undef PMP_CASE
+  return PMP_ERR_UNSUPPORTED;
+}
+
+int do_update(
+  pmp_spray* h, const pmp_box_view* state, const pmp_box_view* source, int nboxes,
+  double flow_dt, int state_ghosts, int source_ghosts, int is_virt, int is_ghost, int do_move,
+  double spray_cfl_lev, cudaStream_t st)
+{
+  (void)is_virt;
+  memset(&h->stats, 0, sizeof(h->stats));
+  if (!h->have_data || !h->have_comps || !h->have_geom) {
+    return set_err(h, PMP_ERR_INVALID, "setup, comps and geometry must be set before update");
+  }
+  if (nboxes != (int)h->boxes.size()) {
+    return set_err(h, PMP_ERR_INVALID, "nboxes differs from the grids given to set_grids");
+  }
+  if (h->mode != PMP_MODE_FP64) {
+    return set_err(h, PMP_ERR_UNSUPPORTED, "this method form is not available");
+  }
+  if (h->data.do_breakup != 0 || h->data.do_splash) {
+    return set_err(h, PMP_ERR_UNSUPPORTED, "breakup and splash models are not supported");
+  }
+  if (!(flow_dt > 0.)) {
+    return set_err(h, PMP_ERR_INVALID, "flow_dt must be positive");
+  }
+  int rc = pack(h);
+  if (rc != PMP_OK) {
+    return rc;
+  }
+  rc = ensure_boxes_cap(h, nboxes);
+  if (rc != PMP_OK) {
+    return rc;
+  }
+  const pmp_spray_comps& c = h->comps;
+  const int NS = h->nspec;
+  const int NF = h->nfuel;
+  const int need_state = 1 + std::max({c.rhoIndx, c.momIndx + 2, c.utempIndx, c.specIndx + NS - 1});
+  const int need_src = 1 + std::max({c.rhoSrcIndx, c.momSrcIndx + 2, c.engSrcIndx, c.specSrcIndx + NF - 1});
+  for (int b = 0; b < nboxes; ++b) {
+    const pmp_box& bx = h->boxes[b];
+    BoxEntry& e = h->h_boxes[b];
+    memset(&e, 0, sizeof(e));
+    for (int d = 0; d < 3; ++d) {
+      e.state_lo[d] = bx.lo[d] - state_ghosts;
+      e.state_hi[d] = bx.hi[d] + state_ghosts;
+      e.src_lo[d] = bx.lo[d] - source_ghosts;
+      e.src_hi[d] = bx.hi[d] + source_ghosts;
+    }
+    if (!view_covers(state[b], e.state_lo, e.state_hi, need_state)) {
+      return set_err(h, PMP_ERR_INVALID, "state view does not cover the grown box", b);
+    }
+    if (!view_covers(source[b], e.src_lo, e.src_hi, need_src)) {
+      return set_err(h, PMP_ERR_INVALID, "source view does not cover the grown box", b);
+    }
+    e.st = state[b].p;
+    e.sr = source[b].p;
+    for (int d = 0; d < 3; ++d) {
+      e.st_lo[d] = state[b].lo[d];
+      e.sr_lo[d] = source[b].lo[d];
+      e.sr_alo[d] = source[b].lo[d];
+      e.sr_ahi[d] = source[b].hi[d];
+    }
+    e.st_js = state[b].jstride;
+    e.st_ks = state[b].kstride;
+    e.st_ns = state[b].nstride;
+    e.sr_js = source[b].jstride;
+    e.sr_ks = source[b].kstride;
+    e.sr_ns = source[b].nstride;
+    e.at_bounds = tile_at_bndry(bx, h->geom);
+    e.p_begin = h->box_begin[b];
+    e.p_end = h->box_begin[b + 1];
+  }
+  PMP_CUDA(h, cudaMemcpyAsync(h->d_boxes, h->h_boxes, sizeof(BoxEntry) * nboxes,
+                              cudaMemcpyHostToDevice, st));
+  PMP_CUDA(h, cudaMemsetAsync(h->d_status, 0, sizeof(DevStatus), st));
+  KParams P;
+  memset(&P, 0, sizeof(P));
+  P.m = h->dmech;
+  P.f = h->dfuel;
+  const long long T = h->total;
+  for (int d = 0; d < 3; ++d) {
+    P.parts.pos[d] = h->soa + (long long)d * T;
+  }
+  for (int r = 0; r < h->nr(); ++r) {
+    P.parts.rd[r] = h->soa + (long long)(3 + r) * T;
+  }
+  P.parts.id = h->ids;
+  const pmp_geometry& g = h->geom;
+  for (int d = 0; d < 3; ++d) {
+    P.plo[d] = g.plo[d];
+    P.phi[d] = g.phi[d];
+    P.dx[d] = g.dx[d];
+    P.dxi[d] = 1. / g.dx[d];
+    P.bndry_lo[d] = g.bndry_lo[d];
+    P.bndry_hi[d] = g.bndry_hi[d];
+  }
+  const double vol = g.dx[0] * g.dx[1] * g.dx[2];
+  P.inv_vol = 1. / vol;
+  P.c_rho = c.rhoIndx;
+  P.c_mom = c.momIndx;
+  P.c_T = c.utempIndx;
+  P.c_spec = c.specIndx;
+  P.s_rho = c.rhoSrcIndx;
+  P.s_mom = c.momSrcIndx;
+  P.s_eng = c.engSrcIndx;
+  P.s_spec = c.specSrcIndx;
+  // sub-cycling (SprayParticles.cpp:221-229)
+  const double sub_cfl = 0.5;
+  P.flow_dt = flow_dt;
+  P.sub_dt = flow_dt;
+  P.num_iter = 1;
+  if (do_move && spray_cfl_lev > sub_cfl) {
+    P.num_iter = static_cast<int>(std::ceil(spray_cfl_lev / sub_cfl));
+    P.sub_dt = flow_dt / static_cast<double>(P.num_iter);
+  }
+  P.do_move = do_move;
+  P.is_ghost = is_ghost;
+  P.nboxes = nboxes;
+  P.boxes = h->d_boxes;
+  P.cta_box = h->d_cta_box;
+  P.cta_start = h->d_cta_start;
+  P.status = h->d_status;
+  PMP_CUDA(h, cudaEventRecord(h->ev0, st));
+  if (h->ncta > 0) {
+    rc = dispatch_fp64(NS, NF, P, h->ncta, st);
+    if (rc != PMP_OK) {
+      return set_err(h, rc, "no kernel for this species / fuel count");
+    }
+    PMP_CUDA(h, cudaGetLastError());
+  }
+  PMP_CUDA(h, cudaEventRecord(h->ev1, st));
+  PMP_CUDA(h, cudaMemcpyAsync(h->h_status, h->d_status, sizeof(DevStatus), cudaMemcpyDeviceToHost, st));
+  PMP_CUDA(h, cudaStreamSynchronize(st));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+  h->stats.kernel_ms = ms;
+  h->stats.substeps = (long long)h->h_status->substeps;
+  h->stats.killed = (long long)h->h_status->killed;
+  h->stats.inner_steps = (long long)h->h_status->inner;
+  h->stats.fallback = (long long)h->h_status->fallback;
+  if (h->h_status->code != 0) {
+    const int b = h->h_status->box;
+    long long caller = -1;
+    const long long slot = h->h_status->slot;
+    if (slot >= 0 && slot < h->total) {
+      cudaMemcpy(&caller, h->perm + slot, sizeof(long long), cudaMemcpyDeviceToHost);
+    }
+    double pos[3] = {0, 0, 0};
+    for (int d = 0; d < 3; ++d) {
+      cudaMemcpy(&pos[d], h->soa + (long long)d * T + slot, sizeof(double), cudaMemcpyDeviceToHost);
+    }
+    static const char* names[] = {"ok", "droplet left the domain", "state box too small",
+                                  "source box too small", "unsupported droplet state", "timeout"};
+    const int code = h->h_status->code;
+    set_err(h, code, code < 6 ? names[code] : "error", b, caller);
+    for (int d = 0; d < 3; ++d) {
+      h->last_err.pos[d] = pos[d];
+    }
+    return code;
+  }
+  memset(&h->last_err, 0, sizeof(h->last_err));
+  h->last_err.particle = -1;
+  return PMP_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+
+extern "C" {
+
+const char* pmp_spray_version(void) { return "pmp-spray-b200 0.1 (sm_100a)"; }
+
+int pmp_spray_create(const pmp_spray_config* cfg, pmp_spray** out)
+{
+  if (!cfg || !out) {
+    return PMP_ERR_INVALID;
+  }
+  *out = nullptr;
+  if (cfg->nfuel < 1 || cfg->nfuel > PMP_MAX_FUEL || cfg->nspec < 1 || cfg->nspec > PMP_MAX_SPEC) {
+    return PMP_ERR_INVALID;
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || cfg->device < 0 || cfg->device >= ndev) {
+    cudaGetLastError();
+    return PMP_ERR_NO_DEVICE;
+  }
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, cfg->device) != cudaSuccess || prop.major != 10) {
+    return PMP_ERR_NO_DEVICE;
+  }
+  pmp_spray* h = new pmp_spray();
+  h->device = cfg->device;
+  h->nfuel = cfg->nfuel;
+  h->nspec = cfg->nspec;
+  int idx[PMP_MAX_SPEC];
+  for (int k = 0; k < cfg->nspec; ++k) {
+    memcpy(h->species[k], cfg->species[k], PMP_NAME_LEN);
+    h->species[k][PMP_NAME_LEN - 1] = 0;
+    idx[k] = pmp_db_lookup(h->species[k]);
+    if (idx[k] < 0) {
+      delete h;
+      return PMP_ERR_INVALID;
+    }
+  }
+  if (pmp_mech_build(&h->mech, cfg->nspec, idx) != 0) {
+    delete h;
+    return PMP_ERR_INVALID;
+  }
+  memset(&h->last_err, 0, sizeof(h->last_err));
+  memset(&h->stats, 0, sizeof(h->stats));
+  if (cudaSetDevice(h->device) != cudaSuccess ||
+      cudaMalloc(&h->d_status, sizeof(DevStatus)) != cudaSuccess ||
+      cudaMallocHost(&h->h_status, sizeof(DevStatus)) != cudaSuccess ||
+      cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess) {
+    delete h;
+    return PMP_ERR_CUDA;
+  }
+  *out = h;
+  return PMP_OK;
+}
+
+int pmp_spray_destroy(pmp_spray* h)
+{
+  if (!h) {
+    return PMP_OK;
+  }
+  cudaSetDevice(h->device);
+  for (auto& s : h->staged) {
+    free_store(s);
+  }
+  free_packed(h);
+  for (double* p : h->stage_state) {
+    cudaFree(p);
+  }
+  for (double* p : h->stage_src) {
+    cudaFree(p);
+  }
+  cudaFree(h->d_boxes);
+  cudaFreeHost(h->h_boxes);
+  cudaFree(h->d_status);
+  cudaFreeHost(h->h_status);
+  if (h->ev0) {
+    cudaEventDestroy(h->ev0);
+  }
+  if (h->ev1) {
+    cudaEventDestroy(h->ev1);
+  }
+  delete h;
+  return PMP_OK;
+}
+
+int pmp_spray_setup(pmp_spray* h, const pmp_spray_inputs* in)
+{
+  if (!h || !in) {
+    return PMP_ERR_INVALID;
+  }
+  // readSprayParams (SpraySetup.cpp:73-253)
+  if (in->nfuel != h->nfuel) {
+    return set_err(h, PMP_ERR_INVALID, "Number of fuel species in input file must match SPRAY_FUEL_NUM");
+  }
+  if (in->cfl > 2.) {
+    return set_err(h, PMP_ERR_INVALID, "particles.cfl must be <= 2");
+  }
+  if (in->use_breakup_model != 0 || in->use_splash_model) {
+    return set_err(h, PMP_ERR_UNSUPPORTED, "breakup and splash models are not supported");
+  }
+  pmp_spray_data d;
+  memset(&d, 0, sizeof(d));
+  d.nfuel = in->nfuel;
+  d.mass_trans = in->mass_transfer;
+  d.mom_trans = in->mom_transfer;
+  d.fixed_parts = in->fixed_parts;
+  d.min_eb_vfrac = 0.05;
+  d.sigma = -1.;
+  d.wall_T = -1.;
+  d.theta_c = -1.;
+  d.dtmod = 0.5;
+  const int NF = in->nfuel;
+  for (int f = 0; f < NF; ++f) {
+    d.critT[f] = in->crit_temp[f];
+    d.boilT[f] = in->boil_temp[f];
+    d.cp[f] = in->cp[f];
+    d.ref_latent[f] = in->latent[f];
+    const int* nc[4] = {in->ncoef_lambda, in->ncoef_psat, in->ncoef_rho, in->ncoef_mu};
+    const double(*src[4])[4] = {in->lambda, in->psat, in->rho, in->mu};
+    double* dst[4] = {d.lambda_coef, d.psat_coef, d.rho_coef, d.mu_coef};
+    for (int q = 0; q < 4; ++q) {
+      if (nc[q][f] == 4) {
+        for (int i = 0; i < 4; ++i) {
+          dst[q][4 * f + i] = src[q][f][i];
+        }
+      } else if (nc[q][f] == 1) {
+        for (int i = 0; i < 4; ++i) {
+          dst[q][4 * f + i] = 0.;
+        }
+        dst[q][4 * f] = src[q][f][0];
+      } else if (q == 2) {
+        return set_err(h, PMP_ERR_INVALID, "particles.<fuel>_rho is required");
+      }
+    }
+    d.latent[f] = d.ref_latent[f];
+  }
+  d.ref_T = in->fuel_ref_temp;
+  // spraySetup (SpraySetup.cpp:255-297)
+  for (int f = 0; f < NF; ++f) {
+    d.indx[f] = -1;
+    d.dep_indx[f] = -1;
+    const char* dep = in->dep_fuel_species[f][0] ? in->dep_fuel_species[f] : in->fuel_species[f];
+    for (int ns = 0; ns < h->nspec; ++ns) {
+      if (strncmp(h->species[ns], in->fuel_species[f], PMP_NAME_LEN) == 0) {
+        d.indx[f] = ns;
+      }
+      if (strncmp(h->species[ns], dep, PMP_NAME_LEN) == 0) {
+        d.dep_indx[f] = ns;
+      }
+    }
+    if (d.indx[f] < 0 || d.dep_indx[f] < 0) {
+      return set_err(h, PMP_ERR_INVALID, "Fuel not found in species list");
+    }
+  }
+  double fuelEnth[PMP_MAX_SPEC];
+  pmp_eos_T2Hi(&h->mech, d.ref_T, fuelEnth);
+  for (int ns = 0; ns < NF; ++ns) {
+    d.latent[ns] -= fuelEnth[d.indx[ns]] * pmp::kEngConv;
+  }
+  for (int i = 0; i < 3; ++i) {
+    d.body_force[i] = in->body_force[i];
+  }
+  return pmp_spray_set_data(h, &d);
+}
+
+int pmp_spray_set_data(pmp_spray* h, const pmp_spray_data* data)
+{
+  if (!h || !data) {
+    return PMP_ERR_INVALID;
+  }
+  if (data->nfuel != h->nfuel) {
+    return set_err(h, PMP_ERR_INVALID, "SprayData fuel count differs from the handle's");
+  }
+  if (data->do_breakup != 0 || data->do_splash) {
+    return set_err(h, PMP_ERR_UNSUPPORTED, "breakup and splash models are not supported");
+  }
+  h->data = *data;
+  const int rc = build_device_tables(h);
+  h->have_data = rc == PMP_OK;
+  return rc;
+}
+
+int pmp_spray_get_data(const pmp_spray* h, pmp_spray_data* data)
+{
+  if (!h || !data || !h->have_data) {
+    return PMP_ERR_INVALID;
+  }
+  *data = h->data;
+  return PMP_OK;
+}
+
+int pmp_spray_set_comps(pmp_spray* h, const pmp_spray_comps* comps)
+{
+  if (!h || !comps) {
+    return PMP_ERR_INVALID;
+  }
+  h->comps = *comps;
+  h->have_comps = true;
+  return PMP_OK;
+}
+
+int pmp_spray_set_geometry(pmp_spray* h, const pmp_geometry* geom)
+{
+  if (!h || !geom) {
+    return PMP_ERR_INVALID;
+  }
+  for (int d = 0; d < 3; ++d) {
+    if (!(geom->dx[d] > 0.) || geom->domain_hi[d] < geom->domain_lo[d]) {
+      return set_err(h, PMP_ERR_INVALID, "bad geometry");
+    }
+    const int bl = geom->bndry_lo[d];
+    const int bh = geom->bndry_hi[d];
+    if (bl < -1 || bl > 1 || bh < -1 || bh > 1 || ((bl == 0) != (bh == 0))) {
+      return set_err(h, PMP_ERR_INVALID, "bad boundary designation");
+    }
+  }
+  h->geom = *geom;
+  h->have_geom = true;
+  return PMP_OK;
+}
+
+int pmp_spray_set_grids(pmp_spray* h, int nboxes, const pmp_box* boxes)
+{
+  if (!h || nboxes < 0 || (nboxes > 0 && !boxes)) {
+    return PMP_ERR_INVALID;
+  }
+  cudaSetDevice(h->device);
+  for (auto& s : h->staged) {
+    free_store(s);
+  }
+  free_packed(h);
+  h->boxes.assign(boxes, boxes + nboxes);
+  h->staged.assign(nboxes, BoxStore{});
+  h->box_set.assign(nboxes, false);
+  return PMP_OK;
+}
+
+int pmp_spray_set_particles(pmp_spray* h, int box, const pmp_particles* p)
+{
+  if (!h || !p || box < 0 || box >= (int)h->boxes.size() || p->n < 0) {
+    return PMP_ERR_INVALID;
+  }
+  if (!h->have_geom) {
+    return set_err(h, PMP_ERR_INVALID, "set_geometry must precede set_particles");
+  }
+  cudaSetDevice(h->device);
+  // unpack the other boxes first if the layout changes
+  if (h->packed) {
+    const int nb = (int)h->boxes.size();
+    const int nc = h->ncomp();
+    for (int b = 0; b < nb; ++b) {
+      const long long n = h->box_begin[b + 1] - h->box_begin[b];
+      BoxStore s;
+      s.n = n;
+      if (n > 0) {
+        PMP_CUDA(h, cudaMalloc(&s.d, sizeof(double) * nc * n));
+        PMP_CUDA(h, cudaMalloc(&s.id, sizeof(int) * n));
+        PMP_CUDA(h, cudaMalloc(&s.perm, sizeof(long long) * n));
+        const long long o = h->box_begin[b];
+        PMP_CUDA(h, cudaMemcpy2D(s.d, sizeof(double) * n, h->soa + o, sizeof(double) * h->total,
+                                 sizeof(double) * n, nc, cudaMemcpyDeviceToDevice));
+        PMP_CUDA(h, cudaMemcpy(s.id, h->ids + o, sizeof(int) * n, cudaMemcpyDeviceToDevice));
+        PMP_CUDA(h, cudaMemcpy(s.perm, h->perm + o, sizeof(long long) * n, cudaMemcpyDeviceToDevice));
+      }
+      h->staged[b] = s;
+    }
+    free_packed(h);
+  }
+  BoxStore& s = h->staged[box];
+  free_store(s);
+  const long long n = p->n;
+  const int nc = h->ncomp();
+  const int nr = h->nr();
+  s.n = n;
+  h->box_set[box] = true;
+  if (n == 0) {
+    return PMP_OK;
+  }
+  double* raw = nullptr;
+  int* rid = nullptr;
+  PMP_CUDA(h, cudaMalloc(&raw, sizeof(double) * nc * n));
+  PMP_CUDA(h, cudaMalloc(&rid, sizeof(int) * n));
+  const cudaMemcpyKind kind =
+    p->where == PMP_WHERE_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+  if (p->layout == PMP_LAYOUT_SOA) {
+    for (int d = 0; d < 3; ++d) {
+      if (!p->pos[d]) {
+        cudaFree(raw);
+        cudaFree(rid);
+        return set_err(h, PMP_ERR_INVALID, "missing position array");
+      }
+      PMP_CUDA(h, cudaMemcpy(raw + (long long)d * n, p->pos[d], sizeof(double) * n, kind));
+    }
+    for (int r = 0; r < nr; ++r) {
+      if (p->rdata[r]) {
+        PMP_CUDA(h, cudaMemcpy(raw + (long long)(3 + r) * n, p->rdata[r], sizeof(double) * n, kind));
+      } else {
+        PMP_CUDA(h, cudaMemset(raw + (long long)(3 + r) * n, 0, sizeof(double) * n));
+      }
+    }
+    if (!p->id) {
+      cudaFree(raw);
+      cudaFree(rid);
+      return set_err(h, PMP_ERR_INVALID, "missing id array");
+    }
+    PMP_CUDA(h, cudaMemcpy(rid, p->id, sizeof(int) * n, kind));
+  } else if (p->layout == PMP_LAYOUT_AOS) {
+    const size_t rec = sizeof(double) * nc + 2 * sizeof(int);
+    char* tmp = nullptr;
+    PMP_CUDA(h, cudaMalloc(&tmp, rec * n));
+    PMP_CUDA(h, cudaMemcpy(tmp, p->aos, rec * n, kind));
+    k_aos_to_soa<<<nblk(n), 256>>>(tmp, n, nr, raw, rid);
+    PMP_CUDA(h, cudaGetLastError());
+    PMP_CUDA(h, cudaDeviceSynchronize());
+    cudaFree(tmp);
+  } else {
+    cudaFree(raw);
+    cudaFree(rid);
+    return set_err(h, PMP_ERR_INVALID, "unknown particle layout");
+  }
+  // sort by the cell holding the droplet (margin kSortPad around the box)
+  const pmp_box& bx = h->boxes[box];
+  const int ext[3] = {bx.hi[0] - bx.lo[0] + 1 + 2 * kSortPad, bx.hi[1] - bx.lo[1] + 1 + 2 * kSortPad,
+                      bx.hi[2] - bx.lo[2] + 1 + 2 * kSortPad};
+  unsigned *keys = nullptr, *keys2 = nullptr;
+  long long* idx = nullptr;
+  PMP_CUDA(h, cudaMalloc(&keys, sizeof(unsigned) * n));
+  PMP_CUDA(h, cudaMalloc(&keys2, sizeof(unsigned) * n));
+  PMP_CUDA(h, cudaMalloc(&idx, sizeof(long long) * n));
+  PMP_CUDA(h, cudaMalloc(&s.perm, sizeof(long long) * n));
+  const pmp_geometry& g = h->geom;
+  k_cell_keys<<<nblk(n), 256>>>(raw, raw + n, raw + 2 * n, n, g.plo[0], g.plo[1], g.plo[2],
+                                1. / g.dx[0], 1. / g.dx[1], 1. / g.dx[2], bx.lo[0], bx.lo[1],
+                                bx.lo[2], ext[0], ext[1], ext[2], keys, idx);
+  PMP_CUDA(h, cudaGetLastError());
+  size_t tbytes = 0;
+  const long long maxkey = (long long)ext[0] * ext[1] * ext[2];
+  int end_bit = 1;
+  while ((1LL << end_bit) < maxkey && end_bit < 32) {
+    ++end_bit;
+  }
+  PMP_CUDA(h, cub::DeviceRadixSort::SortPairs(nullptr, tbytes, keys, keys2, idx, s.perm, (int)n, 0, end_bit));
+  void* tmp = nullptr;
+  PMP_CUDA(h, cudaMalloc(&tmp, tbytes));
+  PMP_CUDA(h, cub::DeviceRadixSort::SortPairs(tmp, tbytes, keys, keys2, idx, s.perm, (int)n, 0, end_bit));
+  PMP_CUDA(h, cudaMalloc(&s.d, sizeof(double) * nc * n));
+  PMP_CUDA(h, cudaMalloc(&s.id, sizeof(int) * n));
+  k_gather<<<nblk(n), 256>>>(raw, rid, s.perm, n, nc, s.d, s.id);
+  PMP_CUDA(h, cudaGetLastError());
+  PMP_CUDA(h, cudaDeviceSynchronize());
+  cudaFree(tmp);
+  cudaFree(keys);
+  cudaFree(keys2);
+  cudaFree(idx);
+  cudaFree(raw);
+  cudaFree(rid);
+  return PMP_OK;
+}
+
+int pmp_spray_num_particles(const pmp_spray* h, int box, long long* n)
+{
+  if (!h || !n || box < 0 || box >= (int)h->boxes.size()) {
+    return PMP_ERR_INVALID;
+  }
+  *n = h->packed ? h->box_begin[box + 1] - h->box_begin[box] : h->staged[box].n;
+  return PMP_OK;
+}
+
+int pmp_spray_get_particles(pmp_spray* h, int box, pmp_particles* out)
+{
+  if (!h || !out || box < 0 || box >= (int)h->boxes.size()) {
+    return PMP_ERR_INVALID;
+  }
+  cudaSetDevice(h->device);
+  long long n = 0;
+  pmp_spray_num_particles(h, box, &n);
+  if (out->n != n) {
+    return set_err(h, PMP_ERR_INVALID, "output count differs from the box's droplet count", box);
+  }
+  if (n == 0) {
+    return PMP_OK;
+  }
+  const int nc = h->ncomp();
+  const int nr = h->nr();
+  double* d = nullptr;
+  int* id = nullptr;
+  PMP_CUDA(h, cudaMalloc(&d, sizeof(double) * nc * n));
+  PMP_CUDA(h, cudaMalloc(&id, sizeof(int) * n));
+  int rc = unsort_box(h, box, d, id, n);
+  if (rc == PMP_OK) {
+    const cudaMemcpyKind kind =
+      out->where == PMP_WHERE_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    if (out->layout == PMP_LAYOUT_SOA) {
+      for (int dd = 0; dd < 3; ++dd) {
+        if (out->pos[dd]) {
+          PMP_CUDA(h, cudaMemcpy(out->pos[dd], d + (long long)dd * n, sizeof(double) * n, kind));
+        }
+      }
+      for (int r = 0; r < nr; ++r) {
+        if (out->rdata[r]) {
+          PMP_CUDA(h, cudaMemcpy(out->rdata[r], d + (long long)(3 + r) * n, sizeof(double) * n, kind));
+        }
+      }
+      if (out->id) {
+        PMP_CUDA(h, cudaMemcpy(out->id, id, sizeof(int) * n, kind));
+      }
+    } else {
+      const size_t rec = sizeof(double) * nc + 2 * sizeof(int);
+      char* tmp = nullptr;
+      PMP_CUDA(h, cudaMalloc(&tmp, rec * n));
+      k_soa_to_aos<<<nblk(n), 256>>>(d, id, n, nr, tmp);
+      PMP_CUDA(h, cudaGetLastError());
+      PMP_CUDA(h, cudaMemcpy(out->aos, tmp, rec * n, kind));
+      cudaFree(tmp);
+    }
+  }
+  cudaFree(d);
+  cudaFree(id);
+  return rc;
+}
+
+int pmp_spray_update(
+  pmp_spray* h, const pmp_box_view* state, const pmp_box_view* source, int nboxes, double flow_dt,
+  double time, int state_ghosts, int source_ghosts, int is_virt, int is_ghost, int do_move,
+  double spray_cfl_lev, void* stream)
+{
+  (void)time;
+  if (!h || (nboxes > 0 && (!state || !source))) {
+    return PMP_ERR_INVALID;
+  }
+  cudaSetDevice(h->device);
+  return do_update(h, state, source, nboxes, flow_dt, state_ghosts, source_ghosts, is_virt, is_ghost,
+                   do_move, spray_cfl_lev, (cudaStream_t)stream);
+}
+
+int pmp_spray_update_host(
+  pmp_spray* h, const pmp_box_view* state, const pmp_box_view* source, int nboxes, double flow_dt,
+  double time, int state_ghosts, int source_ghosts, int is_virt, int is_ghost, int do_move,
+  double spray_cfl_lev, void* stream)
+{
+  (void)time;
+  if (!h || nboxes < 0 || (nboxes > 0 && (!state || !source))) {
+    return PMP_ERR_INVALID;
+  }
+  cudaSetDevice(h->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  if ((int)h->stage_state.size() < nboxes) {
+    h->stage_state.resize(nboxes, nullptr);
+    h->stage_src.resize(nboxes, nullptr);
+    h->stage_state_n.resize(nboxes, 0);
+    h->stage_src_n.resize(nboxes, 0);
+  }
+  std::vector<pmp_box_view> dst(nboxes), dsr(nboxes);
+  for (int b = 0; b < nboxes; ++b) {
+    if (!state[b].p || !source[b].p || state[b].ncomp < 1 || source[b].ncomp < 1) {
+      return set_err(h, PMP_ERR_INVALID, "null host view", b);
+    }
+    const size_t ns = view_extent(state[b]);
+    const size_t nsr = view_extent(source[b]);
+    if (h->stage_state_n[b] < ns) {
+      cudaFree(h->stage_state[b]);
+      h->stage_state[b] = nullptr;
+      PMP_CUDA(h, cudaMalloc(&h->stage_state[b], sizeof(double) * ns));
+      h->stage_state_n[b] = ns;
+    }
+    if (h->stage_src_n[b] < nsr) {
+      cudaFree(h->stage_src[b]);
+      h->stage_src[b] = nullptr;
+      PMP_CUDA(h, cudaMalloc(&h->stage_src[b], sizeof(double) * nsr));
+      h->stage_src_n[b] = nsr;
+    }
+    PMP_CUDA(h, cudaMemcpyAsync(h->stage_state[b], state[b].p, sizeof(double) * ns,
+                                cudaMemcpyHostToDevice, st));
+    PMP_CUDA(h, cudaMemcpyAsync(h->stage_src[b], source[b].p, sizeof(double) * nsr,
+                                cudaMemcpyHostToDevice, st));
+    dst[b] = state[b];
+    dst[b].p = h->stage_state[b];
+    dsr[b] = source[b];
+    dsr[b].p = h->stage_src[b];
+  }
+  const int rc = do_update(h, dst.data(), dsr.data(), nboxes, flow_dt, state_ghosts, source_ghosts,
+                           is_virt, is_ghost, do_move, spray_cfl_lev, st);
+  if (rc != PMP_OK) {
+    return rc;
+  }
+  for (int b = 0; b < nboxes; ++b) {
+    PMP_CUDA(h, cudaMemcpyAsync(source[b].p, h->stage_src[b], sizeof(double) * view_extent(source[b]),
+                                cudaMemcpyDeviceToHost, st));
+  }
+  PMP_CUDA(h, cudaStreamSynchronize(st));
+  return PMP_OK;
+}
+
+int pmp_spray_move_kick_drift(
+  pmp_spray* h, const pmp_box_view* state, const pmp_box_view* source, int nboxes, double dt,
+  double time, int is_virt, int is_ghost, int state_ghosts, int source_ghosts, int do_move,
+  double spray_cfl_lev, void* stream)
+{
+  return pmp_spray_update(h, state, source, nboxes, dt, time, state_ghosts, source_ghosts, is_virt,
+                          is_ghost, do_move, spray_cfl_lev, stream);
+}
+
+int pmp_spray_move_kick(
+  pmp_spray* h, const pmp_box_view* state, const pmp_box_view* source, int nboxes, double dt,
+  double time, int is_virt, int is_ghost, int state_ghosts, int source_ghosts, double spray_cfl_lev,
+  void* stream)
+{
+  return pmp_spray_update(h, state, source, nboxes, dt, time, state_ghosts, source_ghosts, is_virt,
+                          is_ghost, 0, spray_cfl_lev, stream);
+}
+
+int pmp_spray_set_mode(pmp_spray* h, int mode)
+{
+  if (!h || mode < PMP_MODE_FP64 || mode > PMP_MODE_LEARNED) {
+    return PMP_ERR_INVALID;
+  }
+  h->mode = mode;
+  return PMP_OK;
+}
+
+int pmp_spray_last_error(const pmp_spray* h, pmp_error_info* info)
+{
+  if (!h || !info) {
+    return PMP_ERR_INVALID;
+  }
+  *info = h->last_err;
+  return PMP_OK;
+}
+
+int pmp_spray_get_stats(const pmp_spray* h, pmp_stats* stats)
+{
+  if (!h || !stats) {
+    return PMP_ERR_INVALID;
+  }
+  *stats = h->stats;
+  return PMP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,809 @@
+// spray_fp64.cuh -- the plain FP64 spray update kernel.
+//
+// One thread per droplet, droplets in the library's cell-sorted SoA, one CTA
+// per chunk of a box.  Per droplet the kernel runs the device lambda of
+// SprayParticleContainer::updateParticles (Source/PP_Spray/SprayParticles.cpp:324-481):
+// cell location, bounds check, then for each sub-cycle the trilinear gather
+// (SprayInterpolation.H:99-199), calcBoilT (SprayFuelData.H:178-200),
+// calculateSpraySource (Drag.H:138-441) with calcVaporState and
+// calcHeatCoeff, the atomic source scatter and the move with wall handling
+// (WallFunctions.H:89-234).  All droplet state stays in registers; register
+// arrays are only indexed by compile-time indices (fuel species are picked
+// with unrolled selects).
+//
+// Exactness: this file is compiled with -fmad=false and evaluates every
+// expression in the reference's order with the project math library, the
+// same functions the CPU oracle uses.  Each droplet's new state and its
+// deposit increments are therefore bit-identical to the oracle's; only the
+// order in which atomics add the increments into a cell differs.
+#pragma once
+
+#include <cfloat>
+
+#include "phys/pmp_math.h"
+#include "pmp_device.cuh"
+
+namespace pmp {
+
+__device__ __forceinline__ double dmin(double a, double b) { return (b < a) ? b : a; }
+__device__ __forceinline__ double dmax(double a, double b) { return (a < b) ? b : a; }
+
+__device__ __forceinline__ double cubic(const double* c, double x)
+{
+  return fma(fma(fma(c[3], x, c[2]), x, c[1]), x, c[0]);
+}
+
+// a[i] for a runtime i without indexing a register array
+template <int N>
+__device__ __forceinline__ double sel(const double (&a)[N], int i)
+{
+  double v = a[0];
+#pragma unroll
+  for (int k = 1; k < N; ++k) {
+    v = (k == i) ? a[k] : v;
+  }
+  return v;
+}
+
+// a[i] = v for a runtime i
+template <int N>
+__device__ __forceinline__ void put(double (&a)[N], int i, double v)
+{
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+    a[k] = (k == i) ? v : a[k];
+  }
+}
+
+template <int NS, int NF>
+struct GasVals {
+  double vel[3];
+  double T;
+  double rho;
+  double p;
+  double Y[NS];
+  double mw_mix;
+  double mom_src[3];
+  double mass_src;
+  double Ydot[NF];
+  double eng_src;
+};
+
+__device__ __forceinline__ double rhoL(const DevFuel& f, double T, int spf)
+{
+  const double a = f.rho_coef[4 * spf];
+  const double b = f.rho_coef[4 * spf + 1];
+  const double c = f.rho_coef[4 * spf + 2];
+  const double d = f.rho_coef[4 * spf + 3];
+  return a + T * (b + T * (c + T * d));
+}
+
+// calcHeatCoeff (Drag.H:6-45); pow(BM1, phi) = exp(phi log BM1) with the
+// loop-invariant log hoisted (bit-identical to pmp_pow)
+__device__ __forceinline__ double heat_coeff(
+  double ratio, double B_M, double B_eps, double C_eps, double Nu_0)
+{
+  if (B_M <= C_eps) {
+    return 0.;
+  }
+  const int maxIter = 100;
+  const double NU2 = Nu_0 - 2.;
+  const double BM1 = 1. + B_M;
+  const double lnBM1 = pmp_log(BM1);
+  double phi = ratio / Nu_0;
+  double B_T_old = pmp_exp(phi * lnBM1) - 1.;
+  double logB = pmp_log1p(B_T_old);
+  double invFT = B_T_old / (logB * pmp_pow(1. + B_T_old, 0.7));
+  double Nu_num = 2. + NU2 * invFT;
+  phi = ratio / Nu_num;
+  double B_T = pmp_exp(phi * lnBM1) - 1.;
+  double error = fabs(B_T - B_T_old);
+  int k = 0;
+  while (k < maxIter && error > B_eps) {
+    B_T_old = B_T;
+    logB = pmp_log1p(B_T);
+    invFT = B_T / (logB * pmp_pow(1. + B_T, 0.7));
+    Nu_num = 2. + NU2 * invFT;
+    phi = ratio / Nu_num;
+    B_T = pmp_exp(phi * lnBM1) - 1.;
+    error = fabs(B_T - B_T_old);
+    k++;
+  }
+  logB = pmp_log1p(B_T);
+  invFT = B_T / (logB * pmp_pow(1. + B_T, 0.7));
+  Nu_num = 2. + NU2 * invFT;
+  return Nu_num * logB / B_T;
+}
+
+// calculateSpraySource (Drag.H:138-441), PeleLMeX branch.  Updates vel, T,
+// dia, Y in place; returns the number of inner sub-steps taken.
+template <int NS, int NF>
+__device__ __forceinline__ int spray_source_fp64(
+  const KParams& P, double flow_dt, GasVals<NS, NF>& gpv, double* vel_io, double& T_io,
+  double& dia_io, double* Y_io, double num_ppp, int& id, const double* cBoilT)
+{
+  const DevMech& m = P.m;
+  const DevFuel& fdat = P.f;
+  const double rule = 1. / 3.;
+  const double C_eps = 1.E-15;
+  const double B_eps = 1.E-7;
+  const double min_mass = 1.E-13 * kMassConv;
+  const int nSubMax = 100;
+  double Y_skin[NS];
+  double h_part[NS];
+  double cp_n[NS];
+  double Ddiag[NF];  // fuel rows only
+  double L_fuel[NF];
+  double mi_dot[NF];
+  double Y_part[NF];
+  double X_vapor[NF];
+#pragma unroll
+  for (int spf = 0; spf < NF; ++spf) {
+    L_fuel[spf] = 0.;
+    mi_dot[spf] = 0.;
+    X_vapor[spf] = 0.;
+  }
+  const double num_ppp_ = num_ppp;
+  double vel_part[3] = {vel_io[0], vel_io[1], vel_io[2]};
+  if (fdat.fixed_parts) {
+    vel_part[0] = vel_part[1] = vel_part[2] = 0.;
+  }
+  double T_part = T_io;
+  double dia_part = dia_io;
+  double rho_part = 0.;
+#pragma unroll
+  for (int spf = 0; spf < NF; ++spf) {
+    Y_part[spf] = Y_io[spf];
+    rho_part += Y_part[spf] / rhoL(fdat, dmin(T_part, cBoilT[spf]), spf);
+  }
+  rho_part = 1. / rho_part;
+  double dt = flow_dt;
+  int isub = 1;
+  int nsub = 1;
+  double pmass = PMP_PI / 6. * rho_part * pmp_pow(dia_part, 3.);
+  const double startmass = pmass;
+  double part_vel_src[3];
+  while (isub <= nsub) {
+    double cp_part = 0.;
+    double Tboil = 0.;
+    double mw_part = 0.;
+#pragma unroll
+    for (int spf = 0; spf < NF; ++spf) {
+      Tboil += Y_part[spf] * cBoilT[spf];
+      cp_part += Y_part[spf] * fdat.cp[spf];
+      mw_part += Y_part[spf] / m.mw_kg[fdat.indx[spf]];
+    }
+    mw_part = 1. / mw_part;
+    const double delT = dmax(gpv.T - T_part, 0.);
+    double T_skin = gpv.T;
+    if (fdat.mass_trans) {
+      T_skin = T_part + rule * delT;
+    }
+    // eos.T2Cpi(T_skin), eos.T2Hi(T_part) (pmp_thermo.h), then *= eng_conv
+#pragma unroll
+    for (int n = 0; n < NS; ++n) {
+      const double* a = m.cp[n];
+      const double cpr = fma(fma(fma(fma(a[4], T_skin, a[3]), T_skin, a[2]), T_skin, a[1]), T_skin, a[0]);
+      cp_n[n] = cpr * m.ru_w[n];
+      const double* hc = m.hc[n];
+      const double hp = fma(fma(fma(fma(hc[4], T_part, hc[3]), T_part, hc[2]), T_part, hc[1]), T_part, hc[0]);
+      h_part[n] = fma(hp, T_part, hc[5]) * m.ru_w[n];
+      Y_skin[n] = 0.;
+      h_part[n] *= kEngConv;
+      cp_n[n] *= kEngConv;
+    }
+    double cp_skin = 0.;
+    double mw_skin = 0.;
+    double B_M = 0.;
+    double sumXVap = 0.;
+    if (fdat.mass_trans) {
+      // calcVaporState (Drag.H:48-135)
+      const double RU = kRuCgs * kRuConv;
+      const double PATM = kPatmCgs * kPresConv;
+      double mbar_vap = 0.;
+#pragma unroll
+      for (int spf = 0; spf < NF; ++spf) {
+        const int fspec = fdat.indx[spf];
+        const int fdspec = fdat.dep[spf];
+        const double boilT_ref = fdat.boilT[spf];
+        const double mw_fuel = m.mw_kg[fspec];
+        const double Tp = dmin(T_part, 0.99 * cBoilT[spf]);
+        const double part_latent = sel(h_part, fspec) + fdat.latent[spf] - fdat.cp[spf] * (Tp - fdat.ref_T);
+        L_fuel[spf] = part_latent;
+        double pres_sat = 0.;
+        if (fdat.psat_coef[4 * spf + 3] == 0.) {
+          pres_sat = PATM * pmp_exp(part_latent * mw_fuel / RU * (1. / boilT_ref - 1. / Tp));
+        } else {
+          const double a = fdat.psat_coef[4 * spf];
+          const double b = fdat.psat_coef[4 * spf + 1];
+          const double c = fdat.psat_coef[4 * spf + 2];
+          const double d = fdat.psat_coef[4 * spf + 3];
+          pres_sat = d * pmp_exp((a - b / (Tp + c)) * fdat.ln10);
+        }
+        const double X_fluid = sel(gpv.Y, fdspec) * gpv.mw_mix / mw_fuel;
+        if (pres_sat > X_fluid * gpv.p) {
+          const double Xl = Y_part[spf] * mw_part / mw_fuel;
+          const double Xv = Xl * pres_sat / gpv.p;
+          mbar_vap += Xv * mw_fuel;
+          sumXVap += Xv;
+          X_vapor[spf] = Xv;
+        } else {
+          X_vapor[spf] = 0.;
+        }
+      }
+      const double totalmwx = mbar_vap + (1. - sumXVap) * gpv.mw_mix;
+      double sumYSkin = 0.;
+      double sumYfFluid = 0.;
+      double sumYVap = 0.;
+#pragma unroll
+      for (int spf = 0; spf < NF; ++spf) {
+        if (X_vapor[spf] > 0.) {
+          const int fspec = fdat.indx[spf];
+          const double mw_fuel = m.mw_kg[fspec];
+          const double Yfv = X_vapor[spf] * mw_fuel / totalmwx;
+          sumYVap += Yfv;
+          const double gasY = sel(gpv.Y, fdat.dep[spf]);
+          sumYfFluid += gasY;
+          const double Ysk = Yfv + rule * (gasY - Yfv);
+          put(Y_skin, fspec, Ysk);
+          sumYSkin += Ysk;
+        }
+      }
+      const double renorm = (1. - sumYSkin) / (1. - sumYfFluid);
+#pragma unroll
+      for (int n = 0; n < NS; ++n) {
+        if (Y_skin[n] == 0.) {
+          Y_skin[n] = gpv.Y[n] * renorm;
+        }
+        cp_skin += Y_skin[n] * cp_n[n];
+        mw_skin += Y_skin[n] / m.mw_kg[n];
+      }
+      mw_skin = 1. / mw_skin;
+      B_M = (sumYVap - sumYfFluid) / dmax(C_eps, (1. - sumYVap));
+      B_M = dmin(20., B_M);
+    } else {
+#pragma unroll
+      for (int n = 0; n < NS; ++n) {
+        Y_skin[n] = gpv.Y[n];
+        cp_skin += gpv.Y[n] * cp_n[n];
+      }
+      mw_skin = gpv.mw_mix;
+    }
+    double lambda_skin = 0.;
+    double mu_skin = 0.;
+    double rho_skin = gpv.rho;
+    if (fdat.mass_trans) {
+      rho_skin = mw_skin * gpv.p / (kRuCgs * kRuConv * T_skin);
+    }
+    // trans.transport at (T_skin, Y_skin) (pmp_thermo.h), fuel rows of Ddiag
+    {
+      double X[NS];
+      double sumYW = 0.;
+#pragma unroll
+      for (int k = 0; k < NS; ++k) {
+        sumYW += Y_skin[k] / m.mw_g[k];
+      }
+      const double wbar = 1.0 / sumYW;
+#pragma unroll
+      for (int k = 0; k < NS; ++k) {
+        X[k] = Y_skin[k] * wbar / m.mw_g[k];
+      }
+      const double lnT = pmp_log(T_skin);
+      double s = 0.0;
+#pragma unroll
+      for (int k = 0; k < NS; ++k) {
+        s = fma(X[k], pmp_exp(6.0 * cubic(m.mu[k], lnT)), s);
+      }
+      mu_skin = pmp_exp(pmp_log(s) * (1.0 / 6.0));
+      if (fdat.mass_trans) {
+        double sl = 0.0;
+#pragma unroll
+        for (int k = 0; k < NS; ++k) {
+          sl = fma(X[k], pmp_exp(0.25 * cubic(m.lam[k], lnT)), sl);
+        }
+        const double s2 = sl * sl;
+        lambda_skin = s2 * s2;
+        const double rt = kRuCgs * T_skin;
+#pragma unroll
+        for (int f = 0; f < NF; ++f) {
+          const int i = fdat.indx[f];
+          double term1 = 0.0;
+          double term2 = 0.0;
+#pragma unroll
+          for (int j = 0; j < NS; ++j) {
+            if (j != i) {
+              term1 += Y_skin[j];
+              term2 = fma(X[j], pmp_exp(-cubic(m.dbin[f][j], lnT)), term2);
+            }
+          }
+          Ddiag[f] = m.mw_g[i] * term1 / (term2 * rt);
+        }
+      }
+    }
+    mu_skin *= kMuConv;
+    lambda_skin *= kLambdaConv;
+    double diff_vel[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      diff_vel[d] = gpv.vel[d] - vel_part[d];
+    }
+    const double diff_vel_mag =
+      sqrt(diff_vel[0] * diff_vel[0] + diff_vel[1] * diff_vel[1] + diff_vel[2] * diff_vel[2]);
+    const double Reyn = rho_skin * diff_vel_mag * dia_part / mu_skin;
+    const double inv_pmass = 1. / pmass;
+    double drag_coef = 0.;
+    if (Reyn > 1000.) {
+      drag_coef = 0.424;
+    } else if (Reyn > 1.) {
+      drag_coef = 24. / Reyn * (1. + pmp_cbrt(Reyn * Reyn) / 6.);
+    } else if (Reyn > 0.) {
+      drag_coef = 24. / Reyn;
+    }
+    drag_coef *= (1. + 2.6432 * 0.);
+    const double drag_force =
+      0.125 * rho_skin * drag_coef * PMP_PI * dia_part * dia_part * diff_vel_mag;
+    const double drag_force_p = 0.75 * rho_skin * drag_coef * diff_vel_mag / (dia_part * rho_part);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      part_vel_src[d] = drag_force_p * diff_vel[d] + fdat.body_force[d];
+    }
+    if (fdat.mom_trans) {
+      const double nd = num_ppp_ * drag_force;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        gpv.mom_src[d] += nd * diff_vel[d];
+      }
+      if (isub == 1) {
+        const double inv_tau_var = drag_force_p;
+        nsub = min(max(nsub, static_cast<int>(flow_dt * inv_tau_var) + 1), nSubMax);
+      }
+    }
+    double part_temp_src = 0.;
+    double m_dot = 0.;
+    if (fdat.mass_trans) {
+      const double Pr_skin = mu_skin * cp_skin / lambda_skin;
+      const double powR = dmax(pmp_pow(dmin(400., Reyn), 0.077), 1.);
+      double Nu_num = 0.;
+      double sumL = 0.;
+      const double Nu_0 = 1. + powR * pmp_cbrt(1. + Reyn * Pr_skin);
+      if (sumXVap > 0.) {
+        double rhoDtotal = 0.;
+        double cp_fuel = 0.;
+        double sumYSkin = 0.;
+#pragma unroll
+        for (int spf = 0; spf < NF; ++spf) {
+          const int fspec = fdat.indx[spf];
+          Ddiag[spf] *= mw_skin / m.mw_kg[fspec] * kRhodConv;
+          const double X_norm = X_vapor[spf] / sumXVap;
+          Ddiag[spf] *= X_norm;
+          rhoDtotal += Ddiag[spf];
+          const double ysk = sel(Y_skin, fspec);
+          cp_fuel += ysk * sel(cp_n, fspec);
+          sumYSkin += ysk;
+        }
+        cp_fuel /= sumYSkin;
+        const double Sc_skin = mu_skin / rhoDtotal;
+        const double logB = pmp_log1p(B_M);
+        const double invFM = B_M / (logB * pmp_pow(1. + B_M, 0.7));
+        const double Sh_0 = 1. + powR * pmp_cbrt(1. + Reyn * Sc_skin);
+        const double Sh_num = 2. + (Sh_0 - 2.) * invFM;
+        const double mdotcoeff = PMP_PI * dia_part * Sh_num * logB;
+        const double ratio = cp_fuel * Sh_num * rhoDtotal / lambda_skin;
+        Nu_num = heat_coeff(ratio, B_M, B_eps, C_eps, Nu_0);
+#pragma unroll
+        for (int spf = 0; spf < NF; ++spf) {
+          if (X_vapor[spf] > 0.) {
+            mi_dot[spf] = -dmax(Ddiag[spf] * mdotcoeff, 0.);
+            m_dot += mi_dot[spf];
+            sumL += mi_dot[spf] * L_fuel[spf];
+          }
+        }
+      } else {
+        Nu_num = Nu_0;
+      }
+      const double conv_src = PMP_PI * lambda_skin * dia_part * delT * Nu_num;
+      gpv.eng_src += num_ppp_ * conv_src;
+      part_temp_src = (sumL + conv_src) * inv_pmass / cp_part;
+      if (isub == 1 && delT > C_eps) {
+        const double inv_tau_d = -m_dot / (0.2 * pmass);
+        const double inv_tau_T = conv_src * inv_pmass / (cp_part * delT);
+        nsub = min(
+          max(nsub, max(static_cast<int>(flow_dt * inv_tau_d), static_cast<int>(flow_dt * inv_tau_T)) + 1),
+          nSubMax);
+      }
+    }
+    if (isub == 1) {
+      dt = flow_dt / static_cast<double>(nsub);
+    }
+    const double part_dt = fdat.dtmod * dt;
+    if (!fdat.fixed_parts) {
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        vel_part[d] += part_dt * part_vel_src[d];
+      }
+    }
+    if (fdat.mass_trans) {
+      const double newT = T_part + part_dt * part_temp_src;
+      const double new_mass = pmass + m_dot * part_dt;
+      if (new_mass > min_mass && newT < Tboil) {
+        T_part = newT;
+        if (NF > 1) {
+          rho_part = 0.;
+          double sumY = 0.;
+#pragma unroll
+          for (int spf = 0; spf < NF; ++spf) {
+            Y_part[spf] = dmin(1., dmax(0., (Y_part[spf] * pmass + mi_dot[spf] * part_dt) / new_mass));
+            if (Y_part[spf] <= 1.E-12) {
+              Y_part[spf] = 0.;
+            }
+            sumY += Y_part[spf];
+          }
+#pragma unroll
+          for (int spf = 0; spf < NF; ++spf) {
+            Y_part[spf] /= sumY;
+            rho_part += Y_part[spf] / rhoL(fdat, dmin(T_part, cBoilT[spf]), spf);
+          }
+          rho_part = 1. / rho_part;
+        } else {
+          rho_part = rhoL(fdat, dmin(T_part, cBoilT[0]), 0);
+        }
+        pmass = new_mass;
+        dia_part = pmp_cbrt(6. * pmass / (PMP_PI * rho_part));
+      } else {
+        pmass = 0.;
+        id = -1;
+        nsub = isub;
+        isub = nsub + 1;
+      }
+    }
+    ++isub;
+  }
+  if (nsub > 1) {
+    gpv.eng_src /= static_cast<double>(nsub);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      gpv.mom_src[d] /= static_cast<double>(nsub);
+    }
+  }
+  const double mdot_total = (pmass - startmass) / (fdat.dtmod * flow_dt);
+  gpv.mass_src = num_ppp_ * mdot_total;
+  if (fdat.mom_trans) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      gpv.mom_src[d] += num_ppp_ * vel_part[d] * mdot_total;
+    }
+  }
+#pragma unroll
+  for (int spf = 0; spf < NF; ++spf) {
+    const double oldY = Y_io[spf];
+    const double newY = Y_part[spf];
+    const double midot = (newY * pmass - oldY * startmass) / (fdat.dtmod * flow_dt);
+    gpv.Ydot[spf] = num_ppp_ * midot;
+    gpv.eng_src += num_ppp_ * midot * sel(h_part, fdat.dep[spf]);
+    Y_io[spf] = Y_part[spf];
+  }
+  vel_io[0] = vel_part[0];
+  vel_io[1] = vel_part[1];
+  vel_io[2] = vel_part[2];
+  T_io = T_part;
+  dia_io = dia_part;
+  return nsub;
+}
+
+// check_bounds (SprayInterpolation.H:64-97)
+__device__ __forceinline__ bool check_bounds(const KParams& P, const double* pos, int* bflags)
+{
+#pragma unroll
+  for (int hilo = 0; hilo < 2; ++hilo) {
+    const int fact = (hilo == 0) ? 1 : -1;
+#pragma unroll
+    for (int dir = 0; dir < 3; ++dir) {
+      const double dom_loc = (hilo == 0) ? P.plo[dir] : P.phi[dir];
+      const int bflag = (hilo == 0) ? P.bndry_lo[dir] : P.bndry_hi[dir];
+      if (bflag != 0) {
+        const double diff = static_cast<double>(fact) * (pos[dir] - dom_loc);
+        if (diff < 0.) {
+          if (bflag == 1) {
+            bflags[dir] = -fact;
+          } else {
+            return true;
+          }
+        } else if (diff < 0.5 * P.dx[dir]) {
+          bflags[dir] = -2 * fact;
+        }
+      }
+    }
+  }
+  return false;
+}
+
+// impose_wall without splash or EB (WallFunctions.H:89-234)
+__device__ __forceinline__ void impose_wall(const KParams& P, double* pos, double* vel, const int* bflags)
+{
+  double normpos[3];
+  int ijkc[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    normpos[d] = (pos[d] - P.plo[d]) / P.dx[d];
+    ijkc[d] = static_cast<int>(floor(normpos[d]));
+  }
+  bool wall_check = false;
+  double normal[3];
+  double bcentv[3];
+#pragma unroll
+  for (int dir = 0; dir < 3; ++dir) {
+    if ((bflags[dir] == -1 || bflags[dir] == 1) && !wall_check) {
+      normal[dir] = -static_cast<double>(bflags[dir]);
+      bcentv[dir] = static_cast<double>(ijkc[dir]) + 0.5 * static_cast<double>(1 - bflags[dir]);
+      wall_check = true;
+    } else {
+      normal[dir] = 0.;
+      bcentv[dir] = 0.;
+    }
+  }
+  if (!wall_check) {
+    return;
+  }
+  const double par_dot = (normpos[0] - bcentv[0]) * P.dx[0] * normal[0] +
+                         (normpos[1] - bcentv[1]) * P.dx[1] * normal[1] +
+                         (normpos[2] - bcentv[2]) * P.dx[2] * normal[2];
+  if (par_dot < DBL_EPSILON) {
+    const double Nw_Vp = normal[0] * vel[0] + normal[1] * vel[1] + normal[2] * vel[2];
+#pragma unroll
+    for (int dir = 0; dir < 3; ++dir) {
+      vel[dir] -= 2. * Nw_Vp * normal[dir];
+      pos[dir] -= 2. * par_dot * normal[dir];
+    }
+  }
+}
+
+__device__ __forceinline__ void set_error(const KParams& P, int code, int box, long long slot)
+{
+  if (atomicCAS(&P.status->code, 0, code) == 0) {
+    P.status->box = box;
+    P.status->slot = slot;
+  }
+}
+
+__device__ __forceinline__ bool in_box(const int* lo, const int* hi, int i, int j, int k)
+{
+  return i >= lo[0] && i <= hi[0] && j >= lo[1] && j <= hi[1] && k >= lo[2] && k <= hi[2];
+}
+
+template <int NS, int NF, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) spray_update_fp64(const __grid_constant__ KParams P)
+{
+  const int b = P.cta_box[blockIdx.x];
+  const BoxEntry& B = P.boxes[b];
+  const long long s = P.cta_start[blockIdx.x] + threadIdx.x;
+  unsigned long long my_sub = 0, my_killed = 0, my_inner = 0;
+  if (s < B.p_end) {
+    int id = P.parts.id[s];
+    if (id > 0) {
+      double pos[3], vel[3], Y[NF];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        pos[d] = P.parts.pos[d][s];
+        vel[d] = P.parts.rd[PMP_PSTATE_VEL + d][s];
+      }
+      double T = P.parts.rd[PMP_PSTATE_T][s];
+      double dia = P.parts.rd[PMP_PSTATE_DIA][s];
+#pragma unroll
+      for (int spf = 0; spf < NF; ++spf) {
+        Y[spf] = P.parts.rd[PMP_PSTATE_Y + spf][s];
+      }
+      const double num_ppp = P.parts.rd[PMP_PSTATE_NUMDENS(NF)][s];
+      const double film = P.parts.rd[PMP_PSTATE_FILMHGHT(NF)][s];
+      // cell of the upper stencil centre and cell holding the droplet (SprayParticles.cpp:340-343)
+      double lx[3];
+      int ijk[3], ijkc[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        lx[d] = (pos[d] - P.plo[d]) * P.dxi[d] + 0.5;
+        ijk[d] = static_cast<int>(floor(lx[d]));
+        ijkc[d] = static_cast<int>(floor((pos[d] - P.plo[d]) * P.dxi[d]));
+      }
+      int bflags[3] = {0, 0, 0};
+      bool ok = true;
+      if (B.at_bounds) {
+        if (check_bounds(P, pos, bflags)) {
+          set_error(P, PMP_ERR_LEFT_DOMAIN, b, s);
+          ok = false;
+        }
+      }
+      for (int cur_iter = 0; ok && cur_iter < P.num_iter && id > 0; ++cur_iter) {
+        if (film > 0.) {
+          set_error(P, PMP_ERR_UNSUPPORTED, b, s);
+          ok = false;
+          break;
+        }
+        // trilinear_interp (SprayInterpolation.H:158-199)
+        double ssv[2][3];
+#pragma unroll
+        for (int dir = 0; dir < 3; ++dir) {
+          const double sx_hi = lx[dir] - static_cast<double>(ijk[dir]);
+          const double sx_lo = 1. - sx_hi;
+          if (bflags[dir] > 1) {
+            ssv[0][dir] = 1.;
+            ssv[1][dir] = 0.;
+          } else if (bflags[dir] < -1) {
+            ssv[0][dir] = 0.;
+            ssv[1][dir] = 1.;
+          } else {
+            ssv[0][dir] = sx_lo;
+            ssv[1][dir] = sx_hi;
+          }
+        }
+        // InterpolateGasPhase (SprayInterpolation.H:99-150), PeleLMeX branch
+        GasVals<NS, NF> gpv;
+        gpv.rho = 0.;
+        gpv.T = 0.;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          gpv.vel[d] = 0.;
+          gpv.mom_src[d] = 0.;
+        }
+#pragma unroll
+        for (int n = 0; n < NS; ++n) {
+          gpv.Y[n] = 0.;
+        }
+#pragma unroll
+        for (int spf = 0; spf < NF; ++spf) {
+          gpv.Ydot[spf] = 0.;
+        }
+        gpv.eng_src = 0.;
+        gpv.mass_src = 0.;
+        bool state_ok = true;
+#pragma unroll
+        for (int kk = -1; kk < 1; ++kk) {
+#pragma unroll
+          for (int jj = -1; jj < 1; ++jj) {
+#pragma unroll
+            for (int ii = -1; ii < 1; ++ii) {
+              const double cw = ssv[ii + 1][0] * ssv[jj + 1][1] * ssv[kk + 1][2];
+              if (cw > 0.) {
+                const int ci = ijk[0] + ii;
+                const int cj = ijk[1] + jj;
+                const int ck = ijk[2] + kk;
+                if (!in_box(B.state_lo, B.state_hi, ci, cj, ck)) {
+                  state_ok = false;
+                } else {
+                  const double* q = B.st + (long long)(ci - B.st_lo[0]) +
+                                    (long long)(cj - B.st_lo[1]) * B.st_js +
+                                    (long long)(ck - B.st_lo[2]) * B.st_ks;
+                  const double cur_rho = __ldg(q + (long long)P.c_rho * B.st_ns);
+                  gpv.rho += cw * cur_rho;
+                  const double inv_rho = 1. / cur_rho;
+#pragma unroll
+                  for (int n = 0; n < NS; ++n) {
+                    const double cur_mf = __ldg(q + (long long)(P.c_spec + n) * B.st_ns) * inv_rho;
+                    gpv.Y[n] += cw * cur_mf;
+                  }
+#pragma unroll
+                  for (int dir = 0; dir < 3; ++dir) {
+                    gpv.vel[dir] += cw * __ldg(q + (long long)(P.c_mom + dir) * B.st_ns);
+                  }
+                  gpv.T += cw * __ldg(q + (long long)P.c_T * B.st_ns);
+                }
+              }
+            }
+          }
+        }
+        if (!state_ok) {
+          set_error(P, PMP_ERR_STATE_BOX, b, s);
+          ok = false;
+          break;
+        }
+        // GasPhaseVals::define (SprayFuelData.H:101-111)
+        double mw_mix = 0.;
+#pragma unroll
+        for (int n = 0; n < NS; ++n) {
+          mw_mix += gpv.Y[n] / P.m.mw_kg[n];
+        }
+        gpv.p = gpv.rho * kRuCgs * mw_mix * gpv.T * kRuConv;
+        gpv.mw_mix = 1. / mw_mix;
+        // SprayData::calcBoilT (SprayFuelData.H:178-200)
+        double cBoilT[NF];
+        {
+          const double RU = kRuCgs * kRuConv;
+          const double PATM = kPatmCgs * kPresConv;
+          const double lp = pmp_log(PATM / gpv.p);
+#pragma unroll
+          for (int spf = 0; spf < NF; ++spf) {
+            const double mw_fuel = P.m.mw_kg[P.f.indx[spf]];
+            const double c = 1. / (lp * RU / (P.f.hboil_ref[spf] * mw_fuel) + 1. / P.f.boilT[spf]);
+            cBoilT[spf] = dmin(P.f.critT[spf], c);
+          }
+        }
+        const int nsub = spray_source_fp64<NS, NF>(P, P.sub_dt, gpv, vel, T, dia, Y, num_ppp, id, cBoilT);
+        my_sub += 1;
+        my_inner += static_cast<unsigned long long>(nsub);
+        // source scatter into the cell holding the droplet (SprayParticles.cpp:419-441)
+        const double cur_coef = -P.inv_vol * P.sub_dt / P.flow_dt;
+        if (!in_box(B.src_lo, B.src_hi, ijkc[0], ijkc[1], ijkc[2])) {
+          if (!P.is_ghost || !in_box(B.sr_alo, B.sr_ahi, ijkc[0], ijkc[1], ijkc[2])) {
+            set_error(P, PMP_ERR_SOURCE_BOX, b, s);
+            ok = false;
+            break;
+          }
+        }
+        double* q = B.sr + (long long)(ijkc[0] - B.sr_lo[0]) + (long long)(ijkc[1] - B.sr_lo[1]) * B.sr_js +
+                    (long long)(ijkc[2] - B.sr_lo[2]) * B.sr_ks;
+        if (P.f.mom_trans) {
+#pragma unroll
+          for (int dir = 0; dir < 3; ++dir) {
+            atomicAdd(q + (long long)(P.s_mom + dir) * B.sr_ns, cur_coef * gpv.mom_src[dir]);
+          }
+        }
+        if (P.f.mass_trans) {
+          atomicAdd(q + (long long)P.s_rho * B.sr_ns, cur_coef * gpv.mass_src);
+#pragma unroll
+          for (int spf = 0; spf < NF; ++spf) {
+            atomicAdd(q + (long long)(P.s_spec + spf) * B.sr_ns, cur_coef * gpv.Ydot[spf]);
+          }
+        }
+        atomicAdd(q + (long long)P.s_eng * B.sr_ns, cur_coef * gpv.eng_src);
+        // move (SprayParticles.cpp:444-476)
+        if (P.do_move && !P.f.fixed_parts && id > 0) {
+#pragma unroll
+          for (int dir = 0; dir < 3; ++dir) {
+            pos[dir] += P.sub_dt * vel[dir];
+          }
+          if (B.at_bounds) {
+            if (check_bounds(P, pos, bflags)) {
+              id = -1;
+            } else {
+              impose_wall(P, pos, vel, bflags);
+            }
+          }
+#pragma unroll
+          for (int d = 0; d < 3; ++d) {
+            lx[d] = (pos[d] - P.plo[d]) * P.dxi[d] + 0.5;
+            ijk[d] = static_cast<int>(floor(lx[d]));
+            ijkc[d] = static_cast<int>(floor((pos[d] - P.plo[d]) * P.dxi[d]));
+          }
+        }
+        if (P.is_ghost && !in_box(B.src_lo, B.src_hi, ijkc[0], ijkc[1], ijkc[2])) {
+          id = -1;
+        }
+      }
+      if (ok) {
+        if (P.do_move) {
+#pragma unroll
+          for (int d = 0; d < 3; ++d) {
+            P.parts.pos[d][s] = pos[d];
+          }
+        }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          P.parts.rd[PMP_PSTATE_VEL + d][s] = vel[d];
+        }
+        P.parts.rd[PMP_PSTATE_T][s] = T;
+        P.parts.rd[PMP_PSTATE_DIA][s] = dia;
+#pragma unroll
+        for (int spf = 0; spf < NF; ++spf) {
+          P.parts.rd[PMP_PSTATE_Y + spf][s] = Y[spf];
+        }
+        if (id <= 0) {
+          P.parts.id[s] = id;
+          my_killed = 1;
+        }
+      }
+    }
+  }
+  // per-warp counter reduction, one atomic per warp
+  const unsigned mask = 0xffffffffu;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    my_sub += __shfl_down_sync(mask, my_sub, o);
+    my_killed += __shfl_down_sync(mask, my_killed, o);
+    my_inner += __shfl_down_sync(mask, my_inner, o);
+  }
+  if ((threadIdx.x & 31) == 0 && (my_sub | my_killed | my_inner)) {
+    atomicAdd(&P.status->substeps, my_sub);
+    atomicAdd(&P.status->killed, my_killed);
+    atomicAdd(&P.status->inner, my_inner);
+  }
+}
+
+}  // namespace pmp

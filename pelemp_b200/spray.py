@@ -1,0 +1,284 @@
+"""Python mirror of PeleMP's SprayParticleContainer update surface over the C ABI.
+
+Method names follow the reference (Source/PP_Spray/SprayParticles.H:195-243,
+SpraySetup.cpp:73-297): ``spray_setup`` (readSprayParams + spraySetup),
+``assign_spray_comps``, ``update_particles``, ``move_kick_drift``,
+``move_kick``.  Errors the reference reports with amrex::Abort raise
+``SprayError`` carrying the library's status code.
+
+The native library (pelemp_b200/libpmpspray.so, sm_100a) is required: there
+is no CPU path behind this class.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import capi
+from .workloads import view_of
+
+_LIB = None
+_LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libpmpspray.so")
+
+# exported C ABI functions and their argument types
+_SIGS = {
+    "pmp_spray_create": [C.POINTER(capi.SprayConfig), C.POINTER(C.c_void_p)],
+    "pmp_spray_destroy": [C.c_void_p],
+    "pmp_spray_setup": [C.c_void_p, C.POINTER(capi.SprayInputs)],
+    "pmp_spray_set_data": [C.c_void_p, C.POINTER(capi.SprayData)],
+    "pmp_spray_get_data": [C.c_void_p, C.POINTER(capi.SprayData)],
+    "pmp_spray_set_comps": [C.c_void_p, C.POINTER(capi.SprayComps)],
+    "pmp_spray_set_geometry": [C.c_void_p, C.POINTER(capi.Geometry)],
+    "pmp_spray_set_grids": [C.c_void_p, C.c_int, C.POINTER(capi.Box)],
+    "pmp_spray_set_particles": [C.c_void_p, C.c_int, C.POINTER(capi.Particles)],
+    "pmp_spray_get_particles": [C.c_void_p, C.c_int, C.POINTER(capi.Particles)],
+    "pmp_spray_num_particles": [C.c_void_p, C.c_int, C.POINTER(C.c_longlong)],
+    "pmp_spray_update": [C.c_void_p, C.POINTER(capi.BoxView), C.POINTER(capi.BoxView), C.c_int,
+                         C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                         C.c_double, C.c_void_p],
+    "pmp_spray_update_host": [C.c_void_p, C.POINTER(capi.BoxView), C.POINTER(capi.BoxView),
+                              C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int,
+                              C.c_int, C.c_int, C.c_double, C.c_void_p],
+    "pmp_spray_move_kick_drift": [C.c_void_p, C.POINTER(capi.BoxView), C.POINTER(capi.BoxView),
+                                  C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int,
+                                  C.c_int, C.c_int, C.c_double, C.c_void_p],
+    "pmp_spray_move_kick": [C.c_void_p, C.POINTER(capi.BoxView), C.POINTER(capi.BoxView),
+                            C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int,
+                            C.c_double, C.c_void_p],
+    "pmp_spray_set_mode": [C.c_void_p, C.c_int],
+    "pmp_spray_last_error": [C.c_void_p, C.POINTER(capi.ErrorInfo)],
+    "pmp_spray_get_stats": [C.c_void_p, C.POINTER(capi.Stats)],
+    "pmp_spray_version": [],
+}
+
+
+class SprayError(RuntimeError):
+    def __init__(self, code, info=None):
+        self.code = code
+        self.info = info
+        msg = capi.STATUS_NAMES.get(code, str(code))
+        if info is not None:
+            msg += f" (box {info.box}, droplet {info.particle}: {info.message.decode(errors='replace')})"
+        super().__init__(msg)
+
+
+def lib():
+    """Load libpmpspray.so (raises if it is not built)."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(_LIB_PATH):
+            raise RuntimeError(f"{_LIB_PATH} is not built: run `python -m pelemp_b200.build`")
+        L = C.CDLL(_LIB_PATH)
+        for name, args in _SIGS.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = C.c_char_p if name == "pmp_spray_version" else C.c_int
+        _LIB = L
+    return _LIB
+
+
+def _ptr(a):
+    """Data pointer of a numpy array or a torch tensor."""
+    if hasattr(a, "data_ptr"):
+        return a.data_ptr()
+    return a.ctypes.data
+
+
+def _is_cuda(a):
+    return hasattr(a, "is_cuda") and a.is_cuda
+
+
+def views(arrays, los):
+    """pmp_box_view array of per-box (ncomp, nz, ny, nx) arrays (numpy or torch)."""
+    out = (capi.BoxView * len(arrays))()
+    for b, (a, lo) in enumerate(zip(arrays, los)):
+        if hasattr(a, "data_ptr"):
+            nc, nz, ny, nx = a.shape
+            v = out[b]
+            v.p = a.data_ptr()
+            for d in range(3):
+                v.lo[d] = int(lo[d])
+            v.hi[0], v.hi[1], v.hi[2] = lo[0] + nx - 1, lo[1] + ny - 1, lo[2] + nz - 1
+            st = a.stride()
+            v.nstride, v.kstride, v.jstride = st[0], st[1], st[2]
+            v.ncomp = nc
+        else:
+            out[b] = view_of(a, lo)
+    return out
+
+
+class SprayParticleContainer:
+    """One level's spray droplets on one GPU (the reference's container, update path)."""
+
+    def __init__(self, species, nfuel, device=0):
+        L = lib()
+        cfg = capi.SprayConfig()
+        cfg.nfuel = nfuel
+        cfg.nspec = len(species)
+        for i, s in enumerate(species):
+            cfg.species[i].value = s.encode()
+        cfg.device = device
+        h = C.c_void_p()
+        rc = L.pmp_spray_create(C.byref(cfg), C.byref(h))
+        if rc != 0:
+            raise SprayError(rc)
+        self._h = h
+        self.species = list(species)
+        self.nfuel = nfuel
+        self.nboxes = 0
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().pmp_spray_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc != 0:
+            info = capi.ErrorInfo()
+            lib().pmp_spray_last_error(self._h, C.byref(info))
+            raise SprayError(rc, info)
+
+    # --- setup (SpraySetup.cpp) -------------------------------------------
+    def spray_setup(self, inputs):
+        self._check(lib().pmp_spray_setup(self._h, C.byref(inputs)))
+
+    def set_spray_data(self, data):
+        self._check(lib().pmp_spray_set_data(self._h, C.byref(data)))
+
+    def spray_data(self):
+        d = capi.SprayData()
+        self._check(lib().pmp_spray_get_data(self._h, C.byref(d)))
+        return d
+
+    def assign_spray_comps(self, comps):
+        self._check(lib().pmp_spray_set_comps(self._h, C.byref(comps)))
+
+    def set_geometry(self, geom):
+        self._check(lib().pmp_spray_set_geometry(self._h, C.byref(geom)))
+
+    def set_grids(self, boxes):
+        arr = (capi.Box * len(boxes))()
+        for b, (lo, hi) in enumerate(boxes):
+            for d in range(3):
+                arr[b].lo[d] = int(lo[d])
+                arr[b].hi[d] = int(hi[d])
+        self.nboxes = len(boxes)
+        self._check(lib().pmp_spray_set_grids(self._h, len(boxes), arr))
+
+    def set_mode(self, mode):
+        self._check(lib().pmp_spray_set_mode(self._h, mode))
+
+    # --- droplets ---------------------------------------------------------
+    def set_particles(self, box, pos, rdata, ids):
+        """pos (3,n), rdata (10+F,n) float64, ids (n,) int32: numpy or CUDA tensors."""
+        p = capi.Particles()
+        p.layout = capi.PMP_LAYOUT_SOA
+        p.where = capi.PMP_WHERE_DEVICE if _is_cuda(pos) else capi.PMP_WHERE_HOST
+        p.n = int(ids.shape[0])
+        for d in range(3):
+            p.pos[d] = _ptr(pos[d])
+        for r in range(rdata.shape[0]):
+            p.rdata[r] = _ptr(rdata[r])
+        p.id = _ptr(ids)
+        self._check(lib().pmp_spray_set_particles(self._h, box, C.byref(p)))
+
+    def set_particles_aos(self, box, aos, n, on_device=False):
+        p = capi.Particles()
+        p.layout = capi.PMP_LAYOUT_AOS
+        p.where = capi.PMP_WHERE_DEVICE if on_device else capi.PMP_WHERE_HOST
+        p.n = n
+        p.aos = _ptr(aos)
+        self._check(lib().pmp_spray_set_particles(self._h, box, C.byref(p)))
+
+    def num_particles(self, box):
+        n = C.c_longlong()
+        self._check(lib().pmp_spray_num_particles(self._h, box, C.byref(n)))
+        return n.value
+
+    def get_particles(self, box):
+        """Droplets of `box` in the caller's order as host numpy arrays."""
+        n = self.num_particles(box)
+        nr = capi.pstate_num(self.nfuel)
+        pos = np.zeros((3, n))
+        rdata = np.zeros((nr, n))
+        ids = np.zeros(n, dtype=np.int32)
+        p = capi.Particles()
+        p.layout = capi.PMP_LAYOUT_SOA
+        p.where = capi.PMP_WHERE_HOST
+        p.n = n
+        for d in range(3):
+            p.pos[d] = pos[d].ctypes.data
+        for r in range(nr):
+            p.rdata[r] = rdata[r].ctypes.data
+        p.id = ids.ctypes.data
+        self._check(lib().pmp_spray_get_particles(self._h, box, C.byref(p)))
+        return dict(pos=pos, rdata=rdata, id=ids)
+
+    def get_particles_aos(self, box):
+        n = self.num_particles(box)
+        rec = 8 * (3 + capi.pstate_num(self.nfuel)) + 8
+        buf = np.zeros(n * rec, dtype=np.uint8)
+        p = capi.Particles()
+        p.layout = capi.PMP_LAYOUT_AOS
+        p.where = capi.PMP_WHERE_HOST
+        p.n = n
+        p.aos = buf.ctypes.data
+        self._check(lib().pmp_spray_get_particles(self._h, box, C.byref(p)))
+        return buf
+
+    # --- the update (SprayParticles.cpp:37-87,142-502) --------------------
+    def update_particles(self, state, source, flow_dt, time, state_ghosts, source_ghosts,
+                         is_virt, is_ghost, do_move, spray_cfl_lev, stream=0):
+        """state/source: pmp_box_view arrays (device memory)."""
+        self._check(lib().pmp_spray_update(
+            self._h, state, source, len(state), flow_dt, time, state_ghosts, source_ghosts,
+            int(is_virt), int(is_ghost), int(do_move), spray_cfl_lev, C.c_void_p(stream)))
+
+    def update_particles_host(self, state, source, flow_dt, time, state_ghosts, source_ghosts,
+                              is_virt, is_ghost, do_move, spray_cfl_lev, stream=0):
+        """Same call with host-memory views (copies inside)."""
+        self._check(lib().pmp_spray_update_host(
+            self._h, state, source, len(state), flow_dt, time, state_ghosts, source_ghosts,
+            int(is_virt), int(is_ghost), int(do_move), spray_cfl_lev, C.c_void_p(stream)))
+
+    def move_kick_drift(self, state, source, dt, time, is_virt, is_ghost, state_ghosts,
+                        source_ghosts, do_move=True, spray_cfl_lev=-1.0, stream=0):
+        self._check(lib().pmp_spray_move_kick_drift(
+            self._h, state, source, len(state), dt, time, int(is_virt), int(is_ghost),
+            state_ghosts, source_ghosts, int(do_move), spray_cfl_lev, C.c_void_p(stream)))
+
+    def move_kick(self, state, source, dt, time, is_virt, is_ghost, state_ghosts, source_ghosts,
+                  spray_cfl_lev=-1.0, stream=0):
+        self._check(lib().pmp_spray_move_kick(
+            self._h, state, source, len(state), dt, time, int(is_virt), int(is_ghost),
+            state_ghosts, source_ghosts, spray_cfl_lev, C.c_void_p(stream)))
+
+    def last_error(self):
+        info = capi.ErrorInfo()
+        lib().pmp_spray_last_error(self._h, C.byref(info))
+        return info
+
+    def stats(self):
+        s = capi.Stats()
+        lib().pmp_spray_get_stats(self._h, C.byref(s))
+        return s
+
+
+def from_problem(prob, device=0, mode=capi.PMP_MODE_FP64, set_droplets=True):
+    """Container set up for a workloads.Problem (droplets copied from host)."""
+    sp = SprayParticleContainer(prob.species, prob.nfuel, device)
+    sp.spray_setup(prob.inputs())
+    sp.assign_spray_comps(prob.comps())
+    sp.set_geometry(prob.geometry())
+    sp.set_grids(prob.boxes)
+    sp.set_mode(mode)
+    if set_droplets:
+        for b, p in enumerate(prob.parts):
+            sp.set_particles(b, p["pos"], p["rdata"], p["id"])
+    return sp
