@@ -202,6 +202,20 @@ extern "C" int pmp_ref_update(
     splash_breakup* N_SB = nullptr;
     const bool do_splash_box = false;
     const bool eb_in_box = false;
+    // Gpu::Atomic::Add: an OpenMP atomic when droplets run on several threads
+    const bool atomic = nthreads > 1;
+    auto atomic_add = [atomic](Real& dst, Real v) {
+      if (atomic) {
+#pragma omp atomic
+        dst += v;
+      } else {
+        dst += v;
+      }
+    };
+    long long first_bad = -1;
+    int bad_code = 0;
+    long long box_subs = 0;
+#pragma omp parallel for schedule(dynamic, 256) num_threads(nthreads > 1 ? nthreads : 1) reduction(+ : box_subs)
     for (long long pid = 0; pid < Np; ++pid) {
       RefParticle& p = aos[pid];
       try {
@@ -244,7 +258,7 @@ extern "C" int pmp_ref_update(
             gpv.define();
             fdat->calcBoilT(gpv, cBoilT.data());
             calculateSpraySource(sub_dt, gpv, *fdat, p, cBoilT.data(), ltransparm);
-            ++nsubs;
+            ++box_subs;
             IntVect cur_indx = ijkc;
             Real cvol = inv_vol;
             Real cur_coef = -cvol * sub_dt / flow_dt;
@@ -255,16 +269,16 @@ extern "C" int pmp_ref_update(
             }
             if (fdat->mom_trans) {
               for (int dir = 0; dir < AMREX_SPACEDIM; ++dir) {
-                momSrcarr(cur_indx, dir) += cur_coef * gpv.fluid_mom_src[dir];
+                atomic_add(momSrcarr(cur_indx, dir), cur_coef * gpv.fluid_mom_src[dir]);
               }
             }
             if (fdat->mass_trans) {
-              rhoSrcarr(cur_indx) += cur_coef * gpv.fluid_mass_src;
+              atomic_add(rhoSrcarr(cur_indx), cur_coef * gpv.fluid_mass_src);
               for (int spf = 0; spf < SPRAY_FUEL_NUM; ++spf) {
-                rhoYSrcarr(cur_indx, spf) += cur_coef * gpv.fluid_Y_dot[spf];
+                atomic_add(rhoYSrcarr(cur_indx, spf), cur_coef * gpv.fluid_Y_dot[spf]);
               }
             }
-            engSrcarr(cur_indx) += cur_coef * gpv.fluid_eng_src;
+            atomic_add(engSrcarr(cur_indx), cur_coef * gpv.fluid_eng_src);
             if (do_move && !fdat->fixed_parts && p.id() > 0) {
               for (int dir = 0; dir < AMREX_SPACEDIM; ++dir) {
                 const Real cvel = p.rdata(SprayComps::pstateVel + dir);
@@ -293,17 +307,27 @@ extern "C" int pmp_ref_update(
           }
         }
       } catch (const std::pair<int, long long>& e) {
-        if (err) {
-          err->code = e.first;
-          err->box = b;
-          err->particle = e.second;
-          std::snprintf(err->message, sizeof(err->message), "reference: error %d", e.first);
+#pragma omp critical
+        {
+          if (first_bad < 0 || e.second < first_bad) {
+            first_bad = e.second;
+            bad_code = e.first;
+          }
         }
-        if (substeps) {
-          *substeps = nsubs;
-        }
-        return e.first;
       }
+    }
+    nsubs += box_subs;
+    if (first_bad >= 0) {
+      if (err) {
+        err->code = bad_code;
+        err->box = b;
+        err->particle = first_bad;
+        std::snprintf(err->message, sizeof(err->message), "reference: error %d", bad_code);
+      }
+      if (substeps) {
+        *substeps = nsubs;
+      }
+      return bad_code;
     }
     for (long long i = 0; i < Np; ++i) {
       for (int d = 0; d < 3; ++d) {

@@ -1,0 +1,58 @@
+"""Helpers for the GPU tests: run a workloads.Problem through the C ABI."""
+import numpy as np
+
+from pelemp_b200 import capi
+from pelemp_b200.spray import from_problem, views
+
+
+def device_state(prob):
+    import torch
+    st = [torch.from_numpy(s).cuda() for s in prob.state]
+    return st, views(st, [prob.grown(b, prob.state_ghosts)[0] for b in range(len(prob.boxes))])
+
+
+def device_sources(prob):
+    import torch
+    src = [torch.zeros(s.shape, dtype=torch.float64, device="cuda") for s in prob.new_sources()]
+    return src, views(src, [prob.grown(b, prob.source_ghosts)[0] for b in range(len(prob.boxes))])
+
+
+def gpu_run(prob, steps, mode=capi.PMP_MODE_FP64, is_ghost=0, keep=None):
+    """steps x (MKD + MK) on the GPU; returns (parts per box, sources per call, container)."""
+    import torch
+    sp = from_problem(prob, mode=mode)
+    st_keep, st_v = device_state(prob)  # keep the tensors alive while the views are used
+    srcs = []
+    for _step in range(steps):
+        for do_move in (1, 0):
+            src, src_v = device_sources(prob)
+            sp.update_particles(st_v, src_v, prob.flow_dt, 0.0, prob.state_ghosts,
+                                prob.source_ghosts, 0, is_ghost, do_move, prob.spray_cfl_lev,
+                                torch.cuda.current_stream().cuda_stream)
+            srcs.append([s.cpu().numpy() for s in src])
+    parts = [sp.get_particles(b) for b in range(len(prob.boxes))]
+    del st_keep
+    return parts, srcs, sp
+
+
+def oracle_run(oracle, prob, steps, is_ghost=0):
+    mech = oracle.mech(prob.species)
+    rc, fdat = oracle.setup(prob, mech)
+    assert rc == 0
+    parts = prob.copy_parts()
+    srcs = []
+    for _ in range(steps):
+        for do_move in (1, 0):
+            src = prob.new_sources()
+            rc, err, _ = oracle.update(prob, mech, fdat, parts, src, do_move, is_ghost=is_ghost)
+            assert rc == 0, (rc, err.message)
+            srcs.append(src)
+    return parts, srcs
+
+
+def assert_bitwise(pa, pb):
+    for a, b in zip(pa, pb):
+        for k in ("pos", "rdata", "id"):
+            if not np.array_equal(a[k], b[k]):
+                diff = np.nonzero(~np.all(a[k] == b[k], axis=0) if a[k].ndim > 1 else a[k] != b[k])[0]
+                raise AssertionError(f"{k} differs at {diff[:10]} (of {diff.size})")
