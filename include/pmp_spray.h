@@ -279,6 +279,33 @@ int pmp_spray_get_stats(const pmp_spray* h, pmp_stats* stats);
 /* Library version string. */
 const char* pmp_spray_version(void);
 
+/* Allocation-free update.  No counterpart in the reference: PeleMP relies on
+ * AMReX allocating as it goes.  For hosts that cannot call cudaMalloc when the
+ * update runs -- every byte of device memory already handed to their own
+ * pre-sized pool, or work being issued into a CUDA stream capture, where
+ * allocation is not allowed.  The caller passes everything: the gas species
+ * (cfg; cfg->device is ignored, the current device is used), a built SprayData,
+ * the component indices, geometry and boxes, the droplets of each box as
+ * DEVICE SoA arrays (updated in place, caller's order, not sorted), and
+ * device state/source views.  The plain FP64 kernel runs with its working
+ * data in one fixed device array inside the library (about 90 KB per device,
+ * held until the process exits); nothing is allocated or freed.
+ *  - nboxes <= PMP_STATIC_MAX_BOXES, else PMP_ERR_INVALID;
+ *  - the first call on a device looks up that array's address (with the
+ *    device current): make it before any stream capture;
+ *  - all calls share the array: calls whose GPU work overlaps race, so
+ *    serialise them;
+ *  - err (may be NULL) receives the status, box and droplet index. */
+#define PMP_STATIC_MAX_BOXES 256
+int pmp_spray_update_static(
+  const pmp_spray_config* cfg, const pmp_spray_data* data,
+  const pmp_spray_comps* comps, const pmp_geometry* geom, int nboxes,
+  const pmp_box* boxes, const pmp_particles* parts,
+  const pmp_box_view* state, const pmp_box_view* source, double flow_dt,
+  double time, int state_ghosts, int source_ghosts, int is_virt,
+  int is_ghost, int do_move, double spray_cfl_lev, void* stream,
+  pmp_error_info* err);
+
 #ifdef __cplusplus
 }
 #endif

@@ -15,7 +15,7 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libpmpspray.so")
-SOURCES = ["pmp_spray.cu"]
+SOURCES = ["pmp_spray.cu", "pmp_static.cu"]
 HEADERS = ["pmp_device.cuh", "spray_fp64.cuh", "phys/pmp_math.h", "phys/pmp_thermo.h",
            "phys/pmp_thermo_data.h"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
