@@ -16,7 +16,7 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libpmpspray.so")
 SOURCES = ["pmp_spray.cu", "pmp_static.cu"]
-HEADERS = ["pmp_device.cuh", "spray_fp64.cuh", "phys/pmp_math.h", "phys/pmp_thermo.h",
+HEADERS = ["pmp_device.cuh", "spray_fp64.cuh", "phys/pmp_math.h", "phys/pmp_math_tables.h", "phys/pmp_thermo.h",
            "phys/pmp_thermo_data.h"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -48,12 +48,30 @@ def build_lib(force=False, ptxas_verbose=False):
     return LIB
 
 
+DRIVER = os.path.join(PKG, "pmp_spray_driver")
+
+
+def build_driver(force=False):
+    """The C++ host driver over the C ABI (links libpmpspray.so)."""
+    src = os.path.join(CSRC, "host", "spray_driver.cpp")
+    deps = [src, os.path.join(CSRC, "host", "SprayParticleContainer.H"),
+            os.path.join(ROOT, "include", "pmp_spray.h"), LIB]
+    if not (force or _newer(DRIVER, deps)):
+        return DRIVER
+    subprocess.run(["g++", "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"),
+                    "-I", os.path.join(CSRC, "host"), "-o", DRIVER + ".tmp", src,
+                    "-L", PKG, "-lpmpspray", "-Wl,-rpath,$ORIGIN"], check=True)
+    os.replace(DRIVER + ".tmp", DRIVER)
+    return DRIVER
+
+
 def build_oracle():
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
 
 
 def main(argv):
     build_lib(force="--force" in argv, ptxas_verbose="--verbose-ptxas" in argv)
+    build_driver(force="--force" in argv)
     if "--no-oracle" not in argv:
         build_oracle()
 

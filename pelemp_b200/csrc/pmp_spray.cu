@@ -75,6 +75,8 @@ struct pmp_spray {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   pmp_error_info last_err;
   pmp_stats stats;
+  // view pointers already checked to be device-accessible
+  std::vector<const double*> checked_state, checked_src;
   // device mirrors of host views for pmp_spray_update_host
   std::vector<double*> stage_state, stage_src;
   std::vector<size_t> stage_state_n, stage_src_n;
@@ -386,6 +388,19 @@ int unsort_box(pmp_spray* h, int b, double* out_d, int* out_id, long long n)
   return PMP_OK;
 }
 
+// Device memory, managed memory or pinned (mapped) host memory; a plain host
+// pointer would fault in the kernel.
+bool device_accessible(const void* p)
+{
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged ||
+         a.type == cudaMemoryTypeHost;
+}
+
 bool view_covers(const pmp_box_view& v, const int* lo, const int* hi, int ncomp_needed)
 {
   if (v.p == nullptr || v.ncomp < ncomp_needed) {
@@ -502,6 +517,22 @@ int do_update(
     }
     if (!view_covers(source[b], e.src_lo, e.src_hi, need_src)) {
       return set_err(h, PMP_ERR_INVALID, "source view does not cover the grown box", b);
+    }
+    if ((int)h->checked_state.size() != nboxes) {
+      h->checked_state.assign(nboxes, nullptr);
+      h->checked_src.assign(nboxes, nullptr);
+    }
+    if (h->checked_state[b] != state[b].p) {
+      if (!device_accessible(state[b].p)) {
+        return set_err(h, PMP_ERR_INVALID, "state view is not device memory (use pmp_spray_update_host)", b);
+      }
+      h->checked_state[b] = state[b].p;
+    }
+    if (h->checked_src[b] != source[b].p) {
+      if (!device_accessible(source[b].p)) {
+        return set_err(h, PMP_ERR_INVALID, "source view is not device memory (use pmp_spray_update_host)", b);
+      }
+      h->checked_src[b] = source[b].p;
     }
     e.st = state[b].p;
     e.sr = source[b].p;

@@ -78,6 +78,16 @@ __device__ __forceinline__ double rhoL(const DevFuel& f, double T, int spf)
   return a + T * (b + T * (c + T * d));
 }
 
+// log1p(x) and (1 + x)^0.7 sharing one log(1 + x); bit-identical to
+// pmp_log1p(x) and pmp_pow(1. + x, 0.7) for x > -1
+__device__ __forceinline__ void log1p_pow07(double x, double& l1p, double& p07)
+{
+  const double u = 1. + x;
+  const double lu = pmp_log(u);
+  l1p = (fabs(x) < 0.0078125) ? pmp_log1p_core(x) : pmp_log1p_from(x, u, lu);
+  p07 = pmp_exp(0.7 * lu);
+}
+
 // calcHeatCoeff (Drag.H:6-45); pow(BM1, phi) = exp(phi log BM1) with the
 // loop-invariant log hoisted (bit-identical to pmp_pow)
 __device__ __forceinline__ double heat_coeff(
@@ -92,8 +102,9 @@ __device__ __forceinline__ double heat_coeff(
   const double lnBM1 = pmp_log(BM1);
   double phi = ratio / Nu_0;
   double B_T_old = pmp_exp(phi * lnBM1) - 1.;
-  double logB = pmp_log1p(B_T_old);
-  double invFT = B_T_old / (logB * pmp_pow(1. + B_T_old, 0.7));
+  double logB, p07;
+  log1p_pow07(B_T_old, logB, p07);
+  double invFT = B_T_old / (logB * p07);
   double Nu_num = 2. + NU2 * invFT;
   phi = ratio / Nu_num;
   double B_T = pmp_exp(phi * lnBM1) - 1.;
@@ -101,16 +112,16 @@ __device__ __forceinline__ double heat_coeff(
   int k = 0;
   while (k < maxIter && error > B_eps) {
     B_T_old = B_T;
-    logB = pmp_log1p(B_T);
-    invFT = B_T / (logB * pmp_pow(1. + B_T, 0.7));
+    log1p_pow07(B_T, logB, p07);
+    invFT = B_T / (logB * p07);
     Nu_num = 2. + NU2 * invFT;
     phi = ratio / Nu_num;
     B_T = pmp_exp(phi * lnBM1) - 1.;
     error = fabs(B_T - B_T_old);
     k++;
   }
-  logB = pmp_log1p(B_T);
-  invFT = B_T / (logB * pmp_pow(1. + B_T, 0.7));
+  log1p_pow07(B_T, logB, p07);
+  invFT = B_T / (logB * p07);
   Nu_num = 2. + NU2 * invFT;
   return Nu_num * logB / B_T;
 }
@@ -383,8 +394,9 @@ __device__ __forceinline__ int spray_source_fp64(
         }
         cp_fuel /= sumYSkin;
         const double Sc_skin = mu_skin / rhoDtotal;
-        const double logB = pmp_log1p(B_M);
-        const double invFM = B_M / (logB * pmp_pow(1. + B_M, 0.7));
+        double logB, pBM07;
+        log1p_pow07(B_M, logB, pBM07);
+        const double invFM = B_M / (logB * pBM07);
         const double Sh_0 = 1. + powR * pmp_cbrt(1. + Reyn * Sc_skin);
         const double Sh_num = 2. + (Sh_0 - 2.) * invFM;
         const double mdotcoeff = PMP_PI * dia_part * Sh_num * logB;
@@ -570,8 +582,12 @@ __device__ __forceinline__ bool in_box(const int* lo, const int* hi, int i, int 
   return i >= lo[0] && i <= hi[0] && j >= lo[1] && j <= hi[1] && k >= lo[2] && k <= hi[2];
 }
 
+#ifndef PMP_FP64_MIN_BLOCKS
+#define PMP_FP64_MIN_BLOCKS 5  /* 96 registers: 5 CTAs of 128 per SM (measured best) */
+#endif
+
 template <int NS, int NF, int BLOCK>
-__global__ void __launch_bounds__(BLOCK) spray_update_fp64(const __grid_constant__ KParams P)
+__global__ void __launch_bounds__(BLOCK, PMP_FP64_MIN_BLOCKS) spray_update_fp64(const __grid_constant__ KParams P)
 {
   const int b = P.cta_box[blockIdx.x];
   const BoxEntry& B = P.boxes[b];

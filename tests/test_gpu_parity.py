@@ -129,6 +129,20 @@ def test_error_film_unsupported():
     _expect_error(prob, capi.PMP_ERR_UNSUPPORTED, 3, box=1)
 
 
+def test_host_pointer_rejected_by_device_entry_point():
+    """Plain host arrays given to pmp_spray_update are refused before launch."""
+    import torch
+    prob = W.config1(n=100, steps=1)
+    sp = from_problem(prob)
+    st_h = views(prob.state, [prob.grown(0, prob.state_ghosts)[0]])
+    src, src_v = device_sources(prob)
+    with pytest.raises(SprayError) as e:
+        sp.update_particles(st_h, src_v, prob.flow_dt, 0.0, prob.state_ghosts, prob.source_ghosts,
+                            0, 0, 1, prob.spray_cfl_lev, torch.cuda.current_stream().cuda_stream)
+    assert e.value.code == capi.PMP_ERR_INVALID
+    sp.close()
+
+
 def test_empty_boxes_and_zero_droplets():
     prob = W.config2(n=0, steps=1, ncells=(32, 32, 32), box=(16, 16, 16))
     pg, sg, sp = gpu_run(prob, 1)
