@@ -222,6 +222,7 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=100_000)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--mode", default="fp64", choices=["fp64", "mixed"])
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -249,7 +250,8 @@ def main():
     prob = W.config2(n=args.droplets, seed=rank, steps=args.steps)
     nboxes = len(prob.boxes)
     ncells = int(np.prod([prob.domain_hi[d] - prob.domain_lo[d] + 1 for d in range(3)]))
-    sp = from_problem(prob, device=local)
+    mode = {"fp64": capi.PMP_MODE_FP64, "mixed": capi.PMP_MODE_MIXED}[args.mode]
+    sp = from_problem(prob, device=local, mode=mode)
     stream = torch.cuda.current_stream()
     st = [torch.from_numpy(s).cuda() for s in prob.state]
     st_v = views(st, [prob.grown(b, prob.state_ghosts)[0] for b in range(nboxes)])
@@ -371,7 +373,7 @@ def main():
                                    "as 8 boxes of 64^3, 5 gas species, dt=5e-7 s, MKD 4 sub-cycles "
                                    "+ MK 1 sub-cycle per step",
                        "droplets_per_gpu": prob.n_droplets, "boxes": nboxes,
-                       "form": "plain FP64",
+                       "form": {"fp64": "plain FP64", "mixed": "mixed FP32/FP64"}[args.mode],
                        "l2": "inputs larger than L2 (1.9 GB droplet SoA, 0.24 GB state per GPU)",
                        "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

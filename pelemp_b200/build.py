@@ -15,11 +15,18 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libpmpspray.so")
-SOURCES = ["pmp_spray.cu", "pmp_static.cu"]
-HEADERS = ["pmp_device.cuh", "spray_fp64.cuh", "phys/pmp_math.h", "phys/pmp_math_tables.h", "phys/pmp_thermo.h",
+# (source, contraction flag): the FP64 kernels reproduce the oracle's
+# arithmetic exactly, so their units are compiled without multiply-add
+# contraction (their multiply-adds are explicit fma() calls); the mixed and
+# learned forms allow it.
+SOURCES = [("pmp_spray.cu", "-fmad=false"), ("pmp_static.cu", "-fmad=false"),
+           ("pmp_mixed.cu", "-fmad=true")]
+HEADERS = ["pmp_device.cuh", "spray_fp64.cuh", "spray_mixed.cuh", "spray_kernels.cuh",
+           "phys/pmp_math.h", "phys/pmp_math_tables.h", "phys/pmp_thermo.h",
            "phys/pmp_thermo_data.h"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+OBJDIR = os.path.join(ROOT, "_build")
 
 
 def _newer(target, deps):
@@ -29,21 +36,28 @@ def _newer(target, deps):
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build_lib(force=False, ptxas_verbose=False):
-    deps = [os.path.join(CSRC, s) for s in SOURCES + HEADERS]
+def build_lib(force=False, ptxas_verbose=False, extra=()):
+    deps = [os.path.join(CSRC, s) for s, _ in SOURCES] + [os.path.join(CSRC, h) for h in HEADERS]
     deps.append(os.path.join(ROOT, "include", "pmp_spray.h"))
     deps.append(os.path.abspath(__file__))
-    if not (force or ptxas_verbose or _newer(LIB, deps)):
+    if not (force or ptxas_verbose or extra or _newer(LIB, deps)):
         return LIB
-    # -fmad=false: the FP64 kernel reproduces the oracle's arithmetic exactly
-    # (its multiply-adds are explicit fma() calls)
-    cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC",
-           "-shared",
-           "--expt-relaxed-constexpr", "-I", os.path.join(ROOT, "include"), "-I", CSRC,
-           "-o", LIB + ".tmp"] + [os.path.join(CSRC, s) for s in SOURCES]
-    if ptxas_verbose:
-        cmd.insert(1, "-Xptxas=-v")
-    subprocess.run(cmd, check=True)
+    os.makedirs(OBJDIR, exist_ok=True)
+    procs = []
+    objs = []
+    for src, fmad in SOURCES:
+        obj = os.path.join(OBJDIR, src.replace(".cu", ".o"))
+        cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", fmad, "-Xcompiler", "-fPIC",
+               "--expt-relaxed-constexpr", "-I", os.path.join(ROOT, "include"), "-I", CSRC,
+               *extra, "-c", "-o", obj, os.path.join(CSRC, src)]
+        if ptxas_verbose:
+            cmd.insert(1, "-Xptxas=-v")
+        procs.append(subprocess.Popen(cmd))
+        objs.append(obj)
+    for p in procs:
+        if p.wait() != 0:
+            raise subprocess.CalledProcessError(p.returncode, "nvcc")
+    subprocess.run([NVCC, *ARCH, "-shared", "-o", LIB + ".tmp", *objs], check=True)
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

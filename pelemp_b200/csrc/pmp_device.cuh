@@ -110,6 +110,8 @@ struct KParams {
   const BoxEntry* boxes;
   const int* cta_box;
   const long long* cta_start;
+  const long long* box_begin;  // nboxes + 1 slot offsets
+  long long* fb_list;          // slots handed to the FP64 fallback kernel
   DevStatus* status;
 };
 

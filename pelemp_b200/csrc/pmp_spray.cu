@@ -18,7 +18,12 @@
 
 #include "phys/pmp_thermo.h"
 #include "pmp_device.cuh"
-#include "spray_fp64.cuh"
+#include "spray_kernels.cuh"
+
+namespace pmp {
+// pmp_mixed.cu
+int launch_mixed(int ns, int nf, const KParams& P, int ncta, int block, cudaStream_t st);
+}  // namespace pmp
 
 using pmp::BoxEntry;
 using pmp::DevStatus;
@@ -67,6 +72,8 @@ struct pmp_spray {
   int ncta = 0;
   int* d_cta_box = nullptr;
   long long* d_cta_start = nullptr;
+  long long* d_box_begin = nullptr;
+  long long* fb_list = nullptr;  // fallback slots (mixed / learned forms)
   BoxEntry* d_boxes = nullptr;
   BoxEntry* h_boxes = nullptr;
   int boxes_cap = 0;
@@ -218,11 +225,15 @@ void free_packed(pmp_spray* h)
   cudaFree(h->perm);
   cudaFree(h->d_cta_box);
   cudaFree(h->d_cta_start);
+  cudaFree(h->d_box_begin);
+  cudaFree(h->fb_list);
   h->soa = nullptr;
   h->ids = nullptr;
   h->perm = nullptr;
   h->d_cta_box = nullptr;
   h->d_cta_start = nullptr;
+  h->d_box_begin = nullptr;
+  h->fb_list = nullptr;
   h->packed = false;
   h->ncta = 0;
 }
@@ -365,6 +376,10 @@ int pack(pmp_spray* h)
     PMP_CUDA(h, cudaMemcpy(h->d_cta_box, cb.data(), sizeof(int) * h->ncta, cudaMemcpyHostToDevice));
     PMP_CUDA(h, cudaMemcpy(h->d_cta_start, cs.data(), sizeof(long long) * h->ncta, cudaMemcpyHostToDevice));
   }
+  PMP_CUDA(h, cudaMalloc(&h->d_box_begin, sizeof(long long) * (nb + 1)));
+  PMP_CUDA(h, cudaMemcpy(h->d_box_begin, h->box_begin.data(), sizeof(long long) * (nb + 1),
+                         cudaMemcpyHostToDevice));
+  PMP_CUDA(h, cudaMalloc(&h->fb_list, sizeof(long long) * cap));
   h->packed = true;
   return PMP_OK;
 }
@@ -467,6 +482,25 @@ int dispatch_fp64(int ns, int nf, const KParams& P, int ncta, cudaStream_t st)
   return PMP_ERR_UNSUPPORTED;
 }
 
+// the FP64 kernel over the fallback list filled by the mixed / learned kernels
+int dispatch_fp64_list(int ns, int nf, const KParams& P, long long total, cudaStream_t st)
+{
+  const long long need = (total + kBlock - 1) / kBlock;
+  const int grid = (int)std::max(1LL, std::min(need, 148LL * 4));
+#define PMP_CASE(S, F)                                                              \
+  if (ns == S && nf == F) {                                                         \
+    pmp::spray_update_fp64_list<S, F, kBlock><<<grid, kBlock, 0, st>>>(P);          \
+    return PMP_OK;                                                                  \
+  }
+  PMP_CASE(3, 1)
+  PMP_CASE(5, 1)
+  PMP_CASE(5, 2)
+  PMP_CASE(4, 1)
+  PMP_CASE(4, 2)
+#undef PMP_CASE
+  return PMP_ERR_UNSUPPORTED;
+}
+
 int do_update(
   pmp_spray* h, const pmp_box_view* state, const pmp_box_view* source, int nboxes,
   double flow_dt, int state_ghosts, int source_ghosts, int is_virt, int is_ghost, int do_move,
@@ -480,7 +514,7 @@ int do_update(
   if (nboxes != (int)h->boxes.size()) {
     return set_err(h, PMP_ERR_INVALID, "nboxes differs from the grids given to set_grids");
   }
-  if (h->mode != PMP_MODE_FP64) {
+  if (h->mode != PMP_MODE_FP64 && h->mode != PMP_MODE_MIXED) {
     return set_err(h, PMP_ERR_UNSUPPORTED, "this method form is not available");
   }
   if (h->data.do_breakup != 0 || h->data.do_splash) {
@@ -602,9 +636,19 @@ int do_update(
   P.cta_box = h->d_cta_box;
   P.cta_start = h->d_cta_start;
   P.status = h->d_status;
+  P.box_begin = h->d_box_begin;
+  P.fb_list = h->fb_list;
   PMP_CUDA(h, cudaEventRecord(h->ev0, st));
   if (h->ncta > 0) {
-    rc = dispatch_fp64(NS, NF, P, h->ncta, st);
+    if (h->mode == PMP_MODE_MIXED) {
+      rc = pmp::launch_mixed(NS, NF, P, h->ncta, kBlock, st);
+      if (rc == PMP_OK) {
+        PMP_CUDA(h, cudaGetLastError());
+        rc = dispatch_fp64_list(NS, NF, P, h->total, st);
+      }
+    } else {
+      rc = dispatch_fp64(NS, NF, P, h->ncta, st);
+    }
     if (rc != PMP_OK) {
       return set_err(h, rc, "no kernel for this species / fuel count");
     }

@@ -582,244 +582,4 @@ __device__ __forceinline__ bool in_box(const int* lo, const int* hi, int i, int 
   return i >= lo[0] && i <= hi[0] && j >= lo[1] && j <= hi[1] && k >= lo[2] && k <= hi[2];
 }
 
-#ifndef PMP_FP64_MIN_BLOCKS
-#define PMP_FP64_MIN_BLOCKS 5  /* 96 registers: 5 CTAs of 128 per SM (measured best) */
-#endif
-
-template <int NS, int NF, int BLOCK>
-__global__ void __launch_bounds__(BLOCK, PMP_FP64_MIN_BLOCKS) spray_update_fp64(const __grid_constant__ KParams P)
-{
-  const int b = P.cta_box[blockIdx.x];
-  const BoxEntry& B = P.boxes[b];
-  const long long s = P.cta_start[blockIdx.x] + threadIdx.x;
-  unsigned long long my_sub = 0, my_killed = 0, my_inner = 0;
-  if (s < B.p_end) {
-    int id = P.parts.id[s];
-    if (id > 0) {
-      double pos[3], vel[3], Y[NF];
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        pos[d] = P.parts.pos[d][s];
-        vel[d] = P.parts.rd[PMP_PSTATE_VEL + d][s];
-      }
-      double T = P.parts.rd[PMP_PSTATE_T][s];
-      double dia = P.parts.rd[PMP_PSTATE_DIA][s];
-#pragma unroll
-      for (int spf = 0; spf < NF; ++spf) {
-        Y[spf] = P.parts.rd[PMP_PSTATE_Y + spf][s];
-      }
-      const double num_ppp = P.parts.rd[PMP_PSTATE_NUMDENS(NF)][s];
-      const double film = P.parts.rd[PMP_PSTATE_FILMHGHT(NF)][s];
-      // cell of the upper stencil centre and cell holding the droplet (SprayParticles.cpp:340-343)
-      double lx[3];
-      int ijk[3], ijkc[3];
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        lx[d] = (pos[d] - P.plo[d]) * P.dxi[d] + 0.5;
-        ijk[d] = static_cast<int>(floor(lx[d]));
-        ijkc[d] = static_cast<int>(floor((pos[d] - P.plo[d]) * P.dxi[d]));
-      }
-      int bflags[3] = {0, 0, 0};
-      bool ok = true;
-      if (B.at_bounds) {
-        if (check_bounds(P, pos, bflags)) {
-          set_error(P, PMP_ERR_LEFT_DOMAIN, b, s);
-          ok = false;
-        }
-      }
-      for (int cur_iter = 0; ok && cur_iter < P.num_iter && id > 0; ++cur_iter) {
-        if (film > 0.) {
-          set_error(P, PMP_ERR_UNSUPPORTED, b, s);
-          ok = false;
-          break;
-        }
-        // trilinear_interp (SprayInterpolation.H:158-199)
-        double ssv[2][3];
-#pragma unroll
-        for (int dir = 0; dir < 3; ++dir) {
-          const double sx_hi = lx[dir] - static_cast<double>(ijk[dir]);
-          const double sx_lo = 1. - sx_hi;
-          if (bflags[dir] > 1) {
-            ssv[0][dir] = 1.;
-            ssv[1][dir] = 0.;
-          } else if (bflags[dir] < -1) {
-            ssv[0][dir] = 0.;
-            ssv[1][dir] = 1.;
-          } else {
-            ssv[0][dir] = sx_lo;
-            ssv[1][dir] = sx_hi;
-          }
-        }
-        // InterpolateGasPhase (SprayInterpolation.H:99-150), PeleLMeX branch
-        GasVals<NS, NF> gpv;
-        gpv.rho = 0.;
-        gpv.T = 0.;
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          gpv.vel[d] = 0.;
-          gpv.mom_src[d] = 0.;
-        }
-#pragma unroll
-        for (int n = 0; n < NS; ++n) {
-          gpv.Y[n] = 0.;
-        }
-#pragma unroll
-        for (int spf = 0; spf < NF; ++spf) {
-          gpv.Ydot[spf] = 0.;
-        }
-        gpv.eng_src = 0.;
-        gpv.mass_src = 0.;
-        bool state_ok = true;
-#pragma unroll
-        for (int kk = -1; kk < 1; ++kk) {
-#pragma unroll
-          for (int jj = -1; jj < 1; ++jj) {
-#pragma unroll
-            for (int ii = -1; ii < 1; ++ii) {
-              const double cw = ssv[ii + 1][0] * ssv[jj + 1][1] * ssv[kk + 1][2];
-              if (cw > 0.) {
-                const int ci = ijk[0] + ii;
-                const int cj = ijk[1] + jj;
-                const int ck = ijk[2] + kk;
-                if (!in_box(B.state_lo, B.state_hi, ci, cj, ck)) {
-                  state_ok = false;
-                } else {
-                  const double* q = B.st + (long long)(ci - B.st_lo[0]) +
-                                    (long long)(cj - B.st_lo[1]) * B.st_js +
-                                    (long long)(ck - B.st_lo[2]) * B.st_ks;
-                  const double cur_rho = __ldg(q + (long long)P.c_rho * B.st_ns);
-                  gpv.rho += cw * cur_rho;
-                  const double inv_rho = 1. / cur_rho;
-#pragma unroll
-                  for (int n = 0; n < NS; ++n) {
-                    const double cur_mf = __ldg(q + (long long)(P.c_spec + n) * B.st_ns) * inv_rho;
-                    gpv.Y[n] += cw * cur_mf;
-                  }
-#pragma unroll
-                  for (int dir = 0; dir < 3; ++dir) {
-                    gpv.vel[dir] += cw * __ldg(q + (long long)(P.c_mom + dir) * B.st_ns);
-                  }
-                  gpv.T += cw * __ldg(q + (long long)P.c_T * B.st_ns);
-                }
-              }
-            }
-          }
-        }
-        if (!state_ok) {
-          set_error(P, PMP_ERR_STATE_BOX, b, s);
-          ok = false;
-          break;
-        }
-        // GasPhaseVals::define (SprayFuelData.H:101-111)
-        double mw_mix = 0.;
-#pragma unroll
-        for (int n = 0; n < NS; ++n) {
-          mw_mix += gpv.Y[n] / P.m.mw_kg[n];
-        }
-        gpv.p = gpv.rho * kRuCgs * mw_mix * gpv.T * kRuConv;
-        gpv.mw_mix = 1. / mw_mix;
-        // SprayData::calcBoilT (SprayFuelData.H:178-200)
-        double cBoilT[NF];
-        {
-          const double RU = kRuCgs * kRuConv;
-          const double PATM = kPatmCgs * kPresConv;
-          const double lp = pmp_log(PATM / gpv.p);
-#pragma unroll
-          for (int spf = 0; spf < NF; ++spf) {
-            const double mw_fuel = P.m.mw_kg[P.f.indx[spf]];
-            const double c = 1. / (lp * RU / (P.f.hboil_ref[spf] * mw_fuel) + 1. / P.f.boilT[spf]);
-            cBoilT[spf] = dmin(P.f.critT[spf], c);
-          }
-        }
-        const int nsub = spray_source_fp64<NS, NF>(P, P.sub_dt, gpv, vel, T, dia, Y, num_ppp, id, cBoilT);
-        my_sub += 1;
-        my_inner += static_cast<unsigned long long>(nsub);
-        // source scatter into the cell holding the droplet (SprayParticles.cpp:419-441)
-        const double cur_coef = -P.inv_vol * P.sub_dt / P.flow_dt;
-        if (!in_box(B.src_lo, B.src_hi, ijkc[0], ijkc[1], ijkc[2])) {
-          if (!P.is_ghost || !in_box(B.sr_alo, B.sr_ahi, ijkc[0], ijkc[1], ijkc[2])) {
-            set_error(P, PMP_ERR_SOURCE_BOX, b, s);
-            ok = false;
-            break;
-          }
-        }
-        double* q = B.sr + (long long)(ijkc[0] - B.sr_lo[0]) + (long long)(ijkc[1] - B.sr_lo[1]) * B.sr_js +
-                    (long long)(ijkc[2] - B.sr_lo[2]) * B.sr_ks;
-        if (P.f.mom_trans) {
-#pragma unroll
-          for (int dir = 0; dir < 3; ++dir) {
-            atomicAdd(q + (long long)(P.s_mom + dir) * B.sr_ns, cur_coef * gpv.mom_src[dir]);
-          }
-        }
-        if (P.f.mass_trans) {
-          atomicAdd(q + (long long)P.s_rho * B.sr_ns, cur_coef * gpv.mass_src);
-#pragma unroll
-          for (int spf = 0; spf < NF; ++spf) {
-            atomicAdd(q + (long long)(P.s_spec + spf) * B.sr_ns, cur_coef * gpv.Ydot[spf]);
-          }
-        }
-        atomicAdd(q + (long long)P.s_eng * B.sr_ns, cur_coef * gpv.eng_src);
-        // move (SprayParticles.cpp:444-476)
-        if (P.do_move && !P.f.fixed_parts && id > 0) {
-#pragma unroll
-          for (int dir = 0; dir < 3; ++dir) {
-            pos[dir] += P.sub_dt * vel[dir];
-          }
-          if (B.at_bounds) {
-            if (check_bounds(P, pos, bflags)) {
-              id = -1;
-            } else {
-              impose_wall(P, pos, vel, bflags);
-            }
-          }
-#pragma unroll
-          for (int d = 0; d < 3; ++d) {
-            lx[d] = (pos[d] - P.plo[d]) * P.dxi[d] + 0.5;
-            ijk[d] = static_cast<int>(floor(lx[d]));
-            ijkc[d] = static_cast<int>(floor((pos[d] - P.plo[d]) * P.dxi[d]));
-          }
-        }
-        if (P.is_ghost && !in_box(B.src_lo, B.src_hi, ijkc[0], ijkc[1], ijkc[2])) {
-          id = -1;
-        }
-      }
-      if (ok) {
-        if (P.do_move) {
-#pragma unroll
-          for (int d = 0; d < 3; ++d) {
-            P.parts.pos[d][s] = pos[d];
-          }
-        }
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          P.parts.rd[PMP_PSTATE_VEL + d][s] = vel[d];
-        }
-        P.parts.rd[PMP_PSTATE_T][s] = T;
-        P.parts.rd[PMP_PSTATE_DIA][s] = dia;
-#pragma unroll
-        for (int spf = 0; spf < NF; ++spf) {
-          P.parts.rd[PMP_PSTATE_Y + spf][s] = Y[spf];
-        }
-        if (id <= 0) {
-          P.parts.id[s] = id;
-          my_killed = 1;
-        }
-      }
-    }
-  }
-  // per-warp counter reduction, one atomic per warp
-  const unsigned mask = 0xffffffffu;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    my_sub += __shfl_down_sync(mask, my_sub, o);
-    my_killed += __shfl_down_sync(mask, my_killed, o);
-    my_inner += __shfl_down_sync(mask, my_inner, o);
-  }
-  if ((threadIdx.x & 31) == 0 && (my_sub | my_killed | my_inner)) {
-    atomicAdd(&P.status->substeps, my_sub);
-    atomicAdd(&P.status->killed, my_killed);
-    atomicAdd(&P.status->inner, my_inner);
-  }
-}
-
 }  // namespace pmp

@@ -1,0 +1,343 @@
+// spray_kernels.cuh -- the droplet driver loop and the update kernels.
+//
+// update_one<NS, NF, FORM> is the body of the device lambda of
+// SprayParticleContainer::updateParticles (SprayParticles.cpp:324-481) for
+// one droplet slot: cell location, bounds check, and per sub-cycle the
+// trilinear gather (SprayInterpolation.H:99-199), GasPhaseVals::define,
+// calcBoilT (SprayFuelData.H:178-200), the droplet physics of the chosen form
+// (spray_source_fp64 or spray_source_mixed), the atomic scatter into the cell
+// holding the droplet (SprayParticles.cpp:419-441) and the move with wall
+// handling (SprayParticles.cpp:444-479).
+//
+// Cell indices and positions are formed with explicit round-to-nearest
+// intrinsics, so they are bit-exact whatever the translation unit's
+// contraction setting.
+//
+// Kernels
+//  - spray_update_fp64<NS,NF,BLOCK>: plain FP64, one thread per droplet, CTA
+//    -> (box, first slot) from the work map;
+//  - spray_update_mixed<NS,NF,BLOCK>: mixed precision; droplets entering the
+//    call with d < 2 um are appended to the fallback list instead;
+//  - spray_update_fp64_list<NS,NF,BLOCK>: plain FP64 over the fallback list
+//    (grid-stride; the list length is read on the device).
+#pragma once
+
+#include "spray_fp64.cuh"
+#include "spray_mixed.cuh"
+
+namespace pmp {
+
+enum class Form { FP64 = 0, MIXED = 1 };
+
+struct Counters {
+  unsigned long long sub = 0;
+  unsigned long long killed = 0;
+  unsigned long long inner = 0;
+};
+
+__device__ __forceinline__ void cell_of(const KParams& P, const double* pos, double* lx, int* ijk, int* ijkc)
+{
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const double l = __dmul_rn(__dsub_rn(pos[d], P.plo[d]), P.dxi[d]);
+    lx[d] = __dadd_rn(l, 0.5);
+    ijk[d] = static_cast<int>(floor(lx[d]));
+    ijkc[d] = static_cast<int>(floor(l));
+  }
+}
+
+// Returns false if the droplet was handed to the fallback list (MIXED only).
+template <int NS, int NF, Form FORM>
+__device__ __forceinline__ void update_one(const KParams& P, int b, long long s, Counters& c)
+{
+  const BoxEntry& B = P.boxes[b];
+  int id = P.parts.id[s];
+  if (!(id > 0)) {
+    return;
+  }
+  double dia = P.parts.rd[PMP_PSTATE_DIA][s];
+  if (FORM == Form::MIXED && dia < kMixedMinDia) {
+    const unsigned long long k = atomicAdd(&P.status->fallback, 1ULL);
+    P.fb_list[k] = s;
+    return;
+  }
+  double pos[3], vel[3], Y[NF];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    pos[d] = P.parts.pos[d][s];
+    vel[d] = P.parts.rd[PMP_PSTATE_VEL + d][s];
+  }
+  double T = P.parts.rd[PMP_PSTATE_T][s];
+#pragma unroll
+  for (int spf = 0; spf < NF; ++spf) {
+    Y[spf] = P.parts.rd[PMP_PSTATE_Y + spf][s];
+  }
+  const double num_ppp = P.parts.rd[PMP_PSTATE_NUMDENS(NF)][s];
+  const double film = P.parts.rd[PMP_PSTATE_FILMHGHT(NF)][s];
+  double lx[3];
+  int ijk[3], ijkc[3];
+  cell_of(P, pos, lx, ijk, ijkc);
+  int bflags[3] = {0, 0, 0};
+  bool ok = true;
+  if (B.at_bounds) {
+    if (check_bounds(P, pos, bflags)) {
+      set_error(P, PMP_ERR_LEFT_DOMAIN, b, s);
+      ok = false;
+    }
+  }
+  for (int cur_iter = 0; ok && cur_iter < P.num_iter && id > 0; ++cur_iter) {
+    if (film > 0.) {
+      set_error(P, PMP_ERR_UNSUPPORTED, b, s);
+      ok = false;
+      break;
+    }
+    // trilinear_interp (SprayInterpolation.H:158-199)
+    double ssv[2][3];
+#pragma unroll
+    for (int dir = 0; dir < 3; ++dir) {
+      const double sx_hi = __dsub_rn(lx[dir], static_cast<double>(ijk[dir]));
+      const double sx_lo = __dsub_rn(1., sx_hi);
+      if (bflags[dir] > 1) {
+        ssv[0][dir] = 1.;
+        ssv[1][dir] = 0.;
+      } else if (bflags[dir] < -1) {
+        ssv[0][dir] = 0.;
+        ssv[1][dir] = 1.;
+      } else {
+        ssv[0][dir] = sx_lo;
+        ssv[1][dir] = sx_hi;
+      }
+    }
+    // InterpolateGasPhase (SprayInterpolation.H:99-150), PeleLMeX branch
+    GasVals<NS, NF> gpv;
+    gpv.rho = 0.;
+    gpv.T = 0.;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      gpv.vel[d] = 0.;
+      gpv.mom_src[d] = 0.;
+    }
+#pragma unroll
+    for (int n = 0; n < NS; ++n) {
+      gpv.Y[n] = 0.;
+    }
+#pragma unroll
+    for (int spf = 0; spf < NF; ++spf) {
+      gpv.Ydot[spf] = 0.;
+    }
+    gpv.eng_src = 0.;
+    gpv.mass_src = 0.;
+    bool state_ok = true;
+#pragma unroll
+    for (int kk = -1; kk < 1; ++kk) {
+#pragma unroll
+      for (int jj = -1; jj < 1; ++jj) {
+#pragma unroll
+        for (int ii = -1; ii < 1; ++ii) {
+          const double cw = __dmul_rn(__dmul_rn(ssv[ii + 1][0], ssv[jj + 1][1]), ssv[kk + 1][2]);
+          if (cw > 0.) {
+            const int ci = ijk[0] + ii;
+            const int cj = ijk[1] + jj;
+            const int ck = ijk[2] + kk;
+            if (!in_box(B.state_lo, B.state_hi, ci, cj, ck)) {
+              state_ok = false;
+            } else {
+              const double* q = B.st + (long long)(ci - B.st_lo[0]) + (long long)(cj - B.st_lo[1]) * B.st_js +
+                                (long long)(ck - B.st_lo[2]) * B.st_ks;
+              const double cur_rho = __ldg(q + (long long)P.c_rho * B.st_ns);
+              gpv.rho = __dadd_rn(gpv.rho, __dmul_rn(cw, cur_rho));
+              const double inv_rho = 1. / cur_rho;
+#pragma unroll
+              for (int n = 0; n < NS; ++n) {
+                const double cur_mf = __dmul_rn(__ldg(q + (long long)(P.c_spec + n) * B.st_ns), inv_rho);
+                gpv.Y[n] = __dadd_rn(gpv.Y[n], __dmul_rn(cw, cur_mf));
+              }
+#pragma unroll
+              for (int dir = 0; dir < 3; ++dir) {
+                gpv.vel[dir] = __dadd_rn(gpv.vel[dir], __dmul_rn(cw, __ldg(q + (long long)(P.c_mom + dir) * B.st_ns)));
+              }
+              gpv.T = __dadd_rn(gpv.T, __dmul_rn(cw, __ldg(q + (long long)P.c_T * B.st_ns)));
+            }
+          }
+        }
+      }
+    }
+    if (!state_ok) {
+      set_error(P, PMP_ERR_STATE_BOX, b, s);
+      ok = false;
+      break;
+    }
+    // GasPhaseVals::define (SprayFuelData.H:101-111)
+    double mw_mix = 0.;
+#pragma unroll
+    for (int n = 0; n < NS; ++n) {
+      mw_mix = __dadd_rn(mw_mix, gpv.Y[n] / P.m.mw_kg[n]);
+    }
+    gpv.p = __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(gpv.rho, kRuCgs), mw_mix), gpv.T), kRuConv);
+    gpv.mw_mix = 1. / mw_mix;
+    // SprayData::calcBoilT (SprayFuelData.H:178-200)
+    double cBoilT[NF];
+    {
+      const double RU = kRuCgs * kRuConv;
+      const double PATM = kPatmCgs * kPresConv;
+      const double lp = pmp_log(PATM / gpv.p);
+#pragma unroll
+      for (int spf = 0; spf < NF; ++spf) {
+        const double mw_fuel = P.m.mw_kg[P.f.indx[spf]];
+        const double cc = 1. / __dadd_rn(__dmul_rn(lp, RU) / (P.f.hboil_ref[spf] * mw_fuel), 1. / P.f.boilT[spf]);
+        cBoilT[spf] = dmin(P.f.critT[spf], cc);
+      }
+    }
+    int nsub;
+    if (FORM == Form::FP64) {
+      nsub = spray_source_fp64<NS, NF>(P, P.sub_dt, gpv, vel, T, dia, Y, num_ppp, id, cBoilT);
+    } else {
+      nsub = spray_source_mixed<NS, NF>(P, P.sub_dt, gpv, vel, T, dia, Y, num_ppp, id, cBoilT);
+    }
+    c.sub += 1;
+    c.inner += static_cast<unsigned long long>(nsub);
+    // source scatter into the cell holding the droplet (SprayParticles.cpp:419-441)
+    const double cur_coef = __dmul_rn(-P.inv_vol, P.sub_dt) / P.flow_dt;
+    if (!in_box(B.src_lo, B.src_hi, ijkc[0], ijkc[1], ijkc[2])) {
+      if (!P.is_ghost || !in_box(B.sr_alo, B.sr_ahi, ijkc[0], ijkc[1], ijkc[2])) {
+        set_error(P, PMP_ERR_SOURCE_BOX, b, s);
+        ok = false;
+        break;
+      }
+    }
+    double* q = B.sr + (long long)(ijkc[0] - B.sr_lo[0]) + (long long)(ijkc[1] - B.sr_lo[1]) * B.sr_js +
+                (long long)(ijkc[2] - B.sr_lo[2]) * B.sr_ks;
+    if (P.f.mom_trans) {
+#pragma unroll
+      for (int dir = 0; dir < 3; ++dir) {
+        atomicAdd(q + (long long)(P.s_mom + dir) * B.sr_ns, __dmul_rn(cur_coef, gpv.mom_src[dir]));
+      }
+    }
+    if (P.f.mass_trans) {
+      atomicAdd(q + (long long)P.s_rho * B.sr_ns, __dmul_rn(cur_coef, gpv.mass_src));
+#pragma unroll
+      for (int spf = 0; spf < NF; ++spf) {
+        atomicAdd(q + (long long)(P.s_spec + spf) * B.sr_ns, __dmul_rn(cur_coef, gpv.Ydot[spf]));
+      }
+    }
+    atomicAdd(q + (long long)P.s_eng * B.sr_ns, __dmul_rn(cur_coef, gpv.eng_src));
+    // move (SprayParticles.cpp:444-476)
+    if (P.do_move && !P.f.fixed_parts && id > 0) {
+#pragma unroll
+      for (int dir = 0; dir < 3; ++dir) {
+        pos[dir] = __dadd_rn(pos[dir], __dmul_rn(P.sub_dt, vel[dir]));
+      }
+      if (B.at_bounds) {
+        if (check_bounds(P, pos, bflags)) {
+          id = -1;
+        } else {
+          impose_wall(P, pos, vel, bflags);
+        }
+      }
+      cell_of(P, pos, lx, ijk, ijkc);
+    }
+    if (P.is_ghost && !in_box(B.src_lo, B.src_hi, ijkc[0], ijkc[1], ijkc[2])) {
+      id = -1;
+    }
+  }
+  if (ok) {
+    if (P.do_move) {
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        P.parts.pos[d][s] = pos[d];
+      }
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      P.parts.rd[PMP_PSTATE_VEL + d][s] = vel[d];
+    }
+    P.parts.rd[PMP_PSTATE_T][s] = T;
+    P.parts.rd[PMP_PSTATE_DIA][s] = dia;
+#pragma unroll
+    for (int spf = 0; spf < NF; ++spf) {
+      P.parts.rd[PMP_PSTATE_Y + spf][s] = Y[spf];
+    }
+    if (id <= 0) {
+      P.parts.id[s] = id;
+      c.killed += 1;
+    }
+  }
+}
+
+__device__ __forceinline__ void flush_counters(const KParams& P, Counters& c)
+{
+  const unsigned mask = 0xffffffffu;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    c.sub += __shfl_down_sync(mask, c.sub, o);
+    c.killed += __shfl_down_sync(mask, c.killed, o);
+    c.inner += __shfl_down_sync(mask, c.inner, o);
+  }
+  if ((threadIdx.x & 31) == 0 && (c.sub | c.killed | c.inner)) {
+    atomicAdd(&P.status->substeps, c.sub);
+    atomicAdd(&P.status->killed, c.killed);
+    atomicAdd(&P.status->inner, c.inner);
+  }
+}
+
+#ifndef PMP_FP64_MIN_BLOCKS
+#define PMP_FP64_MIN_BLOCKS 5  /* 96 registers: 5 CTAs of 128 per SM (measured best) */
+#endif
+#ifndef PMP_MIXED_MIN_BLOCKS
+#define PMP_MIXED_MIN_BLOCKS 4
+#endif
+
+template <int NS, int NF, int BLOCK>
+__global__ void __launch_bounds__(BLOCK, PMP_FP64_MIN_BLOCKS) spray_update_fp64(const __grid_constant__ KParams P)
+{
+  const int b = P.cta_box[blockIdx.x];
+  const long long s = P.cta_start[blockIdx.x] + threadIdx.x;
+  Counters c;
+  if (s < P.boxes[b].p_end) {
+    update_one<NS, NF, Form::FP64>(P, b, s, c);
+  }
+  flush_counters(P, c);
+}
+
+template <int NS, int NF, int BLOCK>
+__global__ void __launch_bounds__(BLOCK, PMP_MIXED_MIN_BLOCKS) spray_update_mixed(const __grid_constant__ KParams P)
+{
+  const int b = P.cta_box[blockIdx.x];
+  const long long s = P.cta_start[blockIdx.x] + threadIdx.x;
+  Counters c;
+  if (s < P.boxes[b].p_end) {
+    update_one<NS, NF, Form::MIXED>(P, b, s, c);
+  }
+  flush_counters(P, c);
+}
+
+// box holding slot s (box_begin has nboxes + 1 entries)
+__device__ __forceinline__ int box_of_slot(const KParams& P, long long s)
+{
+  int lo = 0;
+  int hi = P.nboxes;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) / 2;
+    if (P.box_begin[mid] <= s) {
+      lo = mid;
+    } else {
+      hi = mid;
+    }
+  }
+  return lo;
+}
+
+template <int NS, int NF, int BLOCK>
+__global__ void __launch_bounds__(BLOCK, PMP_FP64_MIN_BLOCKS) spray_update_fp64_list(const __grid_constant__ KParams P)
+{
+  const unsigned long long n = *reinterpret_cast<volatile unsigned long long*>(&P.status->fallback);
+  Counters c;
+  for (unsigned long long i = blockIdx.x * (unsigned long long)BLOCK + threadIdx.x; i < n;
+       i += (unsigned long long)gridDim.x * BLOCK) {
+    const long long s = P.fb_list[i];
+    update_one<NS, NF, Form::FP64>(P, box_of_slot(P, s), s, c);
+  }
+  flush_counters(P, c);
+}
+
+}  // namespace pmp

@@ -1,0 +1,543 @@
+// spray_mixed.cuh -- the mixed-precision spray update (PMP_MODE_MIXED).
+//
+// Same driver loop as the FP64 kernel (SprayParticles.cpp:324-481), with the
+// per-droplet physics of calculateSpraySource (Drag.H:138-441) evaluated in
+// FP32: gas thermo and transport, vapour state, the B_T fixed point, drag,
+// Nusselt/Sherwood numbers.  FP64 is kept where precision is structural:
+//  - cell indices and positions (bit-exact cells, as in the FP64 form);
+//  - the trilinear gather of the FP64 mesh;
+//  - the droplet state update: velocity, temperature, mass, mass fractions
+//    and diameter are integrated in FP64 from the FP32 rates;
+//  - the deposits: mass and species sources are FP64 differences of FP64
+//    droplet masses, so the liquid + gas mass balance closes to FP64
+//    round-off exactly as in the plain form;
+//  - droplets that enter a call with d < 2 um (approaching complete
+//    evaporation) are not touched here: their slots go to a fallback list
+//    and the FP64 kernel updates them (spray_update_fp64_list).
+// FP32 transcendentals use the SFU (ex2/lg2) with exact power-of-two range
+// reduction: relative error ~3e-7 independent of the argument.
+//
+// One deliberate difference from the FP64 algorithm: the B_T fixed point
+// stops when |dB_T| <= max(1e-7, 8 eps_f32 |B_T|) -- FP32 cannot resolve
+// 1e-7 once B_T > 1, and the reference threshold would then run to its
+// 100-iteration cap.
+#pragma once
+
+#include "spray_fp64.cuh"
+
+namespace pmp {
+
+constexpr double kMixedMinDia = 2e-6;  // below: FP64 path
+
+// 2^x for |x| < 126: SFU ex2 on the fraction, exact 2^k scaling
+__device__ __forceinline__ float fexp2(float x)
+{
+  const float k = rintf(x);
+  const float f = x - k;
+  float r;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(f));
+  return r * __int_as_float((static_cast<int>(k) + 127) << 23);
+}
+
+__device__ __forceinline__ float fexp(float x)
+{
+  // x log2(e) as hi + lo so that the fraction keeps full precision
+  const float t = x * 1.44269502f;
+  const float k = rintf(t);
+  float f = fmaf(x, 1.44269502f, -k);
+  f = fmaf(x, 1.925963e-8f, f);
+  float r;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(f));
+  return r * __int_as_float((static_cast<int>(k) + 127) << 23);
+}
+
+// log2(x) for positive normal x: SFU lg2 on the mantissa in [sqrt(1/2),sqrt(2)), exact exponent
+__device__ __forceinline__ float flog2(float x)
+{
+  int b = __float_as_int(x);
+  int e = ((b >> 23) & 0xff) - 127;
+  int mb = (b & 0x007fffff) | 0x3f800000;
+  if (mb > 0x3fb504f3) {  // m > sqrt(2)
+    mb -= 0x00800000;
+    e += 1;
+  }
+  float r;
+  asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(__int_as_float(mb)));
+  return r + static_cast<float>(e);
+}
+
+__device__ __forceinline__ float flog(float x) { return flog2(x) * 0.693147181f; }
+
+__device__ __forceinline__ float fpow(float x, float y)
+{
+  return (x == 0.f) ? 0.f : fexp2(y * flog2(x));
+}
+
+__device__ __forceinline__ float fcbrt(float x)
+{
+  if (x == 0.f) {
+    return 0.f;
+  }
+  float y = fexp2(flog2(fabsf(x)) * (1.f / 3.f));
+  y = y - (y * y * y - fabsf(x)) / (3.f * y * y);
+  return x < 0.f ? -y : y;
+}
+
+__device__ __forceinline__ float flog1p(float x)
+{
+  if (fabsf(x) < 1e-2f) {
+    // x - x^2/2 + x^3/3 - x^4/4 + x^5/5
+    return x * fmaf(x, fmaf(x, fmaf(x, fmaf(x, 0.2f, -0.25f), 1.f / 3.f), -0.5f), 1.f);
+  }
+  return flog(1.f + x);
+}
+
+// cbrt in FP64 from an FP32 estimate and one Newton step (error ~1e-16)
+__device__ __forceinline__ double dcbrt_from_f(double a)
+{
+  double y = static_cast<double>(fcbrt(static_cast<float>(a)));
+  const double y2 = y * y;
+  const double r = fma(y2, y, -a);
+  return y - r / (3.0 * y2);
+}
+
+__device__ __forceinline__ float fcubic(const double* c, float x)
+{
+  return fmaf(fmaf(fmaf((float)c[3], x, (float)c[2]), x, (float)c[1]), x, (float)c[0]);
+}
+
+template <int N>
+__device__ __forceinline__ float fsel(const float (&a)[N], int i)
+{
+  float v = a[0];
+#pragma unroll
+  for (int k = 1; k < N; ++k) {
+    v = (k == i) ? a[k] : v;
+  }
+  return v;
+}
+
+template <int N>
+__device__ __forceinline__ void fput(float (&a)[N], int i, float v)
+{
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+    a[k] = (k == i) ? v : a[k];
+  }
+}
+
+__device__ __forceinline__ float heat_coeff_f(float ratio, float B_M, float Nu_0)
+{
+  if (B_M <= 1e-15f) {
+    return 0.f;
+  }
+  const float NU2 = Nu_0 - 2.f;
+  const float lnBM1 = flog(1.f + B_M);
+  float phi = ratio / Nu_0;
+  float B_T_old = fexp(phi * lnBM1) - 1.f;
+  float logB = flog1p(B_T_old);
+  float invFT = B_T_old / (logB * fpow(1.f + B_T_old, 0.7f));
+  float Nu_num = 2.f + NU2 * invFT;
+  phi = ratio / Nu_num;
+  float B_T = fexp(phi * lnBM1) - 1.f;
+  float error = fabsf(B_T - B_T_old);
+  int k = 0;
+  while (k < 100 && error > fmaxf(1e-7f, 8.f * 1.1920929e-7f * fabsf(B_T))) {
+    B_T_old = B_T;
+    logB = flog1p(B_T);
+    invFT = B_T / (logB * fpow(1.f + B_T, 0.7f));
+    Nu_num = 2.f + NU2 * invFT;
+    phi = ratio / Nu_num;
+    B_T = fexp(phi * lnBM1) - 1.f;
+    error = fabsf(B_T - B_T_old);
+    k++;
+  }
+  logB = flog1p(B_T);
+  invFT = B_T / (logB * fpow(1.f + B_T, 0.7f));
+  Nu_num = 2.f + NU2 * invFT;
+  return Nu_num * logB / B_T;
+}
+
+// calculateSpraySource with FP32 physics and FP64 state (see the file header).
+template <int NS, int NF>
+__device__ __forceinline__ int spray_source_mixed(
+  const KParams& P, double flow_dt, GasVals<NS, NF>& gpv, double* vel_io, double& T_io,
+  double& dia_io, double* Y_io, double num_ppp, int& id, const double* cBoilT)
+{
+  const DevMech& m = P.m;
+  const DevFuel& fdat = P.f;
+  const float rule = 1.f / 3.f;
+  const float C_eps = 1.E-15f;
+  const double min_mass = 1.E-13 * kMassConv;
+  const int nSubMax = 100;
+  const float RU = (float)(kRuCgs * kRuConv);
+  const float PATM = (float)(kPatmCgs * kPresConv);
+  // gas state in FP32
+  const float Tg = (float)gpv.T;
+  const float pg = (float)gpv.p;
+  const float mw_mix = (float)gpv.mw_mix;
+  float Yg[NS];
+#pragma unroll
+  for (int n = 0; n < NS; ++n) {
+    Yg[n] = (float)gpv.Y[n];
+  }
+  float Y_skin[NS];
+  float h_part[NS];
+  float cp_n[NS];
+  float Ddiag[NF];
+  float L_fuel[NF];
+  float mi_dot[NF];
+  float X_vapor[NF];
+  double Y_part[NF];
+#pragma unroll
+  for (int spf = 0; spf < NF; ++spf) {
+    L_fuel[spf] = 0.f;
+    mi_dot[spf] = 0.f;
+    X_vapor[spf] = 0.f;
+  }
+  double vel_part[3] = {vel_io[0], vel_io[1], vel_io[2]};
+  if (fdat.fixed_parts) {
+    vel_part[0] = vel_part[1] = vel_part[2] = 0.;
+  }
+  double T_part = T_io;
+  double dia_part = dia_io;
+  double rho_part = 0.;
+#pragma unroll
+  for (int spf = 0; spf < NF; ++spf) {
+    Y_part[spf] = Y_io[spf];
+    rho_part += Y_part[spf] / rhoL(fdat, dmin(T_part, cBoilT[spf]), spf);
+  }
+  rho_part = 1. / rho_part;
+  double dt = flow_dt;
+  int isub = 1;
+  int nsub = 1;
+  double pmass = PMP_PI / 6. * rho_part * (dia_part * dia_part * dia_part);
+  const double startmass = pmass;
+  double eng_acc = 0.;
+  double mom_acc[3] = {0., 0., 0.};
+  while (isub <= nsub) {
+    const float Tp_f = (float)T_part;
+    const float dia_f = (float)dia_part;
+    float cp_part = 0.f;
+    double Tboil = 0.;
+    float mw_part = 0.f;
+#pragma unroll
+    for (int spf = 0; spf < NF; ++spf) {
+      Tboil += Y_part[spf] * cBoilT[spf];
+      cp_part += (float)Y_part[spf] * (float)fdat.cp[spf];
+      mw_part += (float)Y_part[spf] / (float)m.mw_kg[fdat.indx[spf]];
+    }
+    mw_part = 1.f / mw_part;
+    const float delT = fmaxf(Tg - Tp_f, 0.f);
+    float T_skin = Tg;
+    if (fdat.mass_trans) {
+      T_skin = Tp_f + rule * delT;
+    }
+#pragma unroll
+    for (int n = 0; n < NS; ++n) {
+      const double* a = m.cp[n];
+      const float cpr = fmaf(fmaf(fmaf(fmaf((float)a[4], T_skin, (float)a[3]), T_skin, (float)a[2]), T_skin,
+                                  (float)a[1]), T_skin, (float)a[0]);
+      cp_n[n] = cpr * (float)(m.ru_w[n] * kEngConv);
+      const double* hc = m.hc[n];
+      const float hp = fmaf(fmaf(fmaf(fmaf((float)hc[4], Tp_f, (float)hc[3]), Tp_f, (float)hc[2]), Tp_f,
+                                 (float)hc[1]), Tp_f, (float)hc[0]);
+      h_part[n] = fmaf(hp, Tp_f, (float)hc[5]) * (float)(m.ru_w[n] * kEngConv);
+      Y_skin[n] = 0.f;
+    }
+    float cp_skin = 0.f;
+    float mw_skin = 0.f;
+    float B_M = 0.f;
+    float sumXVap = 0.f;
+    if (fdat.mass_trans) {
+      float mbar_vap = 0.f;
+#pragma unroll
+      for (int spf = 0; spf < NF; ++spf) {
+        const int fspec = fdat.indx[spf];
+        const float mw_fuel = (float)m.mw_kg[fspec];
+        const float Tp = fminf(Tp_f, 0.99f * (float)cBoilT[spf]);
+        const float part_latent =
+          fsel(h_part, fspec) + (float)fdat.latent[spf] - (float)fdat.cp[spf] * (Tp - (float)fdat.ref_T);
+        L_fuel[spf] = part_latent;
+        float pres_sat;
+        if (fdat.psat_coef[4 * spf + 3] == 0.) {
+          pres_sat = PATM * fexp(part_latent * mw_fuel / RU * (1.f / (float)fdat.boilT[spf] - 1.f / Tp));
+        } else {
+          const float a = (float)fdat.psat_coef[4 * spf];
+          const float b = (float)fdat.psat_coef[4 * spf + 1];
+          const float c = (float)fdat.psat_coef[4 * spf + 2];
+          pres_sat = (float)fdat.psat_coef[4 * spf + 3] * fexp2((a - b / (Tp + c)) * 3.32192809f);
+        }
+        const float X_fluid = fsel(Yg, fdat.dep[spf]) * mw_mix / mw_fuel;
+        if (pres_sat > X_fluid * pg) {
+          const float Xl = (float)Y_part[spf] * mw_part / mw_fuel;
+          const float Xv = Xl * pres_sat / pg;
+          mbar_vap += Xv * mw_fuel;
+          sumXVap += Xv;
+          X_vapor[spf] = Xv;
+        } else {
+          X_vapor[spf] = 0.f;
+        }
+      }
+      const float totalmwx = mbar_vap + (1.f - sumXVap) * mw_mix;
+      float sumYSkin = 0.f;
+      float sumYfFluid = 0.f;
+      float sumYVap = 0.f;
+#pragma unroll
+      for (int spf = 0; spf < NF; ++spf) {
+        if (X_vapor[spf] > 0.f) {
+          const int fspec = fdat.indx[spf];
+          const float Yfv = X_vapor[spf] * (float)m.mw_kg[fspec] / totalmwx;
+          sumYVap += Yfv;
+          const float gasY = fsel(Yg, fdat.dep[spf]);
+          sumYfFluid += gasY;
+          const float Ysk = Yfv + rule * (gasY - Yfv);
+          fput(Y_skin, fspec, Ysk);
+          sumYSkin += Ysk;
+        }
+      }
+      const float renorm = (1.f - sumYSkin) / (1.f - sumYfFluid);
+#pragma unroll
+      for (int n = 0; n < NS; ++n) {
+        if (Y_skin[n] == 0.f) {
+          Y_skin[n] = Yg[n] * renorm;
+        }
+        cp_skin += Y_skin[n] * cp_n[n];
+        mw_skin += Y_skin[n] / (float)m.mw_kg[n];
+      }
+      mw_skin = 1.f / mw_skin;
+      B_M = (sumYVap - sumYfFluid) / fmaxf(C_eps, (1.f - sumYVap));
+      B_M = fminf(20.f, B_M);
+    } else {
+#pragma unroll
+      for (int n = 0; n < NS; ++n) {
+        Y_skin[n] = Yg[n];
+        cp_skin += Yg[n] * cp_n[n];
+      }
+      mw_skin = mw_mix;
+    }
+    float lambda_skin = 0.f;
+    float mu_skin = 0.f;
+    float rho_skin = (float)gpv.rho;
+    if (fdat.mass_trans) {
+      rho_skin = mw_skin * pg / (RU * T_skin);
+    }
+    {
+      float X[NS];
+      float sumYW = 0.f;
+#pragma unroll
+      for (int k = 0; k < NS; ++k) {
+        sumYW += Y_skin[k] / (float)m.mw_g[k];
+      }
+      const float wbar = 1.f / sumYW;
+#pragma unroll
+      for (int k = 0; k < NS; ++k) {
+        X[k] = Y_skin[k] * wbar / (float)m.mw_g[k];
+      }
+      const float lnT = flog(T_skin);
+      float s = 0.f;
+#pragma unroll
+      for (int k = 0; k < NS; ++k) {
+        s = fmaf(X[k], fexp(6.f * fcubic(m.mu[k], lnT)), s);
+      }
+      mu_skin = fexp(flog(s) * (1.f / 6.f));
+      if (fdat.mass_trans) {
+        float sl = 0.f;
+#pragma unroll
+        for (int k = 0; k < NS; ++k) {
+          sl = fmaf(X[k], fexp(0.25f * fcubic(m.lam[k], lnT)), sl);
+        }
+        const float s2 = sl * sl;
+        lambda_skin = s2 * s2;
+        const float rt = (float)kRuCgs * T_skin;
+#pragma unroll
+        for (int f = 0; f < NF; ++f) {
+          const int i = fdat.indx[f];
+          float term1 = 0.f;
+          float term2 = 0.f;
+#pragma unroll
+          for (int j = 0; j < NS; ++j) {
+            if (j != i) {
+              term1 += Y_skin[j];
+              term2 = fmaf(X[j], fexp(-fcubic(m.dbin[f][j], lnT)), term2);
+            }
+          }
+          Ddiag[f] = (float)m.mw_g[i] * term1 / (term2 * rt);
+        }
+      }
+    }
+    mu_skin *= (float)kMuConv;
+    lambda_skin *= (float)kLambdaConv;
+    float diff_vel[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      diff_vel[d] = (float)(gpv.vel[d] - vel_part[d]);
+    }
+    const float diff_vel_mag =
+      sqrtf(diff_vel[0] * diff_vel[0] + diff_vel[1] * diff_vel[1] + diff_vel[2] * diff_vel[2]);
+    const float Reyn = rho_skin * diff_vel_mag * dia_f / mu_skin;
+    const float inv_pmass = (float)(1. / pmass);
+    float drag_coef = 0.f;
+    if (Reyn > 1000.f) {
+      drag_coef = 0.424f;
+    } else if (Reyn > 1.f) {
+      drag_coef = 24.f / Reyn * (1.f + fcbrt(Reyn * Reyn) / 6.f);
+    } else if (Reyn > 0.f) {
+      drag_coef = 24.f / Reyn;
+    }
+    const float drag_force =
+      0.125f * rho_skin * drag_coef * (float)PMP_PI * dia_f * dia_f * diff_vel_mag;
+    const float drag_force_p = 0.75f * rho_skin * drag_coef * diff_vel_mag / (dia_f * (float)rho_part);
+    float part_vel_src[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      part_vel_src[d] = drag_force_p * diff_vel[d] + (float)fdat.body_force[d];
+    }
+    if (fdat.mom_trans) {
+      const double nd = num_ppp * (double)drag_force;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        mom_acc[d] += nd * (double)diff_vel[d];
+      }
+      if (isub == 1) {
+        nsub = min(max(nsub, static_cast<int>((float)flow_dt * drag_force_p) + 1), nSubMax);
+      }
+    }
+    float part_temp_src = 0.f;
+    float m_dot = 0.f;
+    if (fdat.mass_trans) {
+      const float Pr_skin = mu_skin * cp_skin / lambda_skin;
+      const float powR = fmaxf(fpow(fminf(400.f, Reyn), 0.077f), 1.f);
+      float Nu_num = 0.f;
+      float sumL = 0.f;
+      const float Nu_0 = 1.f + powR * fcbrt(1.f + Reyn * Pr_skin);
+      if (sumXVap > 0.f) {
+        float rhoDtotal = 0.f;
+        float cp_fuel = 0.f;
+        float sumYSkin = 0.f;
+#pragma unroll
+        for (int spf = 0; spf < NF; ++spf) {
+          const int fspec = fdat.indx[spf];
+          Ddiag[spf] *= mw_skin / (float)m.mw_kg[fspec] * (float)kRhodConv;
+          const float X_norm = X_vapor[spf] / sumXVap;
+          Ddiag[spf] *= X_norm;
+          rhoDtotal += Ddiag[spf];
+          const float ysk = fsel(Y_skin, fspec);
+          cp_fuel += ysk * fsel(cp_n, fspec);
+          sumYSkin += ysk;
+        }
+        cp_fuel /= sumYSkin;
+        const float Sc_skin = mu_skin / rhoDtotal;
+        const float logB = flog1p(B_M);
+        const float invFM = B_M / (logB * fpow(1.f + B_M, 0.7f));
+        const float Sh_0 = 1.f + powR * fcbrt(1.f + Reyn * Sc_skin);
+        const float Sh_num = 2.f + (Sh_0 - 2.f) * invFM;
+        const float mdotcoeff = (float)PMP_PI * dia_f * Sh_num * logB;
+        const float ratio = cp_fuel * Sh_num * rhoDtotal / lambda_skin;
+        Nu_num = heat_coeff_f(ratio, B_M, Nu_0);
+#pragma unroll
+        for (int spf = 0; spf < NF; ++spf) {
+          if (X_vapor[spf] > 0.f) {
+            mi_dot[spf] = -fmaxf(Ddiag[spf] * mdotcoeff, 0.f);
+            m_dot += mi_dot[spf];
+            sumL += mi_dot[spf] * L_fuel[spf];
+          }
+        }
+      } else {
+        Nu_num = Nu_0;
+      }
+      const float conv_src = (float)PMP_PI * lambda_skin * dia_f * delT * Nu_num;
+      eng_acc += num_ppp * (double)conv_src;
+      part_temp_src = (sumL + conv_src) * inv_pmass / cp_part;
+      if (isub == 1 && delT > C_eps) {
+        const float inv_tau_d = -m_dot / (0.2f * (float)pmass);
+        const float inv_tau_T = conv_src * inv_pmass / (cp_part * delT);
+        nsub = min(max(nsub, max(static_cast<int>((float)flow_dt * inv_tau_d),
+                                 static_cast<int>((float)flow_dt * inv_tau_T)) + 1),
+                   nSubMax);
+      }
+    }
+    if (isub == 1) {
+      dt = flow_dt / static_cast<double>(nsub);
+    }
+    const double part_dt = fdat.dtmod * dt;
+    if (!fdat.fixed_parts) {
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        vel_part[d] += part_dt * (double)part_vel_src[d];
+      }
+    }
+    if (fdat.mass_trans) {
+      const double newT = T_part + part_dt * (double)part_temp_src;
+      const double new_mass = pmass + (double)m_dot * part_dt;
+      if (new_mass > min_mass && newT < Tboil) {
+        T_part = newT;
+        if (NF > 1) {
+          rho_part = 0.;
+          double sumY = 0.;
+#pragma unroll
+          for (int spf = 0; spf < NF; ++spf) {
+            Y_part[spf] = dmin(1., dmax(0., (Y_part[spf] * pmass + (double)mi_dot[spf] * part_dt) / new_mass));
+            if (Y_part[spf] <= 1.E-12) {
+              Y_part[spf] = 0.;
+            }
+            sumY += Y_part[spf];
+          }
+#pragma unroll
+          for (int spf = 0; spf < NF; ++spf) {
+            Y_part[spf] /= sumY;
+            rho_part += Y_part[spf] / rhoL(fdat, dmin(T_part, cBoilT[spf]), spf);
+          }
+          rho_part = 1. / rho_part;
+        } else {
+          rho_part = rhoL(fdat, dmin(T_part, cBoilT[0]), 0);
+        }
+        pmass = new_mass;
+        dia_part = dcbrt_from_f(6. * pmass / (PMP_PI * rho_part));
+      } else {
+        pmass = 0.;
+        id = -1;
+        nsub = isub;
+        isub = nsub + 1;
+      }
+    }
+    ++isub;
+  }
+  gpv.eng_src = eng_acc;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    gpv.mom_src[d] = mom_acc[d];
+  }
+  if (nsub > 1) {
+    gpv.eng_src /= static_cast<double>(nsub);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      gpv.mom_src[d] /= static_cast<double>(nsub);
+    }
+  }
+  const double mdot_total = (pmass - startmass) / (fdat.dtmod * flow_dt);
+  gpv.mass_src = num_ppp * mdot_total;
+  if (fdat.mom_trans) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      gpv.mom_src[d] += num_ppp * vel_part[d] * mdot_total;
+    }
+  }
+#pragma unroll
+  for (int spf = 0; spf < NF; ++spf) {
+    const double oldY = Y_io[spf];
+    const double newY = Y_part[spf];
+    const double midot = (newY * pmass - oldY * startmass) / (fdat.dtmod * flow_dt);
+    gpv.Ydot[spf] = num_ppp * midot;
+    gpv.eng_src += num_ppp * midot * (double)fsel(h_part, fdat.dep[spf]);
+    Y_io[spf] = Y_part[spf];
+  }
+  vel_io[0] = vel_part[0];
+  vel_io[1] = vel_part[1];
+  vel_io[2] = vel_part[2];
+  T_io = T_part;
+  dia_io = dia_part;
+  return nsub;
+}
+
+}  // namespace pmp
