@@ -60,6 +60,36 @@ struct DevFuel {
   int fixed_parts;
 };
 
+// FP32 copies of the tables for the mixed-precision and learned forms
+// (converted once on the host; scaled where the physics always scales them)
+struct DevMechF {
+  float mw_kg[kMaxSpec];
+  float inv_mw_kg[kMaxSpec];
+  float inv_mw_g[kMaxSpec];
+  float mw_g[kMaxSpec];
+  float ru_w_eng[kMaxSpec];          // RU/W * eng_conv
+  float cp[kMaxSpec][5];
+  float hc[kMaxSpec][6];
+  float mu6[kMaxSpec][4];            // 6 ln mu(lnT)
+  float lam4[kMaxSpec][4];           // ln lambda(lnT) / 4
+  float dbinm[kMaxFuel][kMaxSpec][4];// -ln(P D)(lnT)
+};
+
+struct DevFuelF {
+  float cp[kMaxFuel];
+  float latent[kMaxFuel];
+  float boilT[kMaxFuel];
+  float inv_boilT[kMaxFuel];
+  float critT[kMaxFuel];
+  float hb[kMaxFuel];        // RU / (Hboil_ref * W_fuel)
+  float psat_a[kMaxFuel];
+  float psat_b[kMaxFuel];
+  float psat_c[kMaxFuel];
+  float psat_d[kMaxFuel];
+  float ref_T;
+  float body_force[3];
+};
+
 struct BoxEntry {
   const double* st;          // state fab, component 0
   double* sr;                // source fab, component 0
@@ -96,6 +126,8 @@ struct DevParts {
 struct KParams {
   DevMech m;
   DevFuel f;
+  DevMechF mf;
+  DevFuelF ff;
   DevParts parts;
   // geometry
   double plo[3], phi[3], dx[3], dxi[3];

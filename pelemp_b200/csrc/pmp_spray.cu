@@ -59,6 +59,8 @@ struct pmp_spray {
   int mode = PMP_MODE_FP64;
   pmp::DevMech dmech;
   pmp::DevFuel dfuel;
+  pmp::DevMechF dmechf;
+  pmp::DevFuelF dfuelf;
   // per-box staged droplets (before packing)
   std::vector<BoxStore> staged;
   std::vector<bool> box_set;
@@ -306,6 +308,49 @@ int build_device_tables(pmp_spray* h)
   F.mass_trans = d.mass_trans;
   F.mom_trans = d.mom_trans;
   F.fixed_parts = d.fixed_parts;
+  // FP32 tables of the mixed / learned forms
+  pmp::DevMechF& mf = h->dmechf;
+  pmp::DevFuelF& ff = h->dfuelf;
+  memset(&mf, 0, sizeof(mf));
+  memset(&ff, 0, sizeof(ff));
+  for (int k = 0; k < NS; ++k) {
+    mf.mw_kg[k] = (float)m.mw_kg[k];
+    mf.inv_mw_kg[k] = (float)(1. / m.mw_kg[k]);
+    mf.inv_mw_g[k] = (float)(1. / m.mw_g[k]);
+    mf.mw_g[k] = (float)m.mw_g[k];
+    mf.ru_w_eng[k] = (float)(m.ru_w[k] * pmp::kEngConv);
+    for (int n = 0; n < 5; ++n) {
+      mf.cp[k][n] = (float)m.cp[k][n];
+    }
+    for (int n = 0; n < 6; ++n) {
+      mf.hc[k][n] = (float)m.hc[k][n];
+    }
+    for (int n = 0; n < 4; ++n) {
+      mf.mu6[k][n] = (float)(6. * m.mu[k][n]);
+      mf.lam4[k][n] = (float)(0.25 * m.lam[k][n]);
+    }
+  }
+  for (int f = 0; f < NF; ++f) {
+    for (int j = 0; j < NS; ++j) {
+      for (int n = 0; n < 4; ++n) {
+        mf.dbinm[f][j][n] = (float)(-m.dbin[f][j][n]);
+      }
+    }
+    ff.cp[f] = (float)d.cp[f];
+    ff.latent[f] = (float)d.latent[f];
+    ff.boilT[f] = (float)d.boilT[f];
+    ff.inv_boilT[f] = (float)(1. / d.boilT[f]);
+    ff.critT[f] = (float)d.critT[f];
+    ff.hb[f] = (float)(pmp::kRuCgs * pmp::kRuConv / (F.hboil_ref[f] * m.mw_kg[d.indx[f]]));
+    ff.psat_a[f] = (float)d.psat_coef[4 * f];
+    ff.psat_b[f] = (float)d.psat_coef[4 * f + 1];
+    ff.psat_c[f] = (float)d.psat_coef[4 * f + 2];
+    ff.psat_d[f] = (float)d.psat_coef[4 * f + 3];
+  }
+  ff.ref_T = (float)d.ref_T;
+  for (int i = 0; i < 3; ++i) {
+    ff.body_force[i] = (float)d.body_force[i];
+  }
   return PMP_OK;
 }
 
@@ -593,6 +638,8 @@ int do_update(
   memset(&P, 0, sizeof(P));
   P.m = h->dmech;
   P.f = h->dfuel;
+  P.mf = h->dmechf;
+  P.ff = h->dfuelf;
   const long long T = h->total;
   for (int d = 0; d < 3; ++d) {
     P.parts.pos[d] = h->soa + (long long)d * T;

@@ -126,6 +126,23 @@ __device__ __forceinline__ double heat_coeff(
   return Nu_num * logB / B_T;
 }
 
+// eos.T2Cpi / eos.T2Hi of species n at T (pmp_thermo.h, same operation
+// order), converted to MKS: evaluated where needed instead of kept in
+// per-species register arrays
+__device__ __forceinline__ double cp_mks(const DevMech& m, int n, double T)
+{
+  const double* a = m.cp[n];
+  const double cpr = fma(fma(fma(fma(a[4], T, a[3]), T, a[2]), T, a[1]), T, a[0]);
+  return (cpr * m.ru_w[n]) * kEngConv;
+}
+
+__device__ __forceinline__ double h_mks(const DevMech& m, int n, double T)
+{
+  const double* hc = m.hc[n];
+  const double hp = fma(fma(fma(fma(hc[4], T, hc[3]), T, hc[2]), T, hc[1]), T, hc[0]);
+  return (fma(hp, T, hc[5]) * m.ru_w[n]) * kEngConv;
+}
+
 // calculateSpraySource (Drag.H:138-441), PeleLMeX branch.  Updates vel, T,
 // dia, Y in place; returns the number of inner sub-steps taken.
 template <int NS, int NF>
@@ -141,8 +158,7 @@ __device__ __forceinline__ int spray_source_fp64(
   const double min_mass = 1.E-13 * kMassConv;
   const int nSubMax = 100;
   double Y_skin[NS];
-  double h_part[NS];
-  double cp_n[NS];
+  double T_h = T_io;  // temperature of the last h_part evaluation (Drag.H:221)
   double Ddiag[NF];  // fuel rows only
   double L_fuel[NF];
   double mi_dot[NF];
@@ -190,18 +206,12 @@ __device__ __forceinline__ int spray_source_fp64(
     if (fdat.mass_trans) {
       T_skin = T_part + rule * delT;
     }
-    // eos.T2Cpi(T_skin), eos.T2Hi(T_part) (pmp_thermo.h), then *= eng_conv
+    // eos.T2Cpi(T_skin) and eos.T2Hi(T_part) (Drag.H:220-226): cp_mks(n, T_skin)
+    // and h_mks(n, T_part) below
+    T_h = T_part;
 #pragma unroll
     for (int n = 0; n < NS; ++n) {
-      const double* a = m.cp[n];
-      const double cpr = fma(fma(fma(fma(a[4], T_skin, a[3]), T_skin, a[2]), T_skin, a[1]), T_skin, a[0]);
-      cp_n[n] = cpr * m.ru_w[n];
-      const double* hc = m.hc[n];
-      const double hp = fma(fma(fma(fma(hc[4], T_part, hc[3]), T_part, hc[2]), T_part, hc[1]), T_part, hc[0]);
-      h_part[n] = fma(hp, T_part, hc[5]) * m.ru_w[n];
       Y_skin[n] = 0.;
-      h_part[n] *= kEngConv;
-      cp_n[n] *= kEngConv;
     }
     double cp_skin = 0.;
     double mw_skin = 0.;
@@ -219,7 +229,7 @@ __device__ __forceinline__ int spray_source_fp64(
         const double boilT_ref = fdat.boilT[spf];
         const double mw_fuel = m.mw_kg[fspec];
         const double Tp = dmin(T_part, 0.99 * cBoilT[spf]);
-        const double part_latent = sel(h_part, fspec) + fdat.latent[spf] - fdat.cp[spf] * (Tp - fdat.ref_T);
+        const double part_latent = h_mks(m, fspec, T_part) + fdat.latent[spf] - fdat.cp[spf] * (Tp - fdat.ref_T);
         L_fuel[spf] = part_latent;
         double pres_sat = 0.;
         if (fdat.psat_coef[4 * spf + 3] == 0.) {
@@ -266,7 +276,7 @@ __device__ __forceinline__ int spray_source_fp64(
         if (Y_skin[n] == 0.) {
           Y_skin[n] = gpv.Y[n] * renorm;
         }
-        cp_skin += Y_skin[n] * cp_n[n];
+        cp_skin += Y_skin[n] * cp_mks(m, n, T_skin);
         mw_skin += Y_skin[n] / m.mw_kg[n];
       }
       mw_skin = 1. / mw_skin;
@@ -276,7 +286,7 @@ __device__ __forceinline__ int spray_source_fp64(
 #pragma unroll
       for (int n = 0; n < NS; ++n) {
         Y_skin[n] = gpv.Y[n];
-        cp_skin += gpv.Y[n] * cp_n[n];
+        cp_skin += gpv.Y[n] * cp_mks(m, n, T_skin);
       }
       mw_skin = gpv.mw_mix;
     }
@@ -389,7 +399,7 @@ __device__ __forceinline__ int spray_source_fp64(
           Ddiag[spf] *= X_norm;
           rhoDtotal += Ddiag[spf];
           const double ysk = sel(Y_skin, fspec);
-          cp_fuel += ysk * sel(cp_n, fspec);
+          cp_fuel += ysk * cp_mks(m, fspec, T_skin);
           sumYSkin += ysk;
         }
         cp_fuel /= sumYSkin;
@@ -491,7 +501,7 @@ __device__ __forceinline__ int spray_source_fp64(
     const double newY = Y_part[spf];
     const double midot = (newY * pmass - oldY * startmass) / (fdat.dtmod * flow_dt);
     gpv.Ydot[spf] = num_ppp_ * midot;
-    gpv.eng_src += num_ppp_ * midot * sel(h_part, fdat.dep[spf]);
+    gpv.eng_src += num_ppp_ * midot * h_mks(m, fdat.dep[spf], T_h);
     Y_io[spf] = Y_part[spf];
   }
   vel_io[0] = vel_part[0];

@@ -108,91 +108,167 @@ __device__ __forceinline__ void update_one(const KParams& P, int b, long long s,
         ssv[1][dir] = sx_hi;
       }
     }
-    // InterpolateGasPhase (SprayInterpolation.H:99-150), PeleLMeX branch
-    GasVals<NS, NF> gpv;
-    gpv.rho = 0.;
-    gpv.T = 0.;
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      gpv.vel[d] = 0.;
-      gpv.mom_src[d] = 0.;
-    }
-#pragma unroll
-    for (int n = 0; n < NS; ++n) {
-      gpv.Y[n] = 0.;
-    }
-#pragma unroll
-    for (int spf = 0; spf < NF; ++spf) {
-      gpv.Ydot[spf] = 0.;
-    }
-    gpv.eng_src = 0.;
-    gpv.mass_src = 0.;
+    // InterpolateGasPhase (SprayInterpolation.H:99-150), PeleLMeX branch, then
+    // GasPhaseVals::define, calcBoilT and the droplet physics of the form
+    SrcD<NF> src;
+    int nsub = 0;
     bool state_ok = true;
+    if (FORM == Form::FP64) {
+      GasVals<NS, NF> gpv;
+      gpv.rho = 0.;
+      gpv.T = 0.;
 #pragma unroll
-    for (int kk = -1; kk < 1; ++kk) {
+      for (int d = 0; d < 3; ++d) {
+        gpv.vel[d] = 0.;
+        gpv.mom_src[d] = 0.;
+      }
 #pragma unroll
-      for (int jj = -1; jj < 1; ++jj) {
+      for (int n = 0; n < NS; ++n) {
+        gpv.Y[n] = 0.;
+      }
 #pragma unroll
-        for (int ii = -1; ii < 1; ++ii) {
-          const double cw = __dmul_rn(__dmul_rn(ssv[ii + 1][0], ssv[jj + 1][1]), ssv[kk + 1][2]);
-          if (cw > 0.) {
-            const int ci = ijk[0] + ii;
-            const int cj = ijk[1] + jj;
-            const int ck = ijk[2] + kk;
-            if (!in_box(B.state_lo, B.state_hi, ci, cj, ck)) {
-              state_ok = false;
-            } else {
-              const double* q = B.st + (long long)(ci - B.st_lo[0]) + (long long)(cj - B.st_lo[1]) * B.st_js +
-                                (long long)(ck - B.st_lo[2]) * B.st_ks;
-              const double cur_rho = __ldg(q + (long long)P.c_rho * B.st_ns);
-              gpv.rho = __dadd_rn(gpv.rho, __dmul_rn(cw, cur_rho));
-              const double inv_rho = 1. / cur_rho;
+      for (int spf = 0; spf < NF; ++spf) {
+        gpv.Ydot[spf] = 0.;
+      }
+      gpv.eng_src = 0.;
+      gpv.mass_src = 0.;
 #pragma unroll
-              for (int n = 0; n < NS; ++n) {
-                const double cur_mf = __dmul_rn(__ldg(q + (long long)(P.c_spec + n) * B.st_ns), inv_rho);
-                gpv.Y[n] = __dadd_rn(gpv.Y[n], __dmul_rn(cw, cur_mf));
+      for (int kk = -1; kk < 1; ++kk) {
+#pragma unroll
+        for (int jj = -1; jj < 1; ++jj) {
+#pragma unroll
+          for (int ii = -1; ii < 1; ++ii) {
+            const double cw = __dmul_rn(__dmul_rn(ssv[ii + 1][0], ssv[jj + 1][1]), ssv[kk + 1][2]);
+            if (cw > 0.) {
+              const int ci = ijk[0] + ii;
+              const int cj = ijk[1] + jj;
+              const int ck = ijk[2] + kk;
+              if (!in_box(B.state_lo, B.state_hi, ci, cj, ck)) {
+                state_ok = false;
+              } else {
+                const double* q = B.st + (long long)(ci - B.st_lo[0]) + (long long)(cj - B.st_lo[1]) * B.st_js +
+                                  (long long)(ck - B.st_lo[2]) * B.st_ks;
+                const double cur_rho = __ldg(q + (long long)P.c_rho * B.st_ns);
+                gpv.rho = __dadd_rn(gpv.rho, __dmul_rn(cw, cur_rho));
+                const double inv_rho = 1. / cur_rho;
+#pragma unroll
+                for (int n = 0; n < NS; ++n) {
+                  const double cur_mf = __dmul_rn(__ldg(q + (long long)(P.c_spec + n) * B.st_ns), inv_rho);
+                  gpv.Y[n] = __dadd_rn(gpv.Y[n], __dmul_rn(cw, cur_mf));
+                }
+#pragma unroll
+                for (int dir = 0; dir < 3; ++dir) {
+                  gpv.vel[dir] =
+                    __dadd_rn(gpv.vel[dir], __dmul_rn(cw, __ldg(q + (long long)(P.c_mom + dir) * B.st_ns)));
+                }
+                gpv.T = __dadd_rn(gpv.T, __dmul_rn(cw, __ldg(q + (long long)P.c_T * B.st_ns)));
               }
-#pragma unroll
-              for (int dir = 0; dir < 3; ++dir) {
-                gpv.vel[dir] = __dadd_rn(gpv.vel[dir], __dmul_rn(cw, __ldg(q + (long long)(P.c_mom + dir) * B.st_ns)));
-              }
-              gpv.T = __dadd_rn(gpv.T, __dmul_rn(cw, __ldg(q + (long long)P.c_T * B.st_ns)));
             }
           }
         }
       }
-    }
-    if (!state_ok) {
-      set_error(P, PMP_ERR_STATE_BOX, b, s);
-      ok = false;
-      break;
-    }
-    // GasPhaseVals::define (SprayFuelData.H:101-111)
-    double mw_mix = 0.;
+      if (!state_ok) {
+        set_error(P, PMP_ERR_STATE_BOX, b, s);
+        ok = false;
+        break;
+      }
+      double mw_mix = 0.;
 #pragma unroll
-    for (int n = 0; n < NS; ++n) {
-      mw_mix = __dadd_rn(mw_mix, gpv.Y[n] / P.m.mw_kg[n]);
-    }
-    gpv.p = __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(gpv.rho, kRuCgs), mw_mix), gpv.T), kRuConv);
-    gpv.mw_mix = 1. / mw_mix;
-    // SprayData::calcBoilT (SprayFuelData.H:178-200)
-    double cBoilT[NF];
-    {
-      const double RU = kRuCgs * kRuConv;
-      const double PATM = kPatmCgs * kPresConv;
-      const double lp = pmp_log(PATM / gpv.p);
+      for (int n = 0; n < NS; ++n) {
+        mw_mix = __dadd_rn(mw_mix, gpv.Y[n] / P.m.mw_kg[n]);
+      }
+      gpv.p = __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(gpv.rho, kRuCgs), mw_mix), gpv.T), kRuConv);
+      gpv.mw_mix = 1. / mw_mix;
+      double cBoilT[NF];
+      {
+        const double RU = kRuCgs * kRuConv;
+        const double PATM = kPatmCgs * kPresConv;
+        const double lp = pmp_log(PATM / gpv.p);
+#pragma unroll
+        for (int spf = 0; spf < NF; ++spf) {
+          const double mw_fuel = P.m.mw_kg[P.f.indx[spf]];
+          const double cc = 1. / __dadd_rn(__dmul_rn(lp, RU) / (P.f.hboil_ref[spf] * mw_fuel), 1. / P.f.boilT[spf]);
+          cBoilT[spf] = dmin(P.f.critT[spf], cc);
+        }
+      }
+      nsub = spray_source_fp64<NS, NF>(P, P.sub_dt, gpv, vel, T, dia, Y, num_ppp, id, cBoilT);
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        src.mom[d] = gpv.mom_src[d];
+      }
+      src.mass = gpv.mass_src;
 #pragma unroll
       for (int spf = 0; spf < NF; ++spf) {
-        const double mw_fuel = P.m.mw_kg[P.f.indx[spf]];
-        const double cc = 1. / __dadd_rn(__dmul_rn(lp, RU) / (P.f.hboil_ref[spf] * mw_fuel), 1. / P.f.boilT[spf]);
-        cBoilT[spf] = dmin(P.f.critT[spf], cc);
+        src.Ydot[spf] = gpv.Ydot[spf];
       }
-    }
-    int nsub;
-    if (FORM == Form::FP64) {
-      nsub = spray_source_fp64<NS, NF>(P, P.sub_dt, gpv, vel, T, dia, Y, num_ppp, id, cBoilT);
+      src.eng = gpv.eng_src;
     } else {
-      nsub = spray_source_mixed<NS, NF>(P, P.sub_dt, gpv, vel, T, dia, Y, num_ppp, id, cBoilT);
+      // FP64 gather with fused multiply-adds, then the FP32 gas state
+      double rho = 0., Tg = 0., vel_g[3] = {0., 0., 0.}, Yg[NS];
+#pragma unroll
+      for (int n = 0; n < NS; ++n) {
+        Yg[n] = 0.;
+      }
+#pragma unroll
+      for (int kk = -1; kk < 1; ++kk) {
+#pragma unroll
+        for (int jj = -1; jj < 1; ++jj) {
+#pragma unroll
+          for (int ii = -1; ii < 1; ++ii) {
+            const double cw = ssv[ii + 1][0] * ssv[jj + 1][1] * ssv[kk + 1][2];
+            if (cw > 0.) {
+              const int ci = ijk[0] + ii;
+              const int cj = ijk[1] + jj;
+              const int ck = ijk[2] + kk;
+              if (!in_box(B.state_lo, B.state_hi, ci, cj, ck)) {
+                state_ok = false;
+              } else {
+                const double* q = B.st + (long long)(ci - B.st_lo[0]) + (long long)(cj - B.st_lo[1]) * B.st_js +
+                                  (long long)(ck - B.st_lo[2]) * B.st_ks;
+                const double cur_rho = __ldg(q + (long long)P.c_rho * B.st_ns);
+                rho = fma(cw, cur_rho, rho);
+                const double w_rho = cw / cur_rho;
+#pragma unroll
+                for (int n = 0; n < NS; ++n) {
+                  Yg[n] = fma(w_rho, __ldg(q + (long long)(P.c_spec + n) * B.st_ns), Yg[n]);
+                }
+#pragma unroll
+                for (int dir = 0; dir < 3; ++dir) {
+                  vel_g[dir] = fma(cw, __ldg(q + (long long)(P.c_mom + dir) * B.st_ns), vel_g[dir]);
+                }
+                Tg = fma(cw, __ldg(q + (long long)P.c_T * B.st_ns), Tg);
+              }
+            }
+          }
+        }
+      }
+      if (!state_ok) {
+        set_error(P, PMP_ERR_STATE_BOX, b, s);
+        ok = false;
+        break;
+      }
+      GasF<NS> g;
+      g.rho = (float)rho;
+      g.T = (float)Tg;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        g.vel[d] = (float)vel_g[d];
+      }
+      float mwinv = 0.f;
+#pragma unroll
+      for (int n = 0; n < NS; ++n) {
+        g.Y[n] = (float)Yg[n];
+        mwinv = fmaf(g.Y[n], P.mf.inv_mw_kg[n], mwinv);
+      }
+      g.p = g.rho * (float)(kRuCgs * kRuConv) * mwinv * g.T;
+      g.mw_mix = fdiv(1.f, mwinv);
+      float cBoilT[NF];
+      const float lp = flog(fdiv((float)(kPatmCgs * kPresConv), g.p));
+#pragma unroll
+      for (int spf = 0; spf < NF; ++spf) {
+        cBoilT[spf] = fminf(P.ff.critT[spf], fdiv(1.f, fmaf(lp, P.ff.hb[spf], P.ff.inv_boilT[spf])));
+      }
+      nsub = spray_source_mixed<NS, NF>(P, P.sub_dt, g, cBoilT, vel, T, dia, Y, num_ppp, id, src);
     }
     c.sub += 1;
     c.inner += static_cast<unsigned long long>(nsub);
@@ -210,17 +286,17 @@ __device__ __forceinline__ void update_one(const KParams& P, int b, long long s,
     if (P.f.mom_trans) {
 #pragma unroll
       for (int dir = 0; dir < 3; ++dir) {
-        atomicAdd(q + (long long)(P.s_mom + dir) * B.sr_ns, __dmul_rn(cur_coef, gpv.mom_src[dir]));
+        atomicAdd(q + (long long)(P.s_mom + dir) * B.sr_ns, __dmul_rn(cur_coef, src.mom[dir]));
       }
     }
     if (P.f.mass_trans) {
-      atomicAdd(q + (long long)P.s_rho * B.sr_ns, __dmul_rn(cur_coef, gpv.mass_src));
+      atomicAdd(q + (long long)P.s_rho * B.sr_ns, __dmul_rn(cur_coef, src.mass));
 #pragma unroll
       for (int spf = 0; spf < NF; ++spf) {
-        atomicAdd(q + (long long)(P.s_spec + spf) * B.sr_ns, __dmul_rn(cur_coef, gpv.Ydot[spf]));
+        atomicAdd(q + (long long)(P.s_spec + spf) * B.sr_ns, __dmul_rn(cur_coef, src.Ydot[spf]));
       }
     }
-    atomicAdd(q + (long long)P.s_eng * B.sr_ns, __dmul_rn(cur_coef, gpv.eng_src));
+    atomicAdd(q + (long long)P.s_eng * B.sr_ns, __dmul_rn(cur_coef, src.eng));
     // move (SprayParticles.cpp:444-476)
     if (P.do_move && !P.f.fixed_parts && id > 0) {
 #pragma unroll

@@ -3,9 +3,10 @@
 // Same driver loop as the FP64 kernel (SprayParticles.cpp:324-481), with the
 // per-droplet physics of calculateSpraySource (Drag.H:138-441) evaluated in
 // FP32: gas thermo and transport, vapour state, the B_T fixed point, drag,
-// Nusselt/Sherwood numbers.  FP64 is kept where precision is structural:
+// Nusselt/Sherwood numbers, from FP32 copies of the tables (DevMechF,
+// DevFuelF).  FP64 is kept where precision is structural:
 //  - cell indices and positions (bit-exact cells, as in the FP64 form);
-//  - the trilinear gather of the FP64 mesh;
+//  - the trilinear gather of the FP64 mesh (FP64 fused multiply-adds);
 //  - the droplet state update: velocity, temperature, mass, mass fractions
 //    and diameter are integrated in FP64 from the FP32 rates;
 //  - the deposits: mass and species sources are FP64 differences of FP64
@@ -41,7 +42,7 @@ __device__ __forceinline__ float fexp2(float x)
 
 __device__ __forceinline__ float fexp(float x)
 {
-  // x log2(e) as hi + lo so that the fraction keeps full precision
+  // x log2(e) with a two-part constant so the fraction keeps full precision
   const float t = x * 1.44269502f;
   const float k = rintf(t);
   float f = fmaf(x, 1.44269502f, -k);
@@ -54,7 +55,7 @@ __device__ __forceinline__ float fexp(float x)
 // log2(x) for positive normal x: SFU lg2 on the mantissa in [sqrt(1/2),sqrt(2)), exact exponent
 __device__ __forceinline__ float flog2(float x)
 {
-  int b = __float_as_int(x);
+  const int b = __float_as_int(x);
   int e = ((b >> 23) & 0xff) - 127;
   int mb = (b & 0x007fffff) | 0x3f800000;
   if (mb > 0x3fb504f3) {  // m > sqrt(2)
@@ -73,13 +74,16 @@ __device__ __forceinline__ float fpow(float x, float y)
   return (x == 0.f) ? 0.f : fexp2(y * flog2(x));
 }
 
+__device__ __forceinline__ float fdiv(float a, float b) { return __fdividef(a, b); }
+
 __device__ __forceinline__ float fcbrt(float x)
 {
   if (x == 0.f) {
     return 0.f;
   }
-  float y = fexp2(flog2(fabsf(x)) * (1.f / 3.f));
-  y = y - (y * y * y - fabsf(x)) / (3.f * y * y);
+  const float a = fabsf(x);
+  float y = fexp2(flog2(a) * (1.f / 3.f));
+  y = y - fdiv(y * y * y - a, 3.f * y * y);
   return x < 0.f ? -y : y;
 }
 
@@ -95,15 +99,15 @@ __device__ __forceinline__ float flog1p(float x)
 // cbrt in FP64 from an FP32 estimate and one Newton step (error ~1e-16)
 __device__ __forceinline__ double dcbrt_from_f(double a)
 {
-  double y = static_cast<double>(fcbrt(static_cast<float>(a)));
+  const double y = static_cast<double>(fcbrt(static_cast<float>(a)));
   const double y2 = y * y;
   const double r = fma(y2, y, -a);
-  return y - r / (3.0 * y2);
+  return y - r * static_cast<double>(__frcp_rn(static_cast<float>(3.0 * y2)));
 }
 
-__device__ __forceinline__ float fcubic(const double* c, float x)
+__device__ __forceinline__ float fcubic(const float* c, float x)
 {
-  return fmaf(fmaf(fmaf((float)c[3], x, (float)c[2]), x, (float)c[1]), x, (float)c[0]);
+  return fmaf(fmaf(fmaf(c[3], x, c[2]), x, c[1]), x, c[0]);
 }
 
 template <int N>
@@ -126,6 +130,19 @@ __device__ __forceinline__ void fput(float (&a)[N], int i, float v)
   }
 }
 
+__device__ __forceinline__ float cpf(const DevMechF& m, int n, float T)
+{
+  const float* a = m.cp[n];
+  return fmaf(fmaf(fmaf(fmaf(a[4], T, a[3]), T, a[2]), T, a[1]), T, a[0]) * m.ru_w_eng[n];
+}
+
+__device__ __forceinline__ float hf(const DevMechF& m, int n, float T)
+{
+  const float* c = m.hc[n];
+  const float hp = fmaf(fmaf(fmaf(fmaf(c[4], T, c[3]), T, c[2]), T, c[1]), T, c[0]);
+  return fmaf(hp, T, c[5]) * m.ru_w_eng[n];
+}
+
 __device__ __forceinline__ float heat_coeff_f(float ratio, float B_M, float Nu_0)
 {
   if (B_M <= 1e-15f) {
@@ -133,38 +150,59 @@ __device__ __forceinline__ float heat_coeff_f(float ratio, float B_M, float Nu_0
   }
   const float NU2 = Nu_0 - 2.f;
   const float lnBM1 = flog(1.f + B_M);
-  float phi = ratio / Nu_0;
+  float phi = fdiv(ratio, Nu_0);
   float B_T_old = fexp(phi * lnBM1) - 1.f;
   float logB = flog1p(B_T_old);
-  float invFT = B_T_old / (logB * fpow(1.f + B_T_old, 0.7f));
+  float invFT = fdiv(B_T_old, logB * fpow(1.f + B_T_old, 0.7f));
   float Nu_num = 2.f + NU2 * invFT;
-  phi = ratio / Nu_num;
+  phi = fdiv(ratio, Nu_num);
   float B_T = fexp(phi * lnBM1) - 1.f;
   float error = fabsf(B_T - B_T_old);
   int k = 0;
   while (k < 100 && error > fmaxf(1e-7f, 8.f * 1.1920929e-7f * fabsf(B_T))) {
     B_T_old = B_T;
     logB = flog1p(B_T);
-    invFT = B_T / (logB * fpow(1.f + B_T, 0.7f));
+    invFT = fdiv(B_T, logB * fpow(1.f + B_T, 0.7f));
     Nu_num = 2.f + NU2 * invFT;
-    phi = ratio / Nu_num;
+    phi = fdiv(ratio, Nu_num);
     B_T = fexp(phi * lnBM1) - 1.f;
     error = fabsf(B_T - B_T_old);
     k++;
   }
   logB = flog1p(B_T);
-  invFT = B_T / (logB * fpow(1.f + B_T, 0.7f));
+  invFT = fdiv(B_T, logB * fpow(1.f + B_T, 0.7f));
   Nu_num = 2.f + NU2 * invFT;
-  return Nu_num * logB / B_T;
+  return fdiv(Nu_num * logB, B_T);
 }
+
+// interpolated gas state in FP32
+template <int NS>
+struct GasF {
+  float vel[3];
+  float T;
+  float rho;
+  float p;
+  float Y[NS];
+  float mw_mix;
+};
+
+// FP64 deposits of one sub-cycle
+template <int NF>
+struct SrcD {
+  double mom[3];
+  double mass;
+  double Ydot[NF];
+  double eng;
+};
 
 // calculateSpraySource with FP32 physics and FP64 state (see the file header).
 template <int NS, int NF>
 __device__ __forceinline__ int spray_source_mixed(
-  const KParams& P, double flow_dt, GasVals<NS, NF>& gpv, double* vel_io, double& T_io,
-  double& dia_io, double* Y_io, double num_ppp, int& id, const double* cBoilT)
+  const KParams& P, double flow_dt, const GasF<NS>& g, const float* cBoilT, double* vel_io,
+  double& T_io, double& dia_io, double* Y_io, double num_ppp, int& id, SrcD<NF>& src)
 {
-  const DevMech& m = P.m;
+  const DevMechF& m = P.mf;
+  const DevFuelF& ff = P.ff;
   const DevFuel& fdat = P.f;
   const float rule = 1.f / 3.f;
   const float C_eps = 1.E-15f;
@@ -172,18 +210,7 @@ __device__ __forceinline__ int spray_source_mixed(
   const int nSubMax = 100;
   const float RU = (float)(kRuCgs * kRuConv);
   const float PATM = (float)(kPatmCgs * kPresConv);
-  // gas state in FP32
-  const float Tg = (float)gpv.T;
-  const float pg = (float)gpv.p;
-  const float mw_mix = (float)gpv.mw_mix;
-  float Yg[NS];
-#pragma unroll
-  for (int n = 0; n < NS; ++n) {
-    Yg[n] = (float)gpv.Y[n];
-  }
   float Y_skin[NS];
-  float h_part[NS];
-  float cp_n[NS];
   float Ddiag[NF];
   float L_fuel[NF];
   float mi_dot[NF];
@@ -205,7 +232,7 @@ __device__ __forceinline__ int spray_source_mixed(
 #pragma unroll
   for (int spf = 0; spf < NF; ++spf) {
     Y_part[spf] = Y_io[spf];
-    rho_part += Y_part[spf] / rhoL(fdat, dmin(T_part, cBoilT[spf]), spf);
+    rho_part += Y_part[spf] / rhoL(fdat, dmin(T_part, (double)cBoilT[spf]), spf);
   }
   rho_part = 1. / rho_part;
   double dt = flow_dt;
@@ -215,34 +242,29 @@ __device__ __forceinline__ int spray_source_mixed(
   const double startmass = pmass;
   double eng_acc = 0.;
   double mom_acc[3] = {0., 0., 0.};
+  float T_h = (float)T_part;
   while (isub <= nsub) {
     const float Tp_f = (float)T_part;
+    T_h = Tp_f;
     const float dia_f = (float)dia_part;
     float cp_part = 0.f;
     double Tboil = 0.;
     float mw_part = 0.f;
 #pragma unroll
     for (int spf = 0; spf < NF; ++spf) {
-      Tboil += Y_part[spf] * cBoilT[spf];
-      cp_part += (float)Y_part[spf] * (float)fdat.cp[spf];
-      mw_part += (float)Y_part[spf] / (float)m.mw_kg[fdat.indx[spf]];
+      const float yp = (float)Y_part[spf];
+      Tboil += Y_part[spf] * (double)cBoilT[spf];
+      cp_part += yp * ff.cp[spf];
+      mw_part += yp * m.inv_mw_kg[fdat.indx[spf]];
     }
-    mw_part = 1.f / mw_part;
-    const float delT = fmaxf(Tg - Tp_f, 0.f);
-    float T_skin = Tg;
+    mw_part = fdiv(1.f, mw_part);
+    const float delT = fmaxf(g.T - Tp_f, 0.f);
+    float T_skin = g.T;
     if (fdat.mass_trans) {
       T_skin = Tp_f + rule * delT;
     }
 #pragma unroll
     for (int n = 0; n < NS; ++n) {
-      const double* a = m.cp[n];
-      const float cpr = fmaf(fmaf(fmaf(fmaf((float)a[4], T_skin, (float)a[3]), T_skin, (float)a[2]), T_skin,
-                                  (float)a[1]), T_skin, (float)a[0]);
-      cp_n[n] = cpr * (float)(m.ru_w[n] * kEngConv);
-      const double* hc = m.hc[n];
-      const float hp = fmaf(fmaf(fmaf(fmaf((float)hc[4], Tp_f, (float)hc[3]), Tp_f, (float)hc[2]), Tp_f,
-                                 (float)hc[1]), Tp_f, (float)hc[0]);
-      h_part[n] = fmaf(hp, Tp_f, (float)hc[5]) * (float)(m.ru_w[n] * kEngConv);
       Y_skin[n] = 0.f;
     }
     float cp_skin = 0.f;
@@ -254,24 +276,20 @@ __device__ __forceinline__ int spray_source_mixed(
 #pragma unroll
       for (int spf = 0; spf < NF; ++spf) {
         const int fspec = fdat.indx[spf];
-        const float mw_fuel = (float)m.mw_kg[fspec];
-        const float Tp = fminf(Tp_f, 0.99f * (float)cBoilT[spf]);
-        const float part_latent =
-          fsel(h_part, fspec) + (float)fdat.latent[spf] - (float)fdat.cp[spf] * (Tp - (float)fdat.ref_T);
+        const float mw_fuel = m.mw_kg[fspec];
+        const float Tp = fminf(Tp_f, 0.99f * cBoilT[spf]);
+        const float part_latent = hf(m, fspec, Tp_f) + ff.latent[spf] - ff.cp[spf] * (Tp - ff.ref_T);
         L_fuel[spf] = part_latent;
         float pres_sat;
-        if (fdat.psat_coef[4 * spf + 3] == 0.) {
-          pres_sat = PATM * fexp(part_latent * mw_fuel / RU * (1.f / (float)fdat.boilT[spf] - 1.f / Tp));
+        if (ff.psat_d[spf] == 0.f) {
+          pres_sat = PATM * fexp(part_latent * mw_fuel / RU * (ff.inv_boilT[spf] - fdiv(1.f, Tp)));
         } else {
-          const float a = (float)fdat.psat_coef[4 * spf];
-          const float b = (float)fdat.psat_coef[4 * spf + 1];
-          const float c = (float)fdat.psat_coef[4 * spf + 2];
-          pres_sat = (float)fdat.psat_coef[4 * spf + 3] * fexp2((a - b / (Tp + c)) * 3.32192809f);
+          pres_sat = ff.psat_d[spf] * fexp2((ff.psat_a[spf] - fdiv(ff.psat_b[spf], Tp + ff.psat_c[spf])) * 3.32192809f);
         }
-        const float X_fluid = fsel(Yg, fdat.dep[spf]) * mw_mix / mw_fuel;
-        if (pres_sat > X_fluid * pg) {
-          const float Xl = (float)Y_part[spf] * mw_part / mw_fuel;
-          const float Xv = Xl * pres_sat / pg;
+        const float X_fluid = fsel(g.Y, fdat.dep[spf]) * g.mw_mix * m.inv_mw_kg[fspec];
+        if (pres_sat > X_fluid * g.p) {
+          const float Xl = (float)Y_part[spf] * mw_part * m.inv_mw_kg[fspec];
+          const float Xv = fdiv(Xl * pres_sat, g.p);
           mbar_vap += Xv * mw_fuel;
           sumXVap += Xv;
           X_vapor[spf] = Xv;
@@ -279,7 +297,7 @@ __device__ __forceinline__ int spray_source_mixed(
           X_vapor[spf] = 0.f;
         }
       }
-      const float totalmwx = mbar_vap + (1.f - sumXVap) * mw_mix;
+      const float inv_totalmwx = fdiv(1.f, mbar_vap + (1.f - sumXVap) * g.mw_mix);
       float sumYSkin = 0.f;
       float sumYfFluid = 0.f;
       float sumYVap = 0.f;
@@ -287,69 +305,69 @@ __device__ __forceinline__ int spray_source_mixed(
       for (int spf = 0; spf < NF; ++spf) {
         if (X_vapor[spf] > 0.f) {
           const int fspec = fdat.indx[spf];
-          const float Yfv = X_vapor[spf] * (float)m.mw_kg[fspec] / totalmwx;
+          const float Yfv = X_vapor[spf] * m.mw_kg[fspec] * inv_totalmwx;
           sumYVap += Yfv;
-          const float gasY = fsel(Yg, fdat.dep[spf]);
+          const float gasY = fsel(g.Y, fdat.dep[spf]);
           sumYfFluid += gasY;
           const float Ysk = Yfv + rule * (gasY - Yfv);
           fput(Y_skin, fspec, Ysk);
           sumYSkin += Ysk;
         }
       }
-      const float renorm = (1.f - sumYSkin) / (1.f - sumYfFluid);
+      const float renorm = fdiv(1.f - sumYSkin, 1.f - sumYfFluid);
 #pragma unroll
       for (int n = 0; n < NS; ++n) {
         if (Y_skin[n] == 0.f) {
-          Y_skin[n] = Yg[n] * renorm;
+          Y_skin[n] = g.Y[n] * renorm;
         }
-        cp_skin += Y_skin[n] * cp_n[n];
-        mw_skin += Y_skin[n] / (float)m.mw_kg[n];
+        cp_skin += Y_skin[n] * cpf(m, n, T_skin);
+        mw_skin += Y_skin[n] * m.inv_mw_kg[n];
       }
-      mw_skin = 1.f / mw_skin;
-      B_M = (sumYVap - sumYfFluid) / fmaxf(C_eps, (1.f - sumYVap));
+      mw_skin = fdiv(1.f, mw_skin);
+      B_M = fdiv(sumYVap - sumYfFluid, fmaxf(C_eps, (1.f - sumYVap)));
       B_M = fminf(20.f, B_M);
     } else {
 #pragma unroll
       for (int n = 0; n < NS; ++n) {
-        Y_skin[n] = Yg[n];
-        cp_skin += Yg[n] * cp_n[n];
+        Y_skin[n] = g.Y[n];
+        cp_skin += g.Y[n] * cpf(m, n, T_skin);
       }
-      mw_skin = mw_mix;
+      mw_skin = g.mw_mix;
     }
     float lambda_skin = 0.f;
     float mu_skin = 0.f;
-    float rho_skin = (float)gpv.rho;
+    float rho_skin = g.rho;
     if (fdat.mass_trans) {
-      rho_skin = mw_skin * pg / (RU * T_skin);
+      rho_skin = fdiv(mw_skin * g.p, RU * T_skin);
     }
     {
       float X[NS];
       float sumYW = 0.f;
 #pragma unroll
       for (int k = 0; k < NS; ++k) {
-        sumYW += Y_skin[k] / (float)m.mw_g[k];
+        sumYW += Y_skin[k] * m.inv_mw_g[k];
       }
-      const float wbar = 1.f / sumYW;
+      const float wbar = fdiv(1.f, sumYW);
 #pragma unroll
       for (int k = 0; k < NS; ++k) {
-        X[k] = Y_skin[k] * wbar / (float)m.mw_g[k];
+        X[k] = Y_skin[k] * wbar * m.inv_mw_g[k];
       }
       const float lnT = flog(T_skin);
       float s = 0.f;
 #pragma unroll
       for (int k = 0; k < NS; ++k) {
-        s = fmaf(X[k], fexp(6.f * fcubic(m.mu[k], lnT)), s);
+        s = fmaf(X[k], fexp(fcubic(m.mu6[k], lnT)), s);
       }
       mu_skin = fexp(flog(s) * (1.f / 6.f));
       if (fdat.mass_trans) {
         float sl = 0.f;
 #pragma unroll
         for (int k = 0; k < NS; ++k) {
-          sl = fmaf(X[k], fexp(0.25f * fcubic(m.lam[k], lnT)), sl);
+          sl = fmaf(X[k], fexp(fcubic(m.lam4[k], lnT)), sl);
         }
         const float s2 = sl * sl;
         lambda_skin = s2 * s2;
-        const float rt = (float)kRuCgs * T_skin;
+        const float inv_rt = fdiv(1.f, (float)kRuCgs * T_skin);
 #pragma unroll
         for (int f = 0; f < NF; ++f) {
           const int i = fdat.indx[f];
@@ -359,10 +377,10 @@ __device__ __forceinline__ int spray_source_mixed(
           for (int j = 0; j < NS; ++j) {
             if (j != i) {
               term1 += Y_skin[j];
-              term2 = fmaf(X[j], fexp(-fcubic(m.dbin[f][j], lnT)), term2);
+              term2 = fmaf(X[j], fexp(fcubic(m.dbinm[f][j], lnT)), term2);
             }
           }
-          Ddiag[f] = (float)m.mw_g[i] * term1 / (term2 * rt);
+          Ddiag[f] = fdiv(m.mw_g[i] * term1 * inv_rt, term2);
         }
       }
     }
@@ -371,27 +389,26 @@ __device__ __forceinline__ int spray_source_mixed(
     float diff_vel[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      diff_vel[d] = (float)(gpv.vel[d] - vel_part[d]);
+      diff_vel[d] = g.vel[d] - (float)vel_part[d];
     }
     const float diff_vel_mag =
       sqrtf(diff_vel[0] * diff_vel[0] + diff_vel[1] * diff_vel[1] + diff_vel[2] * diff_vel[2]);
-    const float Reyn = rho_skin * diff_vel_mag * dia_f / mu_skin;
+    const float Reyn = fdiv(rho_skin * diff_vel_mag * dia_f, mu_skin);
     const float inv_pmass = (float)(1. / pmass);
     float drag_coef = 0.f;
     if (Reyn > 1000.f) {
       drag_coef = 0.424f;
     } else if (Reyn > 1.f) {
-      drag_coef = 24.f / Reyn * (1.f + fcbrt(Reyn * Reyn) / 6.f);
+      drag_coef = fdiv(24.f, Reyn) * (1.f + fcbrt(Reyn * Reyn) * (1.f / 6.f));
     } else if (Reyn > 0.f) {
-      drag_coef = 24.f / Reyn;
+      drag_coef = fdiv(24.f, Reyn);
     }
-    const float drag_force =
-      0.125f * rho_skin * drag_coef * (float)PMP_PI * dia_f * dia_f * diff_vel_mag;
-    const float drag_force_p = 0.75f * rho_skin * drag_coef * diff_vel_mag / (dia_f * (float)rho_part);
+    const float drag_force = 0.125f * rho_skin * drag_coef * (float)PMP_PI * dia_f * dia_f * diff_vel_mag;
+    const float drag_force_p = fdiv(0.75f * rho_skin * drag_coef * diff_vel_mag, dia_f * (float)rho_part);
     float part_vel_src[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      part_vel_src[d] = drag_force_p * diff_vel[d] + (float)fdat.body_force[d];
+      part_vel_src[d] = drag_force_p * diff_vel[d] + ff.body_force[d];
     }
     if (fdat.mom_trans) {
       const double nd = num_ppp * (double)drag_force;
@@ -406,7 +423,7 @@ __device__ __forceinline__ int spray_source_mixed(
     float part_temp_src = 0.f;
     float m_dot = 0.f;
     if (fdat.mass_trans) {
-      const float Pr_skin = mu_skin * cp_skin / lambda_skin;
+      const float Pr_skin = fdiv(mu_skin * cp_skin, lambda_skin);
       const float powR = fmaxf(fpow(fminf(400.f, Reyn), 0.077f), 1.f);
       float Nu_num = 0.f;
       float sumL = 0.f;
@@ -415,25 +432,24 @@ __device__ __forceinline__ int spray_source_mixed(
         float rhoDtotal = 0.f;
         float cp_fuel = 0.f;
         float sumYSkin = 0.f;
+        const float inv_sumX = fdiv(1.f, sumXVap);
 #pragma unroll
         for (int spf = 0; spf < NF; ++spf) {
           const int fspec = fdat.indx[spf];
-          Ddiag[spf] *= mw_skin / (float)m.mw_kg[fspec] * (float)kRhodConv;
-          const float X_norm = X_vapor[spf] / sumXVap;
-          Ddiag[spf] *= X_norm;
+          Ddiag[spf] *= mw_skin * m.inv_mw_kg[fspec] * (float)kRhodConv * (X_vapor[spf] * inv_sumX);
           rhoDtotal += Ddiag[spf];
           const float ysk = fsel(Y_skin, fspec);
-          cp_fuel += ysk * fsel(cp_n, fspec);
+          cp_fuel += ysk * cpf(m, fspec, T_skin);
           sumYSkin += ysk;
         }
-        cp_fuel /= sumYSkin;
-        const float Sc_skin = mu_skin / rhoDtotal;
+        cp_fuel = fdiv(cp_fuel, sumYSkin);
+        const float Sc_skin = fdiv(mu_skin, rhoDtotal);
         const float logB = flog1p(B_M);
-        const float invFM = B_M / (logB * fpow(1.f + B_M, 0.7f));
+        const float invFM = fdiv(B_M, logB * fpow(1.f + B_M, 0.7f));
         const float Sh_0 = 1.f + powR * fcbrt(1.f + Reyn * Sc_skin);
         const float Sh_num = 2.f + (Sh_0 - 2.f) * invFM;
         const float mdotcoeff = (float)PMP_PI * dia_f * Sh_num * logB;
-        const float ratio = cp_fuel * Sh_num * rhoDtotal / lambda_skin;
+        const float ratio = fdiv(cp_fuel * Sh_num * rhoDtotal, lambda_skin);
         Nu_num = heat_coeff_f(ratio, B_M, Nu_0);
 #pragma unroll
         for (int spf = 0; spf < NF; ++spf) {
@@ -448,10 +464,10 @@ __device__ __forceinline__ int spray_source_mixed(
       }
       const float conv_src = (float)PMP_PI * lambda_skin * dia_f * delT * Nu_num;
       eng_acc += num_ppp * (double)conv_src;
-      part_temp_src = (sumL + conv_src) * inv_pmass / cp_part;
+      part_temp_src = fdiv((sumL + conv_src) * inv_pmass, cp_part);
       if (isub == 1 && delT > C_eps) {
-        const float inv_tau_d = -m_dot / (0.2f * (float)pmass);
-        const float inv_tau_T = conv_src * inv_pmass / (cp_part * delT);
+        const float inv_tau_d = fdiv(-m_dot, 0.2f * (float)pmass);
+        const float inv_tau_T = fdiv(conv_src * inv_pmass, cp_part * delT);
         nsub = min(max(nsub, max(static_cast<int>((float)flow_dt * inv_tau_d),
                                  static_cast<int>((float)flow_dt * inv_tau_T)) + 1),
                    nSubMax);
@@ -486,11 +502,11 @@ __device__ __forceinline__ int spray_source_mixed(
 #pragma unroll
           for (int spf = 0; spf < NF; ++spf) {
             Y_part[spf] /= sumY;
-            rho_part += Y_part[spf] / rhoL(fdat, dmin(T_part, cBoilT[spf]), spf);
+            rho_part += Y_part[spf] / rhoL(fdat, dmin(T_part, (double)cBoilT[spf]), spf);
           }
           rho_part = 1. / rho_part;
         } else {
-          rho_part = rhoL(fdat, dmin(T_part, cBoilT[0]), 0);
+          rho_part = rhoL(fdat, dmin(T_part, (double)cBoilT[0]), 0);
         }
         pmass = new_mass;
         dia_part = dcbrt_from_f(6. * pmass / (PMP_PI * rho_part));
@@ -503,33 +519,32 @@ __device__ __forceinline__ int spray_source_mixed(
     }
     ++isub;
   }
-  gpv.eng_src = eng_acc;
+  src.eng = eng_acc;
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
-    gpv.mom_src[d] = mom_acc[d];
+    src.mom[d] = mom_acc[d];
   }
   if (nsub > 1) {
-    gpv.eng_src /= static_cast<double>(nsub);
+    src.eng /= static_cast<double>(nsub);
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      gpv.mom_src[d] /= static_cast<double>(nsub);
+      src.mom[d] /= static_cast<double>(nsub);
     }
   }
-  const double mdot_total = (pmass - startmass) / (fdat.dtmod * flow_dt);
-  gpv.mass_src = num_ppp * mdot_total;
+  const double inv_dtf = 1. / (fdat.dtmod * flow_dt);
+  const double mdot_total = (pmass - startmass) * inv_dtf;
+  src.mass = num_ppp * mdot_total;
   if (fdat.mom_trans) {
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      gpv.mom_src[d] += num_ppp * vel_part[d] * mdot_total;
+      src.mom[d] += num_ppp * vel_part[d] * mdot_total;
     }
   }
 #pragma unroll
   for (int spf = 0; spf < NF; ++spf) {
-    const double oldY = Y_io[spf];
-    const double newY = Y_part[spf];
-    const double midot = (newY * pmass - oldY * startmass) / (fdat.dtmod * flow_dt);
-    gpv.Ydot[spf] = num_ppp * midot;
-    gpv.eng_src += num_ppp * midot * (double)fsel(h_part, fdat.dep[spf]);
+    const double midot = (Y_part[spf] * pmass - Y_io[spf] * startmass) * inv_dtf;
+    src.Ydot[spf] = num_ppp * midot;
+    src.eng += num_ppp * midot * (double)hf(m, fdat.dep[spf], T_h);
     Y_io[spf] = Y_part[spf];
   }
   vel_io[0] = vel_part[0];
