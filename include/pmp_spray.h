@@ -205,7 +205,8 @@ typedef struct pmp_stats {
   long long substeps;        /* droplet-substeps executed (live droplets x sub-cycles) */
   long long killed;          /* droplets that evaporated or left the domain */
   long long inner_steps;     /* sum over droplet-substeps of the inner nsub */
-  long long fallback;        /* learned form: droplet-substeps sent to the plain path */
+  long long fallback;        /* mixed / learned forms: droplets handed to the
+                                plain FP64 kernel (small, out of range) */
   double kernel_ms;          /* device time of the update kernels */
 } pmp_stats;
 
@@ -305,6 +306,82 @@ int pmp_spray_update_static(
   double time, int state_ghosts, int source_ghosts, int is_virt,
   int is_ghost, int do_move, double spray_cfl_lev, void* stream,
   pmp_error_info* err);
+
+/* ---------------------------------------------------------------------------
+ * Learned form (PMP_MODE_LEARNED).  No counterpart in the reference.  A
+ * 10-64-64-64-5 SiLU network replaces the film-property and heat/mass
+ * transfer evaluation of each inner sub-step of calculateSpraySource
+ * (Drag.H:212-360); the drag law, sub-step count, explicit FP64 update,
+ * deposits and move stay exact.  Droplets whose inputs fall outside the
+ * training range (widened by gate_margin), or whose predicted outputs are
+ * not sane, and droplets below 2 um, run the plain FP64 kernel instead.
+ * Workflow: set grids and droplets, call pmp_spray_learn_generate on one or
+ * more representative states (the FP64 teacher labels the droplets there),
+ * pmp_spray_learn_train, then pmp_spray_set_mode(h, PMP_MODE_LEARNED). */
+typedef struct pmp_learn_config {
+  int epochs;              /* passes over the training tuples (0: 20) */
+  int batch;               /* rows per Adam step (0: 8192) */
+  double lr;               /* initial learning rate (0: 2e-3), decays x0.01 */
+  double gate_margin;      /* accepted input range = training range widened
+                              by this fraction of its span (0: 0.05) */
+  double audit_fraction;   /* share of droplets re-labelled by the teacher in
+                              every learned update to measure the error (0: none) */
+  int no_quant;            /* 1: train without bf16 rounding (diagnostics) */
+  unsigned long long seed; /* initialisation / batch order (0: 1) */
+} pmp_learn_config;
+
+typedef struct pmp_learn_report {
+  long long tuples;        /* training + validation rows */
+  long long steps;         /* Adam steps */
+  double loss_first;       /* normalised MSE of the first / last batch */
+  double loss_last;
+  double val_rel_rms[5];   /* held-out RMS error per output; the outputs are
+                              logarithms (fuel mass fluxes, heat transfer,
+                              film viscosity, film density), so this is
+                              their relative error */
+  double train_ms;         /* wall time of pmp_spray_learn_train */
+} pmp_learn_report;
+
+/* Label droplets for training: every sample_stride-th droplet (offset from
+ * seed) at the given device state, plus `augment` perturbed copies of each
+ * (temperature towards boiling, diameter, slip and composition).  Tuples
+ * accumulate over calls.  Views and arguments as for pmp_spray_update; no
+ * droplet or state is modified. */
+int pmp_spray_learn_generate(
+  pmp_spray* h, const pmp_box_view* state, int nboxes, double flow_dt,
+  int state_ghosts, int do_move, double spray_cfl_lev,
+  long long sample_stride, int augment, unsigned long long seed,
+  void* stream);
+int pmp_spray_learn_count(const pmp_spray* h, long long* n);
+/* Copy up to *n tuples to buf (16 floats each: the 10 raw inputs, the 5
+ * targets, one pad); *n receives the number copied.  With buf NULL, *n
+ * receives the number held. */
+int pmp_spray_learn_tuples(const pmp_spray* h, float* buf, long long* n);
+/* Train the network on the GPU (own forward / backward / Adam kernels; the
+ * forward pass rounds weights and activations to bf16 as inference does). */
+int pmp_spray_learn_train(pmp_spray* h, const pmp_learn_config* cfg,
+                          pmp_learn_report* report);
+/* get = 1: copy the trained parameters and normalisation to buf; get = 0:
+ * install them from buf.  With buf NULL, *count receives the length. */
+int pmp_spray_learn_weights(pmp_spray* h, int get, float* buf,
+                            long long* count);
+/* Share of droplets audited by the teacher in each learned update. */
+int pmp_spray_learn_set_audit(pmp_spray* h, double audit_fraction);
+/* Result of the audit of the last learned update: droplets audited and the
+ * RMS error of each of the 5 surrogate outputs, measured as val_rel_rms. */
+int pmp_spray_learn_audit(const pmp_spray* h, long long* audited,
+                          double rel_rms[5]);
+/* Check of the training kernels: MSE loss and its gradient for n rows of
+ * normalised inputs x[n][10] and targets y[n][5] at the flat parameter
+ * vector params[pmp_learn_param_count()] (quant = 1 rounds to bf16 as the
+ * training forward pass does).  Runs on the current device. */
+int pmp_learn_debug_grad(const float* params, const float* x, const float* y,
+                         int n, int quant, float* grads, double* loss);
+/* Check of the inference: the tensor-core network of the learned kernel on n
+ * rows of normalised inputs xn[n][10] at params; outputs y[n][5]. */
+int pmp_learn_debug_infer(const float* params, const float* xn, int n,
+                          float* y);
+int pmp_learn_param_count(void);
 
 #ifdef __cplusplus
 }

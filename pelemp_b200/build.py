@@ -20,8 +20,9 @@ LIB = os.path.join(PKG, "libpmpspray.so")
 # contraction (their multiply-adds are explicit fma() calls); the mixed and
 # learned forms allow it.
 SOURCES = [("pmp_spray.cu", "-fmad=false"), ("pmp_static.cu", "-fmad=false"),
-           ("pmp_mixed.cu", "-fmad=true")]
-HEADERS = ["pmp_device.cuh", "spray_fp64.cuh", "spray_mixed.cuh", "spray_kernels.cuh",
+           ("pmp_mixed.cu", "-fmad=true"), ("pmp_learn.cu", "-fmad=true")]
+HEADERS = ["pmp_device.cuh", "pmp_handle.h", "spray_fp64.cuh", "spray_mixed.cuh",
+           "spray_kernels.cuh", "learn/learn_common.cuh", "learn/mlp_mma.cuh",
            "phys/pmp_math.h", "phys/pmp_math_tables.h", "phys/pmp_thermo.h",
            "phys/pmp_thermo_data.h"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")

@@ -152,6 +152,26 @@ class Stats(C.Structure):
     ]
 
 
+class LearnConfig(C.Structure):
+    _fields_ = [
+        ("epochs", C.c_int), ("batch", C.c_int), ("lr", C.c_double),
+        ("gate_margin", C.c_double), ("audit_fraction", C.c_double),
+        ("no_quant", C.c_int), ("seed", C.c_ulonglong),
+    ]
+
+
+class LearnReport(C.Structure):
+    _fields_ = [
+        ("tuples", C.c_longlong), ("steps", C.c_longlong),
+        ("loss_first", C.c_double), ("loss_last", C.c_double),
+        ("val_rel_rms", C.c_double * 5), ("train_ms", C.c_double),
+    ]
+
+
+LEARN_IN = 10
+LEARN_OUT = 5
+
+
 # pmp_mech of pelemp_b200/csrc/phys/pmp_thermo.h (opaque blob of the right size
 # for the oracle bindings; the layout is checked in the tests)
 class Mech(C.Structure):

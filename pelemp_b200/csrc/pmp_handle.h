@@ -1,0 +1,95 @@
+// pmp_handle.h -- the library's private handle (struct pmp_spray) and the
+// helpers shared by its translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "phys/pmp_thermo.h"
+#include "pmp_device.cuh"
+
+namespace pmp {
+
+constexpr int kBlock = 128;
+constexpr int kSortPad = 8;  // cells of margin in the sort key around a box
+
+struct BoxStore {
+  long long n = 0;
+  double* d = nullptr;  // (3 + NR) * n doubles, sorted by cell
+  int* id = nullptr;
+  long long* perm = nullptr;  // sorted slot -> caller index
+};
+
+struct LearnState;  // learned form (pmp_learn.cu)
+
+}  // namespace pmp
+
+struct pmp_spray {
+  int device = 0;
+  int nfuel = 0;
+  int nspec = 0;
+  char species[PMP_MAX_SPEC][PMP_NAME_LEN];
+  pmp_mech mech;
+  pmp_spray_data data;
+  bool have_data = false;
+  pmp_spray_comps comps;
+  bool have_comps = false;
+  pmp_geometry geom;
+  bool have_geom = false;
+  std::vector<pmp_box> boxes;
+  int mode = PMP_MODE_FP64;
+  pmp::DevMech dmech;
+  pmp::DevFuel dfuel;
+  pmp::DevMechF dmechf;
+  pmp::DevFuelF dfuelf;
+  // per-box staged droplets (before packing)
+  std::vector<pmp::BoxStore> staged;
+  std::vector<bool> box_set;
+  // packed droplets
+  bool packed = false;
+  long long total = 0;
+  double* soa = nullptr;  // (3 + NR) arrays of length total
+  int* ids = nullptr;
+  long long* perm = nullptr;
+  std::vector<long long> box_begin;
+  int ncta = 0;
+  int* d_cta_box = nullptr;
+  long long* d_cta_start = nullptr;
+  long long* d_box_begin = nullptr;
+  long long* fb_list = nullptr;  // fallback slots (mixed / learned forms)
+  pmp::BoxEntry* d_boxes = nullptr;
+  pmp::BoxEntry* h_boxes = nullptr;
+  int boxes_cap = 0;
+  pmp::DevStatus* d_status = nullptr;
+  pmp::DevStatus* h_status = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  pmp_error_info last_err;
+  pmp_stats stats;
+  // view pointers already checked to be device-accessible
+  std::vector<const double*> checked_state, checked_src;
+  // device mirrors of host views for pmp_spray_update_host
+  std::vector<double*> stage_state, stage_src;
+  std::vector<size_t> stage_state_n, stage_src_n;
+  pmp::LearnState* learn = nullptr;
+  int nr() const { return PMP_PSTATE_NUM(nfuel); }
+  int ncomp() const { return 3 + nr(); }
+};
+
+namespace pmp {
+
+// pmp_spray.cu
+int set_err(pmp_spray* h, int code, const char* msg, int box = -1, long long particle = -1);
+// validate views, pack droplets, upload the box table, reset the status
+// block and fill the kernel parameters of one update call
+int prepare_update(
+  pmp_spray* h, const pmp_box_view* state, const pmp_box_view* source, int nboxes,
+  double flow_dt, int state_ghosts, int source_ghosts, int is_ghost, int do_move,
+  double spray_cfl_lev, cudaStream_t st, KParams& P);
+int run_fp64_list(int ns, int nf, const KParams& P, long long total, cudaStream_t st);
+// pmp_learn.cu
+int launch_learned(pmp_spray* h, const KParams& P, cudaStream_t st);
+bool learn_ready(const pmp_spray* h);
+void learn_free(pmp_spray* h);
+
+}  // namespace pmp

@@ -29,73 +29,13 @@ using pmp::BoxEntry;
 using pmp::DevStatus;
 using pmp::KParams;
 
-namespace {
+#include "pmp_handle.h"
 
-constexpr int kBlock = 128;
-constexpr int kSortPad = 8;  // cells of margin in the sort key around a box
+using pmp::BoxStore;
+using pmp::kBlock;
+using pmp::kSortPad;
 
-struct BoxStore {
-  long long n = 0;
-  double* d = nullptr;  // (3 + NR) * n doubles, sorted by cell
-  int* id = nullptr;
-  long long* perm = nullptr;  // sorted slot -> caller index
-};
-
-}  // namespace
-
-struct pmp_spray {
-  int device = 0;
-  int nfuel = 0;
-  int nspec = 0;
-  char species[PMP_MAX_SPEC][PMP_NAME_LEN];
-  pmp_mech mech;
-  pmp_spray_data data;
-  bool have_data = false;
-  pmp_spray_comps comps;
-  bool have_comps = false;
-  pmp_geometry geom;
-  bool have_geom = false;
-  std::vector<pmp_box> boxes;
-  int mode = PMP_MODE_FP64;
-  pmp::DevMech dmech;
-  pmp::DevFuel dfuel;
-  pmp::DevMechF dmechf;
-  pmp::DevFuelF dfuelf;
-  // per-box staged droplets (before packing)
-  std::vector<BoxStore> staged;
-  std::vector<bool> box_set;
-  // packed droplets
-  bool packed = false;
-  long long total = 0;
-  double* soa = nullptr;  // (3 + NR) arrays of length total
-  int* ids = nullptr;
-  long long* perm = nullptr;
-  std::vector<long long> box_begin;
-  int ncta = 0;
-  int* d_cta_box = nullptr;
-  long long* d_cta_start = nullptr;
-  long long* d_box_begin = nullptr;
-  long long* fb_list = nullptr;  // fallback slots (mixed / learned forms)
-  BoxEntry* d_boxes = nullptr;
-  BoxEntry* h_boxes = nullptr;
-  int boxes_cap = 0;
-  DevStatus* d_status = nullptr;
-  DevStatus* h_status = nullptr;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  pmp_error_info last_err;
-  pmp_stats stats;
-  // view pointers already checked to be device-accessible
-  std::vector<const double*> checked_state, checked_src;
-  // device mirrors of host views for pmp_spray_update_host
-  std::vector<double*> stage_state, stage_src;
-  std::vector<size_t> stage_state_n, stage_src_n;
-  int nr() const { return PMP_PSTATE_NUM(nfuel); }
-  int ncomp() const { return 3 + nr(); }
-};
-
-namespace {
-
-int set_err(pmp_spray* h, int code, const char* msg, int box = -1, long long particle = -1)
+int pmp::set_err(pmp_spray* h, int code, const char* msg, int box, long long particle)
 {
   if (h) {
     memset(&h->last_err, 0, sizeof(h->last_err));
@@ -106,6 +46,10 @@ int set_err(pmp_spray* h, int code, const char* msg, int box = -1, long long par
   }
   return code;
 }
+
+namespace {
+
+using pmp::set_err;
 
 #define PMP_CUDA(h, call)                                                   \
   do {                                                                      \
@@ -546,12 +490,11 @@ int dispatch_fp64_list(int ns, int nf, const KParams& P, long long total, cudaSt
   return PMP_ERR_UNSUPPORTED;
 }
 
-int do_update(
+int prepare_update_impl(
   pmp_spray* h, const pmp_box_view* state, const pmp_box_view* source, int nboxes,
-  double flow_dt, int state_ghosts, int source_ghosts, int is_virt, int is_ghost, int do_move,
-  double spray_cfl_lev, cudaStream_t st)
+  double flow_dt, int state_ghosts, int source_ghosts, int is_ghost, int do_move,
+  double spray_cfl_lev, cudaStream_t st, KParams& P)
 {
-  (void)is_virt;
   memset(&h->stats, 0, sizeof(h->stats));
   if (!h->have_data || !h->have_comps || !h->have_geom) {
     return set_err(h, PMP_ERR_INVALID, "setup, comps and geometry must be set before update");
@@ -559,8 +502,8 @@ int do_update(
   if (nboxes != (int)h->boxes.size()) {
     return set_err(h, PMP_ERR_INVALID, "nboxes differs from the grids given to set_grids");
   }
-  if (h->mode != PMP_MODE_FP64 && h->mode != PMP_MODE_MIXED) {
-    return set_err(h, PMP_ERR_UNSUPPORTED, "this method form is not available");
+  if (h->mode == PMP_MODE_LEARNED && !pmp::learn_ready(h)) {
+    return set_err(h, PMP_ERR_INVALID, "the learned form needs a trained surrogate (pmp_spray_learn_train)");
   }
   if (h->data.do_breakup != 0 || h->data.do_splash) {
     return set_err(h, PMP_ERR_UNSUPPORTED, "breakup and splash models are not supported");
@@ -634,7 +577,6 @@ int do_update(
   PMP_CUDA(h, cudaMemcpyAsync(h->d_boxes, h->h_boxes, sizeof(BoxEntry) * nboxes,
                               cudaMemcpyHostToDevice, st));
   PMP_CUDA(h, cudaMemsetAsync(h->d_status, 0, sizeof(DevStatus), st));
-  KParams P;
   memset(&P, 0, sizeof(P));
   P.m = h->dmech;
   P.f = h->dfuel;
@@ -685,9 +627,33 @@ int do_update(
   P.status = h->d_status;
   P.box_begin = h->d_box_begin;
   P.fb_list = h->fb_list;
+  return PMP_OK;
+}
+
+int do_update(
+  pmp_spray* h, const pmp_box_view* state, const pmp_box_view* source, int nboxes,
+  double flow_dt, int state_ghosts, int source_ghosts, int is_virt, int is_ghost, int do_move,
+  double spray_cfl_lev, cudaStream_t st)
+{
+  (void)is_virt;
+  KParams P;
+  int rc = prepare_update_impl(h, state, source, nboxes, flow_dt, state_ghosts, source_ghosts,
+                               is_ghost, do_move, spray_cfl_lev, st, P);
+  if (rc != PMP_OK) {
+    return rc;
+  }
+  const int NS = h->nspec;
+  const int NF = h->nfuel;
+  const long long T = h->total;
   PMP_CUDA(h, cudaEventRecord(h->ev0, st));
   if (h->ncta > 0) {
-    if (h->mode == PMP_MODE_MIXED) {
+    if (h->mode == PMP_MODE_LEARNED) {
+      rc = pmp::launch_learned(h, P, st);
+      if (rc == PMP_OK) {
+        PMP_CUDA(h, cudaGetLastError());
+        rc = dispatch_fp64_list(NS, NF, P, h->total, st);
+      }
+    } else if (h->mode == PMP_MODE_MIXED) {
       rc = pmp::launch_mixed(NS, NF, P, h->ncta, kBlock, st);
       if (rc == PMP_OK) {
         PMP_CUDA(h, cudaGetLastError());
@@ -737,6 +703,20 @@ int do_update(
 }
 
 }  // namespace
+
+int pmp::prepare_update(
+  pmp_spray* h, const pmp_box_view* state, const pmp_box_view* source, int nboxes,
+  double flow_dt, int state_ghosts, int source_ghosts, int is_ghost, int do_move,
+  double spray_cfl_lev, cudaStream_t st, KParams& P)
+{
+  return prepare_update_impl(h, state, source, nboxes, flow_dt, state_ghosts, source_ghosts,
+                             is_ghost, do_move, spray_cfl_lev, st, P);
+}
+
+int pmp::run_fp64_list(int ns, int nf, const KParams& P, long long total, cudaStream_t st)
+{
+  return ::dispatch_fp64_list(ns, nf, P, total, st);
+}
 
 // ===========================================================================
 // C ABI
@@ -804,6 +784,7 @@ int pmp_spray_destroy(pmp_spray* h)
     free_store(s);
   }
   free_packed(h);
+  pmp::learn_free(h);
   for (double* p : h->stage_state) {
     cudaFree(p);
   }

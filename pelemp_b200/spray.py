@@ -49,6 +49,19 @@ _SIGS = {
     "pmp_spray_last_error": [C.c_void_p, C.POINTER(capi.ErrorInfo)],
     "pmp_spray_get_stats": [C.c_void_p, C.POINTER(capi.Stats)],
     "pmp_spray_version": [],
+    "pmp_spray_learn_generate": [C.c_void_p, C.POINTER(capi.BoxView), C.c_int, C.c_double, C.c_int,
+                                 C.c_int, C.c_double, C.c_longlong, C.c_int, C.c_ulonglong,
+                                 C.c_void_p],
+    "pmp_spray_learn_count": [C.c_void_p, C.POINTER(C.c_longlong)],
+    "pmp_spray_learn_tuples": [C.c_void_p, C.c_void_p, C.POINTER(C.c_longlong)],
+    "pmp_spray_learn_train": [C.c_void_p, C.POINTER(capi.LearnConfig), C.POINTER(capi.LearnReport)],
+    "pmp_spray_learn_weights": [C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_longlong)],
+    "pmp_spray_learn_set_audit": [C.c_void_p, C.c_double],
+    "pmp_spray_learn_audit": [C.c_void_p, C.POINTER(C.c_longlong), C.POINTER(C.c_double)],
+    "pmp_learn_debug_grad": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p,
+                             C.POINTER(C.c_double)],
+    "pmp_learn_debug_infer": [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p],
+    "pmp_learn_param_count": [],
 }
 
 
@@ -269,6 +282,78 @@ class SprayParticleContainer:
         lib().pmp_spray_get_stats(self._h, C.byref(s))
         return s
 
+    # --- learned form (no counterpart in the reference) -------------------
+    def learn_generate(self, state, flow_dt, state_ghosts, do_move=True, spray_cfl_lev=-1.0,
+                       sample_stride=1, augment=0, seed=1, stream=0):
+        """Label droplets at this state with the FP64 teacher (tuples accumulate)."""
+        self._check(lib().pmp_spray_learn_generate(
+            self._h, state, len(state), flow_dt, state_ghosts, int(do_move), spray_cfl_lev,
+            int(sample_stride), int(augment), int(seed), C.c_void_p(stream)))
+
+    def learn_count(self):
+        n = C.c_longlong(0)
+        self._check(lib().pmp_spray_learn_count(self._h, C.byref(n)))
+        return n.value
+
+    def learn_tuples(self):
+        """(n, 16) float32: 10 raw inputs, 5 targets, pad."""
+        n = C.c_longlong(0)
+        self._check(lib().pmp_spray_learn_tuples(self._h, None, C.byref(n)))
+        buf = np.empty((n.value, 16), np.float32)
+        self._check(lib().pmp_spray_learn_tuples(self._h, buf.ctypes.data, C.byref(n)))
+        return buf[:n.value]
+
+    def learn_train(self, epochs=0, batch=0, lr=0.0, gate_margin=0.0, audit_fraction=0.0,
+                    no_quant=False, seed=0):
+        cfg = capi.LearnConfig(epochs, batch, lr, gate_margin, audit_fraction, int(no_quant), seed)
+        rep = capi.LearnReport()
+        self._check(lib().pmp_spray_learn_train(self._h, C.byref(cfg), C.byref(rep)))
+        return rep
+
+    def learn_weights(self):
+        """Flat float32 vector: parameters, then the normalisation and gate."""
+        n = C.c_longlong(0)
+        self._check(lib().pmp_spray_learn_weights(self._h, 1, None, C.byref(n)))
+        buf = np.empty(n.value, np.float32)
+        self._check(lib().pmp_spray_learn_weights(self._h, 1, buf.ctypes.data, C.byref(n)))
+        return buf
+
+    def set_learn_weights(self, buf):
+        buf = np.ascontiguousarray(buf, np.float32)
+        n = C.c_longlong(buf.size)
+        self._check(lib().pmp_spray_learn_weights(self._h, 0, buf.ctypes.data, C.byref(n)))
+
+    def learn_set_audit(self, fraction):
+        self._check(lib().pmp_spray_learn_set_audit(self._h, float(fraction)))
+
+    def learn_audit(self):
+        """(droplets audited, RMS error per surrogate output) of the last learned update."""
+        n = C.c_longlong(0)
+        e = (C.c_double * 5)()
+        self._check(lib().pmp_spray_learn_audit(self._h, C.byref(n), e))
+        return n.value, np.array(e[:])
+
+
+def learn_param_count():
+    return lib().pmp_learn_param_count()
+
+
+def learn_debug_grad(params, x, y, quant=True):
+    """Loss and gradient of the training kernels (see pmp_learn_debug_grad)."""
+    params = np.ascontiguousarray(params, np.float32)
+    x = np.ascontiguousarray(x, np.float32)
+    y = np.ascontiguousarray(y, np.float32)
+    n = x.shape[0]
+    assert params.size == learn_param_count() and x.shape == (n, capi.LEARN_IN)
+    assert y.shape == (n, capi.LEARN_OUT)
+    g = np.zeros_like(params)
+    loss = C.c_double(0.0)
+    rc = lib().pmp_learn_debug_grad(params.ctypes.data, x.ctypes.data, y.ctypes.data, n,
+                                    int(quant), g.ctypes.data, C.byref(loss))
+    if rc != capi.PMP_OK:
+        raise SprayError(rc)
+    return loss.value, g
+
 
 def from_problem(prob, device=0, mode=capi.PMP_MODE_FP64, set_droplets=True):
     """Container set up for a workloads.Problem (droplets copied from host)."""
@@ -282,3 +367,15 @@ def from_problem(prob, device=0, mode=capi.PMP_MODE_FP64, set_droplets=True):
         for b, p in enumerate(prob.parts):
             sp.set_particles(b, p["pos"], p["rdata"], p["id"])
     return sp
+
+
+def learn_debug_infer(params, xn):
+    """Outputs of the learned kernel's tensor-core network for normalised inputs."""
+    params = np.ascontiguousarray(params, np.float32)
+    xn = np.ascontiguousarray(xn, np.float32)
+    n = xn.shape[0]
+    y = np.zeros((n, capi.LEARN_OUT), np.float32)
+    rc = lib().pmp_learn_debug_infer(params.ctypes.data, xn.ctypes.data, n, y.ctypes.data)
+    if rc != capi.PMP_OK:
+        raise SprayError(rc)
+    return y

@@ -17,10 +17,14 @@ def device_sources(prob):
     return src, views(src, [prob.grown(b, prob.source_ghosts)[0] for b in range(len(prob.boxes))])
 
 
-def gpu_run(prob, steps, mode=capi.PMP_MODE_FP64, is_ghost=0, keep=None):
-    """steps x (MKD + MK) on the GPU; returns (parts per box, sources per call, container)."""
+def gpu_run(prob, steps, mode=capi.PMP_MODE_FP64, is_ghost=0, keep=None, setup=None):
+    """steps x (MKD + MK) on the GPU; returns (parts per box, sources per call, container).
+
+    setup(sp), if given, runs on the new container before the first update."""
     import torch
     sp = from_problem(prob, mode=mode)
+    if setup is not None:
+        setup(sp)
     st_keep, st_v = device_state(prob)  # keep the tensors alive while the views are used
     srcs = []
     for _step in range(steps):

@@ -1,0 +1,225 @@
+"""Learned form (PMP_MODE_LEARNED): the training kernels and the tensor-core
+inference against the CPU oracle (oracle/mlp_oracle.py), then the whole
+update against the FP64 oracle.
+
+* training gradient, FP32 network: loss within 1e-5, gradient within 1e-4
+  (relative 2-norm) of the FP64 oracle; bf16-rounded network: 1e-3 / 1e-2
+  (a rounding tie may resolve differently after FP32 accumulation);
+* inference (bf16 mma.sync): RMS within 1e-2 of the output scale;
+* update after several MKD+MK steps with a surrogate trained on another
+  sample of the same workload: droplet temperature, diameter and mass within
+  1e-4 relative of the FP64 oracle in RMS over the droplets (99.9% of the
+  droplets within 1e-3; the rest are droplets whose sub-step count, an
+  integer the reference derives from the rates, lands one off), total liquid
+  mass within 1e-6, liquid + gas mass balance closed to FP64 round-off,
+  deposits within 5e-2 of the component's largest deposit;
+* droplets outside the training range go to the FP64 kernel: bit-identical
+  to the oracle;
+* the learned update is faster than the plain FP64 update.
+"""
+import numpy as np
+import pytest
+
+from oracle import mlp_oracle as M
+from pelemp_b200 import capi
+from pelemp_b200 import workloads as W
+from pelemp_b200.spray import from_problem, learn_debug_grad, learn_debug_infer
+from tests.gpu_util import device_sources, device_state, gpu_run, oracle_run
+from tests.parity import droplet_mass
+
+pytestmark = pytest.mark.gpu
+
+SMALL = dict(steps=4, ncells=(32, 32, 32), box=(16, 16, 16))
+
+
+def test_training_gradient_fp32_matches_oracle():
+    rng = np.random.default_rng(0)
+    p = M.random_params(11)
+    x = rng.standard_normal((777, M.N_IN)).astype(np.float32)
+    y = rng.standard_normal((777, M.N_OUT)).astype(np.float32)
+    lg, gg = learn_debug_grad(p, x, y, quant=False)
+    lo, go = M.loss_and_grad(p.astype(np.float64), x.astype(np.float64), y.astype(np.float64))
+    print("fp32 loss", lg, lo)
+    assert abs(lg - lo) <= 1e-5 * lo
+    assert np.linalg.norm(gg - go) <= 1e-4 * np.linalg.norm(go)
+    for name, (o, s) in M.OFF.items():
+        a, b = gg[o:o + s], go[o:o + s]
+        nb = np.linalg.norm(b)
+        if nb > 0:
+            assert np.linalg.norm(a - b) <= 1e-3 * nb, name
+
+
+def test_training_gradient_bf16_matches_oracle():
+    rng = np.random.default_rng(1)
+    p = M.random_params(12)
+    x = rng.standard_normal((500, M.N_IN)).astype(np.float32)
+    y = rng.standard_normal((500, M.N_OUT)).astype(np.float32)
+    lg, gg = learn_debug_grad(p, x, y, quant=True)
+    lo, go = M.loss_and_grad(p, x.astype(np.float64), y.astype(np.float64), quant=True)
+    print("bf16 loss", lg, lo, "grad rel", np.linalg.norm(gg - go) / np.linalg.norm(go))
+    assert abs(lg - lo) <= 1e-3 * lo
+    assert np.linalg.norm(gg - go) <= 1e-2 * np.linalg.norm(go)
+
+
+def test_inference_matches_oracle():
+    rng = np.random.default_rng(2)
+    p = M.random_params(13)
+    x = rng.standard_normal((1000, M.N_IN)).astype(np.float32)  # not a whole number of warps
+    yg = learn_debug_infer(p, x)
+    yo = M.infer(p, x.astype(np.float64))
+    scale = np.sqrt(np.mean(yo ** 2))
+    rms = np.sqrt(np.mean((yg - yo) ** 2))
+    print("inference rms / scale", rms / scale, "max", np.max(np.abs(yg - yo)) / scale)
+    assert rms <= 1e-2 * scale
+    assert np.max(np.abs(yg - yo)) <= 6e-2 * scale
+
+
+def _advance(sp, prob, st_v, stream):
+    for do_move in (1, 0):
+        _src, src_v = device_sources(prob)
+        sp.update_particles(st_v, src_v, prob.flow_dt, 0.0, prob.state_ghosts, prob.source_ghosts,
+                            0, 0, do_move, prob.spray_cfl_lev, stream)
+
+
+@pytest.fixture(scope="module")
+def trained():
+    """Surrogate trained on a different sample (seed 1) of the small config-2 workload."""
+    import torch
+    prob = W.config2(n=40_000, seed=1, **SMALL)
+    sp = from_problem(prob)
+    st_keep, st_v = device_state(prob)
+    stream = torch.cuda.current_stream().cuda_stream
+    for step in range(prob.steps):
+        sp.learn_generate(st_v, prob.flow_dt, prob.state_ghosts, True, prob.spray_cfl_lev,
+                          sample_stride=1, augment=3, seed=step + 1, stream=stream)
+        _advance(sp, prob, st_v, stream)
+    rep = sp.learn_train(epochs=60, batch=2048, audit_fraction=0.05)
+    print("training: tuples", rep.tuples, "steps", rep.steps, "loss", rep.loss_first, "->",
+          rep.loss_last, "val", list(rep.val_rel_rms), "ms", rep.train_ms)
+    w = sp.learn_weights()
+    del st_keep
+    sp.close()
+    return w, rep
+
+
+def test_training_converges(trained):
+    _, rep = trained
+    assert rep.loss_last < 1e-3 * rep.loss_first
+    assert max(rep.val_rel_rms) < 5e-3
+
+
+def rel_errors(pg, po, nfuel, rho_l):
+    """Per-droplet relative errors of T, diameter, mass and velocity (alive in both)."""
+    out = {"T": [], "dia": [], "mass": [], "vel": []}
+    for a, b in zip(pg, po):
+        al = (a["id"] > 0) & (b["id"] > 0)
+        ra, rb = a["rdata"][:, al], b["rdata"][:, al]
+        out["T"].append(np.abs(ra[capi.PSTATE_T] / rb[capi.PSTATE_T] - 1))
+        out["dia"].append(np.abs(ra[capi.PSTATE_DIA] / rb[capi.PSTATE_DIA] - 1))
+
+        def mass(r):
+            inv = np.sum(r[capi.PSTATE_Y:capi.PSTATE_Y + nfuel] / np.asarray(rho_l)[:, None], axis=0)
+            return r[capi.PSTATE_DIA] ** 3 / inv
+        out["mass"].append(np.abs(mass(ra) / mass(rb) - 1))
+        sp = np.maximum(np.sqrt(np.sum(rb[0:3] ** 2, axis=0)), 1.0)
+        out["vel"].append(np.sqrt(np.sum((ra[0:3] - rb[0:3]) ** 2, axis=0)) / sp)
+    return {k: np.concatenate(v) for k, v in out.items()}
+
+
+def test_learned_vs_fp64_oracle(trained, oracle):
+    w, _ = trained
+    prob = W.config2(n=40_000, seed=0, **SMALL)
+
+    def setup(sp):
+        sp.set_learn_weights(w)
+        sp.learn_set_audit(0.05)
+
+    pg, sg, sp = gpu_run(prob, prob.steps, mode=capi.PMP_MODE_LEARNED, setup=setup)
+    st = sp.stats()
+    audited, rms = sp.learn_audit()
+    print("learned: substeps", st.substeps, "fallback", st.fallback, "audited", audited, "rms", rms)
+    assert audited > 0 and max(rms) < 1e-2
+    assert st.fallback < 0.05 * st.substeps
+    po, so = oracle_run(oracle, prob, prob.steps)
+    ids_g = np.concatenate([p["id"] for p in pg])
+    ids_o = np.concatenate([p["id"] for p in po])
+    assert np.mean(ids_g == ids_o) > 0.999
+    rho_l = [W.LIQUIDS[f]["rho"] for f in prob.fuels]
+    e = rel_errors(pg, po, prob.nfuel, rho_l)
+    for k, v in e.items():
+        print("learned vs FP64 %-4s rms %.3g p99.9 %.3g max %.3g" % (
+            k, np.sqrt(np.mean(v ** 2)), np.quantile(v, 0.999), v.max()))
+    for k in ("T", "dia", "mass"):
+        assert np.sqrt(np.mean(e[k] ** 2)) <= 1e-4, k
+        assert np.quantile(e[k], 0.999) <= 1e-3, k
+    assert np.sqrt(np.mean(e["vel"] ** 2)) <= 1e-3
+    m_g = sum(float(np.sum(m)) for m in droplet_mass(prob, pg, rho_l))
+    m_o = sum(float(np.sum(m)) for m in droplet_mass(prob, po, rho_l))
+    print("total liquid mass rel error", m_g / m_o - 1)
+    assert abs(m_g / m_o - 1) <= 1e-6
+    worst = 0.0
+    for a, b in zip(sg, so):
+        for x, y in zip(a, b):
+            for c in range(x.shape[0]):
+                scale = np.max(np.abs(y[c]))
+                if scale > 0:
+                    worst = max(worst, float(np.max(np.abs(x[c] - y[c])) / scale))
+    print("learned vs FP64 deposit error:", worst)
+    assert worst <= 5e-2
+
+
+def test_learned_mass_balance_closes(trained):
+    w, _ = trained
+    prob = W.config2(n=40_000, seed=0, **dict(SMALL, steps=1))
+    rho_l = [W.LIQUIDS[f]["rho"] for f in prob.fuels]
+    m0 = droplet_mass(prob, prob.parts, rho_l)
+    pg, sg, _ = gpu_run(prob, 1, mode=capi.PMP_MODE_LEARNED, setup=lambda sp: sp.set_learn_weights(w))
+    m1 = droplet_mass(prob, pg, rho_l)
+    vol = float(np.prod(prob.dx))
+    gas = sum(float(np.sum(s[3])) for call in sg for s in call) * vol * 0.5 * prob.flow_dt
+    liq = sum(float(np.sum(b - a)) for a, b in zip(m0, m1))
+    scale = sum(float(np.sum(np.abs(b - a))) for a, b in zip(m0, m1))
+    assert abs(gas + liq) <= 1e-9 * scale
+
+
+def test_gate_sends_out_of_range_droplets_to_fp64(trained, oracle):
+    w, _ = trained
+    prob = W.config2(n=20_000, seed=0, **dict(SMALL, steps=1))
+    planted = []
+    for b, p in enumerate(prob.parts):
+        idx = np.arange(0, p["id"].shape[0], 7)
+        p["rdata"][capi.PSTATE_T, idx] = 240.0  # below every training temperature
+        planted.append(idx)
+    pg, _, sp = gpu_run(prob, 1, mode=capi.PMP_MODE_LEARNED, setup=lambda s: s.set_learn_weights(w))
+    assert sp.stats().fallback >= sum(i.size for i in planted)
+    po, _ = oracle_run(oracle, prob, 1)
+    for b, idx in enumerate(planted):
+        for k in ("pos", "rdata", "id"):
+            assert np.array_equal(pg[b][k][..., idx], po[b][k][..., idx]), (b, k)
+
+
+def test_learned_faster_than_fp64(trained):
+    import torch
+    w, _ = trained
+    prob = W.config2(n=2_000_000, seed=2, steps=1, ncells=(64, 64, 64), box=(32, 32, 32))
+    times = {}
+    for mode in (capi.PMP_MODE_FP64, capi.PMP_MODE_LEARNED):
+        sp = from_problem(prob, mode=mode)
+        if mode == capi.PMP_MODE_LEARNED:
+            sp.set_learn_weights(w)
+        st_keep, st_v = device_state(prob)
+        stream = torch.cuda.current_stream().cuda_stream
+        ms = []
+        for _ in range(3):
+            _src, src_v = device_sources(prob)
+            sp.update_particles(st_v, src_v, prob.flow_dt, 0.0, prob.state_ghosts, prob.source_ghosts,
+                                0, 0, 0, prob.spray_cfl_lev, stream)
+            ms.append(sp.stats().kernel_ms)
+        times[mode] = min(ms)
+        if mode == capi.PMP_MODE_LEARNED:
+            print("learned fallback", sp.stats().fallback, "of", sp.stats().substeps)
+        del st_keep
+        sp.close()
+    print("MK of 2M droplets: FP64 %.3f ms, learned %.3f ms, speed-up %.2f" % (
+        times[0], times[2], times[0] / times[2]))
+    assert times[2] < times[0]
