@@ -12,9 +12,11 @@ Flat parameter layout (float32, shared with the library):
   W4[8][64]  (outputs 5..7 are padding)    b4[8]
 Row = output unit.  Loss = mean over rows and the 5 outputs of (y_pred - y)^2.
 
-With quant=True the forward pass rounds weights (not biases) and hidden
-activations to bf16 (round to nearest even), and the gradient passes through
-the rounding unchanged (straight-through), as the training kernels do.
+With quant=True the forward pass rounds weights (not biases) to bf16 (round
+to nearest even) and computes each hidden activation as the inference kernel
+does, silu(x) = fma(h, tanh h, h) with h = bf16(x/2), tanh h rounded to bf16
+and the fma rounded once to bf16; the gradient passes through the roundings
+unchanged (straight-through), as the training kernels do.
 """
 import numpy as np
 
@@ -57,6 +59,12 @@ def silu(h):
     return h / (1.0 + np.exp(-h))
 
 
+def silu_bf16(x):
+    """silu(x) with the inference kernel's bf16 roundings."""
+    h = bf16_round(0.5 * np.asarray(x, np.float64))
+    return bf16_round(h * bf16_round(np.tanh(h)) + h)
+
+
 def dsilu(h):
     s = 1.0 / (1.0 + np.exp(-h))
     return s * (1.0 + h * (1.0 - s))
@@ -82,14 +90,15 @@ def forward(p, x, quant=False):
     """x: (n, 10) normalised inputs -> (n, 5) outputs and the saved activations."""
     w = unpack(np.asarray(p, np.float64))
     q = (lambda a: bf16_round(a)) if quant else (lambda a: a)
+    act = silu_bf16 if quant else silu
     X = np.zeros((x.shape[0], 16))
     X[:, :N_IN] = x
     H1 = X @ q(w["W1"]).T + w["b1"]
-    A1 = q(silu(H1))
+    A1 = act(H1)
     H2 = A1 @ q(w["W2"]).T + w["b2"]
-    A2 = q(silu(H2))
+    A2 = act(H2)
     H3 = A2 @ q(w["W3"]).T + w["b3"]
-    A3 = q(silu(H3))
+    A3 = act(H3)
     Y = A3 @ q(w["W4"]).T + w["b4"]
     return Y[:, :N_OUT], (X, H1, A1, H2, A2, H3, A3, Y)
 
@@ -121,16 +130,16 @@ def loss_and_grad(p, x, y, quant=False):
 
 def infer(p, xn):
     """The inference the learned kernel runs, in FP64 apart from its roundings:
-    inputs split into bf16 hi + lo, bf16 weights and activations, FP32-range
-    accumulation (emulated in FP64)."""
+    inputs split into bf16 hi + lo, bf16 weights, the bf16 SiLU of silu_bf16,
+    accumulation emulated in FP64."""
     w = unpack(np.asarray(p, np.float64))
     hi = bf16_round(xn)
     lo = bf16_round(np.asarray(xn, np.float64) - hi)
     x = hi + lo
     X = np.zeros((x.shape[0], 16))
     X[:, :N_IN] = x
-    A = bf16_round(silu(X @ bf16_round(w["W1"]).T + w["b1"]))
-    A = bf16_round(silu(A @ bf16_round(w["W2"]).T + w["b2"]))
-    A = bf16_round(silu(A @ bf16_round(w["W3"]).T + w["b3"]))
+    A = silu_bf16(X @ bf16_round(w["W1"]).T + w["b1"])
+    A = silu_bf16(A @ bf16_round(w["W2"]).T + w["b2"])
+    A = silu_bf16(A @ bf16_round(w["W3"]).T + w["b3"])
     Y = A @ bf16_round(w["W4"]).T + w["b4"]
     return Y[:, :N_OUT]

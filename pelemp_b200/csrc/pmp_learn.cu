@@ -407,7 +407,15 @@ __global__ void __launch_bounds__(256) k_gemm(
 
 __device__ __forceinline__ float silu_exact(float x) { return x / (1.f + expf(-x)); }
 
-// H += bias; A = silu(H), rounded to bf16 when quant
+// silu(x) as the inference kernel rounds it (mlp_mma.cuh): h = bf16(x/2),
+// bf16(fma(h, bf16(tanh h), h))
+__device__ __forceinline__ float silu_bf16(float x)
+{
+  const float h = bf16r(0.5f * x);
+  return bf16r(fmaf(h, bf16r(tanhf(h)), h));
+}
+
+// H += bias; A = silu(H), with the inference's bf16 roundings when quant
 __global__ void k_bias_act(float* H, float* A, const float* bias, int B, int N, int act, int quant)
 {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -418,8 +426,7 @@ __global__ void k_bias_act(float* H, float* A, const float* bias, int B, int N, 
   const float h = H[i] + bias[n];
   H[i] = h;
   if (act) {
-    const float a = silu_exact(h);
-    A[i] = quant ? bf16r(a) : a;
+    A[i] = quant ? silu_bf16(h) : silu_exact(h);
   }
 }
 
@@ -639,18 +646,19 @@ static void build_mlp(const std::vector<float>& p, MlpSmem& S)
   for (int i = 0; i < 8 * kWStride; ++i) {
     S.w4[i] = z;
   }
+  // hidden layers halved (exact): the kernel's SiLU takes h = x/2
   for (int o = 0; o < 64; ++o) {
     for (int k = 0; k < kLearnIn; ++k) {
-      S.w1[o * kW1Stride + k] = host_bf16(p[kP_W1 + o * 16 + k]);
-      S.w1[o * kW1Stride + 16 + k] = host_bf16(p[kP_W1 + o * 16 + k]);
+      S.w1[o * kW1Stride + k] = host_bf16(0.5f * p[kP_W1 + o * 16 + k]);
+      S.w1[o * kW1Stride + 16 + k] = host_bf16(0.5f * p[kP_W1 + o * 16 + k]);
     }
     for (int k = 0; k < 64; ++k) {
-      S.w2[o * kWStride + k] = host_bf16(p[kP_W2 + o * 64 + k]);
-      S.w3[o * kWStride + k] = host_bf16(p[kP_W3 + o * 64 + k]);
+      S.w2[o * kWStride + k] = host_bf16(0.5f * p[kP_W2 + o * 64 + k]);
+      S.w3[o * kWStride + k] = host_bf16(0.5f * p[kP_W3 + o * 64 + k]);
     }
-    S.b1[o] = p[kP_B1 + o];
-    S.b2[o] = p[kP_B2 + o];
-    S.b3[o] = p[kP_B3 + o];
+    S.b1[o] = 0.5f * p[kP_B1 + o];
+    S.b2[o] = 0.5f * p[kP_B2 + o];
+    S.b3[o] = 0.5f * p[kP_B3 + o];
   }
   for (int o = 0; o < 8; ++o) {
     for (int k = 0; k < 64; ++k) {
@@ -663,8 +671,12 @@ static void build_mlp(const std::vector<float>& p, MlpSmem& S)
 // ---------------------------------------------------------------------------
 // the learned update kernel
 
+#ifndef PMP_LEARNED_MIN_BLOCKS
+#define PMP_LEARNED_MIN_BLOCKS 4
+#endif
+
 template <int NS, int NF, int BLOCK>
-__global__ void __launch_bounds__(BLOCK, 4)
+__global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
   spray_update_learned(const __grid_constant__ KParams P, const __grid_constant__ LearnParams L)
 {
   __shared__ MlpSmem S;
@@ -715,9 +727,6 @@ __global__ void __launch_bounds__(BLOCK, 4)
     num_ppp = P.parts.rd[PMP_PSTATE_NUMDENS(NF)][s];
     film = P.parts.rd[PMP_PSTATE_FILMHGHT(NF)][s];
   }
-  double lx[3];
-  int ijk[3], ijkc[3];
-  cell_of(P, pos, lx, ijk, ijkc);
   int bflags[3] = {0, 0, 0};
   bool ok = true;
   if (valid && B.at_bounds) {
@@ -728,6 +737,11 @@ __global__ void __launch_bounds__(BLOCK, 4)
   }
   const unsigned FULL = 0xffffffffu;
   for (int cur_iter = 0; cur_iter < P.num_iter; ++cur_iter) {
+    // cell of the droplet (recomputed from the position each sub-cycle, so
+    // the stencil indices are not live across the network evaluation)
+    double lx[3];
+    int ijk[3], ijkc[3];
+    cell_of(P, pos, lx, ijk, ijkc);
     bool active = valid && ok && id > 0;
     if (active && film > 0.) {
       set_error(P, PMP_ERR_UNSUPPORTED, b, s);
@@ -853,6 +867,7 @@ __global__ void __launch_bounds__(BLOCK, 4)
       float xn[kLearnIn];
       float L_fuel[NF], X_vapor[NF], Yfv[NF];
       float sumXVap, B_M;
+      bool in_range = true;
       vapor_state_f<NS, NF>(m, ff, fdat, g, cBoilT, (float)T_part, Y_part, L_fuel, X_vapor, Yfv, sumXVap, B_M);
       {
         double slip = 0.;
@@ -875,6 +890,7 @@ __global__ void __launch_bounds__(BLOCK, 4)
 #pragma unroll
         for (int k = 0; k < kLearnIn; ++k) {
           xn[k] = pending ? (xin[k] - L.norm.x_mean[k]) * L.norm.x_inv_std[k] : 0.f;
+          in_range = in_range && xin[k] >= L.norm.x_lo[k] && xin[k] <= L.norm.x_hi[k];
         }
       }
       float yo[kLearnOut];
@@ -888,11 +904,7 @@ __global__ void __launch_bounds__(BLOCK, 4)
         if (cur_iter == 0 && isub == 1) {
           // gate: some fuel evaporates, inputs inside the (widened)
           // training range, outputs finite
-          bool in = sumXVap > 0.f;
-#pragma unroll
-          for (int k = 0; k < kLearnIn; ++k) {
-            in = in && xin[k] >= L.norm.x_lo[k] && xin[k] <= L.norm.x_hi[k];
-          }
+          bool in = sumXVap > 0.f && in_range;
 #pragma unroll
           for (int k = 0; k < kLearnOut; ++k) {
             in = in && isfinite(yv[k]);
@@ -1140,6 +1152,13 @@ __global__ void __launch_bounds__(BLOCK, 4)
   flush_counters(P, c);
 }
 
+// silu from the halved pre-activation h2 = x/2, rounded as the kernel does
+__device__ __forceinline__ float silu_half_bf16(float h2)
+{
+  const float h = bf16r(h2);
+  return bf16r(fmaf(h, bf16r(tanhf(h)), h));
+}
+
 // SIMT FP32 forward with the inference weights (audit)
 __device__ void mlp_simt(const MlpSmem& S, const float* xn, float* y)
 {
@@ -1151,21 +1170,21 @@ __device__ void mlp_simt(const MlpSmem& S, const float* xn, float* y)
       const float lo = bf16r(xn[k] - hi);
       a = fmaf(__bfloat162float(S.w1[o * kW1Stride + k]), hi + lo, a);
     }
-    h[o] = bf16r(silu_exact(a));
+    h[o] = silu_half_bf16(a);
   }
   for (int o = 0; o < 64; ++o) {
     float a = S.b2[o];
     for (int k = 0; k < 64; ++k) {
       a = fmaf(__bfloat162float(S.w2[o * kWStride + k]), h[k], a);
     }
-    h2[o] = bf16r(silu_exact(a));
+    h2[o] = silu_half_bf16(a);
   }
   for (int o = 0; o < 64; ++o) {
     float a = S.b3[o];
     for (int k = 0; k < 64; ++k) {
       a = fmaf(__bfloat162float(S.w3[o * kWStride + k]), h2[k], a);
     }
-    h[o] = bf16r(silu_exact(a));
+    h[o] = silu_half_bf16(a);
   }
   for (int o = 0; o < kLearnOut; ++o) {
     float a = S.b4[o];
