@@ -208,6 +208,8 @@ typedef struct pmp_stats {
   long long fallback;        /* mixed / learned forms: droplets handed to the
                                 plain FP64 kernel (small, out of range) */
   double kernel_ms;          /* device time of the update kernels */
+  int graph;                 /* 1: the update replayed a captured CUDA graph,
+                                2: it captured a new one, 0: direct launches */
 } pmp_stats;
 
 typedef struct pmp_spray pmp_spray;
@@ -306,6 +308,59 @@ int pmp_spray_update_static(
   double time, int state_ghosts, int source_ghosts, int is_virt,
   int is_ghost, int do_move, double spray_cfl_lev, void* stream,
   pmp_error_info* err);
+
+/* ---------------------------------------------------------------------------
+ * Launch shape of the FP64 form (the batched form).  No counterpart in the
+ * reference, which launches one kernel per box and synchronises after each
+ * (SprayParticles.cpp:244-248,499).  Here all boxes go in one launch; the
+ * shape only changes speed: droplet results are bit-identical for every
+ * shape (deposits differ by the order of the atomic additions).
+ *  - PMP_LAUNCH_GRID: one CTA per `block` droplet slots of a box;
+ *  - PMP_LAUNCH_PERSISTENT: resident CTAs only (ctas_per_sm per SM, 0 = the
+ *    occupancy limit) taking chunks of `chunk` slots from a device counter;
+ *  - PMP_LAUNCH_PER_BOX: the reference's pattern, one launch per box with a
+ *    stream synchronisation after each (the baseline of the batched form).
+ * block is 64, 128 or 256 threads; regs the register cap, 96 (64 or 128
+ * threads) or 128 (128 or 256 threads).  use_graph = 1 captures the device
+ * work of an update (box table upload, status reset, kernels, status
+ * read-back) in a CUDA graph on an internal stream and replays it while the
+ * call's arguments repeat (PMP_MODE_FP64 and PMP_MODE_MIXED, not with
+ * PMP_LAUNCH_PER_BOX).  The default is GRID, 128 threads, 96 registers, no
+ * graph.  PMP_MODE_MIXED and PMP_MODE_LEARNED use their own launch. */
+enum { PMP_LAUNCH_GRID = 0, PMP_LAUNCH_PERSISTENT = 1, PMP_LAUNCH_PER_BOX = 2 };
+typedef struct pmp_launch_config {
+  int kind;
+  int block;
+  int regs;
+  int chunk;
+  int ctas_per_sm;
+  int use_graph;
+} pmp_launch_config;
+
+typedef struct pmp_tune_report {
+  int cached;                /* 1: taken from the cache file, nothing timed */
+  int ncandidates;           /* launch shapes timed */
+  double best_ms;            /* device time of one update with the chosen shape */
+  double default_ms;         /* with the default shape */
+  double per_box_ms;         /* one launch per box, synchronised after each */
+  pmp_launch_config best;    /* the chosen shape (use_graph as it was set) */
+} pmp_tune_report;
+
+int pmp_spray_set_launch(pmp_spray* h, const pmp_launch_config* cfg);
+int pmp_spray_get_launch(const pmp_spray* h, pmp_launch_config* cfg);
+/* The autotuner: times the FP64 update with each candidate launch shape on
+ * the given views (arguments as pmp_spray_update), keeps the fastest in the
+ * handle and, when cache_path is not NULL, records it in that text file
+ * under a key of device name, species and fuel counts, droplet count (to a
+ * power of two), box count, do_move and sub-cycle count; a later call with
+ * the same key reads it back without timing.  Droplets are restored after
+ * every trial and deposits go to scratch arrays: the handle's droplets and
+ * the caller's source are left as they were. */
+int pmp_spray_autotune(
+  pmp_spray* h, const pmp_box_view* state, const pmp_box_view* source,
+  int nboxes, double flow_dt, int state_ghosts, int source_ghosts,
+  int is_ghost, int do_move, double spray_cfl_lev, const char* cache_path,
+  pmp_tune_report* report, void* stream);
 
 /* ---------------------------------------------------------------------------
  * Learned form (PMP_MODE_LEARNED).  No counterpart in the reference.  A

@@ -20,9 +20,12 @@ LIB = os.path.join(PKG, "libpmpspray.so")
 # contraction (their multiply-adds are explicit fma() calls); the mixed and
 # learned forms allow it.
 SOURCES = [("pmp_spray.cu", "-fmad=false"), ("pmp_static.cu", "-fmad=false"),
-           ("pmp_mixed.cu", "-fmad=true"), ("pmp_learn.cu", "-fmad=true")]
+           ("pmp_mixed.cu", "-fmad=true"), ("pmp_learn.cu", "-fmad=true"),
+           ("pmp_batch.cu", "-fmad=false"), ("batch/pmp_batch_b64.cu", "-fmad=false"),
+           ("batch/pmp_batch_b128.cu", "-fmad=false"), ("batch/pmp_batch_b256.cu", "-fmad=false")]
 HEADERS = ["pmp_device.cuh", "pmp_handle.h", "spray_fp64.cuh", "spray_mixed.cuh",
            "spray_kernels.cuh", "learn/learn_common.cuh", "learn/mlp_mma.cuh",
+           "batch/batch_kernels.cuh",
            "phys/pmp_math.h", "phys/pmp_math_tables.h", "phys/pmp_thermo.h",
            "phys/pmp_thermo_data.h"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
@@ -47,7 +50,7 @@ def build_lib(force=False, ptxas_verbose=False, extra=()):
     procs = []
     objs = []
     for src, fmad in SOURCES:
-        obj = os.path.join(OBJDIR, src.replace(".cu", ".o"))
+        obj = os.path.join(OBJDIR, src.replace("/", "_").replace(".cu", ".o"))
         cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", fmad, "-Xcompiler", "-fPIC",
                "--expt-relaxed-constexpr", "-I", os.path.join(ROOT, "include"), "-I", CSRC,
                *extra, "-c", "-o", obj, os.path.join(CSRC, src)]

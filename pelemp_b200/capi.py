@@ -148,7 +148,23 @@ class Stats(C.Structure):
     _fields_ = [
         ("substeps", C.c_longlong), ("killed", C.c_longlong),
         ("inner_steps", C.c_longlong), ("fallback", C.c_longlong),
-        ("kernel_ms", C.c_double),
+        ("kernel_ms", C.c_double), ("graph", C.c_int),
+    ]
+
+
+PMP_LAUNCH_GRID = 0
+PMP_LAUNCH_PERSISTENT = 1
+PMP_LAUNCH_PER_BOX = 2
+
+
+class LaunchConfig(C.Structure):
+    _fields_ = [(n, C.c_int) for n in ("kind", "block", "regs", "chunk", "ctas_per_sm", "use_graph")]
+
+
+class TuneReport(C.Structure):
+    _fields_ = [
+        ("cached", C.c_int), ("ncandidates", C.c_int), ("best_ms", C.c_double),
+        ("default_ms", C.c_double), ("per_box_ms", C.c_double), ("best", LaunchConfig),
     ]
 
 

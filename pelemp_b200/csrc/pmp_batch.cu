@@ -1,0 +1,532 @@
+// pmp_batch.cu -- the batched form: launch shapes of the FP64 update over many
+// boxes with uneven droplet counts, CUDA-graph capture and replay of an
+// update's device work, and the autotuner that picks the launch shape.
+//
+// The reference runs updateParticles box by box: one kernel per box and a
+// stream synchronisation after each (SprayParticles.cpp:244-248,499), which
+// leaves the GPU idle between boxes and under-filled on small boxes.  Here
+// every box is in one launch (the work map below); PMP_LAUNCH_PER_BOX keeps
+// the reference's pattern as the baseline the batched form is measured
+// against.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "batch/batch_kernels.cuh"
+#include "pmp_handle.h"
+
+namespace pmp {
+
+namespace {
+
+int check(pmp_spray* h, cudaError_t e, const char* what)
+{
+  if (e != cudaSuccess) {
+    char b[160];
+    snprintf(b, sizeof(b), "%s: %s", what, cudaGetErrorString(e));
+    return set_err(h, PMP_ERR_CUDA, b);
+  }
+  return PMP_OK;
+}
+
+#define PMP_TRY(h, call)                        \
+  do {                                          \
+    const int rc_ = check((h), (call), #call);  \
+    if (rc_ != PMP_OK) {                        \
+      return rc_;                               \
+    }                                           \
+  } while (0)
+
+void free_map(WorkMap& m)
+{
+  cudaFree(m.box);
+  cudaFree(m.start);
+  m = WorkMap{};
+}
+
+// work items of `chunk` slots over the packed boxes (built once per chunk size)
+int get_map(pmp_spray* h, int chunk, const WorkMap** out)
+{
+  for (const WorkMap& m : h->batch.maps) {
+    if (m.chunk == chunk) {
+      *out = &m;
+      return PMP_OK;
+    }
+  }
+  const int nb = (int)h->boxes.size();
+  WorkMap m;
+  m.chunk = chunk;
+  std::vector<int> box;
+  std::vector<long long> start;
+  m.item_begin.assign(nb + 1, 0);
+  for (int b = 0; b < nb; ++b) {
+    m.item_begin[b] = (int)box.size();
+    for (long long o = h->box_begin[b]; o < h->box_begin[b + 1]; o += chunk) {
+      box.push_back(b);
+      start.push_back(o);
+    }
+  }
+  m.item_begin[nb] = (int)box.size();
+  m.nitems = (int)box.size();
+  if (m.nitems > 0) {
+    PMP_TRY(h, cudaMalloc(&m.box, sizeof(int) * m.nitems));
+    PMP_TRY(h, cudaMalloc(&m.start, sizeof(long long) * m.nitems));
+    PMP_TRY(h, cudaMemcpy(m.box, box.data(), sizeof(int) * m.nitems, cudaMemcpyHostToDevice));
+    PMP_TRY(h, cudaMemcpy(m.start, start.data(), sizeof(long long) * m.nitems, cudaMemcpyHostToDevice));
+  }
+  h->batch.maps.push_back(m);
+  *out = &h->batch.maps.back();
+  return PMP_OK;
+}
+
+bool launch_variant(int ns, int nf, int block, int regs, bool persistent, const KParams& P, const WorkArgs& W,
+                    int grid, cudaStream_t st)
+{
+  switch (block) {
+    case 64:
+      return batch_launch_b64(ns, nf, regs, persistent, P, W, grid, st);
+    case 128:
+      return batch_launch_b128(ns, nf, regs, persistent, P, W, grid, st);
+    case 256:
+      return batch_launch_b256(ns, nf, regs, persistent, P, W, grid, st);
+    default:
+      return false;
+  }
+}
+
+int occupancy_variant(int ns, int nf, int block, int regs, bool persistent)
+{
+  switch (block) {
+    case 64:
+      return batch_occupancy_b64(ns, nf, regs, persistent);
+    case 128:
+      return batch_occupancy_b128(ns, nf, regs, persistent);
+    case 256:
+      return batch_occupancy_b256(ns, nf, regs, persistent);
+    default:
+      return 0;
+  }
+}
+
+bool valid_shape(const pmp_launch_config& c)
+{
+  const bool shape = (c.block == 64 && c.regs == 96) || (c.block == 128 && (c.regs == 96 || c.regs == 128)) ||
+                     (c.block == 256 && c.regs == 128);
+  if (!shape || c.kind < PMP_LAUNCH_GRID || c.kind > PMP_LAUNCH_PER_BOX) {
+    return false;
+  }
+  if (c.kind == PMP_LAUNCH_PERSISTENT && (c.chunk < c.block || c.chunk % c.block != 0 || c.ctas_per_sm < 0)) {
+    return false;
+  }
+  return true;
+}
+
+constexpr size_t kMaxGraphs = 4;
+
+void destroy_graphs(pmp_spray* h)
+{
+  for (BatchState::Graph& g : h->batch.graphs) {
+    cudaGraphExecDestroy(g.exec);
+  }
+  h->batch.graphs.clear();
+}
+
+// Everything a launch of the current shape needs that is not a stream
+// operation (work map, counter, resident CTA count), done before any graph
+// capture so that the capture holds stream work only.
+int batch_prepare(pmp_spray* h, const WorkMap** map)
+{
+  BatchState& B = h->batch;
+  const pmp_launch_config& c = B.cfg;
+  *map = nullptr;
+  if (c.kind == PMP_LAUNCH_GRID && c.block == 128 && c.regs == 96) {
+    return PMP_OK;  // the default launch uses the handle's own CTA map
+  }
+  const int chunk = c.kind == PMP_LAUNCH_PERSISTENT ? c.chunk : c.block;
+  int rc = get_map(h, chunk, map);
+  if (rc != PMP_OK || c.kind != PMP_LAUNCH_PERSISTENT) {
+    return rc;
+  }
+  if (!B.d_counter) {
+    PMP_TRY(h, cudaMalloc(&B.d_counter, sizeof(int)));
+  }
+  if (B.sm_count == 0) {
+    PMP_TRY(h, cudaDeviceGetAttribute(&B.sm_count, cudaDevAttrMultiProcessorCount, h->device));
+  }
+  if (memcmp(&B.occ_cfg, &c, sizeof(c)) != 0 || B.occ_ns != h->nspec || B.occ_nf != h->nfuel) {
+    const int per_sm = c.ctas_per_sm > 0 ? c.ctas_per_sm
+                                         : occupancy_variant(h->nspec, h->nfuel, c.block, c.regs, true);
+    B.persist_ctas = std::max(per_sm, 1) * B.sm_count;
+    B.occ_cfg = c;
+    B.occ_ns = h->nspec;
+    B.occ_nf = h->nfuel;
+  }
+  return PMP_OK;
+}
+
+}  // namespace
+
+int batch_enqueue_fp64(pmp_spray* h, const KParams& P, int nboxes, cudaStream_t st)
+{
+  const pmp_launch_config& c = h->batch.cfg;
+  const int ns = h->nspec, nf = h->nfuel;
+  const WorkMap* m = nullptr;
+  int rc = batch_prepare(h, &m);
+  if (rc != PMP_OK) {
+    return rc;
+  }
+  if (!m) {
+    return dispatch_fp64_default(ns, nf, P, h->ncta, st);
+  }
+  if (m->nitems == 0) {
+    return PMP_OK;
+  }
+  const int chunk = m->chunk;
+  WorkArgs W{m->box, m->start, m->nitems, chunk, h->batch.d_counter};
+  if (c.kind == PMP_LAUNCH_GRID) {
+    return launch_variant(ns, nf, c.block, c.regs, false, P, W, m->nitems, st) ? PMP_OK : PMP_ERR_UNSUPPORTED;
+  }
+  if (c.kind == PMP_LAUNCH_PERSISTENT) {
+    const int grid = std::min(m->nitems, h->batch.persist_ctas);
+    PMP_TRY(h, cudaMemsetAsync(h->batch.d_counter, 0, sizeof(int), st));
+    return launch_variant(ns, nf, c.block, c.regs, true, P, W, grid, st) ? PMP_OK : PMP_ERR_UNSUPPORTED;
+  }
+  // one launch per box, synchronised after each (the reference's pattern)
+  for (int b = 0; b < nboxes; ++b) {
+    const int i0 = m->item_begin[b], i1 = m->item_begin[b + 1];
+    if (i1 == i0) {
+      continue;
+    }
+    WorkArgs Wb{m->box + i0, m->start + i0, i1 - i0, chunk, nullptr};
+    if (!launch_variant(ns, nf, c.block, c.regs, false, P, Wb, i1 - i0, st)) {
+      return PMP_ERR_UNSUPPORTED;
+    }
+    PMP_TRY(h, cudaStreamSynchronize(st));
+  }
+  return PMP_OK;
+}
+
+// Replay the captured graph when the call repeats (same kernel parameters,
+// box table, mode and launch shape); capture a new one otherwise.
+int graph_update(pmp_spray* h, const KParams& P, int nboxes, cudaStream_t st, int* graph_state)
+{
+  BatchState& B = h->batch;
+  if (!B.gstream) {
+    PMP_TRY(h, cudaStreamCreateWithFlags(&B.gstream, cudaStreamNonBlocking));
+    PMP_TRY(h, cudaEventCreateWithFlags(&B.ev_in, cudaEventDisableTiming));
+    PMP_TRY(h, cudaEventCreateWithFlags(&B.ev_out, cudaEventDisableTiming));
+  }
+  std::vector<unsigned char> key(sizeof(KParams) + sizeof(BoxEntry) * nboxes + sizeof(pmp_launch_config) +
+                                 2 * sizeof(int));
+  unsigned char* k = key.data();
+  memcpy(k, &P, sizeof(KParams));
+  k += sizeof(KParams);
+  memcpy(k, h->h_boxes, sizeof(BoxEntry) * nboxes);
+  k += sizeof(BoxEntry) * nboxes;
+  memcpy(k, &B.cfg, sizeof(pmp_launch_config));
+  k += sizeof(pmp_launch_config);
+  memcpy(k, &h->mode, sizeof(int));
+  k += sizeof(int);
+  memcpy(k, &h->ncta, sizeof(int));
+  *graph_state = 1;
+  BatchState::Graph* G = nullptr;
+  for (BatchState::Graph& g : B.graphs) {
+    if (g.key == key) {
+      G = &g;
+    }
+  }
+  if (!G) {
+    if (h->mode == PMP_MODE_FP64) {
+      const WorkMap* m = nullptr;
+      const int rc = batch_prepare(h, &m);
+      if (rc != PMP_OK) {
+        return rc;
+      }
+    }
+    PMP_TRY(h, cudaStreamBeginCapture(B.gstream, cudaStreamCaptureModeThreadLocal));
+    const int rc = enqueue_update(h, P, nboxes, B.gstream);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(B.gstream, &g);
+    if (rc != PMP_OK || e != cudaSuccess) {
+      if (g) {
+        cudaGraphDestroy(g);
+      }
+      return rc != PMP_OK ? rc : check(h, e, "cudaStreamEndCapture");
+    }
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t ei = cudaGraphInstantiate(&exec, g, 0);
+    cudaGraphDestroy(g);
+    PMP_TRY(h, ei);
+    if (B.graphs.size() >= kMaxGraphs) {
+      auto lru = std::min_element(B.graphs.begin(), B.graphs.end(),
+                                  [](const BatchState::Graph& a, const BatchState::Graph& b) {
+                                    return a.last_use < b.last_use;
+                                  });
+      cudaGraphExecDestroy(lru->exec);
+      B.graphs.erase(lru);
+    }
+    B.graphs.push_back(BatchState::Graph{});
+    G = &B.graphs.back();
+    G->key.swap(key);
+    G->exec = exec;
+    *graph_state = 2;
+  }
+  G->last_use = ++B.use_clock;
+  PMP_TRY(h, cudaEventRecord(B.ev_in, st));
+  PMP_TRY(h, cudaStreamWaitEvent(B.gstream, B.ev_in, 0));
+  PMP_TRY(h, cudaGraphLaunch(G->exec, B.gstream));
+  PMP_TRY(h, cudaEventRecord(B.ev_out, B.gstream));
+  PMP_TRY(h, cudaStreamWaitEvent(st, B.ev_out, 0));
+  return PMP_OK;
+}
+
+void batch_reset(pmp_spray* h)
+{
+  for (WorkMap& m : h->batch.maps) {
+    free_map(m);
+  }
+  h->batch.maps.clear();
+  destroy_graphs(h);
+}
+
+void batch_free(pmp_spray* h)
+{
+  batch_reset(h);
+  cudaFree(h->batch.d_counter);
+  h->batch.d_counter = nullptr;
+  if (h->batch.gstream) {
+    cudaStreamDestroy(h->batch.gstream);
+    cudaEventDestroy(h->batch.ev_in);
+    cudaEventDestroy(h->batch.ev_out);
+    h->batch.gstream = nullptr;
+  }
+}
+
+}  // namespace pmp
+
+using namespace pmp;
+
+extern "C" int pmp_spray_set_launch(pmp_spray* h, const pmp_launch_config* cfg)
+{
+  if (!h || !cfg || !valid_shape(*cfg)) {
+    return set_err(h, PMP_ERR_INVALID, "invalid launch shape");
+  }
+  h->batch.cfg = *cfg;
+  h->batch.cfg.use_graph = cfg->use_graph ? 1 : 0;
+  return PMP_OK;
+}
+
+extern "C" int pmp_spray_get_launch(const pmp_spray* h, pmp_launch_config* cfg)
+{
+  if (!h || !cfg) {
+    return PMP_ERR_INVALID;
+  }
+  *cfg = h->batch.cfg;
+  return PMP_OK;
+}
+
+namespace {
+
+std::string tune_key(pmp_spray* h, int nboxes, int do_move, int num_iter)
+{
+  cudaDeviceProp prop;
+  cudaGetDeviceProperties(&prop, h->device);
+  std::string name(prop.name);
+  for (char& ch : name) {
+    if (ch == ' ' || ch == '\t') {
+      ch = '_';
+    }
+  }
+  const int lg = h->total > 0 ? (int)std::floor(std::log2((double)h->total)) : 0;
+  char b[256];
+  snprintf(b, sizeof(b), "%s|ns=%d|nf=%d|n=2^%d|boxes=%d|move=%d|iter=%d", name.c_str(), h->nspec, h->nfuel, lg,
+           nboxes, do_move, num_iter);
+  return b;
+}
+
+bool read_cache(const char* path, const std::string& key, pmp_launch_config* cfg, double* ms)
+{
+  FILE* f = fopen(path, "r");
+  if (!f) {
+    return false;
+  }
+  char line[512];
+  bool found = false;
+  while (fgets(line, sizeof(line), f)) {
+    const size_t n = key.size();
+    if (strncmp(line, key.c_str(), n) == 0 && line[n] == '\t') {
+      pmp_launch_config c{};
+      double t = 0.;
+      if (sscanf(line + n + 1, "%d %d %d %d %d %lf", &c.kind, &c.block, &c.regs, &c.chunk, &c.ctas_per_sm, &t) ==
+            6 &&
+          valid_shape(c)) {
+        *cfg = c;
+        *ms = t;
+        found = true;  // the last matching line wins
+      }
+    }
+  }
+  fclose(f);
+  return found;
+}
+
+void write_cache(const char* path, const std::string& key, const pmp_launch_config& c, double ms)
+{
+  FILE* f = fopen(path, "a");
+  if (!f) {
+    return;
+  }
+  fprintf(f, "%s\t%d %d %d %d %d %.6f\n", key.c_str(), c.kind, c.block, c.regs, c.chunk, c.ctas_per_sm, ms);
+  fclose(f);
+}
+
+}  // namespace
+
+extern "C" int pmp_spray_autotune(
+  pmp_spray* h, const pmp_box_view* state, const pmp_box_view* source, int nboxes, double flow_dt,
+  int state_ghosts, int source_ghosts, int is_ghost, int do_move, double spray_cfl_lev, const char* cache_path,
+  pmp_tune_report* rep, void* stream)
+{
+  if (!h || !state || !source || !rep) {
+    return PMP_ERR_INVALID;
+  }
+  if (h->mode != PMP_MODE_FP64) {
+    return set_err(h, PMP_ERR_INVALID, "the autotuner tunes the FP64 form (set PMP_MODE_FP64)");
+  }
+  cudaSetDevice(h->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  memset(rep, 0, sizeof(*rep));
+  // validation, packing and the sub-cycle count
+  KParams P;
+  int rc = prepare_update(h, state, source, nboxes, flow_dt, state_ghosts, source_ghosts, is_ghost, do_move,
+                          spray_cfl_lev, st, P);
+  if (rc != PMP_OK) {
+    return rc;
+  }
+  const pmp_launch_config saved = h->batch.cfg;
+  const std::string key = tune_key(h, nboxes, do_move, P.num_iter);
+  if (cache_path) {
+    pmp_launch_config c;
+    double ms = 0.;
+    if (read_cache(cache_path, key, &c, &ms)) {
+      c.use_graph = saved.use_graph;
+      h->batch.cfg = c;
+      rep->cached = 1;
+      rep->best = c;
+      rep->best_ms = ms;
+      return PMP_OK;
+    }
+  }
+  // snapshot of the droplets, scratch sources
+  const long long T = h->total;
+  const int nc = h->ncomp();
+  double* snap = nullptr;
+  int* snap_id = nullptr;
+  std::vector<double*> scratch(nboxes, nullptr);
+  std::vector<size_t> scratch_n(nboxes, 0);
+  std::vector<pmp_box_view> sviews(source, source + nboxes);
+  auto cleanup = [&]() {
+    cudaFree(snap);
+    cudaFree(snap_id);
+    for (double* p : scratch) {
+      cudaFree(p);
+    }
+  };
+  if (T > 0 && (cudaMalloc(&snap, sizeof(double) * nc * (size_t)T) != cudaSuccess ||
+                cudaMalloc(&snap_id, sizeof(int) * (size_t)T) != cudaSuccess)) {
+    cleanup();
+    return set_err(h, PMP_ERR_CUDA, "autotune: snapshot allocation failed");
+  }
+  if (T > 0) {
+    cudaMemcpy(snap, h->soa, sizeof(double) * nc * (size_t)T, cudaMemcpyDeviceToDevice);
+    cudaMemcpy(snap_id, h->ids, sizeof(int) * (size_t)T, cudaMemcpyDeviceToDevice);
+  }
+  for (int b = 0; b < nboxes; ++b) {
+    const pmp_box_view& v = source[b];
+    const size_t n = (size_t)((v.hi[0] - v.lo[0]) + (long long)(v.hi[1] - v.lo[1]) * v.jstride +
+                              (long long)(v.hi[2] - v.lo[2]) * v.kstride + (long long)(v.ncomp - 1) * v.nstride + 1);
+    if (cudaMalloc(&scratch[b], sizeof(double) * n) != cudaSuccess) {
+      cleanup();
+      return set_err(h, PMP_ERR_CUDA, "autotune: scratch allocation failed");
+    }
+    scratch_n[b] = n;
+    sviews[b].p = scratch[b];
+  }
+  auto trial = [&](const pmp_launch_config& c, int reps, double* best) -> int {
+    h->batch.cfg = c;
+    h->batch.cfg.use_graph = 0;
+    double t = 1e300;
+    for (int r = 0; r <= reps; ++r) {  // the first run warms up
+      if (T > 0) {
+        cudaMemcpyAsync(h->soa, snap, sizeof(double) * nc * (size_t)T, cudaMemcpyDeviceToDevice, st);
+        cudaMemcpyAsync(h->ids, snap_id, sizeof(int) * (size_t)T, cudaMemcpyDeviceToDevice, st);
+      }
+      for (int b = 0; b < nboxes; ++b) {
+        cudaMemsetAsync(scratch[b], 0, sizeof(double) * scratch_n[b], st);
+      }
+      const int e = run_update(h, state, sviews.data(), nboxes, flow_dt, state_ghosts, source_ghosts, is_ghost,
+                               do_move, spray_cfl_lev, st);
+      if (e != PMP_OK) {
+        return e;
+      }
+      if (r > 0) {
+        t = std::min(t, h->stats.kernel_ms);
+      }
+    }
+    *best = t;
+    return PMP_OK;
+  };
+  const pmp_launch_config cands[] = {
+    {PMP_LAUNCH_GRID, 128, 96, 128, 0, 0},        {PMP_LAUNCH_GRID, 64, 96, 64, 0, 0},
+    {PMP_LAUNCH_GRID, 128, 128, 128, 0, 0},       {PMP_LAUNCH_GRID, 256, 128, 256, 0, 0},
+    {PMP_LAUNCH_PERSISTENT, 128, 96, 128, 0, 0},  {PMP_LAUNCH_PERSISTENT, 128, 96, 512, 0, 0},
+    {PMP_LAUNCH_PERSISTENT, 128, 96, 2048, 0, 0}, {PMP_LAUNCH_PERSISTENT, 64, 96, 512, 0, 0},
+    {PMP_LAUNCH_PERSISTENT, 128, 128, 512, 0, 0}, {PMP_LAUNCH_PERSISTENT, 256, 128, 1024, 0, 0},
+  };
+  pmp_launch_config best = cands[0];
+  double best_ms = 1e300;
+  for (const pmp_launch_config& c : cands) {
+    double ms = 0.;
+    rc = trial(c, 3, &ms);
+    if (rc != PMP_OK) {
+      break;
+    }
+    if (&c == &cands[0]) {
+      rep->default_ms = ms;
+    }
+    rep->ncandidates += 1;
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = c;
+    }
+  }
+  if (rc == PMP_OK) {
+    double ms = 0.;
+    rc = trial({PMP_LAUNCH_PER_BOX, 128, 96, 128, 0, 0}, 2, &ms);
+    rep->per_box_ms = ms;
+  }
+  // leave the droplets as they were
+  if (T > 0) {
+    cudaMemcpyAsync(h->soa, snap, sizeof(double) * nc * (size_t)T, cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(h->ids, snap_id, sizeof(int) * (size_t)T, cudaMemcpyDeviceToDevice, st);
+  }
+  cudaStreamSynchronize(st);
+  cleanup();
+  if (rc != PMP_OK) {
+    h->batch.cfg = saved;
+    return rc;
+  }
+  best.use_graph = saved.use_graph;
+  h->batch.cfg = best;
+  rep->best = best;
+  rep->best_ms = best_ms;
+  if (cache_path) {
+    write_cache(cache_path, key, best, best_ms);
+  }
+  return PMP_OK;
+}

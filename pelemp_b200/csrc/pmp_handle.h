@@ -23,6 +23,37 @@ struct BoxStore {
 
 struct LearnState;  // learned form (pmp_learn.cu)
 
+// (box, first slot) work items of `chunk` slots (batched form, pmp_batch.cu)
+struct WorkMap {
+  int chunk = 0;
+  int nitems = 0;
+  int* box = nullptr;
+  long long* start = nullptr;
+  std::vector<int> item_begin;  // per box: first work item (nboxes + 1 entries)
+};
+
+struct BatchState {
+  pmp_launch_config cfg{PMP_LAUNCH_GRID, 128, 96, 512, 0, 0};
+  std::vector<WorkMap> maps;
+  int* d_counter = nullptr;
+  int sm_count = 0;
+  // resident CTAs of the persistent launch, for the shape occ_cfg
+  pmp_launch_config occ_cfg{-1, 0, 0, 0, 0, 0};
+  int occ_ns = 0, occ_nf = 0;
+  int persist_ctas = 0;
+  // CUDA graphs of recent updates' device work (a few, so that alternating
+  // calls such as MKD and MK both replay), least recently used evicted
+  struct Graph {
+    std::vector<unsigned char> key;
+    cudaGraphExec_t exec = nullptr;
+    unsigned long long last_use = 0;
+  };
+  std::vector<Graph> graphs;
+  unsigned long long use_clock = 0;
+  cudaStream_t gstream = nullptr;
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+};
+
 }  // namespace pmp
 
 struct pmp_spray {
@@ -72,6 +103,7 @@ struct pmp_spray {
   std::vector<double*> stage_state, stage_src;
   std::vector<size_t> stage_state_n, stage_src_n;
   pmp::LearnState* learn = nullptr;
+  pmp::BatchState batch;
   int nr() const { return PMP_PSTATE_NUM(nfuel); }
   int ncomp() const { return 3 + nr(); }
 };
@@ -87,6 +119,20 @@ int prepare_update(
   double flow_dt, int state_ghosts, int source_ghosts, int is_ghost, int do_move,
   double spray_cfl_lev, cudaStream_t st, KParams& P);
 int run_fp64_list(int ns, int nf, const KParams& P, long long total, cudaStream_t st);
+int dispatch_fp64_default(int ns, int nf, const KParams& P, int ncta, cudaStream_t st);
+// the device work of one update after prepare: box table upload, status
+// reset, timing events, kernels, status read-back (no synchronisation)
+int enqueue_update(pmp_spray* h, const KParams& P, int nboxes, cudaStream_t st);
+// a whole update call (prepare, launch, synchronise, status)
+int run_update(
+  pmp_spray* h, const pmp_box_view* state, const pmp_box_view* source, int nboxes,
+  double flow_dt, int state_ghosts, int source_ghosts, int is_ghost, int do_move,
+  double spray_cfl_lev, cudaStream_t st);
+// pmp_batch.cu
+int batch_enqueue_fp64(pmp_spray* h, const KParams& P, int nboxes, cudaStream_t st);
+int graph_update(pmp_spray* h, const KParams& P, int nboxes, cudaStream_t st, int* graph_state);
+void batch_reset(pmp_spray* h);
+void batch_free(pmp_spray* h);
 // pmp_learn.cu
 int launch_learned(pmp_spray* h, const KParams& P, cudaStream_t st);
 bool learn_ready(const pmp_spray* h);

@@ -182,6 +182,7 @@ void free_packed(pmp_spray* h)
   h->fb_list = nullptr;
   h->packed = false;
   h->ncta = 0;
+  pmp::batch_reset(h);
 }
 
 // DevMech (species in mechanism order) and DevFuel from the mechanism and
@@ -574,9 +575,7 @@ int prepare_update_impl(
     e.p_begin = h->box_begin[b];
     e.p_end = h->box_begin[b + 1];
   }
-  PMP_CUDA(h, cudaMemcpyAsync(h->d_boxes, h->h_boxes, sizeof(BoxEntry) * nboxes,
-                              cudaMemcpyHostToDevice, st));
-  PMP_CUDA(h, cudaMemsetAsync(h->d_status, 0, sizeof(DevStatus), st));
+  (void)st;
   memset(&P, 0, sizeof(P));
   P.m = h->dmech;
   P.f = h->dfuel;
@@ -642,37 +641,23 @@ int do_update(
   if (rc != PMP_OK) {
     return rc;
   }
-  const int NS = h->nspec;
-  const int NF = h->nfuel;
   const long long T = h->total;
-  PMP_CUDA(h, cudaEventRecord(h->ev0, st));
-  if (h->ncta > 0) {
-    if (h->mode == PMP_MODE_LEARNED) {
-      rc = pmp::launch_learned(h, P, st);
-      if (rc == PMP_OK) {
-        PMP_CUDA(h, cudaGetLastError());
-        rc = dispatch_fp64_list(NS, NF, P, h->total, st);
-      }
-    } else if (h->mode == PMP_MODE_MIXED) {
-      rc = pmp::launch_mixed(NS, NF, P, h->ncta, kBlock, st);
-      if (rc == PMP_OK) {
-        PMP_CUDA(h, cudaGetLastError());
-        rc = dispatch_fp64_list(NS, NF, P, h->total, st);
-      }
-    } else {
-      rc = dispatch_fp64(NS, NF, P, h->ncta, st);
-    }
-    if (rc != PMP_OK) {
-      return set_err(h, rc, "no kernel for this species / fuel count");
-    }
-    PMP_CUDA(h, cudaGetLastError());
+  const bool graph = h->batch.cfg.use_graph && h->mode != PMP_MODE_LEARNED &&
+                     h->batch.cfg.kind != PMP_LAUNCH_PER_BOX;
+  int graph_state = 0;
+  rc = graph ? pmp::graph_update(h, P, nboxes, st, &graph_state) : pmp::enqueue_update(h, P, nboxes, st);
+  if (rc != PMP_OK) {
+    return rc;
   }
-  PMP_CUDA(h, cudaEventRecord(h->ev1, st));
-  PMP_CUDA(h, cudaMemcpyAsync(h->h_status, h->d_status, sizeof(DevStatus), cudaMemcpyDeviceToHost, st));
   PMP_CUDA(h, cudaStreamSynchronize(st));
   float ms = 0.f;
-  cudaEventElapsedTime(&ms, h->ev0, h->ev1);
-  h->stats.kernel_ms = ms;
+  if (cudaEventElapsedTime(&ms, h->ev0, h->ev1) == cudaSuccess) {
+    h->stats.kernel_ms = ms;
+  } else {
+    h->stats.kernel_ms = -1.;
+    cudaGetLastError();  // not sticky: clear it so that the next call does not report it
+  }
+  h->stats.graph = graph_state;
   h->stats.substeps = (long long)h->h_status->substeps;
   h->stats.killed = (long long)h->h_status->killed;
   h->stats.inner_steps = (long long)h->h_status->inner;
@@ -709,8 +694,71 @@ int pmp::prepare_update(
   double flow_dt, int state_ghosts, int source_ghosts, int is_ghost, int do_move,
   double spray_cfl_lev, cudaStream_t st, KParams& P)
 {
-  return prepare_update_impl(h, state, source, nboxes, flow_dt, state_ghosts, source_ghosts,
-                             is_ghost, do_move, spray_cfl_lev, st, P);
+  const int rc = prepare_update_impl(h, state, source, nboxes, flow_dt, state_ghosts, source_ghosts,
+                                     is_ghost, do_move, spray_cfl_lev, st, P);
+  if (rc != PMP_OK) {
+    return rc;
+  }
+  PMP_CUDA(h, cudaMemcpyAsync(h->d_boxes, h->h_boxes, sizeof(BoxEntry) * nboxes,
+                              cudaMemcpyHostToDevice, st));
+  PMP_CUDA(h, cudaMemsetAsync(h->d_status, 0, sizeof(DevStatus), st));
+  return PMP_OK;
+}
+
+int pmp::enqueue_update(pmp_spray* h, const KParams& P, int nboxes, cudaStream_t st)
+{
+  // under stream capture the timing events become event-record nodes of the graph
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  PMP_CUDA(h, cudaStreamIsCapturing(st, &cap));
+  const unsigned ev_flags = cap == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : 0u;
+  PMP_CUDA(h, cudaMemcpyAsync(h->d_boxes, h->h_boxes, sizeof(BoxEntry) * nboxes,
+                              cudaMemcpyHostToDevice, st));
+  PMP_CUDA(h, cudaMemsetAsync(h->d_status, 0, sizeof(DevStatus), st));
+  PMP_CUDA(h, cudaEventRecordWithFlags(h->ev0, st, ev_flags));
+  if (h->ncta > 0) {
+    const int NS = h->nspec;
+    const int NF = h->nfuel;
+    int rc = PMP_OK;
+    if (h->mode == PMP_MODE_LEARNED) {
+      rc = pmp::launch_learned(h, P, st);
+      if (rc == PMP_OK) {
+        PMP_CUDA(h, cudaGetLastError());
+        rc = dispatch_fp64_list(NS, NF, P, h->total, st);
+      }
+    } else if (h->mode == PMP_MODE_MIXED) {
+      rc = pmp::launch_mixed(NS, NF, P, h->ncta, kBlock, st);
+      if (rc == PMP_OK) {
+        PMP_CUDA(h, cudaGetLastError());
+        rc = dispatch_fp64_list(NS, NF, P, h->total, st);
+      }
+    } else {
+      rc = pmp::batch_enqueue_fp64(h, P, nboxes, st);
+    }
+    if (rc == PMP_ERR_UNSUPPORTED) {
+      return set_err(h, rc, "no kernel for this species / fuel count");
+    }
+    if (rc != PMP_OK) {
+      return rc;
+    }
+    PMP_CUDA(h, cudaGetLastError());
+  }
+  PMP_CUDA(h, cudaEventRecordWithFlags(h->ev1, st, ev_flags));
+  PMP_CUDA(h, cudaMemcpyAsync(h->h_status, h->d_status, sizeof(DevStatus), cudaMemcpyDeviceToHost, st));
+  return PMP_OK;
+}
+
+int pmp::run_update(
+  pmp_spray* h, const pmp_box_view* state, const pmp_box_view* source, int nboxes,
+  double flow_dt, int state_ghosts, int source_ghosts, int is_ghost, int do_move,
+  double spray_cfl_lev, cudaStream_t st)
+{
+  return do_update(h, state, source, nboxes, flow_dt, state_ghosts, source_ghosts, 0, is_ghost,
+                   do_move, spray_cfl_lev, st);
+}
+
+int pmp::dispatch_fp64_default(int ns, int nf, const KParams& P, int ncta, cudaStream_t st)
+{
+  return dispatch_fp64(ns, nf, P, ncta, st);
 }
 
 int pmp::run_fp64_list(int ns, int nf, const KParams& P, long long total, cudaStream_t st)
@@ -785,6 +833,7 @@ int pmp_spray_destroy(pmp_spray* h)
   }
   free_packed(h);
   pmp::learn_free(h);
+  pmp::batch_free(h);
   for (double* p : h->stage_state) {
     cudaFree(p);
   }

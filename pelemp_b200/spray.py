@@ -49,6 +49,11 @@ _SIGS = {
     "pmp_spray_last_error": [C.c_void_p, C.POINTER(capi.ErrorInfo)],
     "pmp_spray_get_stats": [C.c_void_p, C.POINTER(capi.Stats)],
     "pmp_spray_version": [],
+    "pmp_spray_set_launch": [C.c_void_p, C.POINTER(capi.LaunchConfig)],
+    "pmp_spray_get_launch": [C.c_void_p, C.POINTER(capi.LaunchConfig)],
+    "pmp_spray_autotune": [C.c_void_p, C.POINTER(capi.BoxView), C.POINTER(capi.BoxView), C.c_int,
+                           C.c_double, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_char_p,
+                           C.POINTER(capi.TuneReport), C.c_void_p],
     "pmp_spray_learn_generate": [C.c_void_p, C.POINTER(capi.BoxView), C.c_int, C.c_double, C.c_int,
                                  C.c_int, C.c_double, C.c_longlong, C.c_int, C.c_ulonglong,
                                  C.c_void_p],
@@ -281,6 +286,27 @@ class SprayParticleContainer:
         s = capi.Stats()
         lib().pmp_spray_get_stats(self._h, C.byref(s))
         return s
+
+    # --- launch shape, CUDA graph, autotuner (batched form) ---------------
+    def set_launch(self, kind=capi.PMP_LAUNCH_GRID, block=128, regs=96, chunk=512, ctas_per_sm=0,
+                   use_graph=False):
+        cfg = capi.LaunchConfig(kind, block, regs, chunk, ctas_per_sm, int(use_graph))
+        self._check(lib().pmp_spray_set_launch(self._h, C.byref(cfg)))
+
+    def launch(self):
+        cfg = capi.LaunchConfig()
+        self._check(lib().pmp_spray_get_launch(self._h, C.byref(cfg)))
+        return cfg
+
+    def autotune(self, state, source, flow_dt, state_ghosts, source_ghosts, is_ghost, do_move,
+                 spray_cfl_lev, cache_path=None, stream=0):
+        """Pick the fastest launch shape of the FP64 update for these views."""
+        rep = capi.TuneReport()
+        self._check(lib().pmp_spray_autotune(
+            self._h, state, source, len(state), flow_dt, state_ghosts, source_ghosts, int(is_ghost),
+            int(do_move), spray_cfl_lev, cache_path.encode() if cache_path else None, C.byref(rep),
+            C.c_void_p(stream)))
+        return rep
 
     # --- learned form (no counterpart in the reference) -------------------
     def learn_generate(self, state, flow_dt, state_ghosts, do_move=True, spray_cfl_lev=-1.0,
