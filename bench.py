@@ -9,9 +9,15 @@ PeleLMeX time step asks of the spray container: zero the source
 one execution of the sub-cycle body SprayParticles.cpp:357-480.
 
 Arms
-* default: the B200 library (plain FP64 form), inputs resident in HBM; plus
-  ``e2e``: the same steps through pmp_spray_update_host with the mesh state
-  and source in pinned host memory (copies inside the timed region).
+* default: the B200 library, inputs resident in HBM, in three forms timed on
+  the same initial droplets: plain FP64, mixed (FP32 physics, FP64 state and
+  deposits) and learned (surrogate trained first, untimed, on tuples the FP64
+  teacher labels from a sample of the workload).  ``value`` is the fastest
+  non-FP64 form; ``forms`` lists every form with its speed-up over FP64 and
+  its per-droplet error against the FP64 form (bit-identical to the FP64
+  oracle) after all steps.  ``e2e``: the headline form's steps through
+  pmp_spray_update_host with the mesh state and source in pinned host memory
+  (copies inside the timed region).
 * --impl reference: PeleMP's own spray physics headers (oracle/_ref, built
   from the reference sources) on the host cores, OpenMP over droplets, on a
   bounded random sample of the same workload.
@@ -211,6 +217,45 @@ def cpu_baseline(seconds=12.0):
                                            if have_ref else "CPU oracle, OpenMP"))}
 
 
+FORM_MODE = {"fp64": 0, "mixed": 1, "learned": 2}
+FORM_NAME = {"fp64": "plain FP64", "mixed": "mixed FP32 physics / FP64 state and deposits",
+             "learned": "learned surrogate (bf16 MLP on tensor cores) + FP32 physics / FP64 state"}
+KERNEL = {"fp64": "spray_update_fp64<5,2,128>", "mixed": "spray_update_mixed<5,2,128>",
+          "learned": "spray_update_learned<5,2,128>"}
+
+
+def train_surrogate(sp, prob, st_v, stream, args):
+    """Tuples from the plain FP64 teacher on a sample of the workload's droplets,
+    then GPU training; returns (seconds, report)."""
+    t0 = time.perf_counter()
+    sp.learn_generate(st_v, prob.flow_dt, prob.state_ghosts, True, prob.spray_cfl_lev,
+                      sample_stride=args.learn_stride, augment=3, seed=7, stream=stream)
+    rep = sp.learn_train(epochs=args.learn_epochs, batch=2048, audit_fraction=0.0)
+    return time.perf_counter() - t0, rep
+
+
+def droplet_errors(pa, pb, prob):
+    """Per-droplet relative errors of T and liquid mass (d^3 / sum(Y/rho_l)) of pa vs pb."""
+    from pelemp_b200 import workloads as W
+    nfuel = prob.nfuel
+    rho = np.array([W.LIQUIDS[f]["rho"] for f in prob.fuels])
+    eT, em = [], []
+    for a, b in zip(pa, pb):
+        al = (a["id"] > 0) & (b["id"] > 0)
+        ra, rb = a["rdata"][:, al], b["rdata"][:, al]
+        eT.append(np.abs(ra[3] / rb[3] - 1))
+
+        def mass(r):
+            return r[4] ** 3 / np.sum(r[5:5 + nfuel] / rho[:, None], axis=0)
+        em.append(np.abs(mass(ra) / mass(rb) - 1))
+    eT, em = np.concatenate(eT), np.concatenate(em)
+
+    def q(e):
+        return {"rms": float(np.sqrt(np.mean(e ** 2))), "p99_9": float(np.quantile(e, 0.999)),
+                "max": float(e.max())}
+    return {"T": q(eT), "mass": q(em), "droplets": int(eT.size)}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -222,7 +267,10 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=100_000)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--mode", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--forms", default="fp64,mixed,learned",
+                    help="forms to time; the fastest non-FP64 one is the headline value")
+    ap.add_argument("--learn-stride", type=int, default=64)
+    ap.add_argument("--learn-epochs", type=int, default=40)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -243,22 +291,21 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         pg = dist
 
-    from pelemp_b200 import capi
     from pelemp_b200 import workloads as W
     from pelemp_b200.spray import from_problem, views
 
+    forms = [f for f in args.forms.split(",") if f]
     prob = W.config2(n=args.droplets, seed=rank, steps=args.steps)
     nboxes = len(prob.boxes)
     ncells = int(np.prod([prob.domain_hi[d] - prob.domain_lo[d] + 1 for d in range(3)]))
-    mode = {"fp64": capi.PMP_MODE_FP64, "mixed": capi.PMP_MODE_MIXED}[args.mode]
-    sp = from_problem(prob, device=local, mode=mode)
     stream = torch.cuda.current_stream()
     st = [torch.from_numpy(s).cuda() for s in prob.state]
     st_v = views(st, [prob.grown(b, prob.state_ghosts)[0] for b in range(nboxes)])
     src = [torch.zeros(s.shape, dtype=torch.float64, device="cuda") for s in prob.new_sources()]
     src_v = views(src, [prob.grown(b, prob.source_ghosts)[0] for b in range(nboxes)])
+    peak, peak_src = measured_peaks()
 
-    def step(stats_out=None):
+    def step(sp):
         for s in src:
             s.zero_()
         out = []
@@ -267,53 +314,79 @@ def main():
                                 prob.source_ghosts, 0, 0, do_move, prob.spray_cfl_lev,
                                 stream.cuda_stream)
             s_ = sp.stats()
-            out.append((s_.substeps, s_.kernel_ms))
+            out.append((s_.substeps, s_.kernel_ms, s_.fallback))
         return out
 
-    for _ in range(args.warmup):
-        step()
-    n_live = prob.n_droplets
-    sampler = ClockSampler(local)
-    if pg:
-        pg.barrier()
-    torch.cuda.synchronize()
-    sampler.start()
-    time.sleep(0.3)
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    substeps = 0
-    mkd_ms = []
-    mkd_bytes = []
-    for _ in range(args.steps):
-        rec = step()
-        substeps += rec[0][0] + rec[1][0]
-        mkd_ms.append(rec[0][1])
-        mkd_bytes.append(algorithmic_bytes(n_live, prob.nfuel, prob.nspec, ncells, True))
-        n_live = n_live  # kills are rare at these sizes; counted exactly below
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    if pg:
-        pg.barrier()
-    clocks = sampler.stop()
-    t_ms = ev0.elapsed_time(ev1)
-    t_max = t_ms
-    sub_total = substeps
-    if pg:
-        tt = torch.tensor([t_ms], device="cuda", dtype=torch.float64)
-        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
-        t_max = float(tt.item())
-        ss = torch.tensor([float(substeps)], device="cuda", dtype=torch.float64)
-        pg.all_reduce(ss, op=pg.ReduceOp.SUM)
-        sub_total = int(ss.item())
-    value = sub_total / (t_max * 1e-3)
-    peak, peak_src = measured_peaks()
-    avg_mkd_ms = float(np.mean(mkd_ms))
-    achieved = float(np.mean(mkd_bytes)) / (avg_mkd_ms * 1e-3) / 1e9
+    results = {}
+    containers = {}
+    for form in forms:
+        sp = from_problem(prob, device=local, mode=FORM_MODE[form])
+        containers[form] = sp
+        info = {}
+        if form == "learned":
+            t_train, rep = train_surrogate(sp, prob, st_v, stream.cuda_stream, args)
+            info["train"] = {"seconds": t_train, "tuples": rep.tuples, "adam_steps": rep.steps,
+                             "val_rel_rms": list(rep.val_rel_rms), "epochs": args.learn_epochs,
+                             "sample_stride": args.learn_stride}
+        for _ in range(args.warmup):
+            step(sp)
+        sampler = ClockSampler(local)
+        if pg:
+            pg.barrier()
+        torch.cuda.synchronize()
+        sampler.start()
+        time.sleep(0.3)
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        substeps, fallback, mkd_ms = 0, 0, []
+        for _ in range(args.steps):
+            rec = step(sp)
+            substeps += rec[0][0] + rec[1][0]
+            fallback += rec[0][2] + rec[1][2]
+            mkd_ms.append(rec[0][1])
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        if pg:
+            pg.barrier()
+        c = sampler.stop()
+        t_ms = ev0.elapsed_time(ev1)
+        t_max, sub_total = t_ms, substeps
+        if pg:
+            tt = torch.tensor([t_ms], device="cuda", dtype=torch.float64)
+            pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+            t_max = float(tt.item())
+            ss = torch.tensor([float(substeps)], device="cuda", dtype=torch.float64)
+            pg.all_reduce(ss, op=pg.ReduceOp.SUM)
+            sub_total = int(ss.item())
+        info.update({"value": sub_total / (t_max * 1e-3), "ms_per_step": t_max / args.steps,
+                     "mkd_launch_ms": float(np.mean(mkd_ms)), "substeps": sub_total,
+                     "fallback_frac": fallback / max(substeps, 1), "clocks": c})
+        results[form] = info
 
-    # ---- e2e: host views through pmp_spray_update_host ----
+    fast = [f for f in forms if f != "fp64"]
+    head = max(fast, key=lambda f: results[f]["value"]) if fast else "fp64"
+    value = results[head]["value"]
+    t_max = results[head]["ms_per_step"] * args.steps
+    clocks = results[head]["clocks"]
+
+    # accuracy of the fast forms against the FP64 form (bit-identical to the FP64
+    # oracle): every form advanced the same initial droplets by warmup + steps steps
+    accuracy = {}
+    if "fp64" in containers and rank == 0:
+        ref = [containers["fp64"].get_particles(0)]
+        for f in fast:
+            accuracy[f] = droplet_errors([containers[f].get_particles(0)], ref, prob)
+        accuracy["steps"] = args.warmup + args.steps
+
+    # roofline of the headline form's MKD launch (algorithmic bytes / launch time)
+    mkd_bytes = algorithmic_bytes(prob.n_droplets, prob.nfuel, prob.nspec, ncells, True)
+    achieved = mkd_bytes / (results[head]["mkd_launch_ms"] * 1e-3) / 1e9
+
+    # ---- e2e: host views through pmp_spray_update_host (headline form) ----
     e2e = None
     if not args.no_e2e:
+        sp = containers[head]
         st_h = [torch.from_numpy(s).pin_memory().numpy() for s in prob.state]
         src_h = [torch.zeros(s.shape, dtype=torch.float64).pin_memory().numpy()
                  for s in prob.new_sources()]
@@ -356,7 +429,7 @@ def main():
             ns = int(ss.item())
         e2e = {"value": ns / (te * 1e-3), "unit": "droplet-substeps/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-               "steps": args.e2e_steps,
+               "steps": args.e2e_steps, "form": head,
                "path": "pmp_spray_update_host: pinned host state/source, H2D+D2H inside"}
 
     cpu = None
@@ -364,31 +437,49 @@ def main():
         cpu = cpu_baseline()
 
     if rank == 0:
+        forms_out = {}
+        for f in forms:
+            r = results[f]
+            forms_out[f] = {"value": r["value"], "ms_per_step": r["ms_per_step"],
+                            "mkd_launch_ms": r["mkd_launch_ms"], "fallback_frac": r["fallback_frac"],
+                            "speedup_vs_fp64": (r["value"] / results["fp64"]["value"]
+                                                if "fp64" in results else None)}
+            if "train" in r:
+                forms_out[f]["train"] = r["train"]
+            if f in accuracy:
+                forms_out[f]["error_vs_fp64"] = accuracy[f]
         line = {
             "metric": "droplet-substeps/s", "value": value, "unit": "droplet-substeps/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, numpy PCG64)",
+            "vs_baseline": None,
+            "dtype": {"fp64": "f64", "mixed": "f32 physics, f64 state/deposits",
+                      "learned": "bf16 MLP (f32 accumulate), f32 physics, f64 state/deposits"}[head],
+            "data": "synthetic (seeded, numpy PCG64)",
             "config": {"workload": "config2: 16M two-fuel droplets (decane/heptane), 128^3 mesh "
                                    "as 8 boxes of 64^3, 5 gas species, dt=5e-7 s, MKD 4 sub-cycles "
                                    "+ MK 1 sub-cycle per step",
-                       "droplets_per_gpu": prob.n_droplets, "boxes": nboxes,
-                       "form": {"fp64": "plain FP64", "mixed": "mixed FP32/FP64"}[args.mode],
+                       "droplets_per_gpu": prob.n_droplets, "boxes": nboxes, "form": head,
+                       "form_name": FORM_NAME[head],
                        "l2": "inputs larger than L2 (1.9 GB droplet SoA, 0.24 GB state per GPU)",
                        "parallelism": f"replicas x{world}"},
+            "forms": forms_out,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None,
-                         "kernel": "spray_update_fp64<5,2> (MKD launch)",
-                         "launch_ms": avg_mkd_ms, "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)"
+                         "kernel": KERNEL[head] + " (MKD launch)",
+                         "launch_ms": results[head]["mkd_launch_ms"],
+                         "algorithmic_bytes_per_launch": mkd_bytes,
+                         "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)"
                          if peak_src == "measured" else "fallback 6650 GB/s"},
             "e2e": e2e,
             "cpu_baseline": cpu,
-            "gpu_launches": 2 * args.steps,
+            "gpu_launches": 2 * args.steps * (2 if head != "fp64" else 1),
             "clocks": clocks,
-            "substeps_per_step": sub_total / args.steps,
+            "substeps_per_step": results[head]["substeps"] / args.steps,
         }
         print(json.dumps(line), flush=True)
-    sp.close()
+    for sp in containers.values():
+        sp.close()
     if pg:
         pg.destroy_process_group()
 
