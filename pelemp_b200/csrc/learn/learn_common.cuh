@@ -326,19 +326,18 @@ __device__ __forceinline__ bool learn_gas_fp64(
           if (!in_box(B.state_lo, B.state_hi, ci, cj, ck)) {
             return false;
           }
-          const double* q = B.st + (long long)(ci - B.st_lo[0]) + (long long)(cj - B.st_lo[1]) * B.st_js +
-                            (long long)(ck - B.st_lo[2]) * B.st_ks;
-          const double r = q[(long long)P.c_rho * B.st_ns];
+          const double* q = B.st + ((ci - B.st_lo[0]) + (cj - B.st_lo[1]) * B.st_j32 + (ck - B.st_lo[2]) * B.st_k32);
+          const double r = q[P.c_rho * B.st_n32];
           gpv.rho += cw * r;
 #pragma unroll
           for (int n = 0; n < NS; ++n) {
-            gpv.Y[n] += cw * q[(long long)(P.c_spec + n) * B.st_ns] / r;
+            gpv.Y[n] += cw * q[(P.c_spec + n) * B.st_n32] / r;
           }
 #pragma unroll
           for (int d = 0; d < 3; ++d) {
-            gpv.vel[d] += cw * q[(long long)(P.c_mom + d) * B.st_ns];
+            gpv.vel[d] += cw * q[(P.c_mom + d) * B.st_n32];
           }
-          gpv.T += cw * q[(long long)P.c_T * B.st_ns];
+          gpv.T += cw * q[P.c_T * B.st_n32];
         }
       }
     }

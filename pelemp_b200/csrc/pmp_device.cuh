@@ -103,6 +103,10 @@ struct BoxEntry {
   int at_bounds;
   int pad;
   long long p_begin, p_end;       // droplet slots of this box
+  // the strides again as 32-bit ints (every view is checked to span fewer
+  // than 2^31 elements), for cheaper index arithmetic in the update kernels
+  int st_j32, st_k32, st_n32;
+  int sr_j32, sr_k32, sr_n32;
 };
 
 // Device status word block, zeroed before each update.

@@ -793,20 +793,19 @@ __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
               if (!in_box(B.state_lo, B.state_hi, ci, cj, ck)) {
                 state_ok = false;
               } else {
-                const double* q = B.st + (long long)(ci - B.st_lo[0]) + (long long)(cj - B.st_lo[1]) * B.st_js +
-                                  (long long)(ck - B.st_lo[2]) * B.st_ks;
-                const double cur_rho = __ldg(q + (long long)P.c_rho * B.st_ns);
+                const double* q = B.st + ((ci - B.st_lo[0]) + (cj - B.st_lo[1]) * B.st_j32 + (ck - B.st_lo[2]) * B.st_k32);
+                const double cur_rho = __ldg(q + P.c_rho * B.st_n32);
                 rho = fma(cw, cur_rho, rho);
-                const double w_rho = cw / cur_rho;
+                const double w_rho = cw * drcp_from_f(cur_rho);
 #pragma unroll
                 for (int n = 0; n < NS; ++n) {
-                  Yg[n] = fma(w_rho, __ldg(q + (long long)(P.c_spec + n) * B.st_ns), Yg[n]);
+                  Yg[n] = fma(w_rho, __ldg(q + (P.c_spec + n) * B.st_n32), Yg[n]);
                 }
 #pragma unroll
                 for (int dir = 0; dir < 3; ++dir) {
-                  vg[dir] = fma(cw, __ldg(q + (long long)(P.c_mom + dir) * B.st_ns), vg[dir]);
+                  vg[dir] = fma(cw, __ldg(q + (P.c_mom + dir) * B.st_n32), vg[dir]);
                 }
-                Tg = fma(cw, __ldg(q + (long long)P.c_T * B.st_ns), Tg);
+                Tg = fma(cw, __ldg(q + P.c_T * B.st_n32), Tg);
               }
             }
           }
@@ -1093,20 +1092,19 @@ __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
         set_error(P, PMP_ERR_SOURCE_BOX, b, s);
         ok = false;
       } else {
-        double* q = B.sr + (long long)(ijkc[0] - B.sr_lo[0]) + (long long)(ijkc[1] - B.sr_lo[1]) * B.sr_js +
-                    (long long)(ijkc[2] - B.sr_lo[2]) * B.sr_ks;
+        double* q = B.sr + ((ijkc[0] - B.sr_lo[0]) + (ijkc[1] - B.sr_lo[1]) * B.sr_j32 + (ijkc[2] - B.sr_lo[2]) * B.sr_k32);
         if (fdat.mom_trans) {
 #pragma unroll
           for (int dir = 0; dir < 3; ++dir) {
-            atomicAdd(q + (long long)(P.s_mom + dir) * B.sr_ns, cur_coef * src.mom[dir]);
+            atomicAdd(q + (P.s_mom + dir) * B.sr_n32, cur_coef * src.mom[dir]);
           }
         }
-        atomicAdd(q + (long long)P.s_rho * B.sr_ns, cur_coef * src.mass);
+        atomicAdd(q + P.s_rho * B.sr_n32, cur_coef * src.mass);
 #pragma unroll
         for (int spf = 0; spf < NF; ++spf) {
-          atomicAdd(q + (long long)(P.s_spec + spf) * B.sr_ns, cur_coef * src.Ydot[spf]);
+          atomicAdd(q + (P.s_spec + spf) * B.sr_n32, cur_coef * src.Ydot[spf]);
         }
-        atomicAdd(q + (long long)P.s_eng * B.sr_ns, cur_coef * src.eng);
+        atomicAdd(q + P.s_eng * B.sr_n32, cur_coef * src.eng);
         if (P.do_move && !fdat.fixed_parts && id > 0) {
 #pragma unroll
           for (int dir = 0; dir < 3; ++dir) {

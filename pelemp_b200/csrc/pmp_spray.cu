@@ -571,6 +571,15 @@ int prepare_update_impl(
     e.sr_js = source[b].jstride;
     e.sr_ks = source[b].kstride;
     e.sr_ns = source[b].nstride;
+    if (view_extent(state[b]) >= (1LL << 31) || view_extent(source[b]) >= (1LL << 31)) {
+      return set_err(h, PMP_ERR_INVALID, "a state or source view spans 2^31 elements or more", b);
+    }
+    e.st_j32 = (int)state[b].jstride;
+    e.st_k32 = (int)state[b].kstride;
+    e.st_n32 = (int)state[b].nstride;
+    e.sr_j32 = (int)source[b].jstride;
+    e.sr_k32 = (int)source[b].kstride;
+    e.sr_n32 = (int)source[b].nstride;
     e.at_bounds = tile_at_bndry(bx, h->geom);
     e.p_begin = h->box_begin[b];
     e.p_end = h->box_begin[b + 1];

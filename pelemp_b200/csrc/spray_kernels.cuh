@@ -146,22 +146,21 @@ __device__ __forceinline__ void update_one(const KParams& P, int b, long long s,
               if (!in_box(B.state_lo, B.state_hi, ci, cj, ck)) {
                 state_ok = false;
               } else {
-                const double* q = B.st + (long long)(ci - B.st_lo[0]) + (long long)(cj - B.st_lo[1]) * B.st_js +
-                                  (long long)(ck - B.st_lo[2]) * B.st_ks;
-                const double cur_rho = __ldg(q + (long long)P.c_rho * B.st_ns);
+                const double* q = B.st + ((ci - B.st_lo[0]) + (cj - B.st_lo[1]) * B.st_j32 + (ck - B.st_lo[2]) * B.st_k32);
+                const double cur_rho = __ldg(q + P.c_rho * B.st_n32);
                 gpv.rho = __dadd_rn(gpv.rho, __dmul_rn(cw, cur_rho));
                 const double inv_rho = 1. / cur_rho;
 #pragma unroll
                 for (int n = 0; n < NS; ++n) {
-                  const double cur_mf = __dmul_rn(__ldg(q + (long long)(P.c_spec + n) * B.st_ns), inv_rho);
+                  const double cur_mf = __dmul_rn(__ldg(q + (P.c_spec + n) * B.st_n32), inv_rho);
                   gpv.Y[n] = __dadd_rn(gpv.Y[n], __dmul_rn(cw, cur_mf));
                 }
 #pragma unroll
                 for (int dir = 0; dir < 3; ++dir) {
                   gpv.vel[dir] =
-                    __dadd_rn(gpv.vel[dir], __dmul_rn(cw, __ldg(q + (long long)(P.c_mom + dir) * B.st_ns)));
+                    __dadd_rn(gpv.vel[dir], __dmul_rn(cw, __ldg(q + (P.c_mom + dir) * B.st_n32)));
                 }
-                gpv.T = __dadd_rn(gpv.T, __dmul_rn(cw, __ldg(q + (long long)P.c_T * B.st_ns)));
+                gpv.T = __dadd_rn(gpv.T, __dmul_rn(cw, __ldg(q + P.c_T * B.st_n32)));
               }
             }
           }
@@ -223,20 +222,19 @@ __device__ __forceinline__ void update_one(const KParams& P, int b, long long s,
               if (!in_box(B.state_lo, B.state_hi, ci, cj, ck)) {
                 state_ok = false;
               } else {
-                const double* q = B.st + (long long)(ci - B.st_lo[0]) + (long long)(cj - B.st_lo[1]) * B.st_js +
-                                  (long long)(ck - B.st_lo[2]) * B.st_ks;
-                const double cur_rho = __ldg(q + (long long)P.c_rho * B.st_ns);
+                const double* q = B.st + ((ci - B.st_lo[0]) + (cj - B.st_lo[1]) * B.st_j32 + (ck - B.st_lo[2]) * B.st_k32);
+                const double cur_rho = __ldg(q + P.c_rho * B.st_n32);
                 rho = fma(cw, cur_rho, rho);
-                const double w_rho = cw / cur_rho;
+                const double w_rho = cw * drcp_from_f(cur_rho);
 #pragma unroll
                 for (int n = 0; n < NS; ++n) {
-                  Yg[n] = fma(w_rho, __ldg(q + (long long)(P.c_spec + n) * B.st_ns), Yg[n]);
+                  Yg[n] = fma(w_rho, __ldg(q + (P.c_spec + n) * B.st_n32), Yg[n]);
                 }
 #pragma unroll
                 for (int dir = 0; dir < 3; ++dir) {
-                  vel_g[dir] = fma(cw, __ldg(q + (long long)(P.c_mom + dir) * B.st_ns), vel_g[dir]);
+                  vel_g[dir] = fma(cw, __ldg(q + (P.c_mom + dir) * B.st_n32), vel_g[dir]);
                 }
-                Tg = fma(cw, __ldg(q + (long long)P.c_T * B.st_ns), Tg);
+                Tg = fma(cw, __ldg(q + P.c_T * B.st_n32), Tg);
               }
             }
           }
@@ -281,22 +279,21 @@ __device__ __forceinline__ void update_one(const KParams& P, int b, long long s,
         break;
       }
     }
-    double* q = B.sr + (long long)(ijkc[0] - B.sr_lo[0]) + (long long)(ijkc[1] - B.sr_lo[1]) * B.sr_js +
-                (long long)(ijkc[2] - B.sr_lo[2]) * B.sr_ks;
+    double* q = B.sr + ((ijkc[0] - B.sr_lo[0]) + (ijkc[1] - B.sr_lo[1]) * B.sr_j32 + (ijkc[2] - B.sr_lo[2]) * B.sr_k32);
     if (P.f.mom_trans) {
 #pragma unroll
       for (int dir = 0; dir < 3; ++dir) {
-        atomicAdd(q + (long long)(P.s_mom + dir) * B.sr_ns, __dmul_rn(cur_coef, src.mom[dir]));
+        atomicAdd(q + (P.s_mom + dir) * B.sr_n32, __dmul_rn(cur_coef, src.mom[dir]));
       }
     }
     if (P.f.mass_trans) {
-      atomicAdd(q + (long long)P.s_rho * B.sr_ns, __dmul_rn(cur_coef, src.mass));
+      atomicAdd(q + P.s_rho * B.sr_n32, __dmul_rn(cur_coef, src.mass));
 #pragma unroll
       for (int spf = 0; spf < NF; ++spf) {
-        atomicAdd(q + (long long)(P.s_spec + spf) * B.sr_ns, __dmul_rn(cur_coef, src.Ydot[spf]));
+        atomicAdd(q + (P.s_spec + spf) * B.sr_n32, __dmul_rn(cur_coef, src.Ydot[spf]));
       }
     }
-    atomicAdd(q + (long long)P.s_eng * B.sr_ns, __dmul_rn(cur_coef, src.eng));
+    atomicAdd(q + P.s_eng * B.sr_n32, __dmul_rn(cur_coef, src.eng));
     // move (SprayParticles.cpp:444-476)
     if (P.do_move && !P.f.fixed_parts && id > 0) {
 #pragma unroll
@@ -360,7 +357,8 @@ __device__ __forceinline__ void flush_counters(const KParams& P, Counters& c)
 #define PMP_FP64_MIN_BLOCKS 5  /* 96 registers: 5 CTAs of 128 per SM (measured best) */
 #endif
 #ifndef PMP_MIXED_MIN_BLOCKS
-#define PMP_MIXED_MIN_BLOCKS 4
+#define PMP_MIXED_MIN_BLOCKS 8  /* 64 registers: 8 CTAs of 128 per SM; the spills cost less than the
+                                   latency the extra warps hide (measured against 4, 6, 7) */
 #endif
 
 template <int NS, int NF, int BLOCK>

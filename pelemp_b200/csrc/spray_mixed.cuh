@@ -96,6 +96,14 @@ __device__ __forceinline__ float flog1p(float x)
   return flog(1.f + x);
 }
 
+// 1/x in FP64 from the FP32 reciprocal estimate and one Newton step (relative
+// error ~2^-44): for the gas-state gather, whose result feeds FP32 physics
+__device__ __forceinline__ double drcp_from_f(double x)
+{
+  const double r = (double)__fdividef(1.f, (float)x);
+  return r * fma(-x, r, 2.);
+}
+
 // cbrt in FP64 from an FP32 estimate and one Newton step (error ~1e-16)
 __device__ __forceinline__ double dcbrt_from_f(double a)
 {
