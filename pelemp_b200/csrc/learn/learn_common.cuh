@@ -238,7 +238,7 @@ __device__ __forceinline__ bool learn_teacher(
 // calcVaporState's closed-form part in FP32 (Drag.H:232-288): fuel latent
 // heats, saturation pressures, Raoult vapor mole fractions, surface vapor mass
 // fractions and the Spalding number B_M, for the learned kernel.
-template <int NS, int NF>
+template <int NS, int NF, bool FF>
 __device__ __forceinline__ void vapor_state_f(
   const DevMechF& m, const DevFuelF& ff, const DevFuel& fdat, const GasF<NS>& g, const float* cBoilT,
   float Tp_f, const double* Y_part, float* L_fuel, float* X_vapor, float* Yfv, float& sumXVap, float& B_M)
@@ -248,14 +248,14 @@ __device__ __forceinline__ void vapor_state_f(
   float mw_part = 0.f;
 #pragma unroll
   for (int spf = 0; spf < NF; ++spf) {
-    mw_part += (float)Y_part[spf] * m.inv_mw_kg[fdat.indx[spf]];
+    mw_part += (float)Y_part[spf] * m.inv_mw_kg[fuel_sp<FF>(fdat, spf)];
   }
   mw_part = fdiv(1.f, mw_part);
   float mbar_vap = 0.f;
   sumXVap = 0.f;
 #pragma unroll
   for (int spf = 0; spf < NF; ++spf) {
-    const int fspec = fdat.indx[spf];
+    const int fspec = fuel_sp<FF>(fdat, spf);
     const float mw_fuel = m.mw_kg[fspec];
     const float Tp = fminf(Tp_f, 0.99f * cBoilT[spf]);
     L_fuel[spf] = hf(m, fspec, Tp_f) + ff.latent[spf] - ff.cp[spf] * (Tp - ff.ref_T);
@@ -265,7 +265,7 @@ __device__ __forceinline__ void vapor_state_f(
     } else {
       pres_sat = ff.psat_d[spf] * fexp2((ff.psat_a[spf] - fdiv(ff.psat_b[spf], Tp + ff.psat_c[spf])) * 3.32192809f);
     }
-    const float X_fluid = fsel(g.Y, fdat.dep[spf]) * g.mw_mix * m.inv_mw_kg[fspec];
+    const float X_fluid = fsel(g.Y, dep_sp<FF>(fdat, spf)) * g.mw_mix * m.inv_mw_kg[fspec];
     X_vapor[spf] = 0.f;
     if (pres_sat > X_fluid * g.p) {
       const float Xv = fdiv((float)Y_part[spf] * mw_part * m.inv_mw_kg[fspec] * pres_sat, g.p);
@@ -280,9 +280,9 @@ __device__ __forceinline__ void vapor_state_f(
   for (int spf = 0; spf < NF; ++spf) {
     Yfv[spf] = 0.f;
     if (X_vapor[spf] > 0.f) {
-      Yfv[spf] = X_vapor[spf] * m.mw_kg[fdat.indx[spf]] * inv_totalmwx;
+      Yfv[spf] = X_vapor[spf] * m.mw_kg[fuel_sp<FF>(fdat, spf)] * inv_totalmwx;
       sumYVap += Yfv[spf];
-      sumYfFluid += fsel(g.Y, fdat.dep[spf]);
+      sumYfFluid += fsel(g.Y, dep_sp<FF>(fdat, spf));
     }
   }
   B_M = fminf(20.f, fdiv(sumYVap - sumYfFluid, fmaxf(1.E-15f, 1.f - sumYVap)));

@@ -62,6 +62,10 @@ struct DevFuel {
 
 // FP32 copies of the tables for the mixed-precision and learned forms
 // (converted once on the host; scaled where the physics always scales them)
+// FP32 tables of the mixed and learned forms.  Species are stored in the
+// order spec_perm of KParams: when every fuel deposits into its own gas
+// species (dep_indx == indx), the fuels' gas species come first (fuel f is
+// species f), so that the kernels index them at compile time (fuel_first).
 struct DevMechF {
   float mw_kg[kMaxSpec];
   float inv_mw_kg[kMaxSpec];
@@ -149,6 +153,10 @@ struct KParams {
   const long long* box_begin;  // nboxes + 1 slot offsets
   long long* fb_list;          // slots handed to the FP64 fallback kernel
   DevStatus* status;
+  // mixed / learned forms: species k of DevMechF (and of their gas-state
+  // gather) is mechanism species spec_perm[k]; fuel_first as in DevMechF
+  int spec_perm[kMaxSpec];
+  int fuel_first;
 };
 
 }  // namespace pmp

@@ -73,6 +73,8 @@ struct pmp_spray {
   pmp::DevMech dmech;
   pmp::DevFuel dfuel;
   pmp::DevMechF dmechf;
+  int spec_perm[PMP_MAX_SPEC];  // species order of dmechf (see DevMechF)
+  int fuel_first = 0;
   pmp::DevFuelF dfuelf;
   // per-box staged droplets (before packing)
   std::vector<pmp::BoxStore> staged;

@@ -675,7 +675,7 @@ static void build_mlp(const std::vector<float>& p, MlpSmem& S)
 #define PMP_LEARNED_MIN_BLOCKS 4
 #endif
 
-template <int NS, int NF, int BLOCK>
+template <int NS, int NF, int BLOCK, bool FF>
 __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
   spray_update_learned(const __grid_constant__ KParams P, const __grid_constant__ LearnParams L)
 {
@@ -799,7 +799,7 @@ __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
                 const double w_rho = cw * drcp_from_f(cur_rho);
 #pragma unroll
                 for (int n = 0; n < NS; ++n) {
-                  Yg[n] = fma(w_rho, __ldg(q + (P.c_spec + n) * B.st_n32), Yg[n]);
+                  Yg[n] = fma(w_rho, __ldg(q + (P.c_spec + P.spec_perm[n]) * B.st_n32), Yg[n]);
                 }
 #pragma unroll
                 for (int dir = 0; dir < 3; ++dir) {
@@ -867,7 +867,7 @@ __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
       float L_fuel[NF], X_vapor[NF], Yfv[NF];
       float sumXVap, B_M;
       bool in_range = true;
-      vapor_state_f<NS, NF>(m, ff, fdat, g, cBoilT, (float)T_part, Y_part, L_fuel, X_vapor, Yfv, sumXVap, B_M);
+      vapor_state_f<NS, NF, FF>(m, ff, fdat, g, cBoilT, (float)T_part, Y_part, L_fuel, X_vapor, Yfv, sumXVap, B_M);
       {
         double slip = 0.;
 #pragma unroll
@@ -880,8 +880,8 @@ __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
         xin[1] = (float)T_part;
         xin[2] = g.T;
         xin[3] = flog(g.p * (float)(1. / (kPatmCgs * kPresConv)));
-        xin[4] = fsel(g.Y, fdat.dep[0]);
-        xin[5] = NF > 1 ? fsel(g.Y, fdat.dep[NF > 1 ? 1 : 0]) : 0.f;
+        xin[4] = fsel(g.Y, dep_sp<FF>(fdat, 0));
+        xin[5] = NF > 1 ? fsel(g.Y, dep_sp<FF>(fdat, NF > 1 ? 1 : 0)) : 0.f;
         xin[6] = flog((float)(g.rho * slip * dia_part) + 1e-12f);
         xin[7] = (float)Y_part[0];
         xin[8] = Yfv[0];
@@ -1073,7 +1073,7 @@ __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
       for (int spf = 0; spf < NF; ++spf) {
         const double midot = (Y_part[spf] * pmass - Y[spf] * startmass) * inv_dtf;
         src.Ydot[spf] = num_ppp * midot;
-        src.eng += num_ppp * midot * (double)hf(m, fdat.dep[spf], T_h);
+        src.eng += num_ppp * midot * (double)hf(m, dep_sp<FF>(fdat, spf), T_h);
         Y[spf] = Y_part[spf];
       }
 #pragma unroll
@@ -1261,7 +1261,11 @@ static int launch_learned_t(pmp_spray* h, const KParams& P, const LearnParams& L
       k_learn_audit<NS, NF><<<nb(n, 128), 128, 0, st>>>(P, LP, h->total);
     }
   }
-  spray_update_learned<NS, NF, kBlock><<<h->ncta, kBlock, 0, st>>>(P, LP);
+  if (P.fuel_first) {
+    spray_update_learned<NS, NF, kBlock, true><<<h->ncta, kBlock, 0, st>>>(P, LP);
+  } else {
+    spray_update_learned<NS, NF, kBlock, false><<<h->ncta, kBlock, 0, st>>>(P, LP);
+  }
   return PMP_OK;
 }
 

@@ -16,7 +16,11 @@ int launch_mixed(int ns, int nf, const KParams& P, int ncta, int block, cudaStre
   }
 #define PMP_MIXED_CASE(S, F)                                          \
   if (ns == S && nf == F) {                                           \
-    spray_update_mixed<S, F, 128><<<ncta, 128, 0, st>>>(P);           \
+    if (P.fuel_first) {                                                \
+      spray_update_mixed<S, F, 128, true><<<ncta, 128, 0, st>>>(P);    \
+    } else {                                                           \
+      spray_update_mixed<S, F, 128, false><<<ncta, 128, 0, st>>>(P);   \
+    }                                                                  \
     return PMP_OK;                                                    \
   }
   PMP_MIXED_CASE(3, 1)

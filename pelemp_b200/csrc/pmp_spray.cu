@@ -253,32 +253,55 @@ int build_device_tables(pmp_spray* h)
   F.mass_trans = d.mass_trans;
   F.mom_trans = d.mom_trans;
   F.fixed_parts = d.fixed_parts;
-  // FP32 tables of the mixed / learned forms
+  // FP32 tables of the mixed / learned forms, fuels' species first when
+  // every fuel deposits into its own species
+  h->fuel_first = 1;
+  for (int f = 0; f < NF; ++f) {
+    h->fuel_first = h->fuel_first && d.dep_indx[f] == d.indx[f];
+  }
+  {
+    int k = 0;
+    if (h->fuel_first) {
+      for (int f = 0; f < NF; ++f) {
+        h->spec_perm[k++] = d.indx[f];
+      }
+    }
+    for (int n = 0; n < NS; ++n) {
+      bool fuel = false;
+      for (int f = 0; f < NF; ++f) {
+        fuel = fuel || (h->fuel_first && d.indx[f] == n);
+      }
+      if (!fuel) {
+        h->spec_perm[k++] = n;
+      }
+    }
+  }
   pmp::DevMechF& mf = h->dmechf;
   pmp::DevFuelF& ff = h->dfuelf;
   memset(&mf, 0, sizeof(mf));
   memset(&ff, 0, sizeof(ff));
   for (int k = 0; k < NS; ++k) {
-    mf.mw_kg[k] = (float)m.mw_kg[k];
-    mf.inv_mw_kg[k] = (float)(1. / m.mw_kg[k]);
-    mf.inv_mw_g[k] = (float)(1. / m.mw_g[k]);
-    mf.mw_g[k] = (float)m.mw_g[k];
-    mf.ru_w_eng[k] = (float)(m.ru_w[k] * pmp::kEngConv);
+    const int s = h->spec_perm[k];
+    mf.mw_kg[k] = (float)m.mw_kg[s];
+    mf.inv_mw_kg[k] = (float)(1. / m.mw_kg[s]);
+    mf.inv_mw_g[k] = (float)(1. / m.mw_g[s]);
+    mf.mw_g[k] = (float)m.mw_g[s];
+    mf.ru_w_eng[k] = (float)(m.ru_w[s] * pmp::kEngConv);
     for (int n = 0; n < 5; ++n) {
-      mf.cp[k][n] = (float)m.cp[k][n];
+      mf.cp[k][n] = (float)m.cp[s][n];
     }
     for (int n = 0; n < 6; ++n) {
-      mf.hc[k][n] = (float)m.hc[k][n];
+      mf.hc[k][n] = (float)m.hc[s][n];
     }
     for (int n = 0; n < 4; ++n) {
-      mf.mu6[k][n] = (float)(6. * m.mu[k][n]);
-      mf.lam4[k][n] = (float)(0.25 * m.lam[k][n]);
+      mf.mu6[k][n] = (float)(6. * m.mu[s][n]);
+      mf.lam4[k][n] = (float)(0.25 * m.lam[s][n]);
     }
   }
   for (int f = 0; f < NF; ++f) {
     for (int j = 0; j < NS; ++j) {
       for (int n = 0; n < 4; ++n) {
-        mf.dbinm[f][j][n] = (float)(-m.dbin[f][j][n]);
+        mf.dbinm[f][j][n] = (float)(-m.dbin[f][h->spec_perm[j]][n]);
       }
     }
     ff.cp[f] = (float)d.cp[f];
@@ -589,6 +612,10 @@ int prepare_update_impl(
   P.m = h->dmech;
   P.f = h->dfuel;
   P.mf = h->dmechf;
+  for (int k = 0; k < PMP_MAX_SPEC; ++k) {
+    P.spec_perm[k] = k < h->nspec ? h->spec_perm[k] : k;
+  }
+  P.fuel_first = h->fuel_first;
   P.ff = h->dfuelf;
   const long long T = h->total;
   for (int d = 0; d < 3; ++d) {

@@ -16,7 +16,7 @@
 // Kernels
 //  - spray_update_fp64<NS,NF,BLOCK>: plain FP64, one thread per droplet, CTA
 //    -> (box, first slot) from the work map;
-//  - spray_update_mixed<NS,NF,BLOCK>: mixed precision; droplets entering the
+//  - spray_update_mixed<NS,NF,BLOCK,FF>: mixed precision; droplets entering the
 //    call with d < 2 um are appended to the fallback list instead;
 //  - spray_update_fp64_list<NS,NF,BLOCK>: plain FP64 over the fallback list
 //    (grid-stride; the list length is read on the device).
@@ -47,7 +47,7 @@ __device__ __forceinline__ void cell_of(const KParams& P, const double* pos, dou
 }
 
 // Returns false if the droplet was handed to the fallback list (MIXED only).
-template <int NS, int NF, Form FORM>
+template <int NS, int NF, Form FORM, bool FF = false>
 __device__ __forceinline__ void update_one(const KParams& P, int b, long long s, Counters& c)
 {
   const BoxEntry& B = P.boxes[b];
@@ -228,7 +228,7 @@ __device__ __forceinline__ void update_one(const KParams& P, int b, long long s,
                 const double w_rho = cw * drcp_from_f(cur_rho);
 #pragma unroll
                 for (int n = 0; n < NS; ++n) {
-                  Yg[n] = fma(w_rho, __ldg(q + (P.c_spec + n) * B.st_n32), Yg[n]);
+                  Yg[n] = fma(w_rho, __ldg(q + (P.c_spec + P.spec_perm[n]) * B.st_n32), Yg[n]);
                 }
 #pragma unroll
                 for (int dir = 0; dir < 3; ++dir) {
@@ -266,7 +266,7 @@ __device__ __forceinline__ void update_one(const KParams& P, int b, long long s,
       for (int spf = 0; spf < NF; ++spf) {
         cBoilT[spf] = fminf(P.ff.critT[spf], fdiv(1.f, fmaf(lp, P.ff.hb[spf], P.ff.inv_boilT[spf])));
       }
-      nsub = spray_source_mixed<NS, NF>(P, P.sub_dt, g, cBoilT, vel, T, dia, Y, num_ppp, id, src);
+      nsub = spray_source_mixed<NS, NF, FF>(P, P.sub_dt, g, cBoilT, vel, T, dia, Y, num_ppp, id, src);
     }
     c.sub += 1;
     c.inner += static_cast<unsigned long long>(nsub);
@@ -373,14 +373,14 @@ __global__ void __launch_bounds__(BLOCK, PMP_FP64_MIN_BLOCKS) spray_update_fp64(
   flush_counters(P, c);
 }
 
-template <int NS, int NF, int BLOCK>
+template <int NS, int NF, int BLOCK, bool FF>
 __global__ void __launch_bounds__(BLOCK, PMP_MIXED_MIN_BLOCKS) spray_update_mixed(const __grid_constant__ KParams P)
 {
   const int b = P.cta_box[blockIdx.x];
   const long long s = P.cta_start[blockIdx.x] + threadIdx.x;
   Counters c;
   if (s < P.boxes[b].p_end) {
-    update_one<NS, NF, Form::MIXED>(P, b, s, c);
+    update_one<NS, NF, Form::MIXED, FF>(P, b, s, c);
   }
   flush_counters(P, c);
 }

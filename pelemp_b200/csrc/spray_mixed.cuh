@@ -118,6 +118,20 @@ __device__ __forceinline__ float fcubic(const float* c, float x)
   return fmaf(fmaf(fmaf(c[3], x, c[2]), x, c[1]), x, c[0]);
 }
 
+// Species index (in the DevMechF order) of fuel spf's liquid and of the gas
+// species it deposits into: fuel spf itself when the fuels come first
+template <bool FF>
+__device__ __forceinline__ int fuel_sp(const DevFuel& f, int spf)
+{
+  return FF ? spf : f.indx[spf];
+}
+
+template <bool FF>
+__device__ __forceinline__ int dep_sp(const DevFuel& f, int spf)
+{
+  return FF ? spf : f.dep[spf];
+}
+
 template <int N>
 __device__ __forceinline__ float fsel(const float (&a)[N], int i)
 {
@@ -204,7 +218,7 @@ struct SrcD {
 };
 
 // calculateSpraySource with FP32 physics and FP64 state (see the file header).
-template <int NS, int NF>
+template <int NS, int NF, bool FF>
 __device__ __forceinline__ int spray_source_mixed(
   const KParams& P, double flow_dt, const GasF<NS>& g, const float* cBoilT, double* vel_io,
   double& T_io, double& dia_io, double* Y_io, double num_ppp, int& id, SrcD<NF>& src)
@@ -263,7 +277,7 @@ __device__ __forceinline__ int spray_source_mixed(
       const float yp = (float)Y_part[spf];
       Tboil += Y_part[spf] * (double)cBoilT[spf];
       cp_part += yp * ff.cp[spf];
-      mw_part += yp * m.inv_mw_kg[fdat.indx[spf]];
+      mw_part += yp * m.inv_mw_kg[fuel_sp<FF>(fdat, spf)];
     }
     mw_part = fdiv(1.f, mw_part);
     const float delT = fmaxf(g.T - Tp_f, 0.f);
@@ -283,7 +297,7 @@ __device__ __forceinline__ int spray_source_mixed(
       float mbar_vap = 0.f;
 #pragma unroll
       for (int spf = 0; spf < NF; ++spf) {
-        const int fspec = fdat.indx[spf];
+        const int fspec = fuel_sp<FF>(fdat, spf);
         const float mw_fuel = m.mw_kg[fspec];
         const float Tp = fminf(Tp_f, 0.99f * cBoilT[spf]);
         const float part_latent = hf(m, fspec, Tp_f) + ff.latent[spf] - ff.cp[spf] * (Tp - ff.ref_T);
@@ -294,7 +308,7 @@ __device__ __forceinline__ int spray_source_mixed(
         } else {
           pres_sat = ff.psat_d[spf] * fexp2((ff.psat_a[spf] - fdiv(ff.psat_b[spf], Tp + ff.psat_c[spf])) * 3.32192809f);
         }
-        const float X_fluid = fsel(g.Y, fdat.dep[spf]) * g.mw_mix * m.inv_mw_kg[fspec];
+        const float X_fluid = fsel(g.Y, dep_sp<FF>(fdat, spf)) * g.mw_mix * m.inv_mw_kg[fspec];
         if (pres_sat > X_fluid * g.p) {
           const float Xl = (float)Y_part[spf] * mw_part * m.inv_mw_kg[fspec];
           const float Xv = fdiv(Xl * pres_sat, g.p);
@@ -312,10 +326,10 @@ __device__ __forceinline__ int spray_source_mixed(
 #pragma unroll
       for (int spf = 0; spf < NF; ++spf) {
         if (X_vapor[spf] > 0.f) {
-          const int fspec = fdat.indx[spf];
+          const int fspec = fuel_sp<FF>(fdat, spf);
           const float Yfv = X_vapor[spf] * m.mw_kg[fspec] * inv_totalmwx;
           sumYVap += Yfv;
-          const float gasY = fsel(g.Y, fdat.dep[spf]);
+          const float gasY = fsel(g.Y, dep_sp<FF>(fdat, spf));
           sumYfFluid += gasY;
           const float Ysk = Yfv + rule * (gasY - Yfv);
           fput(Y_skin, fspec, Ysk);
@@ -378,7 +392,7 @@ __device__ __forceinline__ int spray_source_mixed(
         const float inv_rt = fdiv(1.f, (float)kRuCgs * T_skin);
 #pragma unroll
         for (int f = 0; f < NF; ++f) {
-          const int i = fdat.indx[f];
+          const int i = fuel_sp<FF>(fdat, f);
           float term1 = 0.f;
           float term2 = 0.f;
 #pragma unroll
@@ -443,7 +457,7 @@ __device__ __forceinline__ int spray_source_mixed(
         const float inv_sumX = fdiv(1.f, sumXVap);
 #pragma unroll
         for (int spf = 0; spf < NF; ++spf) {
-          const int fspec = fdat.indx[spf];
+          const int fspec = fuel_sp<FF>(fdat, spf);
           Ddiag[spf] *= mw_skin * m.inv_mw_kg[fspec] * (float)kRhodConv * (X_vapor[spf] * inv_sumX);
           rhoDtotal += Ddiag[spf];
           const float ysk = fsel(Y_skin, fspec);
@@ -552,7 +566,7 @@ __device__ __forceinline__ int spray_source_mixed(
   for (int spf = 0; spf < NF; ++spf) {
     const double midot = (Y_part[spf] * pmass - Y_io[spf] * startmass) * inv_dtf;
     src.Ydot[spf] = num_ppp * midot;
-    src.eng += num_ppp * midot * (double)hf(m, fdat.dep[spf], T_h);
+    src.eng += num_ppp * midot * (double)hf(m, dep_sp<FF>(fdat, spf), T_h);
     Y_io[spf] = Y_part[spf];
   }
   vel_io[0] = vel_part[0];
