@@ -43,6 +43,7 @@ struct LearnParams {
   long long audit_stride;
   long long audit_offset;
   double* audit;  // [0] count, [1..5] sum of squared errors, [6..10] sum of squared targets
+  int ncta;       // items of the CTA map
 };
 
 struct LearnState {
@@ -671,16 +672,25 @@ static void build_mlp(const std::vector<float>& p, MlpSmem& S)
 // ---------------------------------------------------------------------------
 // the learned update kernel
 
-#ifndef PMP_LEARNED_MIN_BLOCKS
-#define PMP_LEARNED_MIN_BLOCKS 4
+// 256 threads, 2 CTAs per SM (128 registers): one copy of the weights in
+// shared memory serves 8 warps (measured against 128 threads x 4 CTAs and
+// 256 x 3 or 4 CTAs, whose register caps spill more than they gain)
+#ifndef PMP_LEARNED_THREADS
+#define PMP_LEARNED_THREADS 256
 #endif
+#ifndef PMP_LEARNED_MIN_BLOCKS
+#define PMP_LEARNED_MIN_BLOCKS 2
+#endif
+constexpr int kLearnThreads = PMP_LEARNED_THREADS;  // threads per CTA, a multiple of kBlock
 
 template <int NS, int NF, int BLOCK, bool FF>
 __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
   spray_update_learned(const __grid_constant__ KParams P, const __grid_constant__ LearnParams L)
 {
-  __shared__ MlpSmem S;
-  __shared__ MlpWarpScratch WS[BLOCK / 32];
+  // dynamic shared memory: the network's weights, then one scratch per warp
+  extern __shared__ __align__(16) unsigned char learn_smem[];
+  MlpSmem& S = *reinterpret_cast<MlpSmem*>(learn_smem);
+  MlpWarpScratch* WS = reinterpret_cast<MlpWarpScratch*>(learn_smem + sizeof(MlpSmem));
   {
     const int4* src = reinterpret_cast<const int4*>(L.mlp);
     int4* dst = reinterpret_cast<int4*>(&S);
@@ -693,11 +703,14 @@ __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
   const DevMechF& m = P.mf;
   const DevFuelF& ff = P.ff;
   const DevFuel& fdat = P.f;
-  const int b = P.cta_box[blockIdx.x];
+  // each group of kBlock threads takes one kBlock-slot item of the CTA map
+  const int item = blockIdx.x * (BLOCK / kBlock) + threadIdx.x / kBlock;
+  const bool item_ok = item < L.ncta;
+  const int b = item_ok ? P.cta_box[item] : 0;
   const BoxEntry& B = P.boxes[b];
-  const long long s = P.cta_start[blockIdx.x] + threadIdx.x;
+  const long long s = item_ok ? P.cta_start[item] + threadIdx.x % kBlock : 0;
   Counters c;
-  bool valid = s < B.p_end;
+  bool valid = item_ok && s < B.p_end;
   int id = valid ? P.parts.id[s] : 0;
   valid = valid && id > 0;
   double dia = valid ? P.parts.rd[PMP_PSTATE_DIA][s] : 1e-5;
@@ -1261,11 +1274,19 @@ static int launch_learned_t(pmp_spray* h, const KParams& P, const LearnParams& L
       k_learn_audit<NS, NF><<<nb(n, 128), 128, 0, st>>>(P, LP, h->total);
     }
   }
-  if (P.fuel_first) {
-    spray_update_learned<NS, NF, kBlock, true><<<h->ncta, kBlock, 0, st>>>(P, LP);
-  } else {
-    spray_update_learned<NS, NF, kBlock, false><<<h->ncta, kBlock, 0, st>>>(P, LP);
+  constexpr int per = kLearnThreads / kBlock;
+  const int grid = (h->ncta + per - 1) / per;
+  constexpr size_t smem = sizeof(MlpSmem) + sizeof(MlpWarpScratch) * (kLearnThreads / 32);
+  static_assert(sizeof(MlpSmem) % 16 == 0, "warp scratch must stay 16-byte aligned");
+  auto kern = P.fuel_first ? spray_update_learned<NS, NF, kLearnThreads, true>
+                           : spray_update_learned<NS, NF, kLearnThreads, false>;
+  if (smem > 48 * 1024) {
+    const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) {
+      return PMP_ERR_CUDA;
+    }
   }
+  kern<<<grid, kLearnThreads, smem, st>>>(P, LP);
   return PMP_OK;
 }
 
@@ -1283,6 +1304,7 @@ int launch_learned(pmp_spray* h, const KParams& P, cudaStream_t st)
   LP.norm = L->norm;
   LP.mlp = L->d_mlp;
   LP.audit = L->d_audit;
+  LP.ncta = h->ncta;
   LP.audit_stride = 0;
   if (L->audit_fraction > 0.) {
     LP.audit_stride = std::max(1LL, (long long)llround(1.0 / L->audit_fraction));
