@@ -310,6 +310,54 @@ int pmp_spray_update_static(
   pmp_error_info* err);
 
 /* ---------------------------------------------------------------------------
+ * The operations on either side of the update, on the device. */
+
+/* SprayParticleContainer::estTimestep (SprayParticles.cpp:89-140): min over
+ * the droplets of cfl / max_d(|u_d| / dx_d) (1e50 for a droplet at rest), -1
+ * for any dead droplet still held (the reference's reduction gives dead
+ * droplets -1 too; pmp_spray_redistribute drops them), then
+ * min(dt, cfl dx_0 / max_jet_vel) when max_jet_vel > 0 (the injection jets'
+ * bound).  -1 with fixed_parts; DBL_MAX with no droplets.  cfl is
+ * particles.cfl. */
+int pmp_spray_est_timestep(pmp_spray* h, double cfl, double max_jet_vel,
+                           double* dt, void* stream);
+
+/* computeDerivedVars (SprayDerive.cpp:9-155): adds into vars[b] components
+ * start_indx + (0 spray_mass, 1 spray_density, 2 spray_num, 3 spray_vol,
+ * 4 spray_surf_area, 5 spray_vol_frac, 6 d10, 7 d32, 8 wall_film_hght,
+ * 9 wall_film_mass, 10 spray_temp, 11 num_parcels, 12-14 spray_x/y/z_vel,
+ * then 15.. spray_mass_<fuel> per fuel when with_species and F > 1) from the
+ * droplets of box b at the cell holding each, then divides d10 by the number,
+ * d32 by the surface, temperature and velocity by the mass where the divisor
+ * is non-zero, over every cell of the view.  The caller zeroes vars first, as
+ * the reference's callers do.  PMP_ERR_SOURCE_BOX if a view does not hold a
+ * droplet's cell. */
+int pmp_spray_derive(pmp_spray* h, const pmp_box_view* vars, int nboxes,
+                     int start_indx, int with_species, void* stream);
+
+/* transferSource (SprayParticles.H:250-295) on level 0: SumBoundary of the
+ * temporary source with the domain's periodicity (each ghost cell adds into
+ * the valid cell of the box owning its wrapped location; ghost cells keep
+ * their values), then act += tmp over each box grown by
+ * min(act_ghosts, source_ghosts): all components when tmp and act have the
+ * same count, else addSpraySrc's mapping (momentum, density, energy, and
+ * fuel f's source into species dep_indx[f]); finally tmp = 0 everywhere.
+ * tmp views cover each box grown by source_ghosts. */
+int pmp_spray_transfer_source(pmp_spray* h, const pmp_box_view* tmp_source,
+                              const pmp_box_view* act_source, int nboxes,
+                              int source_ghosts, int act_ghosts, void* stream);
+
+/* Re-bin the droplets after a move, what AMReX's Redistribute does for this
+ * container (AMReX is not in the reference tree; the rule is restated here):
+ * positions are wrapped across periodic faces (while x >= phi: x -= L; while
+ * x < plo: x += L), each droplet goes to the box whose valid region holds its
+ * cell floor((x - plo)/dx), and droplets with id <= 0 or in no box are
+ * dropped (*removed, may be NULL, receives their count).  Afterwards every
+ * box's droplets are in cell order and that order is the box's caller order
+ * for pmp_spray_get_particles. */
+int pmp_spray_redistribute(pmp_spray* h, long long* removed, void* stream);
+
+/* ---------------------------------------------------------------------------
  * Launch shape of the FP64 form (the batched form).  No counterpart in the
  * reference, which launches one kernel per box and synchronises after each
  * (SprayParticles.cpp:244-248,499).  Here all boxes go in one launch; the

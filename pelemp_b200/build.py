@@ -22,7 +22,8 @@ LIB = os.path.join(PKG, "libpmpspray.so")
 SOURCES = [("pmp_spray.cu", "-fmad=false"), ("pmp_static.cu", "-fmad=false"),
            ("pmp_mixed.cu", "-fmad=true"), ("pmp_learn.cu", "-fmad=true"),
            ("pmp_batch.cu", "-fmad=false"), ("batch/pmp_batch_b64.cu", "-fmad=false"),
-           ("batch/pmp_batch_b128.cu", "-fmad=false"), ("batch/pmp_batch_b256.cu", "-fmad=false")]
+           ("batch/pmp_batch_b128.cu", "-fmad=false"), ("batch/pmp_batch_b256.cu", "-fmad=false"),
+           ("pmp_mesh.cu", "-fmad=false")]
 HEADERS = ["pmp_device.cuh", "pmp_handle.h", "spray_fp64.cuh", "spray_mixed.cuh",
            "spray_kernels.cuh", "learn/learn_common.cuh", "learn/mlp_mma.cuh",
            "batch/batch_kernels.cuh",

@@ -157,6 +157,47 @@ public:
     return s;
   }
 
+  /// estTimestep (SprayParticles.cpp:89-140); cfl is particles.cfl, max_jet_vel
+  /// the fastest injection jet (0 without jets).  Single process: the
+  /// ReduceRealMin over ranks is the caller's.
+  Real estTimestep(int /*level*/, Real cfl, Real max_jet_vel = 0., void* stream = nullptr)
+  {
+    double dt = 0.;
+    check(pmp_spray_est_timestep(h_, cfl, max_jet_vel, &dt, stream));
+    return dt;
+  }
+
+  /// computeDerivedVars (SprayDerive.cpp:9-155): one view of mf_var per box.
+  void computeDerivedVars(
+    const std::vector<pmp_box_view>& mf_var, int /*level*/, int start_indx, bool derive_plot_species = true,
+    void* stream = nullptr)
+  {
+    check(pmp_spray_derive(h_, mf_var.data(), static_cast<int>(mf_var.size()), start_indx,
+                           derive_plot_species ? 1 : 0, stream));
+  }
+
+  /// transferSource (SprayParticles.H:250-295), level 0: fold the ghost
+  /// deposits of tmpSource, add into actSource, zero tmpSource.
+  void transferSource(
+    int source_ghosts, int level, const std::vector<pmp_box_view>& tmpSource,
+    const std::vector<pmp_box_view>& actSource, int act_ghosts, void* stream = nullptr)
+  {
+    if (level != 0) {
+      throw SprayAbort(PMP_ERR_UNSUPPORTED, "SprayParticleContainer::transferSource: level 0 only", {});
+    }
+    check(pmp_spray_transfer_source(h_, tmpSource.data(), actSource.data(), static_cast<int>(tmpSource.size()),
+                                    source_ghosts, act_ghosts, stream));
+  }
+
+  /// Redistribute for this container: re-bin moved droplets to their boxes
+  /// (periodic wrap), drop dead ones; returns how many were dropped.
+  long long Redistribute(void* stream = nullptr)
+  {
+    long long removed = 0;
+    check(pmp_spray_redistribute(h_, &removed, stream));
+    return removed;
+  }
+
   pmp_spray* handle() { return h_; }
 
 private:

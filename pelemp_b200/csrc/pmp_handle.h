@@ -106,6 +106,13 @@ struct pmp_spray {
   std::vector<size_t> stage_state_n, stage_src_n;
   pmp::LearnState* learn = nullptr;
   pmp::BatchState batch;
+  // cell -> box map over the domain (pmp_mesh.cu), rebuilt when the grids or
+  // the geometry change
+  int grids_version = 0;
+  int box_map_version = -1;
+  int* d_box_map = nullptr;
+  void* mesh_scratch = nullptr;
+  size_t mesh_scratch_bytes = 0;
   int nr() const { return PMP_PSTATE_NUM(nfuel); }
   int ncomp() const { return 3 + nr(); }
 };
@@ -130,6 +137,14 @@ int run_update(
   pmp_spray* h, const pmp_box_view* state, const pmp_box_view* source, int nboxes,
   double flow_dt, int state_ghosts, int source_ghosts, int is_ghost, int do_move,
   double spray_cfl_lev, cudaStream_t st);
+// pack the staged droplets if needed
+int ensure_packed(pmp_spray* h);
+// replace the packed droplets by soa/ids (device, ncomp arrays of stride
+// box_begin.back(), taken over by the handle), sorted by box and cell; the
+// caller order of every box becomes the stored order
+int install_packed(pmp_spray* h, double* soa, int* ids, const std::vector<long long>& box_begin);
+// pmp_mesh.cu
+void mesh_free(pmp_spray* h);
 // pmp_batch.cu
 int batch_enqueue_fp64(pmp_spray* h, const KParams& P, int nboxes, cudaStream_t st);
 int graph_update(pmp_spray* h, const KParams& P, int nboxes, cudaStream_t st, int* graph_state);

@@ -337,6 +337,8 @@ int ensure_boxes_cap(pmp_spray* h, int n)
   return PMP_OK;
 }
 
+int build_cta_map(pmp_spray* h);
+
 int pack(pmp_spray* h)
 {
   if (h->packed) {
@@ -373,7 +375,14 @@ int pack(pmp_spray* h)
     }
     free_store(s);
   }
-  // CTA -> (box, first slot) map
+  return build_cta_map(h);
+}
+
+// CTA -> (box, first slot) map, box offsets and fallback list of the packed droplets
+int build_cta_map(pmp_spray* h)
+{
+  const int nb = (int)h->boxes.size();
+  const long long cap = h->total > 0 ? h->total : 1;
   std::vector<int> cb;
   std::vector<long long> cs;
   for (int b = 0; b < nb; ++b) {
@@ -741,6 +750,38 @@ int pmp::prepare_update(
   return PMP_OK;
 }
 
+int pmp::ensure_packed(pmp_spray* h) { return pack(h); }
+
+int pmp::install_packed(pmp_spray* h, double* soa, int* ids, const std::vector<long long>& box_begin)
+{
+  const int nb = (int)h->boxes.size();
+  free_packed(h);
+  h->box_begin = box_begin;
+  const long long total = box_begin[nb];
+  h->total = total;
+  h->soa = soa;
+  h->ids = ids;
+  const long long cap = total > 0 ? total : 1;
+  PMP_CUDA(h, cudaMalloc(&h->perm, sizeof(long long) * cap));
+  {
+    std::vector<long long> perm(total);
+    for (int b = 0; b < nb; ++b) {
+      for (long long o = box_begin[b]; o < box_begin[b + 1]; ++o) {
+        perm[o] = o - box_begin[b];
+      }
+    }
+    if (total > 0) {
+      PMP_CUDA(h, cudaMemcpy(h->perm, perm.data(), sizeof(long long) * total, cudaMemcpyHostToDevice));
+    }
+  }
+  for (int b = 0; b < nb; ++b) {
+    free_store(h->staged[b]);
+    h->staged[b].n = box_begin[b + 1] - box_begin[b];
+    h->box_set[b] = true;
+  }
+  return build_cta_map(h);
+}
+
 int pmp::enqueue_update(pmp_spray* h, const KParams& P, int nboxes, cudaStream_t st)
 {
   // under stream capture the timing events become event-record nodes of the graph
@@ -870,6 +911,7 @@ int pmp_spray_destroy(pmp_spray* h)
   free_packed(h);
   pmp::learn_free(h);
   pmp::batch_free(h);
+  pmp::mesh_free(h);
   for (double* p : h->stage_state) {
     cudaFree(p);
   }
@@ -1023,6 +1065,7 @@ int pmp_spray_set_geometry(pmp_spray* h, const pmp_geometry* geom)
   }
   h->geom = *geom;
   h->have_geom = true;
+  h->grids_version += 1;
   return PMP_OK;
 }
 
@@ -1037,6 +1080,7 @@ int pmp_spray_set_grids(pmp_spray* h, int nboxes, const pmp_box* boxes)
   }
   free_packed(h);
   h->boxes.assign(boxes, boxes + nboxes);
+  h->grids_version += 1;
   h->staged.assign(nboxes, BoxStore{});
   h->box_set.assign(nboxes, false);
   return PMP_OK;

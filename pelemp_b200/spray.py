@@ -49,6 +49,11 @@ _SIGS = {
     "pmp_spray_last_error": [C.c_void_p, C.POINTER(capi.ErrorInfo)],
     "pmp_spray_get_stats": [C.c_void_p, C.POINTER(capi.Stats)],
     "pmp_spray_version": [],
+    "pmp_spray_est_timestep": [C.c_void_p, C.c_double, C.c_double, C.POINTER(C.c_double), C.c_void_p],
+    "pmp_spray_derive": [C.c_void_p, C.POINTER(capi.BoxView), C.c_int, C.c_int, C.c_int, C.c_void_p],
+    "pmp_spray_transfer_source": [C.c_void_p, C.POINTER(capi.BoxView), C.POINTER(capi.BoxView), C.c_int,
+                                  C.c_int, C.c_int, C.c_void_p],
+    "pmp_spray_redistribute": [C.c_void_p, C.POINTER(C.c_longlong), C.c_void_p],
     "pmp_spray_set_launch": [C.c_void_p, C.POINTER(capi.LaunchConfig)],
     "pmp_spray_get_launch": [C.c_void_p, C.POINTER(capi.LaunchConfig)],
     "pmp_spray_autotune": [C.c_void_p, C.POINTER(capi.BoxView), C.POINTER(capi.BoxView), C.c_int,
@@ -286,6 +291,28 @@ class SprayParticleContainer:
         s = capi.Stats()
         lib().pmp_spray_get_stats(self._h, C.byref(s))
         return s
+
+    # --- around the update (SprayParticles.cpp:89-140, SprayDerive.cpp,
+    #     SprayParticles.H:250-319, Redistribute) ---------------------------
+    def est_timestep(self, cfl, max_jet_vel=0.0, stream=0):
+        dt = C.c_double(0.0)
+        self._check(lib().pmp_spray_est_timestep(self._h, cfl, max_jet_vel, C.byref(dt),
+                                                 C.c_void_p(stream)))
+        return dt.value
+
+    def compute_derived_vars(self, var_views, start_indx=0, with_species=True, stream=0):
+        self._check(lib().pmp_spray_derive(self._h, var_views, len(var_views), start_indx,
+                                           int(with_species), C.c_void_p(stream)))
+
+    def transfer_source(self, tmp_views, act_views, source_ghosts, act_ghosts, stream=0):
+        self._check(lib().pmp_spray_transfer_source(self._h, tmp_views, act_views, len(tmp_views),
+                                                    source_ghosts, act_ghosts, C.c_void_p(stream)))
+
+    def redistribute(self, stream=0):
+        """Re-bin droplets to boxes (periodic wrap, dead dropped); returns the count dropped."""
+        n = C.c_longlong(0)
+        self._check(lib().pmp_spray_redistribute(self._h, C.byref(n), C.c_void_p(stream)))
+        return n.value
 
     # --- launch shape, CUDA graph, autotuner (batched form) ---------------
     def set_launch(self, kind=capi.PMP_LAUNCH_GRID, block=128, regs=96, chunk=512, ctas_per_sm=0,
