@@ -217,6 +217,16 @@ def cpu_baseline(seconds=12.0):
                                            if have_ref else "CPU oracle, OpenMP"))}
 
 
+WORKLOAD_TEXT = {
+    "config2": "config2: {n:.0f}M two-fuel droplets (decane/heptane), 128^3 mesh as 8 boxes of 64^3, "
+               "5 gas species, dt=5e-7 s, MKD 4 sub-cycles + MK 1 sub-cycle per step",
+    "config4": "config4: {n:.0f}M heptane droplets with config-1 distributions, 256x128x128 mesh as "
+               "8 boxes of 64^3, 3 gas species, dt=1e-6 s, MKD + MK (1 sub-cycle each) per step",
+    "config5": "config5: {n:.0f}M heptane droplets with config-1 distributions, 256x128x128 mesh as "
+               "8 boxes of 64^3, 3 gas species, dt=1e-6 s, MKD + MK (1 sub-cycle each) per step",
+    "config3": "config3: {n:.0f}M heptane droplets in 256 boxes of 32^3 (256x256x128 cells) with "
+               "capped-Zipf counts, config-1 physics, MKD + MK per step, FP64",
+}
 FORM_MODE = {"fp64": 0, "mixed": 1, "learned": 2}
 FORM_NAME = {"fp64": "plain FP64", "mixed": "mixed FP32 physics / FP64 state and deposits",
              "learned": "learned surrogate (bf16 MLP on tensor cores) + FP32 physics / FP64 state"}
@@ -256,13 +266,105 @@ def droplet_errors(pa, pb, prob):
     return {"T": q(eT), "mass": q(em), "droplets": int(eT.size)}
 
 
+def bench_batched(args, world, rank, local, pg):
+    """Config 3: the FP64 form over 256 uneven boxes -- the default launch, the
+    autotuned launch (replayed from a CUDA graph) and one launch per box."""
+    import torch
+    from pelemp_b200 import capi
+    from pelemp_b200 import workloads as W
+    from pelemp_b200.spray import from_problem, views
+    prob = W.config3(total=args.droplets or 16_000_000, seed=rank, steps=args.steps)
+    nboxes = len(prob.boxes)
+    stream = torch.cuda.current_stream()
+    st = [torch.from_numpy(s).cuda() for s in prob.state]
+    st_v = views(st, [prob.grown(b, prob.state_ghosts)[0] for b in range(nboxes)])
+    src = [torch.zeros(s.shape, dtype=torch.float64, device="cuda") for s in prob.new_sources()]
+    src_v = views(src, [prob.grown(b, prob.source_ghosts)[0] for b in range(nboxes)])
+
+    def timed(sp, steps):
+        def step():
+            for s in src:
+                s.zero_()
+            n = 0
+            for do_move in (1, 0):
+                sp.update_particles(st_v, src_v, prob.flow_dt, 0.0, prob.state_ghosts, prob.source_ghosts,
+                                    0, 0, do_move, prob.spray_cfl_lev, stream.cuda_stream)
+                n += sp.stats().substeps
+            return n
+        for _ in range(args.warmup):
+            step()
+        if pg:
+            pg.barrier()
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        n = sum(step() for _ in range(steps))
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        t = ev0.elapsed_time(ev1)
+        if pg:
+            tt = torch.tensor([t], device="cuda", dtype=torch.float64)
+            pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+            t = float(tt.item())
+            nn = torch.tensor([float(n)], device="cuda", dtype=torch.float64)
+            pg.all_reduce(nn, op=pg.ReduceOp.SUM)
+            n = int(nn.item())
+        return n / (t * 1e-3), t / steps
+
+    sp = from_problem(prob, device=local)
+    v_default, ms_default = timed(sp, args.steps)
+    rep = sp.autotune(st_v, src_v, prob.flow_dt, prob.state_ghosts, prob.source_ghosts, 0, 1,
+                      prob.spray_cfl_lev, stream=stream.cuda_stream)
+    best = rep.best
+    sp.set_launch(kind=best.kind, block=best.block, regs=best.regs, chunk=best.chunk,
+                  ctas_per_sm=best.ctas_per_sm, use_graph=True)
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    v_tuned, ms_tuned = timed(sp, args.steps)
+    clocks = sampler.stop()
+    sp.set_launch(kind=capi.PMP_LAUNCH_PER_BOX)
+    v_box, ms_box = timed(sp, max(2, args.steps // 5))
+    if rank == 0:
+        line = {
+            "metric": "droplet-substeps/s", "value": v_tuned, "unit": "droplet-substeps/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_tuned,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded, numpy PCG64)",
+            "config": {"workload": WORKLOAD_TEXT["config3"].format(n=prob.n_droplets / 1e6),
+                       "droplets_per_gpu": prob.n_droplets, "boxes": nboxes,
+                       "largest_box": int(max(prob.meta["counts"])), "smallest_box": int(min(prob.meta["counts"])),
+                       "parallelism": f"replicas x{world}"},
+            "launches": {
+                "autotuned_graph": {"value": v_tuned, "ms_per_step": ms_tuned,
+                                    "shape": {"kind": best.kind, "block": best.block, "regs": best.regs,
+                                              "chunk": best.chunk},
+                                    "tuner": {"candidates": rep.ncandidates, "best_ms": rep.best_ms,
+                                              "default_ms": rep.default_ms, "per_box_ms": rep.per_box_ms}},
+                "default_one_launch": {"value": v_default, "ms_per_step": ms_default},
+                "per_box_baseline": {"value": v_box, "ms_per_step": ms_box,
+                                     "what": "one launch per box, stream synchronised after each "
+                                             "(SprayParticles.cpp:244-248,499)"},
+                "speedup_vs_per_box": v_tuned / v_box},
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    sp.close()
+    if pg:
+        pg.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--droplets", type=int, default=16_000_000)
+    ap.add_argument("--droplets", type=int, default=None,
+                    help="droplets per GPU (default: the workload's, 16M; 32M for config4)")
+    ap.add_argument("--workload", default="config2", choices=["config2", "config3", "config4", "config5"],
+                    help="config2 (default): the headline; config3: batched FP64 launch shapes; "
+                         "config4 / config5: config-1 distributions at 32M / 16M droplets")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-sample", type=int, default=100_000)
     ap.add_argument("--no-cpu", action="store_true")
@@ -294,8 +396,13 @@ def main():
     from pelemp_b200 import workloads as W
     from pelemp_b200.spray import from_problem, views
 
+    if args.workload == "config3":
+        bench_batched(args, world, rank, local, pg)
+        return
     forms = [f for f in args.forms.split(",") if f]
-    prob = W.config2(n=args.droplets, seed=rank, steps=args.steps)
+    ndrop = args.droplets or {"config2": 16_000_000, "config4": 32_000_000,
+                              "config5": 16_000_000}[args.workload]
+    prob = W.CONFIGS[args.workload](n=ndrop, seed=rank, steps=args.steps)
     nboxes = len(prob.boxes)
     ncells = int(np.prod([prob.domain_hi[d] - prob.domain_lo[d] + 1 for d in range(3)]))
     stream = torch.cuda.current_stream()
@@ -456,12 +563,11 @@ def main():
             "dtype": {"fp64": "f64", "mixed": "f32 physics, f64 state/deposits",
                       "learned": "bf16 MLP (f32 accumulate), f32 physics, f64 state/deposits"}[head],
             "data": "synthetic (seeded, numpy PCG64)",
-            "config": {"workload": "config2: 16M two-fuel droplets (decane/heptane), 128^3 mesh "
-                                   "as 8 boxes of 64^3, 5 gas species, dt=5e-7 s, MKD 4 sub-cycles "
-                                   "+ MK 1 sub-cycle per step",
+            "config": {"workload": WORKLOAD_TEXT[args.workload].format(n=prob.n_droplets / 1e6),
                        "droplets_per_gpu": prob.n_droplets, "boxes": nboxes, "form": head,
                        "form_name": FORM_NAME[head],
-                       "l2": "inputs larger than L2 (1.9 GB droplet SoA, 0.24 GB state per GPU)",
+                       "l2": "inputs larger than L2 (droplet SoA %.1f GB per GPU)" % (
+                           prob.n_droplets * 8 * (13 + prob.nfuel) / 1e9),
                        "parallelism": f"replicas x{world}"},
             "forms": forms_out,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -383,6 +383,15 @@ def config4(n=32_000_000, seed=0, steps=10):
     return prob
 
 
+def config5(n=16_000_000, seed=0, steps=10):
+    """Learned-surrogate workload: config-1 distributions (heptane droplets of
+    20 um median at 300 K in 800-1000 K air) at 16M or 64M droplets, on
+    config 4's 256x128x128 mesh of 64^3 boxes."""
+    prob = config4(n=n, seed=seed, steps=steps)
+    prob.name = "config5"
+    return prob
+
+
 def walls(n=20_000, seed=0, steps=2):
     """Non-periodic case: reflective x walls, outflow z, periodic y; 2 boxes."""
     rng = np.random.default_rng(seed)
@@ -398,4 +407,4 @@ def walls(n=20_000, seed=0, steps=2):
 
 
 CONFIGS = {"config1": config1, "config2": config2, "config3": config3,
-           "config4": config4, "walls": walls}
+           "config4": config4, "config5": config5, "walls": walls}
