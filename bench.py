@@ -311,8 +311,12 @@ def bench_batched(args, world, rank, local, pg):
             n = int(nn.item())
         return n / (t * 1e-3), t / steps
 
+    # each phase starts from the initial droplets (no re-binning inside the
+    # timed steps: the ghost widths cover the drift of warmup + steps steps)
     sp = from_problem(prob, device=local)
     v_default, ms_default = timed(sp, args.steps)
+    sp.close()
+    sp = from_problem(prob, device=local)
     rep = sp.autotune(st_v, src_v, prob.flow_dt, prob.state_ghosts, prob.source_ghosts, 0, 1,
                       prob.spray_cfl_lev, stream=stream.cuda_stream)
     best = rep.best
@@ -323,6 +327,8 @@ def bench_batched(args, world, rank, local, pg):
     time.sleep(0.3)
     v_tuned, ms_tuned = timed(sp, args.steps)
     clocks = sampler.stop()
+    sp.close()
+    sp = from_problem(prob, device=local)
     sp.set_launch(kind=capi.PMP_LAUNCH_PER_BOX)
     v_box, ms_box = timed(sp, max(2, args.steps // 5))
     if rank == 0:
