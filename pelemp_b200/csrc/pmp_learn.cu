@@ -1096,7 +1096,7 @@ __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
       T = T_part;
       dia = dia_part;
       c.sub += 1;
-      c.inner += static_cast<unsigned long long>(nsub);
+      c.inner += static_cast<unsigned>(nsub);
       // deposit into the cell holding the droplet (SprayParticles.cpp:419-441)
       const double cur_coef = __dmul_rn(-P.inv_vol, P.sub_dt) / P.flow_dt;
       bool src_ok = in_box(B.src_lo, B.src_hi, ijkc[0], ijkc[1], ijkc[2]) ||

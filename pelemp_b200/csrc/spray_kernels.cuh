@@ -29,10 +29,11 @@ namespace pmp {
 
 enum class Form { FP64 = 0, MIXED = 1 };
 
+// per-thread counts (32-bit: a thread's own counts stay far below 2^32)
 struct Counters {
-  unsigned long long sub = 0;
-  unsigned long long killed = 0;
-  unsigned long long inner = 0;
+  unsigned sub = 0;
+  unsigned killed = 0;
+  unsigned inner = 0;
 };
 
 __device__ __forceinline__ void cell_of(const KParams& P, const double* pos, double* lx, int* ijk, int* ijkc)
@@ -74,9 +75,6 @@ __device__ __forceinline__ void update_one(const KParams& P, int b, long long s,
   }
   const double num_ppp = P.parts.rd[PMP_PSTATE_NUMDENS(NF)][s];
   const double film = P.parts.rd[PMP_PSTATE_FILMHGHT(NF)][s];
-  double lx[3];
-  int ijk[3], ijkc[3];
-  cell_of(P, pos, lx, ijk, ijkc);
   int bflags[3] = {0, 0, 0};
   bool ok = true;
   if (B.at_bounds) {
@@ -86,6 +84,11 @@ __device__ __forceinline__ void update_one(const KParams& P, int b, long long s,
     }
   }
   for (int cur_iter = 0; ok && cur_iter < P.num_iter && id > 0; ++cur_iter) {
+    // cell of the droplet, from its position at the start of the sub-cycle
+    // (recomputed rather than carried, so that it is not live across the physics)
+    double lx[3];
+    int ijk[3], ijkc[3];
+    cell_of(P, pos, lx, ijk, ijkc);
     if (film > 0.) {
       set_error(P, PMP_ERR_UNSUPPORTED, b, s);
       ok = false;
@@ -269,7 +272,7 @@ __device__ __forceinline__ void update_one(const KParams& P, int b, long long s,
       nsub = spray_source_mixed<NS, NF, FF>(P, P.sub_dt, g, cBoilT, vel, T, dia, Y, num_ppp, id, src);
     }
     c.sub += 1;
-    c.inner += static_cast<unsigned long long>(nsub);
+    c.inner += static_cast<unsigned>(nsub);
     // source scatter into the cell holding the droplet (SprayParticles.cpp:419-441)
     const double cur_coef = __dmul_rn(-P.inv_vol, P.sub_dt) / P.flow_dt;
     if (!in_box(B.src_lo, B.src_hi, ijkc[0], ijkc[1], ijkc[2])) {
@@ -307,10 +310,12 @@ __device__ __forceinline__ void update_one(const KParams& P, int b, long long s,
           impose_wall(P, pos, vel, bflags);
         }
       }
-      cell_of(P, pos, lx, ijk, ijkc);
     }
-    if (P.is_ghost && !in_box(B.src_lo, B.src_hi, ijkc[0], ijkc[1], ijkc[2])) {
-      id = -1;
+    if (P.is_ghost) {
+      cell_of(P, pos, lx, ijk, ijkc);
+      if (!in_box(B.src_lo, B.src_hi, ijkc[0], ijkc[1], ijkc[2])) {
+        id = -1;
+      }
     }
   }
   if (ok) {
@@ -347,9 +352,9 @@ __device__ __forceinline__ void flush_counters(const KParams& P, Counters& c)
     c.inner += __shfl_down_sync(mask, c.inner, o);
   }
   if ((threadIdx.x & 31) == 0 && (c.sub | c.killed | c.inner)) {
-    atomicAdd(&P.status->substeps, c.sub);
-    atomicAdd(&P.status->killed, c.killed);
-    atomicAdd(&P.status->inner, c.inner);
+    atomicAdd(&P.status->substeps, (unsigned long long)c.sub);
+    atomicAdd(&P.status->killed, (unsigned long long)c.killed);
+    atomicAdd(&P.status->inner, (unsigned long long)c.inner);
   }
 }
 
