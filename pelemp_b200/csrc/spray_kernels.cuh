@@ -83,17 +83,18 @@ __device__ __forceinline__ void update_one(const KParams& P, int b, long long s,
       ok = false;
     }
   }
+  // a wall-film droplet stops the first sub-cycle (the film height never
+  // changes here, so the check is made once)
+  if (ok && P.num_iter > 0 && id > 0 && film > 0.) {
+    set_error(P, PMP_ERR_UNSUPPORTED, b, s);
+    ok = false;
+  }
   for (int cur_iter = 0; ok && cur_iter < P.num_iter && id > 0; ++cur_iter) {
     // cell of the droplet, from its position at the start of the sub-cycle
     // (recomputed rather than carried, so that it is not live across the physics)
     double lx[3];
     int ijk[3], ijkc[3];
     cell_of(P, pos, lx, ijk, ijkc);
-    if (film > 0.) {
-      set_error(P, PMP_ERR_UNSUPPORTED, b, s);
-      ok = false;
-      break;
-    }
     // trilinear_interp (SprayInterpolation.H:158-199)
     double ssv[2][3];
 #pragma unroll

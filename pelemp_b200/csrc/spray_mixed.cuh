@@ -262,8 +262,9 @@ __device__ __forceinline__ int spray_source_mixed(
   int nsub = 1;
   double pmass = PMP_PI / 6. * rho_part * (dia_part * dia_part * dia_part);
   const double startmass = pmass;
-  double eng_acc = 0.;
-  double mom_acc[3] = {0., 0., 0.};
+  // sums over the inner sub-steps in FP32; times the parcel count in FP64 at the end
+  float eng_acc = 0.f;
+  float mom_acc[3] = {0.f, 0.f, 0.f};
   float T_h = (float)T_part;
   while (isub <= nsub) {
     const float Tp_f = (float)T_part;
@@ -433,10 +434,9 @@ __device__ __forceinline__ int spray_source_mixed(
       part_vel_src[d] = drag_force_p * diff_vel[d] + ff.body_force[d];
     }
     if (fdat.mom_trans) {
-      const double nd = num_ppp * (double)drag_force;
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
-        mom_acc[d] += nd * (double)diff_vel[d];
+        mom_acc[d] = fmaf(drag_force, diff_vel[d], mom_acc[d]);
       }
       if (isub == 1) {
         nsub = min(max(nsub, static_cast<int>((float)flow_dt * drag_force_p) + 1), nSubMax);
@@ -485,7 +485,7 @@ __device__ __forceinline__ int spray_source_mixed(
         Nu_num = Nu_0;
       }
       const float conv_src = (float)PMP_PI * lambda_skin * dia_f * delT * Nu_num;
-      eng_acc += num_ppp * (double)conv_src;
+      eng_acc += conv_src;
       part_temp_src = fdiv((sumL + conv_src) * inv_pmass, cp_part);
       if (isub == 1 && delT > C_eps) {
         const float inv_tau_d = fdiv(-m_dot, 0.2f * (float)pmass);
@@ -541,10 +541,10 @@ __device__ __forceinline__ int spray_source_mixed(
     }
     ++isub;
   }
-  src.eng = eng_acc;
+  src.eng = num_ppp * (double)eng_acc;
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
-    src.mom[d] = mom_acc[d];
+    src.mom[d] = num_ppp * (double)mom_acc[d];
   }
   if (nsub > 1) {
     src.eng /= static_cast<double>(nsub);
