@@ -230,8 +230,16 @@ WORKLOAD_TEXT = {
 FORM_MODE = {"fp64": 0, "mixed": 1, "learned": 2}
 FORM_NAME = {"fp64": "plain FP64", "mixed": "mixed FP32 physics / FP64 state and deposits",
              "learned": "learned surrogate (bf16 MLP on tensor cores) + FP32 physics / FP64 state"}
-KERNEL = {"fp64": "spray_update_fp64<5,2,128>", "mixed": "spray_update_mixed<5,2,128>",
-          "learned": "spray_update_learned<5,2,128>"}
+KERNEL = {"fp64": "spray_update_fp64<5,2,128>", "mixed": "spray_update_mixed<5,2,128,fuel_first>",
+          "learned": "spray_update_learned<5,2,256,fuel_first>"}
+# DRAM bytes per droplet of one config-2 MKD launch, measured by ncu on a
+# 2M-droplet launch (profiles/update_kernels_config2_2M.md): dram read + write
+# minus the mesh's algorithmic bytes (state read once, source read-modify-
+# write), divided by the droplets.  The droplet part grows with the droplet
+# count, the mesh part does not, so a full launch's traffic is estimated as
+# mesh bytes + droplets x this.  Above the 184 algorithmic bytes per droplet
+# for the FP64 and mixed kernels: their register spills reach DRAM.
+DRAM_BYTES_PER_DROPLET = {"fp64": 302.3, "mixed": 300.0, "learned": 184.9}
 
 
 def train_surrogate(sp, prob, st_v, stream, args):
@@ -495,6 +503,10 @@ def main():
     # roofline of the headline form's MKD launch (algorithmic bytes / launch time)
     mkd_bytes = algorithmic_bytes(prob.n_droplets, prob.nfuel, prob.nspec, ncells, True)
     achieved = mkd_bytes / (results[head]["mkd_launch_ms"] * 1e-3) / 1e9
+    traffic = None
+    if args.workload == "config2":
+        mesh = algorithmic_bytes(0, prob.nfuel, prob.nspec, ncells, True)
+        traffic = mesh + prob.n_droplets * DRAM_BYTES_PER_DROPLET[head]
 
     # ---- e2e: host views through pmp_spray_update_host (headline form) ----
     e2e = None
@@ -577,7 +589,10 @@ def main():
                        "parallelism": f"replicas x{world}"},
             "forms": forms_out,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None,
+                         "frac": achieved / peak, "traffic": traffic,
+                         "traffic_source": "ncu dram bytes of a 2M-droplet MKD launch scaled by droplet "
+                                           "count (mesh part fixed); profiles/update_kernels_config2_2M.md"
+                         if traffic else None,
                          "kernel": KERNEL[head] + " (MKD launch)",
                          "launch_ms": results[head]["mkd_launch_ms"],
                          "algorithmic_bytes_per_launch": mkd_bytes,
