@@ -30,6 +30,30 @@ namespace pmp {
 
 constexpr double kMixedMinDia = 2e-6;  // below: FP64 path
 
+#ifndef PMP_MIXED_FULL_RANGE_SFU
+#define PMP_MIXED_FULL_RANGE_SFU 1
+#endif
+
+#if PMP_MIXED_FULL_RANGE_SFU
+// 2^x, e^x, log2 x on the SFU over the full range (ex2.approx / lg2.approx);
+// the relative error of e^x is ~|x| 2^-24 from rounding x log2(e), plus the
+// SFU's own, well inside the form's 1e-4 budget
+__device__ __forceinline__ float fexp2(float x)
+{
+  float r;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
+__device__ __forceinline__ float fexp(float x) { return fexp2(x * 1.44269502f); }
+
+__device__ __forceinline__ float flog2(float x)
+{
+  float r;
+  asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+#else
 // 2^x for |x| < 126: SFU ex2 on the fraction, exact 2^k scaling
 __device__ __forceinline__ float fexp2(float x)
 {
@@ -66,6 +90,8 @@ __device__ __forceinline__ float flog2(float x)
   asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(__int_as_float(mb)));
   return r + static_cast<float>(e);
 }
+
+#endif
 
 __device__ __forceinline__ float flog(float x) { return flog2(x) * 0.693147181f; }
 
