@@ -30,12 +30,14 @@ template <int NS, int NF, int BLOCK, int MINB>
 __global__ void __launch_bounds__(BLOCK, MINB)
   spray_update_fp64_grid(const __grid_constant__ KParams P, const WorkArgs W)
 {
+  __shared__ BoxEntry sB;
   const int item = blockIdx.x;
   const int b = W.box[item];
+  stage_box(P, b, sB);
   const long long s = W.start[item] + threadIdx.x;
   Counters c;
-  if (s < P.boxes[b].p_end) {
-    update_one<NS, NF, Form::FP64>(P, b, s, c);
+  if (s < sB.p_end) {
+    update_one<NS, NF, Form::FP64>(P, sB, b, s, c);
   }
   flush_counters(P, c);
 }
@@ -59,7 +61,7 @@ __global__ void __launch_bounds__(BLOCK, MINB)
     const int b = W.box[item];
     const long long end = min(W.start[item] + W.chunk, P.boxes[b].p_end);
     for (long long s = W.start[item] + threadIdx.x; s < end; s += BLOCK) {
-      update_one<NS, NF, Form::FP64>(P, b, s, c);
+      update_one<NS, NF, Form::FP64>(P, P.boxes[b], b, s, c);
     }
   }
   flush_counters(P, c);

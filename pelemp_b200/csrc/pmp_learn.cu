@@ -707,7 +707,18 @@ __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
   const int item = blockIdx.x * (BLOCK / kBlock) + threadIdx.x / kBlock;
   const bool item_ok = item < L.ncta;
   const int b = item_ok ? P.cta_box[item] : 0;
-  const BoxEntry& B = P.boxes[b];
+  // this item's box entry, staged in shared memory
+  __shared__ BoxEntry sB[BLOCK / kBlock];
+  {
+    const int h = threadIdx.x / kBlock;
+    const int* src = reinterpret_cast<const int*>(P.boxes + b);
+    int* dst = reinterpret_cast<int*>(&sB[h]);
+    for (int i = threadIdx.x % kBlock; i < (int)(sizeof(BoxEntry) / 4); i += kBlock) {
+      dst[i] = src[i];
+    }
+  }
+  __syncthreads();
+  const BoxEntry& B = sB[threadIdx.x / kBlock];
   const long long s = item_ok ? P.cta_start[item] + threadIdx.x % kBlock : 0;
   Counters c;
   bool valid = item_ok && s < B.p_end;

@@ -48,10 +48,12 @@ __device__ __forceinline__ void cell_of(const KParams& P, const double* pos, dou
 }
 
 // Returns false if the droplet was handed to the fallback list (MIXED only).
+// B is box b's entry: the kernel passes a copy in shared memory when the CTA
+// works on one box (read at low latency, without re-deriving addresses), or
+// the global entry otherwise
 template <int NS, int NF, Form FORM, bool FF = false>
-__device__ __forceinline__ void update_one(const KParams& P, int b, long long s, Counters& c)
+__device__ __forceinline__ void update_one(const KParams& P, const BoxEntry& B, int b, long long s, Counters& c)
 {
-  const BoxEntry& B = P.boxes[b];
   int id = P.parts.id[s];
   if (!(id > 0)) {
     return;
@@ -367,14 +369,28 @@ __device__ __forceinline__ void flush_counters(const KParams& P, Counters& c)
                                    latency the extra warps hide (measured against 4, 6, 7) */
 #endif
 
+// copy box b's entry into shared memory (all threads of the CTA call it)
+__device__ __forceinline__ void stage_box(const KParams& P, int b, BoxEntry& sB)
+{
+  static_assert(sizeof(BoxEntry) % 4 == 0, "box entry copied as words");
+  const int* src = reinterpret_cast<const int*>(P.boxes + b);
+  int* dst = reinterpret_cast<int*>(&sB);
+  for (int i = threadIdx.x; i < (int)(sizeof(BoxEntry) / 4); i += blockDim.x) {
+    dst[i] = src[i];
+  }
+  __syncthreads();
+}
+
 template <int NS, int NF, int BLOCK>
 __global__ void __launch_bounds__(BLOCK, PMP_FP64_MIN_BLOCKS) spray_update_fp64(const __grid_constant__ KParams P)
 {
+  __shared__ BoxEntry sB;
   const int b = P.cta_box[blockIdx.x];
+  stage_box(P, b, sB);
   const long long s = P.cta_start[blockIdx.x] + threadIdx.x;
   Counters c;
-  if (s < P.boxes[b].p_end) {
-    update_one<NS, NF, Form::FP64>(P, b, s, c);
+  if (s < sB.p_end) {
+    update_one<NS, NF, Form::FP64>(P, sB, b, s, c);
   }
   flush_counters(P, c);
 }
@@ -382,11 +398,13 @@ __global__ void __launch_bounds__(BLOCK, PMP_FP64_MIN_BLOCKS) spray_update_fp64(
 template <int NS, int NF, int BLOCK, bool FF>
 __global__ void __launch_bounds__(BLOCK, PMP_MIXED_MIN_BLOCKS) spray_update_mixed(const __grid_constant__ KParams P)
 {
+  __shared__ BoxEntry sB;
   const int b = P.cta_box[blockIdx.x];
+  stage_box(P, b, sB);
   const long long s = P.cta_start[blockIdx.x] + threadIdx.x;
   Counters c;
-  if (s < P.boxes[b].p_end) {
-    update_one<NS, NF, Form::MIXED, FF>(P, b, s, c);
+  if (s < sB.p_end) {
+    update_one<NS, NF, Form::MIXED, FF>(P, sB, b, s, c);
   }
   flush_counters(P, c);
 }
@@ -415,7 +433,8 @@ __global__ void __launch_bounds__(BLOCK, PMP_FP64_MIN_BLOCKS) spray_update_fp64_
   for (unsigned long long i = blockIdx.x * (unsigned long long)BLOCK + threadIdx.x; i < n;
        i += (unsigned long long)gridDim.x * BLOCK) {
     const long long s = P.fb_list[i];
-    update_one<NS, NF, Form::FP64>(P, box_of_slot(P, s), s, c);
+    const int b = box_of_slot(P, s);
+    update_one<NS, NF, Form::FP64>(P, P.boxes[b], b, s, c);
   }
   flush_counters(P, c);
 }
