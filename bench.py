@@ -118,6 +118,19 @@ def algorithmic_bytes(n_live, nfuel, nspec, ncells, do_move):
     return n_live * (rp + wp) + ncells * (8 * (5 + nspec) + 16 * (5 + nfuel))
 
 
+def reduce_over_ranks(pg, t_ms, count, device="cuda"):
+    """Whole-job timing of replicas: the max of the ranks' timed milliseconds
+    and the sum of their work (unchanged without a process group)."""
+    if not pg:
+        return t_ms, count
+    import torch
+    tt = torch.tensor([t_ms], device=device, dtype=torch.float64)
+    pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+    nn = torch.tensor([float(count)], device=device, dtype=torch.float64)
+    pg.all_reduce(nn, op=pg.ReduceOp.SUM)
+    return float(tt.item()), int(nn.item())
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -309,14 +322,7 @@ def bench_batched(args, world, rank, local, pg):
         n = sum(step() for _ in range(steps))
         ev1.record(stream)
         torch.cuda.synchronize()
-        t = ev0.elapsed_time(ev1)
-        if pg:
-            tt = torch.tensor([t], device="cuda", dtype=torch.float64)
-            pg.all_reduce(tt, op=pg.ReduceOp.MAX)
-            t = float(tt.item())
-            nn = torch.tensor([float(n)], device="cuda", dtype=torch.float64)
-            pg.all_reduce(nn, op=pg.ReduceOp.SUM)
-            n = int(nn.item())
+        t, n = reduce_over_ranks(pg, ev0.elapsed_time(ev1), n)
         return n / (t * 1e-3), t / steps
 
     # each phase starts from the initial droplets (no re-binning inside the
@@ -471,15 +477,7 @@ def main():
         if pg:
             pg.barrier()
         c = sampler.stop()
-        t_ms = ev0.elapsed_time(ev1)
-        t_max, sub_total = t_ms, substeps
-        if pg:
-            tt = torch.tensor([t_ms], device="cuda", dtype=torch.float64)
-            pg.all_reduce(tt, op=pg.ReduceOp.MAX)
-            t_max = float(tt.item())
-            ss = torch.tensor([float(substeps)], device="cuda", dtype=torch.float64)
-            pg.all_reduce(ss, op=pg.ReduceOp.SUM)
-            sub_total = int(ss.item())
+        t_max, sub_total = reduce_over_ranks(pg, ev0.elapsed_time(ev1), substeps)
         info.update({"value": sub_total / (t_max * 1e-3), "ms_per_step": t_max / args.steps,
                      "mkd_launch_ms": float(np.mean(mkd_ms)), "substeps": sub_total,
                      "fallback_frac": fallback / max(substeps, 1), "clocks": c})
@@ -545,13 +543,7 @@ def main():
         e_ev1.record(stream)
         torch.cuda.synchronize()
         te = max(e_ev0.elapsed_time(e_ev1), 1e3 * (time.perf_counter() - t0))
-        if pg:
-            tt = torch.tensor([te], device="cuda", dtype=torch.float64)
-            pg.all_reduce(tt, op=pg.ReduceOp.MAX)
-            te = float(tt.item())
-            ss = torch.tensor([float(ns)], device="cuda", dtype=torch.float64)
-            pg.all_reduce(ss, op=pg.ReduceOp.SUM)
-            ns = int(ss.item())
+        te, ns = reduce_over_ranks(pg, te, ns)
         e2e = {"value": ns / (te * 1e-3), "unit": "droplet-substeps/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                "steps": args.e2e_steps, "form": head,
