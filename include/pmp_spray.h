@@ -276,6 +276,27 @@ int pmp_spray_move_kick(
 /* Method form (enum pmp_mode), default PMP_MODE_FP64. */
 int pmp_spray_set_mode(pmp_spray* h, int mode);
 
+/* Flow solver the update couples to (replaces the compile-time choice
+ * PELELM_USE_SPRAY: the units of Source/PP_Spray/SprayFuelData.H:41-70, the
+ * gas state of SprayInterpolation.H:111-146, the energy terms of
+ * Drag.H:282-286 and 418-421).
+ *   PMP_COUPLING_LMEX  (default): MKS units; the state holds rho, rho*u,
+ *                      rho*Y and T; the energy source is the enthalpy source.
+ *   PMP_COUPLING_PELEC: CGS units; the state holds rho, rho*u, rho*E, rho*Y
+ *                      and T (the guess for the gas temperature, which is
+ *                      found from e = E - |u|^2/2 and Y, EOS::EY2T); the
+ *                      energy source adds the drag work and the kinetic
+ *                      energy the evaporated mass carries.
+ * Call before pmp_spray_setup / pmp_spray_set_data (the latent heat is
+ * shifted by the fuel enthalpy in the coupling's units there); PMP_ERR_INVALID
+ * after.  The PeleC coupling runs the FP64 form with its default launch
+ * (pmp_spray_set_launch does not apply); the other forms return
+ * PMP_ERR_UNSUPPORTED in it, and pmp_spray_update_static couples to
+ * PeleLMeX only. */
+enum pmp_coupling { PMP_COUPLING_LMEX = 0, PMP_COUPLING_PELEC = 1 };
+int pmp_spray_set_coupling(pmp_spray* h, int coupling);
+int pmp_spray_get_coupling(const pmp_spray* h, int* coupling);
+
 int pmp_spray_last_error(const pmp_spray* h, pmp_error_info* info);
 int pmp_spray_get_stats(const pmp_spray* h, pmp_stats* stats);
 

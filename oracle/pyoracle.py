@@ -8,6 +8,11 @@ bench.py's CPU-baseline leg, as the checker.  The product never imports it.
   (C library math).
 * ``Reference(nspec, nfuel)`` -- oracle/_ref/libref_n{S}_f{F}.so, PeleMP's own
   physics headers compiled in this repository (C library math).
+
+``pelec=True`` selects the PeleC coupling (CGS units, energy state, drag work
+and kinetic-energy source terms): the oracle's process-wide coupling switch is
+set before each call, and the reference build is the one compiled without
+PELELM_USE_SPRAY (oracle/_ref/libref_pelec_n{S}_f{F}.so).
 """
 import ctypes as C
 import os
@@ -45,6 +50,10 @@ def _views(prob, arrays, ghosts):
 
 class _Base:
     _update_name = None
+    pelec = False
+
+    def _couple(self):
+        pass
 
     def _bind_update(self):
         f = getattr(self.lib, self._update_name)
@@ -66,6 +75,7 @@ class _Base:
         pa = _parts_array(prob, parts)
         st = _views(prob, state if state is not None else prob.state, prob.state_ghosts)
         sr = _views(prob, sources, prob.source_ghosts)
+        self._couple()
         rc = self._update(
             C.byref(mech), C.byref(fdat), C.byref(prob.comps()), C.byref(prob.geometry()),
             len(prob.boxes), prob.box_array(), pa, st, sr,
@@ -78,12 +88,15 @@ class _Base:
 class Oracle(_Base):
     _update_name = "pmp_oracle_update"
 
-    def __init__(self, libm=False):
+    def __init__(self, libm=False, pelec=False):
         name = "liboracle_libm.so" if libm else "liboracle.so"
         path = os.path.join(HERE, name)
         if not os.path.exists(path):
             raise RuntimeError(f"{path} missing: run `make -C oracle`")
         self.lib = C.CDLL(path)
+        self.pelec = bool(pelec)
+        self.lib.pmp_oracle_set_coupling.restype = None
+        self.lib.pmp_oracle_set_coupling.argtypes = [C.c_int]
         self._bind_update()
         self.lib.pmp_oracle_mech.restype = C.c_int
         self.lib.pmp_oracle_mech.argtypes = [C.POINTER(capi.Mech), C.c_int, C.c_void_p]
@@ -105,6 +118,9 @@ class Oracle(_Base):
         L.pmp_oracle_math.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_longlong]
         L.pmp_oracle_abi_sizes.restype = None
         L.pmp_oracle_abi_sizes.argtypes = [C.c_void_p]
+
+    def _couple(self):
+        self.lib.pmp_oracle_set_coupling(1 if self.pelec else 0)
 
     def math(self, fn, x, y=None):
         """fn in ('exp','log','log1p','pow','cbrt') over float64 arrays."""
@@ -149,6 +165,7 @@ class Oracle(_Base):
         names = capi.names_array(prob.species)
         out = capi.SprayData()
         inp = inputs if inputs is not None else prob.inputs()
+        self._couple()
         rc = self.lib.pmp_oracle_setup(C.byref(mech), C.cast(names, C.c_void_p),
                                        C.byref(inp), C.byref(out))
         return rc, out
@@ -158,6 +175,7 @@ class Oracle(_Base):
         rd = np.ascontiguousarray(rdata, dtype=np.float64).copy()
         src = np.zeros(5 + fdat.nfuel)
         idv = C.c_int(pid)
+        self._couple()
         re = self.lib.pmp_oracle_droplet_source(
             C.byref(mech), C.byref(fdat), flow_dt, gas.ctypes.data, rd.ctypes.data,
             C.byref(idv), src.ctypes.data)
@@ -167,13 +185,19 @@ class Oracle(_Base):
 class Reference(_Base):
     _update_name = "pmp_ref_update"
 
-    def __init__(self, nspec, nfuel):
-        path = os.path.join(HERE, "_ref", f"libref_n{nspec}_f{nfuel}.so")
+    def __init__(self, nspec, nfuel, pelec=False):
+        path = self._path(nspec, nfuel, pelec)
         if not os.path.exists(path):
             raise RuntimeError(f"{path} missing (needs the PeleMP sources at build time)")
         self.lib = C.CDLL(path)
+        self.pelec = bool(pelec)
         self._bind_update()
 
     @staticmethod
-    def available(nspec, nfuel):
-        return os.path.exists(os.path.join(HERE, "_ref", f"libref_n{nspec}_f{nfuel}.so"))
+    def _path(nspec, nfuel, pelec):
+        tag = "pelec_" if pelec else ""
+        return os.path.join(HERE, "_ref", f"libref_{tag}n{nspec}_f{nfuel}.so")
+
+    @staticmethod
+    def available(nspec, nfuel, pelec=False):
+        return os.path.exists(Reference._path(nspec, nfuel, pelec))

@@ -42,6 +42,10 @@ struct RefEos {
   void molecular_weight(amrex::Real* mw) const { pmp_eos_molecular_weight(&ref_mech(), mw); }
   void T2Cpi(amrex::Real T, amrex::Real* cp) const { pmp_eos_T2Cpi(&ref_mech(), T, cp); }
   void T2Hi(amrex::Real T, amrex::Real* h) const { pmp_eos_T2Hi(&ref_mech(), T, h); }
+  void EY2T(const amrex::Real e, const amrex::Real* Y, amrex::Real& T) const
+  {
+    pmp_eos_EY2T(&ref_mech(), e, Y, &T);
+  }
 };
 
 struct RefTransport {

@@ -13,14 +13,30 @@
 #endif
 
 /* SprayUnits, PeleLMeX branch (Source/PP_Spray/SprayFuelData.H:44-54,66) */
-#define U_RU_CONV 1.E-7
-#define U_ENG_CONV 1.E-4
-#define U_RHO_CONV 1.E3
-#define U_MASS_CONV 1.E-3
-#define U_RHOD_CONV 0.1
-#define U_MU_CONV 0.1
-#define U_LAMBDA_CONV 1.E-5
-#define U_PRES_CONV 0.1
+/* SprayUnits (SprayFuelData.H:42-67): PeleLMeX (PELELM_USE_SPRAY, MKS at
+ * the interface) or PeleC (CGS throughout), chosen by
+ * pmp_oracle_set_coupling; set before any other call, read-only after. */
+typedef struct {
+  double ru, eng, rho, mass, rhod, mu, lambda, pres;
+} units_t;
+static const units_t k_units_lmex = {1.E-7, 1.E-4, 1.E3, 1.E-3, 0.1, 0.1, 1.E-5, 0.1};
+static const units_t k_units_pelec = {1., 1., 1., 1., 1., 1., 1., 1.};
+static units_t g_units = {1.E-7, 1.E-4, 1.E3, 1.E-3, 0.1, 0.1, 1.E-5, 0.1};
+static int g_pelec = 0;
+#define U_RU_CONV (g_units.ru)
+#define U_ENG_CONV (g_units.eng)
+#define U_RHO_CONV (g_units.rho)
+#define U_MASS_CONV (g_units.mass)
+#define U_RHOD_CONV (g_units.rhod)
+#define U_MU_CONV (g_units.mu)
+#define U_LAMBDA_CONV (g_units.lambda)
+#define U_PRES_CONV (g_units.pres)
+
+void pmp_oracle_set_coupling(int pelec)
+{
+  g_pelec = pelec != 0;
+  g_units = g_pelec ? k_units_pelec : k_units_lmex;
+}
 
 /* std::min / std::max semantics (amrex::min/max forward to them) */
 static inline double dmin(double a, double b) { return (b < a) ? b : a; }
@@ -342,6 +358,12 @@ static double calculateSpraySource(
       for (int d = 0; d < 3; ++d) {
         gpv->fluid_mom_src[d] += nd * diff_vel[d];
       }
+      if (g_pelec) {
+        /* drag work s_d,mu . u_d, PeleC branch (Drag.H:282-286) */
+        const double S_dmu_dot_u = diff_vel[0] * vel_part[0] + diff_vel[1] * vel_part[1] +
+                                   diff_vel[2] * vel_part[2];
+        gpv->fluid_eng_src += nd * S_dmu_dot_u;
+      }
       if (isub == 1) {
         const double inv_tau_var = drag_force_p;
         nsub = imin(imax(nsub, (int)(flow_dt * inv_tau_var) + 1), nSubMax);
@@ -452,6 +474,12 @@ static double calculateSpraySource(
   }
   const double mdot_total = (pmass - startmass) / (fdat->dtmod * flow_dt);
   gpv->fluid_mass_src = num_ppp * mdot_total;
+  if (g_pelec) {
+    /* kinetic energy of the mass exchanged, PeleC branch (Drag.H:418-421) */
+    const double part_ke =
+      0.5 * (vel_part[0] * vel_part[0] + vel_part[1] * vel_part[1] + vel_part[2] * vel_part[2]);
+    gpv->fluid_eng_src += num_ppp * part_ke * mdot_total;
+  }
   if (fdat->mom_trans) {
     for (int d = 0; d < 3; ++d) {
       gpv->fluid_mom_src[d] += num_ppp * vel_part[d] * mdot_total;
@@ -673,7 +701,9 @@ static int update_droplet(const ctx_t* c, double* pos, double* rdata, int* id, l
     }
     trilinear_interp(ijk, lx, indx_array, weights, bflags);
     gpv_reset(&gpv, NS, NF);
-    /* InterpolateGasPhase (SprayInterpolation.H:99-150), PeleLMeX branch */
+    /* InterpolateGasPhase (SprayInterpolation.H:99-150): PeleLMeX branch
+     * (velocity and T read directly) or PeleC branch (velocity = mom / rho,
+     * T from the internal energy through eos.EY2T, the cell's T the guess) */
     for (int a = 0; a < 8; ++a) {
       const double cw = weights[a];
       if (cw > 0.) {
@@ -683,16 +713,27 @@ static int update_droplet(const ctx_t* c, double* pos, double* rdata, int* id, l
         }
         const double cur_rho = *vat(c->st, ci[0], ci[1], ci[2], sc->rhoIndx);
         gpv.rho_fluid += cw * cur_rho;
-        const double inv_rho = 1. / cur_rho;
+        double inv_rho = 1. / cur_rho;
+        double mass_frac[PMP_MAX_SPEC];
         for (int n = 0; n < NS; ++n) {
           const double cur_mf = *vat(c->st, ci[0], ci[1], ci[2], sc->specIndx + n) * inv_rho;
           gpv.Y_fluid[n] += cw * cur_mf;
+          mass_frac[n] = cur_mf;
         }
+        if (!g_pelec) {
+          inv_rho = 1.;
+        }
+        double ke = 0.;
         for (int dir = 0; dir < 3; ++dir) {
-          const double vel = *vat(c->st, ci[0], ci[1], ci[2], sc->momIndx + dir) * 1.;
+          const double vel = *vat(c->st, ci[0], ci[1], ci[2], sc->momIndx + dir) * inv_rho;
           gpv.vel_fluid[dir] += cw * vel;
+          ke += vel * vel / 2.;
         }
-        const double T_i = *vat(c->st, ci[0], ci[1], ci[2], sc->utempIndx);
+        double T_i = *vat(c->st, ci[0], ci[1], ci[2], sc->utempIndx);
+        if (g_pelec) {
+          const double intEng = *vat(c->st, ci[0], ci[1], ci[2], sc->engIndx) * inv_rho - ke;
+          pmp_eos_EY2T(c->mech, intEng, mass_frac, &T_i);
+        }
         gpv.T_fluid += cw * T_i;
       }
     }

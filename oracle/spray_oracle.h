@@ -37,6 +37,11 @@
 extern "C" {
 #endif
 
+/* Coupling of every following call: 0 = PeleLMeX (PELELM_USE_SPRAY, the
+ * default), 1 = PeleC (CGS units, energy-based gas temperature, kinetic
+ * energy and drag-work energy sources). */
+void pmp_oracle_set_coupling(int pelec);
+
 /* Build a mechanism from species names; returns 0 or -1. */
 int pmp_oracle_mech(pmp_mech* mech, int nspec, const char (*names)[PMP_NAME_LEN]);
 

@@ -33,6 +33,8 @@ def pstate_filmhght(f):
 
 
 PMP_OK = 0
+PMP_COUPLING_LMEX = 0
+PMP_COUPLING_PELEC = 1
 PMP_ERR_LEFT_DOMAIN = 1
 PMP_ERR_STATE_BOX = 2
 PMP_ERR_SOURCE_BOX = 3

@@ -85,6 +85,8 @@ public:
     return n;
   }
   void setMode(int mode) { check(pmp_spray_set_mode(h_, mode)); }
+  /// the flow solver (PMP_COUPLING_LMEX / PMP_COUPLING_PELEC), before readSprayParams
+  void setCoupling(int coupling) { check(pmp_spray_set_coupling(h_, coupling)); }
 
   /// Update but do not move particles (SprayParticles.cpp:37-57)
   void moveKick(

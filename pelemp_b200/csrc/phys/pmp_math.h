@@ -46,6 +46,10 @@
 #include <stdint.h>
 #include <string.h>
 
+/* Newton iterations at most in the EOS inversion e(T, Y) -> T (pmp_eos_EY2T
+ * in pmp_thermo.h and its device copy); shared so both stop alike. */
+#define PMP_EY2T_MAXIT 20
+
 #if defined(__CUDACC__)
 #define PMP_HD __host__ __device__ __forceinline__
 #else

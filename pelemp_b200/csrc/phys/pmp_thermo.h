@@ -114,6 +114,36 @@ PMP_HD void pmp_eos_T2Hi(const pmp_mech* m, double T, double* hi)
   }
 }
 
+/* eos.EY2T: the temperature at which the mixture's specific internal energy
+ * sum_k Y_k (h_k(T) - R T / W_k) [erg/g] equals e, by Newton iteration from
+ * the guess in *T (at most 20 steps; stops once |dT| <= 1e-11 T).  PelePhysics'
+ * own EY2T is not part of PeleMP; this is the project's EOS inversion, used by
+ * the PeleC coupling's gas-state gather (SprayInterpolation.H:111-146). */
+PMP_HD void pmp_eos_EY2T(const pmp_mech* m, double e, const double* Y, double* T)
+{
+  double t = *T;
+  for (int it = 0; it < PMP_EY2T_MAXIT; ++it) {
+    double em = 0., cv = 0.;
+    for (int k = 0; k < m->nspec; ++k) {
+      const double rw = PMP_RU_CGS / m->mw[k];
+      const double* a = m->hc[k];
+      const double hp = fma(fma(fma(fma(a[4], t, a[3]), t, a[2]), t, a[1]), t, a[0]);
+      const double hk = fma(hp, t, a[5]) * rw;
+      const double* c = m->cp[k];
+      const double cpr = fma(fma(fma(fma(c[4], t, c[3]), t, c[2]), t, c[1]), t, c[0]);
+      const double cpk = cpr * rw;
+      em = fma(Y[k], fma(-rw, t, hk), em);
+      cv = fma(Y[k], cpk - rw, cv);
+    }
+    const double dT = (e - em) / cv;
+    t = t + dT;
+    if (fabs(dT) <= 1e-11 * t) {
+      break;
+    }
+  }
+  *T = t;
+}
+
 PMP_HD double pmp_cubic(const double* c, double x)
 {
   return fma(fma(fma(c[3], x, c[2]), x, c[1]), x, c[0]);

@@ -25,6 +25,19 @@ constexpr double kRhodConv = 0.1;
 constexpr double kMuConv = 0.1;
 constexpr double kLambdaConv = 1.E-5;
 constexpr double kPresConv = 0.1;
+// SprayUnits of either coupling, for the FP64 kernels: PELEC = false is the
+// PeleLMeX branch above (MKS at the interface), PELEC = true the PeleC branch
+// (CGS throughout, every factor 1; SprayFuelData.H:55-64)
+template <bool PELEC>
+struct Units {
+  static constexpr double ru = PELEC ? 1. : kRuConv;
+  static constexpr double eng = PELEC ? 1. : kEngConv;
+  static constexpr double mass = PELEC ? 1. : kMassConv;
+  static constexpr double rhod = PELEC ? 1. : kRhodConv;
+  static constexpr double mu = PELEC ? 1. : kMuConv;
+  static constexpr double lambda = PELEC ? 1. : kLambdaConv;
+  static constexpr double pres = PELEC ? 1. : kPresConv;
+};
 constexpr double kRuCgs = 8.31446261815324e7;
 constexpr double kPatmCgs = 1013250.0;
 
@@ -153,6 +166,8 @@ struct KParams {
   const long long* box_begin;  // nboxes + 1 slot offsets
   long long* fb_list;          // slots handed to the FP64 fallback kernel
   DevStatus* status;
+  // PeleC coupling (FP64 form only): energy component of the state
+  int pelec, c_eng;
   // mixed / learned forms: species k of DevMechF (and of their gas-state
   // gather) is mechanism species spec_perm[k]; fuel_first as in DevMechF
   int spec_perm[kMaxSpec];

@@ -70,6 +70,7 @@ struct pmp_spray {
   bool have_geom = false;
   std::vector<pmp_box> boxes;
   int mode = PMP_MODE_FP64;
+  int pelec = 0;  // enum pmp_coupling
   pmp::DevMech dmech;
   pmp::DevFuel dfuel;
   pmp::DevMechF dmechf;

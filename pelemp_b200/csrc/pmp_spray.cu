@@ -206,7 +206,7 @@ int build_device_tables(pmp_spray* h)
   memset(&m, 0, sizeof(m));
   for (int k = 0; k < NS; ++k) {
     m.mw_g[k] = h->mech.mw[k];
-    m.mw_kg[k] = h->mech.mw[k] * pmp::kMassConv;
+    m.mw_kg[k] = h->mech.mw[k] * (h->pelec ? 1. : pmp::kMassConv);
     m.ru_w[k] = PMP_RU_CGS / h->mech.mw[k];
     for (int n = 0; n < 5; ++n) {
       m.cp[k][n] = h->mech.cp[k][n];
@@ -504,6 +504,22 @@ int dispatch_fp64(int ns, int nf, const KParams& P, int ncta, cudaStream_t st)
   return PMP_ERR_UNSUPPORTED;
 }
 
+int dispatch_fp64_pelec(int ns, int nf, const KParams& P, int ncta, cudaStream_t st)
+{
+#define PMP_CASE(S, F)                                                  \
+  if (ns == S && nf == F) {                                             \
+    pmp::spray_update_fp64_pelec<S, F, kBlock><<<ncta, kBlock, 0, st>>>(P); \
+    return PMP_OK;                                                      \
+  }
+  PMP_CASE(3, 1)
+  PMP_CASE(5, 1)
+  PMP_CASE(5, 2)
+  PMP_CASE(4, 1)
+  PMP_CASE(4, 2)
+#undef PMP_CASE
+  return PMP_ERR_UNSUPPORTED;
+}
+
 // the FP64 kernel over the fallback list filled by the mixed / learned kernels
 int dispatch_fp64_list(int ns, int nf, const KParams& P, long long total, cudaStream_t st)
 {
@@ -535,6 +551,9 @@ int prepare_update_impl(
   if (nboxes != (int)h->boxes.size()) {
     return set_err(h, PMP_ERR_INVALID, "nboxes differs from the grids given to set_grids");
   }
+  if (h->pelec && h->mode != PMP_MODE_FP64) {
+    return set_err(h, PMP_ERR_UNSUPPORTED, "the PeleC coupling runs the FP64 form only");
+  }
   if (h->mode == PMP_MODE_LEARNED && !pmp::learn_ready(h)) {
     return set_err(h, PMP_ERR_INVALID, "the learned form needs a trained surrogate (pmp_spray_learn_train)");
   }
@@ -555,7 +574,8 @@ int prepare_update_impl(
   const pmp_spray_comps& c = h->comps;
   const int NS = h->nspec;
   const int NF = h->nfuel;
-  const int need_state = 1 + std::max({c.rhoIndx, c.momIndx + 2, c.utempIndx, c.specIndx + NS - 1});
+  const int need_state = 1 + std::max({c.rhoIndx, c.momIndx + 2, c.utempIndx, c.specIndx + NS - 1,
+                                       h->pelec ? c.engIndx : 0});
   const int need_src = 1 + std::max({c.rhoSrcIndx, c.momSrcIndx + 2, c.engSrcIndx, c.specSrcIndx + NF - 1});
   for (int b = 0; b < nboxes; ++b) {
     const pmp_box& bx = h->boxes[b];
@@ -648,6 +668,8 @@ int prepare_update_impl(
   P.c_rho = c.rhoIndx;
   P.c_mom = c.momIndx;
   P.c_T = c.utempIndx;
+  P.c_eng = c.engIndx;
+  P.pelec = h->pelec;
   P.c_spec = c.specIndx;
   P.s_rho = c.rhoSrcIndx;
   P.s_mom = c.momSrcIndx;
@@ -808,6 +830,8 @@ int pmp::enqueue_update(pmp_spray* h, const KParams& P, int nboxes, cudaStream_t
         PMP_CUDA(h, cudaGetLastError());
         rc = dispatch_fp64_list(NS, NF, P, h->total, st);
       }
+    } else if (P.pelec) {
+      rc = dispatch_fp64_pelec(NS, NF, P, h->ncta, st);
     } else {
       rc = pmp::batch_enqueue_fp64(h, P, nboxes, st);
     }
@@ -1004,7 +1028,7 @@ int pmp_spray_setup(pmp_spray* h, const pmp_spray_inputs* in)
   double fuelEnth[PMP_MAX_SPEC];
   pmp_eos_T2Hi(&h->mech, d.ref_T, fuelEnth);
   for (int ns = 0; ns < NF; ++ns) {
-    d.latent[ns] -= fuelEnth[d.indx[ns]] * pmp::kEngConv;
+    d.latent[ns] -= fuelEnth[d.indx[ns]] * (h->pelec ? 1. : pmp::kEngConv);
   }
   for (int i = 0; i < 3; ++i) {
     d.body_force[i] = in->body_force[i];
@@ -1366,6 +1390,27 @@ int pmp_spray_set_mode(pmp_spray* h, int mode)
     return PMP_ERR_INVALID;
   }
   h->mode = mode;
+  return PMP_OK;
+}
+
+int pmp_spray_set_coupling(pmp_spray* h, int coupling)
+{
+  if (!h || (coupling != PMP_COUPLING_LMEX && coupling != PMP_COUPLING_PELEC)) {
+    return PMP_ERR_INVALID;
+  }
+  if (h->have_data && coupling != h->pelec) {
+    return set_err(h, PMP_ERR_INVALID, "set the coupling before the spray data");
+  }
+  h->pelec = coupling;
+  return PMP_OK;
+}
+
+int pmp_spray_get_coupling(const pmp_spray* h, int* coupling)
+{
+  if (!h || !coupling) {
+    return PMP_ERR_INVALID;
+  }
+  *coupling = h->pelec;
   return PMP_OK;
 }
 

@@ -129,23 +129,55 @@ __device__ __forceinline__ double heat_coeff(
 // eos.T2Cpi / eos.T2Hi of species n at T (pmp_thermo.h, same operation
 // order), converted to MKS: evaluated where needed instead of kept in
 // per-species register arrays
+template <bool PELEC = false>
 __device__ __forceinline__ double cp_mks(const DevMech& m, int n, double T)
 {
   const double* a = m.cp[n];
   const double cpr = fma(fma(fma(fma(a[4], T, a[3]), T, a[2]), T, a[1]), T, a[0]);
-  return (cpr * m.ru_w[n]) * kEngConv;
+  return (cpr * m.ru_w[n]) * Units<PELEC>::eng;
 }
 
+template <bool PELEC = false>
 __device__ __forceinline__ double h_mks(const DevMech& m, int n, double T)
 {
   const double* hc = m.hc[n];
   const double hp = fma(fma(fma(fma(hc[4], T, hc[3]), T, hc[2]), T, hc[1]), T, hc[0]);
-  return (fma(hp, T, hc[5]) * m.ru_w[n]) * kEngConv;
+  return (fma(hp, T, hc[5]) * m.ru_w[n]) * Units<PELEC>::eng;
+}
+
+// eos.EY2T of the project EOS (pmp_eos_EY2T in phys/pmp_thermo.h, the same
+// operations): temperature of specific internal energy e [erg/g], Newton
+// from the guess T
+template <int NS>
+__device__ __forceinline__ double ey2t(const DevMech& m, double e, const double* Y, double T)
+{
+  double t = T;
+  for (int it = 0; it < PMP_EY2T_MAXIT; ++it) {
+    double em = 0., cv = 0.;
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+      const double rw = m.ru_w[k];
+      const double* a = m.hc[k];
+      const double hp = fma(fma(fma(fma(a[4], t, a[3]), t, a[2]), t, a[1]), t, a[0]);
+      const double hk = fma(hp, t, a[5]) * rw;
+      const double* c = m.cp[k];
+      const double cpr = fma(fma(fma(fma(c[4], t, c[3]), t, c[2]), t, c[1]), t, c[0]);
+      const double cpk = cpr * rw;
+      em = fma(Y[k], fma(-rw, t, hk), em);
+      cv = fma(Y[k], cpk - rw, cv);
+    }
+    const double dT = (e - em) / cv;
+    t = t + dT;
+    if (fabs(dT) <= 1e-11 * t) {
+      break;
+    }
+  }
+  return t;
 }
 
 // calculateSpraySource (Drag.H:138-441), PeleLMeX branch.  Updates vel, T,
 // dia, Y in place; returns the number of inner sub-steps taken.
-template <int NS, int NF>
+template <int NS, int NF, bool PELEC = false>
 __device__ __forceinline__ int spray_source_fp64(
   const KParams& P, double flow_dt, GasVals<NS, NF>& gpv, double* vel_io, double& T_io,
   double& dia_io, double* Y_io, double num_ppp, int& id, const double* cBoilT)
@@ -155,7 +187,7 @@ __device__ __forceinline__ int spray_source_fp64(
   const double rule = 1. / 3.;
   const double C_eps = 1.E-15;
   const double B_eps = 1.E-7;
-  const double min_mass = 1.E-13 * kMassConv;
+  const double min_mass = 1.E-13 * Units<PELEC>::mass;
   const int nSubMax = 100;
   double Y_skin[NS];
   double T_h = T_io;  // temperature of the last h_part evaluation (Drag.H:221)
@@ -219,8 +251,8 @@ __device__ __forceinline__ int spray_source_fp64(
     double sumXVap = 0.;
     if (fdat.mass_trans) {
       // calcVaporState (Drag.H:48-135)
-      const double RU = kRuCgs * kRuConv;
-      const double PATM = kPatmCgs * kPresConv;
+      const double RU = kRuCgs * Units<PELEC>::ru;
+      const double PATM = kPatmCgs * Units<PELEC>::pres;
       double mbar_vap = 0.;
 #pragma unroll
       for (int spf = 0; spf < NF; ++spf) {
@@ -229,7 +261,7 @@ __device__ __forceinline__ int spray_source_fp64(
         const double boilT_ref = fdat.boilT[spf];
         const double mw_fuel = m.mw_kg[fspec];
         const double Tp = dmin(T_part, 0.99 * cBoilT[spf]);
-        const double part_latent = h_mks(m, fspec, T_part) + fdat.latent[spf] - fdat.cp[spf] * (Tp - fdat.ref_T);
+        const double part_latent = h_mks<PELEC>(m, fspec, T_part) + fdat.latent[spf] - fdat.cp[spf] * (Tp - fdat.ref_T);
         L_fuel[spf] = part_latent;
         double pres_sat = 0.;
         if (fdat.psat_coef[4 * spf + 3] == 0.) {
@@ -276,7 +308,7 @@ __device__ __forceinline__ int spray_source_fp64(
         if (Y_skin[n] == 0.) {
           Y_skin[n] = gpv.Y[n] * renorm;
         }
-        cp_skin += Y_skin[n] * cp_mks(m, n, T_skin);
+        cp_skin += Y_skin[n] * cp_mks<PELEC>(m, n, T_skin);
         mw_skin += Y_skin[n] / m.mw_kg[n];
       }
       mw_skin = 1. / mw_skin;
@@ -286,7 +318,7 @@ __device__ __forceinline__ int spray_source_fp64(
 #pragma unroll
       for (int n = 0; n < NS; ++n) {
         Y_skin[n] = gpv.Y[n];
-        cp_skin += gpv.Y[n] * cp_mks(m, n, T_skin);
+        cp_skin += gpv.Y[n] * cp_mks<PELEC>(m, n, T_skin);
       }
       mw_skin = gpv.mw_mix;
     }
@@ -294,7 +326,7 @@ __device__ __forceinline__ int spray_source_fp64(
     double mu_skin = 0.;
     double rho_skin = gpv.rho;
     if (fdat.mass_trans) {
-      rho_skin = mw_skin * gpv.p / (kRuCgs * kRuConv * T_skin);
+      rho_skin = mw_skin * gpv.p / (kRuCgs * Units<PELEC>::ru * T_skin);
     }
     // trans.transport at (T_skin, Y_skin) (pmp_thermo.h), fuel rows of Ddiag
     {
@@ -341,8 +373,8 @@ __device__ __forceinline__ int spray_source_fp64(
         }
       }
     }
-    mu_skin *= kMuConv;
-    lambda_skin *= kLambdaConv;
+    mu_skin *= Units<PELEC>::mu;
+    lambda_skin *= Units<PELEC>::lambda;
     double diff_vel[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
@@ -374,6 +406,12 @@ __device__ __forceinline__ int spray_source_fp64(
       for (int d = 0; d < 3; ++d) {
         gpv.mom_src[d] += nd * diff_vel[d];
       }
+      if (PELEC) {
+        // drag work s_d,mu . u_d (Drag.H:282-286, PeleC branch)
+        const double S_dmu_dot_u =
+          diff_vel[0] * vel_part[0] + diff_vel[1] * vel_part[1] + diff_vel[2] * vel_part[2];
+        gpv.eng_src += nd * S_dmu_dot_u;
+      }
       if (isub == 1) {
         const double inv_tau_var = drag_force_p;
         nsub = min(max(nsub, static_cast<int>(flow_dt * inv_tau_var) + 1), nSubMax);
@@ -394,12 +432,12 @@ __device__ __forceinline__ int spray_source_fp64(
 #pragma unroll
         for (int spf = 0; spf < NF; ++spf) {
           const int fspec = fdat.indx[spf];
-          Ddiag[spf] *= mw_skin / m.mw_kg[fspec] * kRhodConv;
+          Ddiag[spf] *= mw_skin / m.mw_kg[fspec] * Units<PELEC>::rhod;
           const double X_norm = X_vapor[spf] / sumXVap;
           Ddiag[spf] *= X_norm;
           rhoDtotal += Ddiag[spf];
           const double ysk = sel(Y_skin, fspec);
-          cp_fuel += ysk * cp_mks(m, fspec, T_skin);
+          cp_fuel += ysk * cp_mks<PELEC>(m, fspec, T_skin);
           sumYSkin += ysk;
         }
         cp_fuel /= sumYSkin;
@@ -489,6 +527,12 @@ __device__ __forceinline__ int spray_source_fp64(
   }
   const double mdot_total = (pmass - startmass) / (fdat.dtmod * flow_dt);
   gpv.mass_src = num_ppp_ * mdot_total;
+  if (PELEC) {
+    // kinetic energy of the exchanged mass (Drag.H:418-421, PeleC branch)
+    const double part_ke =
+      0.5 * (vel_part[0] * vel_part[0] + vel_part[1] * vel_part[1] + vel_part[2] * vel_part[2]);
+    gpv.eng_src += num_ppp_ * part_ke * mdot_total;
+  }
   if (fdat.mom_trans) {
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
@@ -501,7 +545,7 @@ __device__ __forceinline__ int spray_source_fp64(
     const double newY = Y_part[spf];
     const double midot = (newY * pmass - oldY * startmass) / (fdat.dtmod * flow_dt);
     gpv.Ydot[spf] = num_ppp_ * midot;
-    gpv.eng_src += num_ppp_ * midot * h_mks(m, fdat.dep[spf], T_h);
+    gpv.eng_src += num_ppp_ * midot * h_mks<PELEC>(m, fdat.dep[spf], T_h);
     Y_io[spf] = Y_part[spf];
   }
   vel_io[0] = vel_part[0];

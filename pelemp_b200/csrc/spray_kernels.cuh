@@ -51,7 +51,7 @@ __device__ __forceinline__ void cell_of(const KParams& P, const double* pos, dou
 // B is box b's entry: the kernel passes a copy in shared memory when the CTA
 // works on one box (read at low latency, without re-deriving addresses), or
 // the global entry otherwise
-template <int NS, int NF, Form FORM, bool FF = false>
+template <int NS, int NF, Form FORM, bool FF = false, bool PELEC = false>
 __device__ __forceinline__ void update_one(const KParams& P, const BoxEntry& B, int b, long long s, Counters& c)
 {
   int id = P.parts.id[s];
@@ -156,17 +156,40 @@ __device__ __forceinline__ void update_one(const KParams& P, const BoxEntry& B, 
                 const double cur_rho = __ldg(q + P.c_rho * B.st_n32);
                 gpv.rho = __dadd_rn(gpv.rho, __dmul_rn(cw, cur_rho));
                 const double inv_rho = 1. / cur_rho;
+                if (!PELEC) {
 #pragma unroll
-                for (int n = 0; n < NS; ++n) {
-                  const double cur_mf = __dmul_rn(__ldg(q + (P.c_spec + n) * B.st_n32), inv_rho);
-                  gpv.Y[n] = __dadd_rn(gpv.Y[n], __dmul_rn(cw, cur_mf));
-                }
+                  for (int n = 0; n < NS; ++n) {
+                    const double cur_mf = __dmul_rn(__ldg(q + (P.c_spec + n) * B.st_n32), inv_rho);
+                    gpv.Y[n] = __dadd_rn(gpv.Y[n], __dmul_rn(cw, cur_mf));
+                  }
 #pragma unroll
-                for (int dir = 0; dir < 3; ++dir) {
-                  gpv.vel[dir] =
-                    __dadd_rn(gpv.vel[dir], __dmul_rn(cw, __ldg(q + (P.c_mom + dir) * B.st_n32)));
+                  for (int dir = 0; dir < 3; ++dir) {
+                    gpv.vel[dir] =
+                      __dadd_rn(gpv.vel[dir], __dmul_rn(cw, __ldg(q + (P.c_mom + dir) * B.st_n32)));
+                  }
+                  gpv.T = __dadd_rn(gpv.T, __dmul_rn(cw, __ldg(q + P.c_T * B.st_n32)));
+                } else {
+                  // PeleC branch (SprayInterpolation.H:111-146): velocity from
+                  // momentum, T from the internal energy (eos.EY2T, the cell's
+                  // T as the guess)
+                  double mass_frac[NS];
+#pragma unroll
+                  for (int n = 0; n < NS; ++n) {
+                    const double cur_mf = __dmul_rn(__ldg(q + (P.c_spec + n) * B.st_n32), inv_rho);
+                    gpv.Y[n] = __dadd_rn(gpv.Y[n], __dmul_rn(cw, cur_mf));
+                    mass_frac[n] = cur_mf;
+                  }
+                  double ke = 0.;
+#pragma unroll
+                  for (int dir = 0; dir < 3; ++dir) {
+                    const double vel = __dmul_rn(__ldg(q + (P.c_mom + dir) * B.st_n32), inv_rho);
+                    gpv.vel[dir] = __dadd_rn(gpv.vel[dir], __dmul_rn(cw, vel));
+                    ke = __dadd_rn(ke, __dmul_rn(vel, vel) / 2.);
+                  }
+                  const double intEng = __dsub_rn(__dmul_rn(__ldg(q + P.c_eng * B.st_n32), inv_rho), ke);
+                  const double T_i = ey2t<NS>(P.m, intEng, mass_frac, __ldg(q + P.c_T * B.st_n32));
+                  gpv.T = __dadd_rn(gpv.T, __dmul_rn(cw, T_i));
                 }
-                gpv.T = __dadd_rn(gpv.T, __dmul_rn(cw, __ldg(q + P.c_T * B.st_n32)));
               }
             }
           }
@@ -182,12 +205,12 @@ __device__ __forceinline__ void update_one(const KParams& P, const BoxEntry& B, 
       for (int n = 0; n < NS; ++n) {
         mw_mix = __dadd_rn(mw_mix, gpv.Y[n] / P.m.mw_kg[n]);
       }
-      gpv.p = __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(gpv.rho, kRuCgs), mw_mix), gpv.T), kRuConv);
+      gpv.p = __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(gpv.rho, kRuCgs), mw_mix), gpv.T), Units<PELEC>::ru);
       gpv.mw_mix = 1. / mw_mix;
       double cBoilT[NF];
       {
-        const double RU = kRuCgs * kRuConv;
-        const double PATM = kPatmCgs * kPresConv;
+        const double RU = kRuCgs * Units<PELEC>::ru;
+        const double PATM = kPatmCgs * Units<PELEC>::pres;
         const double lp = pmp_log(PATM / gpv.p);
 #pragma unroll
         for (int spf = 0; spf < NF; ++spf) {
@@ -196,7 +219,7 @@ __device__ __forceinline__ void update_one(const KParams& P, const BoxEntry& B, 
           cBoilT[spf] = dmin(P.f.critT[spf], cc);
         }
       }
-      nsub = spray_source_fp64<NS, NF>(P, P.sub_dt, gpv, vel, T, dia, Y, num_ppp, id, cBoilT);
+      nsub = spray_source_fp64<NS, NF, PELEC>(P, P.sub_dt, gpv, vel, T, dia, Y, num_ppp, id, cBoilT);
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
         src.mom[d] = gpv.mom_src[d];
@@ -391,6 +414,21 @@ __global__ void __launch_bounds__(BLOCK, PMP_FP64_MIN_BLOCKS) spray_update_fp64(
   Counters c;
   if (s < sB.p_end) {
     update_one<NS, NF, Form::FP64>(P, sB, b, s, c);
+  }
+  flush_counters(P, c);
+}
+
+// the PeleC coupling of the FP64 form
+template <int NS, int NF, int BLOCK>
+__global__ void __launch_bounds__(BLOCK, PMP_FP64_MIN_BLOCKS) spray_update_fp64_pelec(const __grid_constant__ KParams P)
+{
+  __shared__ BoxEntry sB;
+  const int b = P.cta_box[blockIdx.x];
+  stage_box(P, b, sB);
+  const long long s = P.cta_start[blockIdx.x] + threadIdx.x;
+  Counters c;
+  if (s < sB.p_end) {
+    update_one<NS, NF, Form::FP64, false, true>(P, sB, b, s, c);
   }
   flush_counters(P, c);
 }

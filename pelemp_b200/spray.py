@@ -46,6 +46,8 @@ _SIGS = {
                             C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int,
                             C.c_double, C.c_void_p],
     "pmp_spray_set_mode": [C.c_void_p, C.c_int],
+    "pmp_spray_set_coupling": [C.c_void_p, C.c_int],
+    "pmp_spray_get_coupling": [C.c_void_p, C.POINTER(C.c_int)],
     "pmp_spray_last_error": [C.c_void_p, C.POINTER(capi.ErrorInfo)],
     "pmp_spray_get_stats": [C.c_void_p, C.POINTER(capi.Stats)],
     "pmp_spray_version": [],
@@ -196,6 +198,16 @@ class SprayParticleContainer:
 
     def set_mode(self, mode):
         self._check(lib().pmp_spray_set_mode(self._h, mode))
+
+    def set_coupling(self, coupling):
+        """capi.PMP_COUPLING_LMEX (default) or PMP_COUPLING_PELEC; before setup."""
+        self._check(lib().pmp_spray_set_coupling(self._h, coupling))
+
+    @property
+    def coupling(self):
+        c = C.c_int(0)
+        self._check(lib().pmp_spray_get_coupling(self._h, C.byref(c)))
+        return c.value
 
     # --- droplets ---------------------------------------------------------
     def set_particles(self, box, pos, rdata, ids):
@@ -411,6 +423,8 @@ def learn_debug_grad(params, x, y, quant=True):
 def from_problem(prob, device=0, mode=capi.PMP_MODE_FP64, set_droplets=True):
     """Container set up for a workloads.Problem (droplets copied from host)."""
     sp = SprayParticleContainer(prob.species, prob.nfuel, device)
+    if getattr(prob, "pelec", False):
+        sp.set_coupling(capi.PMP_COUPLING_PELEC)
     sp.spray_setup(prob.inputs())
     sp.assign_spray_comps(prob.comps())
     sp.set_geometry(prob.geometry())

@@ -17,6 +17,8 @@ generated here from a seed with numpy's PCG64 generator:
 * ``config4`` -- config 1's distributions, 32M droplets on 256x128x128.
 * ``walls``   -- a small non-periodic case (reflective x, outflow z) used to
   exercise the boundary branches.
+* ``to_pelec(prob, mech)`` -- any of the above restated for the PeleC
+  coupling: CGS units, momentum and total energy in the state.
 
 Liquid properties: n-heptane from Exec/SprayTests/PeleC/heptane_evap/input2d:64-77
 (converted to MKS), n-decane from Exec/SprayTests/PeleLMeX/abramzon_test/inputs_2d:65-77.
@@ -28,7 +30,8 @@ Mesh layout (AMReX Array4, x fastest): a box's state is a numpy array of
 shape (ncomp, nz, ny, nx) over the box grown by its ghost width.  State
 components: vel 0..2 (PeleLMeX stores velocity), rho 3, rhoY 4..4+NSP-1,
 rhoH 4+NSP (not read on this path), T 5+NSP.  Source components: mom 0..2,
-rho 3, rhoY_fuel 4..4+F-1, energy 4+F.
+rho 3, rhoY_fuel 4..4+F-1, energy 4+F.  In the PeleC restatement the same
+slots hold rho*u 0..2, rho 3, rhoY, rho*E 4+NSP and the temperature guess.
 """
 from dataclasses import dataclass, field
 
@@ -77,6 +80,7 @@ class Problem:
     mom_trans: int = 1
     fixed_parts: int = 0
     body_force: tuple = (0.0, 0.0, 0.0)
+    pelec: bool = False      # CGS units and the PeleC state (to_pelec)
     meta: dict = field(default_factory=dict)
 
     @property
@@ -129,25 +133,28 @@ class Problem:
         """The particles.* inputs of this problem (pmp_spray_inputs)."""
         s = capi.SprayInputs()
         s.nfuel = self.nfuel
+        # CGS for PeleC: erg/g = 1e4 J/kg, g/cm^3 = 1e3 kg/m^3, dyn/cm^2 = 0.1 Pa
+        eng, rho, pres = (1e4, 1e-3, 10.0) if self.pelec else (1.0, 1.0, 1.0)
         for f, name in enumerate(self.fuels):
             liq = LIQUIDS[name]
             s.fuel_species[f].value = name.encode()
             s.crit_temp[f] = liq["crit_temp"]
             s.boil_temp[f] = liq["boil_temp"]
-            s.latent[f] = liq["latent"]
-            s.cp[f] = liq["cp"]
+            s.latent[f] = liq["latent"] * eng
+            s.cp[f] = liq["cp"] * eng
             s.ncoef_rho[f] = 1
-            s.rho[f][0] = liq["rho"]
+            s.rho[f][0] = liq["rho"] * rho
             s.ncoef_psat[f] = 4
-            for i in range(4):
+            for i in range(3):
                 s.psat[f][i] = liq["psat"][i]
+            s.psat[f][3] = liq["psat"][3] * pres
         s.mass_transfer = self.mass_trans
         s.mom_transfer = self.mom_trans
         s.fixed_parts = self.fixed_parts
         s.cfl = 0.5 if cfl is None else cfl
         s.fuel_ref_temp = self.ref_T
         for d in range(3):
-            s.body_force[d] = self.body_force[d]
+            s.body_force[d] = self.body_force[d] * (100.0 if self.pelec else 1.0)
         return s
 
     def grown(self, b, g):
@@ -408,3 +415,62 @@ def walls(n=20_000, seed=0, steps=2):
 
 CONFIGS = {"config1": config1, "config2": config2, "config3": config3,
            "config4": config4, "config5": config5, "walls": walls}
+
+
+RU_CGS = 8.31446261815324e7   # erg/(mol K)
+
+
+def internal_energy(mech, T, Y):
+    """Mixture specific internal energy [erg/g] of the mechanism's NASA fits:
+    sum_k Y_k (h_k(T) - R T / W_k), h_k = (R/W_k)(sum_n hc_n T^(n+1) + hc_5).
+    T: array; Y: (nspec,) + T.shape."""
+    e = np.zeros_like(T)
+    for k in range(mech.nspec):
+        a = [mech.hc[k][n] for n in range(6)]
+        rw = RU_CGS / mech.mw[k]
+        p = (((a[4] * T + a[3]) * T + a[2]) * T + a[1]) * T + a[0]
+        e += Y[k] * ((p * T + a[5]) * rw - rw * T)
+    return e
+
+
+def to_pelec(prob, mech, guess_offset=-7.0):
+    """The same flow and droplets restated for the PeleC coupling (CGS).
+
+    The state keeps its component slots but holds rho*u [g/(cm^2 s)] in
+    0..2, rho [g/cm^3] in 3, rho*Y in 4.., rho*E = rho (e(T, Y) + |u|^2/2)
+    [erg/cm^3] in 4+NSP and T + guess_offset in 5+NSP: the stored temperature
+    is only the starting guess of the EOS inversion, so the gathered gas
+    temperature comes from the energy.  Lengths x 100, velocities x 100,
+    liquid properties in CGS (Problem.inputs)."""
+    ns = prob.nspec
+    out = Problem(**{k: getattr(prob, k) for k in prob.__dataclass_fields__})
+    out.name = prob.name + "_pelec"
+    out.pelec = True
+    out.plo = prob.plo * 100.0
+    out.phi = prob.phi * 100.0
+    out.dx = prob.dx * 100.0
+    out.meta = dict(prob.meta)
+    states = []
+    for st in prob.state:
+        rho = st[3] * 1e-3
+        vel = st[0:3] * 100.0
+        Y = st[4:4 + ns] / st[3]
+        T = st[5 + ns]
+        q = np.zeros_like(st)
+        q[0:3] = rho * vel
+        q[3] = rho
+        q[4:4 + ns] = rho * Y
+        q[4 + ns] = rho * (internal_energy(mech, T, Y) + 0.5 * np.sum(vel * vel, axis=0))
+        q[5 + ns] = T + guess_offset
+        states.append(np.ascontiguousarray(q))
+    out.state = states
+    nf = prob.nfuel
+    parts = []
+    for p in prob.parts:
+        rd = p["rdata"].copy()
+        rd[0:3] *= 100.0
+        rd[capi.PSTATE_DIA] *= 100.0
+        rd[capi.pstate_filmhght(nf)] *= 100.0
+        parts.append(dict(pos=p["pos"] * 100.0, rdata=rd, id=p["id"].copy()))
+    out.parts = parts
+    return out
