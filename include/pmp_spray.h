@@ -207,7 +207,8 @@ typedef struct pmp_stats {
   long long inner_steps;     /* sum over droplet-substeps of the inner nsub */
   long long fallback;        /* mixed / learned forms: droplets handed to the
                                 plain FP64 kernel (small, out of range) */
-  double kernel_ms;          /* device time of the update kernels */
+  double kernel_ms;          /* device time of the update kernels (host views:
+                                from the first copy in to the last copy out) */
   int graph;                 /* 1: the update replayed a captured CUDA graph,
                                 2: it captured a new one, 0: direct launches */
 } pmp_stats;
@@ -255,7 +256,13 @@ int pmp_spray_update(
   double spray_cfl_lev, void* stream);
 
 /* Same call with HOST views: the state is copied to the device, the source
- * deposits are added into the host source arrays after the update. */
+ * deposits are added into the host source arrays after the update.  The
+ * copies overlap the update: the boxes go in up to 8 groups, each group's
+ * update starting once its views are on the device and its sources copied
+ * back while later groups run (page-locked host memory lets all three
+ * proceed at once).  The FP64 form with a non-default launch shape or CUDA
+ * graph, and the learned form with its audit on, copy, update and copy back
+ * in sequence.  Returns after the sources are back in host memory. */
 int pmp_spray_update_host(
   pmp_spray* h, const pmp_box_view* state, const pmp_box_view* source,
   int nboxes, double flow_dt, double time, int state_ghosts,

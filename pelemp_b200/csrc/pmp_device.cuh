@@ -168,6 +168,9 @@ struct KParams {
   DevStatus* status;
   // PeleC coupling (FP64 form only): energy component of the state
   int pelec, c_eng;
+  // fallback-list kernel: when list_nbox > 0, only the entries of boxes
+  // [list_box0, list_box0 + list_nbox) (one stage of the host-view pipeline)
+  int list_box0, list_nbox;
   // mixed / learned forms: species k of DevMechF (and of their gas-state
   // gather) is mechanism species spec_perm[k]; fuel_first as in DevMechF
   int spec_perm[kMaxSpec];

@@ -105,6 +105,12 @@ struct pmp_spray {
   // device mirrors of host views for pmp_spray_update_host
   std::vector<double*> stage_state, stage_src;
   std::vector<size_t> stage_state_n, stage_src_n;
+  // streams and events of the overlapped host-view update (copy-in, copy-out;
+  // per stage: copied in, updated; start; all copied out)
+  static constexpr int kHostStages = 8;
+  cudaStream_t hs_in = nullptr, hs_out = nullptr;
+  cudaEvent_t hev_in[kHostStages] = {}, hev_done[kHostStages] = {};
+  cudaEvent_t hev_start = nullptr, hev_out = nullptr;
   pmp::LearnState* learn = nullptr;
   pmp::BatchState batch;
   // cell -> box map over the domain (pmp_mesh.cu), rebuilt when the grids or
@@ -152,7 +158,10 @@ int graph_update(pmp_spray* h, const KParams& P, int nboxes, cudaStream_t st, in
 void batch_reset(pmp_spray* h);
 void batch_free(pmp_spray* h);
 // pmp_learn.cu
-int launch_learned(pmp_spray* h, const KParams& P, cudaStream_t st);
+// the learned kernel over CTA-map items [first, first + count) (count < 0: all);
+// the audit runs only with the whole map
+int launch_learned(pmp_spray* h, const KParams& P, cudaStream_t st, int first = 0, int count = -1);
+bool learn_audit_on(const pmp_spray* h);
 bool learn_ready(const pmp_spray* h);
 void learn_free(pmp_spray* h);
 

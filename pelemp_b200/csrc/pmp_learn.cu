@@ -1279,14 +1279,14 @@ __global__ void k_learn_audit(const __grid_constant__ KParams P, const __grid_co
 template <int NS, int NF>
 static int launch_learned_t(pmp_spray* h, const KParams& P, const LearnParams& LP, cudaStream_t st)
 {
-  if (LP.audit_stride > 0) {
+  if (LP.audit_stride > 0 && LP.ncta == h->ncta) {
     const long long n = (h->total + LP.audit_stride - 1) / LP.audit_stride;
     if (n > 0) {
       k_learn_audit<NS, NF><<<nb(n, 128), 128, 0, st>>>(P, LP, h->total);
     }
   }
   constexpr int per = kLearnThreads / kBlock;
-  const int grid = (h->ncta + per - 1) / per;
+  const int grid = (LP.ncta + per - 1) / per;
   constexpr size_t smem = sizeof(MlpSmem) + sizeof(MlpWarpScratch) * (kLearnThreads / 32);
   static_assert(sizeof(MlpSmem) % 16 == 0, "warp scratch must stay 16-byte aligned");
   auto kern = P.fuel_first ? spray_update_learned<NS, NF, kLearnThreads, true>
@@ -1301,8 +1301,18 @@ static int launch_learned_t(pmp_spray* h, const KParams& P, const LearnParams& L
   return PMP_OK;
 }
 
-int launch_learned(pmp_spray* h, const KParams& P, cudaStream_t st)
+int launch_learned(pmp_spray* h, const KParams& P, cudaStream_t st, int first, int count)
 {
+  if (count < 0) {
+    first = 0;
+    count = h->ncta;
+  }
+  if (count == 0) {
+    return PMP_OK;
+  }
+  KParams Q = P;
+  Q.cta_box = P.cta_box + first;
+  Q.cta_start = P.cta_start + first;
   LearnState* L = h->learn;
   if (!L || !L->trained) {
     return PMP_ERR_INVALID;
@@ -1315,9 +1325,9 @@ int launch_learned(pmp_spray* h, const KParams& P, cudaStream_t st)
   LP.norm = L->norm;
   LP.mlp = L->d_mlp;
   LP.audit = L->d_audit;
-  LP.ncta = h->ncta;
+  LP.ncta = count;
   LP.audit_stride = 0;
-  if (L->audit_fraction > 0.) {
+  if (L->audit_fraction > 0. && count == h->ncta) {
     LP.audit_stride = std::max(1LL, (long long)llround(1.0 / L->audit_fraction));
     LP.audit_offset = (long long)(mix64(L->seed++) % (unsigned long long)LP.audit_stride);
     cudaMemsetAsync(L->d_audit, 0, sizeof(double) * 16, st);
@@ -1325,7 +1335,7 @@ int launch_learned(pmp_spray* h, const KParams& P, cudaStream_t st)
   const int ns = h->nspec, nf = h->nfuel;
 #define PMP_LCASE(S, F)                              \
   if (ns == S && nf == F) {                          \
-    return launch_learned_t<S, F>(h, P, LP, st);     \
+    return launch_learned_t<S, F>(h, Q, LP, st);     \
   }
   PMP_LCASE(3, 1)
   PMP_LCASE(5, 1)
@@ -1337,6 +1347,8 @@ int launch_learned(pmp_spray* h, const KParams& P, cudaStream_t st)
 }
 
 bool learn_ready(const pmp_spray* h) { return h->learn && h->learn->trained; }
+
+bool learn_audit_on(const pmp_spray* h) { return h->learn && h->learn->audit_fraction > 0.; }
 
 static void free_state(LearnState* L)
 {

@@ -696,6 +696,8 @@ int prepare_update_impl(
   return PMP_OK;
 }
 
+int finish_update(pmp_spray* h, int graph_state);
+
 int do_update(
   pmp_spray* h, const pmp_box_view* state, const pmp_box_view* source, int nboxes,
   double flow_dt, int state_ghosts, int source_ghosts, int is_virt, int is_ghost, int do_move,
@@ -708,7 +710,6 @@ int do_update(
   if (rc != PMP_OK) {
     return rc;
   }
-  const long long T = h->total;
   const bool graph = h->batch.cfg.use_graph && h->mode != PMP_MODE_LEARNED &&
                      h->batch.cfg.kind != PMP_LAUNCH_PER_BOX;
   int graph_state = 0;
@@ -717,6 +718,167 @@ int do_update(
     return rc;
   }
   PMP_CUDA(h, cudaStreamSynchronize(st));
+  return finish_update(h, graph_state);
+}
+
+// The overlapped form of pmp_spray_update_host.  The boxes are split into up
+// to kHostStages consecutive groups of about equal bytes; group g's state and
+// source are copied in on one stream while the update of the groups before
+// it runs on the caller's stream, and its sources are copied back on a third
+// stream while later groups run.  A droplet reads and deposits only its own
+// box's views, and the CTA map is box-contiguous, so group g's launch (the
+// map's CTA range of its boxes, then the fallback list filtered to its boxes)
+// needs group g's copies only.  hst/hsr are the caller's host views, dst/dsr
+// their device mirrors.
+int update_host_overlapped_impl(
+  pmp_spray* h, const pmp_box_view* hst, const pmp_box_view* hsr, const pmp_box_view* dst,
+  const pmp_box_view* dsr, int nboxes, double flow_dt, int state_ghosts, int source_ghosts,
+  int is_ghost, int do_move, double spray_cfl_lev, cudaStream_t st)
+{
+  KParams P;
+  int rc = prepare_update_impl(h, dst, dsr, nboxes, flow_dt, state_ghosts, source_ghosts,
+                               is_ghost, do_move, spray_cfl_lev, st, P);
+  if (rc != PMP_OK) {
+    return rc;
+  }
+  if (!h->hs_in) {
+    PMP_CUDA(h, cudaStreamCreateWithFlags(&h->hs_in, cudaStreamNonBlocking));
+    PMP_CUDA(h, cudaStreamCreateWithFlags(&h->hs_out, cudaStreamNonBlocking));
+    for (int g = 0; g < pmp_spray::kHostStages; ++g) {
+      PMP_CUDA(h, cudaEventCreateWithFlags(&h->hev_in[g], cudaEventDisableTiming));
+      PMP_CUDA(h, cudaEventCreateWithFlags(&h->hev_done[g], cudaEventDisableTiming));
+    }
+    PMP_CUDA(h, cudaEventCreateWithFlags(&h->hev_start, cudaEventDisableTiming));
+    PMP_CUDA(h, cudaEventCreateWithFlags(&h->hev_out, cudaEventDisableTiming));
+  }
+  // groups of consecutive boxes of about equal bytes
+  std::vector<size_t> bytes(nboxes);
+  size_t total_bytes = 0;
+  for (int b = 0; b < nboxes; ++b) {
+    bytes[b] = sizeof(double) * (view_extent(hst[b]) + 2 * view_extent(hsr[b]));
+    total_bytes += bytes[b];
+  }
+  const int G = std::max(1, std::min(nboxes, (int)pmp_spray::kHostStages));
+  std::vector<int> gfirst(1, 0);
+  {
+    size_t acc = 0;
+    for (int b = 0; b < nboxes; ++b) {
+      acc += bytes[b];
+      const int made = (int)gfirst.size();
+      if (b + 1 < nboxes && made < G && acc * G >= total_bytes * made) {
+        gfirst.push_back(b + 1);
+      }
+    }
+    gfirst.push_back(nboxes);
+  }
+  const int ngroups = (int)gfirst.size() - 1;
+  // first CTA-map item of each box (build_cta_map: ceil(n_b / kBlock) items per box, in box order)
+  std::vector<int> cta_first(nboxes + 1, 0);
+  for (int b = 0; b < nboxes; ++b) {
+    const long long n = h->box_begin[b + 1] - h->box_begin[b];
+    cta_first[b + 1] = cta_first[b] + (int)((n + kBlock - 1) / kBlock);
+  }
+  if (cta_first[nboxes] != h->ncta) {
+    return set_err(h, PMP_ERR_INVALID, "CTA map does not match the boxes");
+  }
+  const int NS = h->nspec;
+  const int NF = h->nfuel;
+  PMP_CUDA(h, cudaMemcpyAsync(h->d_boxes, h->h_boxes, sizeof(BoxEntry) * nboxes,
+                              cudaMemcpyHostToDevice, st));
+  PMP_CUDA(h, cudaMemsetAsync(h->d_status, 0, sizeof(DevStatus), st));
+  PMP_CUDA(h, cudaEventRecord(h->ev0, st));
+  PMP_CUDA(h, cudaEventRecord(h->hev_start, st));
+  PMP_CUDA(h, cudaStreamWaitEvent(h->hs_in, h->hev_start, 0));
+  PMP_CUDA(h, cudaStreamWaitEvent(h->hs_out, h->hev_start, 0));
+  auto copy_in = [&](int g) -> int {
+    for (int b = gfirst[g]; b < gfirst[g + 1]; ++b) {
+      PMP_CUDA(h, cudaMemcpyAsync(dst[b].p, hst[b].p, sizeof(double) * view_extent(hst[b]),
+                                  cudaMemcpyHostToDevice, h->hs_in));
+      PMP_CUDA(h, cudaMemcpyAsync(dsr[b].p, hsr[b].p, sizeof(double) * view_extent(hsr[b]),
+                                  cudaMemcpyHostToDevice, h->hs_in));
+    }
+    PMP_CUDA(h, cudaEventRecord(h->hev_in[g], h->hs_in));
+    return PMP_OK;
+  };
+  rc = copy_in(0);
+  if (rc != PMP_OK) {
+    return rc;
+  }
+  for (int g = 0; g < ngroups; ++g) {
+    PMP_CUDA(h, cudaStreamWaitEvent(st, h->hev_in[g], 0));
+    const int b0 = gfirst[g], b1 = gfirst[g + 1];
+    const int c0 = cta_first[b0], n = cta_first[b1] - c0;
+    KParams Q = P;
+    Q.cta_box = P.cta_box + c0;
+    Q.cta_start = P.cta_start + c0;
+    Q.list_box0 = b0;
+    Q.list_nbox = b1 - b0;
+    if (n > 0) {
+      if (h->mode == PMP_MODE_LEARNED) {
+        rc = pmp::launch_learned(h, P, st, c0, n);
+      } else if (h->mode == PMP_MODE_MIXED) {
+        rc = pmp::launch_mixed(NS, NF, Q, n, kBlock, st);
+      } else if (P.pelec) {
+        rc = dispatch_fp64_pelec(NS, NF, Q, n, st);
+      } else {
+        rc = dispatch_fp64(NS, NF, Q, n, st);
+      }
+      if (rc == PMP_OK && h->mode != PMP_MODE_FP64) {
+        PMP_CUDA(h, cudaGetLastError());
+        rc = dispatch_fp64_list(NS, NF, Q, h->total, st);
+      }
+      if (rc == PMP_ERR_UNSUPPORTED) {
+        return set_err(h, rc, "no kernel for this species / fuel count");
+      }
+      if (rc != PMP_OK) {
+        return rc;
+      }
+      PMP_CUDA(h, cudaGetLastError());
+    }
+    PMP_CUDA(h, cudaEventRecord(h->hev_done[g], st));
+    if (g + 1 < ngroups) {
+      rc = copy_in(g + 1);
+      if (rc != PMP_OK) {
+        return rc;
+      }
+    }
+  }
+  for (int g = 0; g < ngroups; ++g) {
+    PMP_CUDA(h, cudaStreamWaitEvent(h->hs_out, h->hev_done[g], 0));
+    for (int b = gfirst[g]; b < gfirst[g + 1]; ++b) {
+      PMP_CUDA(h, cudaMemcpyAsync(hsr[b].p, dsr[b].p, sizeof(double) * view_extent(hsr[b]),
+                                  cudaMemcpyDeviceToHost, h->hs_out));
+    }
+  }
+  PMP_CUDA(h, cudaEventRecord(h->hev_out, h->hs_out));
+  PMP_CUDA(h, cudaStreamWaitEvent(st, h->hev_out, 0));
+  PMP_CUDA(h, cudaEventRecord(h->ev1, st));
+  PMP_CUDA(h, cudaMemcpyAsync(h->h_status, h->d_status, sizeof(DevStatus), cudaMemcpyDeviceToHost, st));
+  PMP_CUDA(h, cudaStreamSynchronize(st));
+  return finish_update(h, 0);
+}
+
+int update_host_overlapped(
+  pmp_spray* h, const pmp_box_view* hst, const pmp_box_view* hsr, const pmp_box_view* dst,
+  const pmp_box_view* dsr, int nboxes, double flow_dt, int state_ghosts, int source_ghosts,
+  int is_ghost, int do_move, double spray_cfl_lev, cudaStream_t st)
+{
+  const int rc = update_host_overlapped_impl(h, hst, hsr, dst, dsr, nboxes, flow_dt, state_ghosts,
+                                             source_ghosts, is_ghost, do_move, spray_cfl_lev, st);
+  if (rc != PMP_OK && h->hs_in) {
+    // no copy of the caller's host memory may still be in flight on return
+    cudaStreamSynchronize(h->hs_in);
+    cudaStreamSynchronize(h->hs_out);
+    cudaStreamSynchronize(st);
+  }
+  return rc;
+}
+
+// Stats and the error record from the status an update copied back (its
+// stream synchronised).
+int finish_update(pmp_spray* h, int graph_state)
+{
+  const long long T = h->total;
   float ms = 0.f;
   if (cudaEventElapsedTime(&ms, h->ev0, h->ev1) == cudaSuccess) {
     h->stats.kernel_ms = ms;
@@ -951,6 +1113,16 @@ int pmp_spray_destroy(pmp_spray* h)
   }
   if (h->ev1) {
     cudaEventDestroy(h->ev1);
+  }
+  if (h->hs_in) {
+    cudaStreamDestroy(h->hs_in);
+    cudaStreamDestroy(h->hs_out);
+    for (int g = 0; g < pmp_spray::kHostStages; ++g) {
+      cudaEventDestroy(h->hev_in[g]);
+      cudaEventDestroy(h->hev_done[g]);
+    }
+    cudaEventDestroy(h->hev_start);
+    cudaEventDestroy(h->hev_out);
   }
   delete h;
   return PMP_OK;
@@ -1344,14 +1516,27 @@ int pmp_spray_update_host(
       PMP_CUDA(h, cudaMalloc(&h->stage_src[b], sizeof(double) * nsr));
       h->stage_src_n[b] = nsr;
     }
-    PMP_CUDA(h, cudaMemcpyAsync(h->stage_state[b], state[b].p, sizeof(double) * ns,
-                                cudaMemcpyHostToDevice, st));
-    PMP_CUDA(h, cudaMemcpyAsync(h->stage_src[b], source[b].p, sizeof(double) * nsr,
-                                cudaMemcpyHostToDevice, st));
     dst[b] = state[b];
     dst[b].p = h->stage_state[b];
     dsr[b] = source[b];
     dsr[b].p = h->stage_src[b];
+  }
+  // copies overlapped with the update, except for the FP64 form's launch
+  // shapes and graphs and the learned form's audit (whole-map launches)
+  const pmp_launch_config& lc = h->batch.cfg;
+  const bool default_fp64 = lc.kind == PMP_LAUNCH_GRID && lc.block == 128 && lc.regs == 96 && !lc.use_graph;
+  const bool overlapped = h->mode == PMP_MODE_MIXED ||
+                          (h->mode == PMP_MODE_LEARNED && !pmp::learn_audit_on(h)) ||
+                          (h->mode == PMP_MODE_FP64 && (h->pelec || default_fp64));
+  if (overlapped) {
+    return update_host_overlapped(h, state, source, dst.data(), dsr.data(), nboxes, flow_dt,
+                                  state_ghosts, source_ghosts, is_ghost, do_move, spray_cfl_lev, st);
+  }
+  for (int b = 0; b < nboxes; ++b) {
+    PMP_CUDA(h, cudaMemcpyAsync(dst[b].p, state[b].p, sizeof(double) * view_extent(state[b]),
+                                cudaMemcpyHostToDevice, st));
+    PMP_CUDA(h, cudaMemcpyAsync(dsr[b].p, source[b].p, sizeof(double) * view_extent(source[b]),
+                                cudaMemcpyHostToDevice, st));
   }
   const int rc = do_update(h, dst.data(), dsr.data(), nboxes, flow_dt, state_ghosts, source_ghosts,
                            is_virt, is_ghost, do_move, spray_cfl_lev, st);

@@ -472,6 +472,9 @@ __global__ void __launch_bounds__(BLOCK, PMP_FP64_MIN_BLOCKS) spray_update_fp64_
        i += (unsigned long long)gridDim.x * BLOCK) {
     const long long s = P.fb_list[i];
     const int b = box_of_slot(P, s);
+    if (P.list_nbox > 0 && (b < P.list_box0 || b >= P.list_box0 + P.list_nbox)) {
+      continue;
+    }
     update_one<NS, NF, Form::FP64>(P, P.boxes[b], b, s, c);
   }
   flush_counters(P, c);

@@ -39,6 +39,33 @@ def gpu_run(prob, steps, mode=capi.PMP_MODE_FP64, is_ghost=0, keep=None, setup=N
     return parts, srcs, sp
 
 
+def host_run(prob, steps, mode=capi.PMP_MODE_FP64, setup=None, pinned=True):
+    """gpu_run through pmp_spray_update_host: state and sources in host memory
+    (page-locked when pinned)."""
+    import torch
+    sp = from_problem(prob, mode=mode)
+    if setup is not None:
+        setup(sp)
+
+    def host(a):
+        t = torch.from_numpy(np.ascontiguousarray(a))
+        return (t.pin_memory() if pinned else t.clone()).numpy()
+
+    st_h = [host(s) for s in prob.state]
+    st_v = views(st_h, [prob.grown(b, prob.state_ghosts)[0] for b in range(len(prob.boxes))])
+    srcs = []
+    for _step in range(steps):
+        for do_move in (1, 0):
+            src = [host(s) for s in prob.new_sources()]
+            src_v = views(src, [prob.grown(b, prob.source_ghosts)[0] for b in range(len(prob.boxes))])
+            sp.update_particles_host(st_v, src_v, prob.flow_dt, 0.0, prob.state_ghosts,
+                                     prob.source_ghosts, 0, 0, do_move, prob.spray_cfl_lev,
+                                     torch.cuda.current_stream().cuda_stream)
+            srcs.append([s.copy() for s in src])
+    parts = [sp.get_particles(b) for b in range(len(prob.boxes))]
+    return parts, srcs, sp
+
+
 def oracle_run(oracle, prob, steps, is_ghost=0):
     mech = oracle.mech(prob.species)
     rc, fdat = oracle.setup(prob, mech)

@@ -1,0 +1,60 @@
+"""pmp_spray_update_host (host views; the copies overlap the update, in groups
+of boxes) against pmp_spray_update (device views) on a B200.
+
+Each droplet bit-identical after every call; deposits equal up to the order
+of the atomic additions (1e-12 of the component's largest).  Cases: the FP64
+form (several box groups, uneven and empty boxes), the mixed form, the PeleC
+coupling, page-locked and pageable host memory, and the FP64 form with a
+non-default launch shape (copies, update and copy-back in sequence).
+"""
+import numpy as np
+import pytest
+
+from pelemp_b200 import capi
+from pelemp_b200 import workloads as W
+from tests.gpu_util import assert_bitwise, gpu_run, host_run
+from tests.parity import source_errors
+
+pytestmark = pytest.mark.gpu
+
+
+def uneven(total=120_000):
+    """32 boxes of 16^3 with capped-Zipf counts; boxes 3 and 17 emptied."""
+    prob = W.config3(total=total, steps=2, nbox_xyz=(4, 4, 2), box=16)
+    nr = prob.parts[0]["rdata"].shape[0]
+    for b in (3, 17):
+        prob.parts[b] = dict(pos=np.zeros((3, 0)), rdata=np.zeros((nr, 0)),
+                             id=np.zeros(0, dtype=np.int32))
+    return prob
+
+
+def compare(prob, mode=capi.PMP_MODE_FP64, setup=None, pinned=True):
+    pd, sd, _ = gpu_run(prob, prob.steps, mode=mode, setup=setup)
+    ph, sh, sp = host_run(prob, prob.steps, mode=mode, setup=setup, pinned=pinned)
+    assert_bitwise(pd, ph)
+    for a, b in zip(sd, sh):
+        assert source_errors(b, a) <= 1e-12
+    assert sp.stats().substeps > 0
+    return sp
+
+
+@pytest.mark.parametrize("mode", [capi.PMP_MODE_FP64, capi.PMP_MODE_MIXED])
+def test_host_views_uneven_boxes(mode):
+    compare(uneven(), mode)
+
+
+def test_host_views_config2_pageable():
+    prob = W.config2(n=60_000, steps=2, ncells=(32, 32, 32), box=(16, 16, 16))
+    compare(prob, capi.PMP_MODE_MIXED, pinned=False)
+
+
+def test_host_views_pelec():
+    from oracle.pyoracle import Oracle
+    lm = W.config2(n=40_000, steps=2, ncells=(32, 32, 32), box=(16, 16, 16))
+    compare(W.to_pelec(lm, Oracle(pelec=True).mech(lm.species)))
+
+
+def test_host_views_sequential_launch_shape():
+    def persistent(sp):
+        sp.set_launch(kind=capi.PMP_LAUNCH_PERSISTENT, block=128, regs=96, chunk=512)
+    compare(uneven(60_000), setup=persistent)

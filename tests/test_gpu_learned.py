@@ -24,7 +24,8 @@ from oracle import mlp_oracle as M
 from pelemp_b200 import capi
 from pelemp_b200 import workloads as W
 from pelemp_b200.spray import from_problem, learn_debug_grad, learn_debug_infer
-from tests.gpu_util import device_sources, device_state, gpu_run, oracle_run
+from tests.gpu_util import assert_bitwise, device_sources, device_state, gpu_run, host_run, oracle_run
+from tests.parity import source_errors
 from tests.parity import droplet_mass
 
 pytestmark = pytest.mark.gpu
@@ -180,6 +181,22 @@ def test_learned_mass_balance_closes(trained):
     liq = sum(float(np.sum(b - a)) for a, b in zip(m0, m1))
     scale = sum(float(np.sum(np.abs(b - a))) for a, b in zip(m0, m1))
     assert abs(gas + liq) <= 1e-9 * scale
+
+
+def test_learned_host_views_match_device_views(trained):
+    """pmp_spray_update_host's overlapped groups give the device-view result:
+    droplets bit-identical, deposits up to atomic order."""
+    w, _ = trained
+    prob = W.config2(n=30_000, seed=0, **dict(SMALL, steps=2))
+
+    def setup(sp):
+        sp.set_learn_weights(w)
+
+    pd, sd, _ = gpu_run(prob, prob.steps, mode=capi.PMP_MODE_LEARNED, setup=setup)
+    ph, sh, _ = host_run(prob, prob.steps, mode=capi.PMP_MODE_LEARNED, setup=setup)
+    assert_bitwise(pd, ph)
+    for a, b in zip(sd, sh):
+        assert source_errors(b, a) <= 1e-12
 
 
 def test_gate_sends_out_of_range_droplets_to_fp64(trained, oracle):
