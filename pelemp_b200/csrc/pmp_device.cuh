@@ -7,6 +7,8 @@
 // droplet range in the library's cell-sorted SoA.
 #pragma once
 
+#include <cuda_runtime.h>
+
 #include <cstdint>
 
 #include "../../include/pmp_spray.h"
@@ -124,7 +126,34 @@ struct BoxEntry {
   // than 2^31 elements), for cheaper index arithmetic in the update kernels
   int st_j32, st_k32, st_n32;
   int sr_j32, sr_k32, sr_n32;
+  // FP32 gas records of the grown box (mixed and learned forms, written by
+  // k_gas_records before the update): gas_rec4<NS>() float4 per cell,
+  // {rho, T, u, v}, {w, Y_0, Y_1, Y_2}, {Y_3, ...}, mass fractions in the
+  // FP32 tables' species order; cell (i, j, k) is record
+  // (k - state_lo[2]) * gr_k + (j - state_lo[1]) * gr_j + (i - state_lo[0])
+  float4* gr;
+  int gr_j, gr_k;
 };
+
+// float4 records per cell of the FP32 gas records: rho, T, velocity, Y
+__host__ __device__ constexpr int gas_rec4(int ns) { return (8 + ns) / 4; }
+
+#ifdef __CUDACC__
+// Gas record of cell (i, j, k) of box B (inside its grown box), as 4 * R4 floats.
+template <int R4>
+__device__ __forceinline__ void load_gas_rec(const BoxEntry& B, int i, int j, int k, float* rec)
+{
+  const float4* r = B.gr + ((k - B.state_lo[2]) * B.gr_k + (j - B.state_lo[1]) * B.gr_j + (i - B.state_lo[0])) * R4;
+#pragma unroll
+  for (int m = 0; m < R4; ++m) {
+    const float4 v = __ldg(r + m);
+    rec[4 * m] = v.x;
+    rec[4 * m + 1] = v.y;
+    rec[4 * m + 2] = v.z;
+    rec[4 * m + 3] = v.w;
+  }
+}
+#endif
 
 // Device status word block, zeroed before each update.
 struct DevStatus {

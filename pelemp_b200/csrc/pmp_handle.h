@@ -120,6 +120,11 @@ struct pmp_spray {
   int* d_box_map = nullptr;
   void* mesh_scratch = nullptr;
   size_t mesh_scratch_bytes = 0;
+  // FP32 gas records of the mixed and learned forms (BoxEntry::gr): capacity
+  // in float4, and the largest grown box (cells) of the last prepared update
+  float4* gas_rec = nullptr;
+  size_t gas_rec_cap = 0;
+  int gas_rec_max_cells = 0;
   int nr() const { return PMP_PSTATE_NUM(nfuel); }
   int ncomp() const { return 3 + nr(); }
 };

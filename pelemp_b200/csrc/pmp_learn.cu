@@ -799,10 +799,11 @@ __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
         ssv[0][dir] = bflags[dir] > 1 ? 1. : (bflags[dir] < -1 ? 0. : sx_lo);
         ssv[1][dir] = bflags[dir] > 1 ? 0. : (bflags[dir] < -1 ? 1. : sx_hi);
       }
-      double rho = 0., Tg = 0., vg[3] = {0., 0., 0.}, Yg[NS];
+      constexpr int R4 = gas_rec4(NS);
+      float rho = 0.f, Tg = 0.f, vg[3] = {0.f, 0.f, 0.f}, Yg[NS];
 #pragma unroll
       for (int n = 0; n < NS; ++n) {
-        Yg[n] = 0.;
+        Yg[n] = 0.f;
       }
       bool state_ok = true;
 #pragma unroll
@@ -817,19 +818,19 @@ __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
               if (!in_box(B.state_lo, B.state_hi, ci, cj, ck)) {
                 state_ok = false;
               } else {
-                const double* q = B.st + ((ci - B.st_lo[0]) + (cj - B.st_lo[1]) * B.st_j32 + (ck - B.st_lo[2]) * B.st_k32);
-                const double cur_rho = __ldg(q + P.c_rho * B.st_n32);
-                rho = fma(cw, cur_rho, rho);
-                const double w_rho = cw * drcp_from_f(cur_rho);
-#pragma unroll
-                for (int n = 0; n < NS; ++n) {
-                  Yg[n] = fma(w_rho, __ldg(q + (P.c_spec + P.spec_perm[n]) * B.st_n32), Yg[n]);
-                }
+                float rec[4 * R4];
+                load_gas_rec<R4>(B, ci, cj, ck, rec);
+                const float w = (float)cw;
+                rho = fmaf(w, rec[0], rho);
+                Tg = fmaf(w, rec[1], Tg);
 #pragma unroll
                 for (int dir = 0; dir < 3; ++dir) {
-                  vg[dir] = fma(cw, __ldg(q + (P.c_mom + dir) * B.st_n32), vg[dir]);
+                  vg[dir] = fmaf(w, rec[2 + dir], vg[dir]);
                 }
-                Tg = fma(cw, __ldg(q + P.c_T * B.st_n32), Tg);
+#pragma unroll
+                for (int n = 0; n < NS; ++n) {
+                  Yg[n] = fmaf(w, rec[5 + n], Yg[n]);
+                }
               }
             }
           }
@@ -840,16 +841,16 @@ __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
         ok = false;
         active = false;
       } else {
-        g.rho = (float)rho;
-        g.T = (float)Tg;
+        g.rho = rho;
+        g.T = Tg;
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
-          g.vel[d] = (float)vg[d];
+          g.vel[d] = vg[d];
         }
         float mwinv = 0.f;
 #pragma unroll
         for (int n = 0; n < NS; ++n) {
-          g.Y[n] = (float)Yg[n];
+          g.Y[n] = Yg[n];
           mwinv = fmaf(g.Y[n], m.inv_mw_kg[n], mwinv);
         }
         g.p = g.rho * (float)(kRuCgs * kRuConv) * mwinv * g.T;

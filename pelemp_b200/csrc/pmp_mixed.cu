@@ -5,6 +5,8 @@
 // pmp_spray.cu are compiled without it to stay bit-identical to the oracle).
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "spray_kernels.cuh"
 
 namespace pmp {
@@ -29,6 +31,24 @@ int launch_mixed(int ns, int nf, const KParams& P, int ncta, int block, cudaStre
   PMP_MIXED_CASE(4, 1)
   PMP_MIXED_CASE(4, 2)
 #undef PMP_MIXED_CASE
+  return PMP_ERR_UNSUPPORTED;
+}
+
+int launch_gas_records(int ns, const KParams& P, int b0, int nb, int max_cells, cudaStream_t st)
+{
+  if (nb <= 0 || max_cells <= 0) {
+    return PMP_OK;
+  }
+  const dim3 grid((unsigned)std::min((max_cells + 255) / 256, 128), (unsigned)nb);
+#define PMP_REC_CASE(S)                                     \
+  if (ns == S) {                                            \
+    k_gas_records<S><<<grid, 256, 0, st>>>(P, b0);          \
+    return PMP_OK;                                          \
+  }
+  PMP_REC_CASE(3)
+  PMP_REC_CASE(4)
+  PMP_REC_CASE(5)
+#undef PMP_REC_CASE
   return PMP_ERR_UNSUPPORTED;
 }
 

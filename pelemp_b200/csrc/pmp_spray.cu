@@ -23,6 +23,9 @@
 namespace pmp {
 // pmp_mixed.cu
 int launch_mixed(int ns, int nf, const KParams& P, int ncta, int block, cudaStream_t st);
+// FP32 gas records (BoxEntry::gr) of boxes [b0, b0 + nb); max_cells = the
+// largest grown box's cell count
+int launch_gas_records(int ns, const KParams& P, int b0, int nb, int max_cells, cudaStream_t st);
 }  // namespace pmp
 
 using pmp::BoxEntry;
@@ -577,6 +580,32 @@ int prepare_update_impl(
   const int need_state = 1 + std::max({c.rhoIndx, c.momIndx + 2, c.utempIndx, c.specIndx + NS - 1,
                                        h->pelec ? c.engIndx : 0});
   const int need_src = 1 + std::max({c.rhoSrcIndx, c.momSrcIndx + 2, c.engSrcIndx, c.specSrcIndx + NF - 1});
+  // FP32 gas records of the grown boxes for the mixed and learned forms
+  const bool records = h->mode == PMP_MODE_MIXED || h->mode == PMP_MODE_LEARNED;
+  const int R4 = pmp::gas_rec4(NS);
+  size_t rec_total = 0;
+  h->gas_rec_max_cells = 0;
+  if (records) {
+    for (int b = 0; b < nboxes; ++b) {
+      long long cells = 1;
+      for (int d = 0; d < 3; ++d) {
+        cells *= (long long)(h->boxes[b].hi[d] - h->boxes[b].lo[d] + 1 + 2 * state_ghosts);
+      }
+      if (cells * R4 >= (1LL << 31)) {
+        return set_err(h, PMP_ERR_INVALID, "a grown box holds 2^31 gas-record words or more", b);
+      }
+      h->gas_rec_max_cells = std::max(h->gas_rec_max_cells, (int)cells);
+      rec_total += (size_t)cells * R4;
+    }
+    if (rec_total > h->gas_rec_cap) {
+      cudaFree(h->gas_rec);
+      h->gas_rec = nullptr;
+      h->gas_rec_cap = 0;
+      PMP_CUDA(h, cudaMalloc(&h->gas_rec, sizeof(float4) * rec_total));
+      h->gas_rec_cap = rec_total;
+    }
+  }
+  size_t rec_off = 0;
   for (int b = 0; b < nboxes; ++b) {
     const pmp_box& bx = h->boxes[b];
     BoxEntry& e = h->h_boxes[b];
@@ -632,6 +661,15 @@ int prepare_update_impl(
     e.sr_j32 = (int)source[b].jstride;
     e.sr_k32 = (int)source[b].kstride;
     e.sr_n32 = (int)source[b].nstride;
+    if (records) {
+      const int nx = e.state_hi[0] - e.state_lo[0] + 1;
+      const int ny = e.state_hi[1] - e.state_lo[1] + 1;
+      const int nz = e.state_hi[2] - e.state_lo[2] + 1;
+      e.gr = h->gas_rec + rec_off;
+      e.gr_j = nx;
+      e.gr_k = nx * ny;
+      rec_off += (size_t)nx * ny * nz * R4;
+    }
     e.at_bounds = tile_at_bndry(bx, h->geom);
     e.p_begin = h->box_begin[b];
     e.p_end = h->box_begin[b + 1];
@@ -814,6 +852,12 @@ int update_host_overlapped_impl(
     Q.list_box0 = b0;
     Q.list_nbox = b1 - b0;
     if (n > 0) {
+      if (h->mode != PMP_MODE_FP64) {
+        rc = pmp::launch_gas_records(NS, P, b0, b1 - b0, h->gas_rec_max_cells, st);
+        if (rc != PMP_OK) {
+          return set_err(h, rc, "no gas-record kernel for this species count");
+        }
+      }
       if (h->mode == PMP_MODE_LEARNED) {
         rc = pmp::launch_learned(h, P, st, c0, n);
       } else if (h->mode == PMP_MODE_MIXED) {
@@ -981,13 +1025,19 @@ int pmp::enqueue_update(pmp_spray* h, const KParams& P, int nboxes, cudaStream_t
     const int NF = h->nfuel;
     int rc = PMP_OK;
     if (h->mode == PMP_MODE_LEARNED) {
-      rc = pmp::launch_learned(h, P, st);
+      rc = pmp::launch_gas_records(NS, P, 0, nboxes, h->gas_rec_max_cells, st);
+      if (rc == PMP_OK) {
+        rc = pmp::launch_learned(h, P, st);
+      }
       if (rc == PMP_OK) {
         PMP_CUDA(h, cudaGetLastError());
         rc = dispatch_fp64_list(NS, NF, P, h->total, st);
       }
     } else if (h->mode == PMP_MODE_MIXED) {
-      rc = pmp::launch_mixed(NS, NF, P, h->ncta, kBlock, st);
+      rc = pmp::launch_gas_records(NS, P, 0, nboxes, h->gas_rec_max_cells, st);
+      if (rc == PMP_OK) {
+        rc = pmp::launch_mixed(NS, NF, P, h->ncta, kBlock, st);
+      }
       if (rc == PMP_OK) {
         PMP_CUDA(h, cudaGetLastError());
         rc = dispatch_fp64_list(NS, NF, P, h->total, st);
@@ -1104,6 +1154,7 @@ int pmp_spray_destroy(pmp_spray* h)
   for (double* p : h->stage_src) {
     cudaFree(p);
   }
+  cudaFree(h->gas_rec);
   cudaFree(h->d_boxes);
   cudaFreeHost(h->h_boxes);
   cudaFree(h->d_status);

@@ -231,11 +231,12 @@ __device__ __forceinline__ void update_one(const KParams& P, const BoxEntry& B, 
       }
       src.eng = gpv.eng_src;
     } else {
-      // FP64 gather with fused multiply-adds, then the FP32 gas state
-      double rho = 0., Tg = 0., vel_g[3] = {0., 0., 0.}, Yg[NS];
+      // FP32 gather of the cells' gas records (weights from the FP64 position)
+      constexpr int R4 = gas_rec4(NS);
+      float rho = 0.f, Tg = 0.f, vel_g[3] = {0.f, 0.f, 0.f}, Yg[NS];
 #pragma unroll
       for (int n = 0; n < NS; ++n) {
-        Yg[n] = 0.;
+        Yg[n] = 0.f;
       }
 #pragma unroll
       for (int kk = -1; kk < 1; ++kk) {
@@ -251,19 +252,19 @@ __device__ __forceinline__ void update_one(const KParams& P, const BoxEntry& B, 
               if (!in_box(B.state_lo, B.state_hi, ci, cj, ck)) {
                 state_ok = false;
               } else {
-                const double* q = B.st + ((ci - B.st_lo[0]) + (cj - B.st_lo[1]) * B.st_j32 + (ck - B.st_lo[2]) * B.st_k32);
-                const double cur_rho = __ldg(q + P.c_rho * B.st_n32);
-                rho = fma(cw, cur_rho, rho);
-                const double w_rho = cw * drcp_from_f(cur_rho);
-#pragma unroll
-                for (int n = 0; n < NS; ++n) {
-                  Yg[n] = fma(w_rho, __ldg(q + (P.c_spec + P.spec_perm[n]) * B.st_n32), Yg[n]);
-                }
+                float rec[4 * R4];
+                load_gas_rec<R4>(B, ci, cj, ck, rec);
+                const float w = (float)cw;
+                rho = fmaf(w, rec[0], rho);
+                Tg = fmaf(w, rec[1], Tg);
 #pragma unroll
                 for (int dir = 0; dir < 3; ++dir) {
-                  vel_g[dir] = fma(cw, __ldg(q + (P.c_mom + dir) * B.st_n32), vel_g[dir]);
+                  vel_g[dir] = fmaf(w, rec[2 + dir], vel_g[dir]);
                 }
-                Tg = fma(cw, __ldg(q + P.c_T * B.st_n32), Tg);
+#pragma unroll
+                for (int n = 0; n < NS; ++n) {
+                  Yg[n] = fmaf(w, rec[5 + n], Yg[n]);
+                }
               }
             }
           }
@@ -275,16 +276,16 @@ __device__ __forceinline__ void update_one(const KParams& P, const BoxEntry& B, 
         break;
       }
       GasF<NS> g;
-      g.rho = (float)rho;
-      g.T = (float)Tg;
+      g.rho = rho;
+      g.T = Tg;
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
-        g.vel[d] = (float)vel_g[d];
+        g.vel[d] = vel_g[d];
       }
       float mwinv = 0.f;
 #pragma unroll
       for (int n = 0; n < NS; ++n) {
-        g.Y[n] = (float)Yg[n];
+        g.Y[n] = Yg[n];
         mwinv = fmaf(g.Y[n], P.mf.inv_mw_kg[n], mwinv);
       }
       g.p = g.rho * (float)(kRuCgs * kRuConv) * mwinv * g.T;
@@ -461,6 +462,50 @@ __device__ __forceinline__ int box_of_slot(const KParams& P, long long s)
     }
   }
   return lo;
+}
+
+// The FP32 gas records of boxes [b0, b0 + gridDim.y) (BoxEntry::gr), one
+// thread per cell of the grown box, from the FP64 state: the mixed and
+// learned updates then gather 2-3 16-byte records per stencil cell instead of
+// 5 + NS FP64 planes, with rho*Y / rho divided once per cell.
+template <int NS>
+__global__ void __launch_bounds__(256) k_gas_records(const __grid_constant__ KParams P, int b0)
+{
+  constexpr int R4 = gas_rec4(NS);
+  const BoxEntry& B = P.boxes[b0 + blockIdx.y];
+  const int nx = B.state_hi[0] - B.state_lo[0] + 1;
+  const int ny = B.state_hi[1] - B.state_lo[1] + 1;
+  const int nz = B.state_hi[2] - B.state_lo[2] + 1;
+  const int n = nx * ny * nz;
+  for (int c = blockIdx.x * 256 + threadIdx.x; c < n; c += gridDim.x * 256) {
+    const int i = c % nx;
+    const int t = c / nx;
+    const int j = t % ny;
+    const int k = t / ny;
+    const double* q = B.st + ((i + B.state_lo[0] - B.st_lo[0]) + (j + B.state_lo[1] - B.st_lo[1]) * B.st_j32 +
+                              (k + B.state_lo[2] - B.st_lo[2]) * B.st_k32);
+    const double rho = __ldg(q + P.c_rho * B.st_n32);
+    float v[4 * R4];
+    v[0] = (float)rho;
+    v[1] = (float)__ldg(q + P.c_T * B.st_n32);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      v[2 + d] = (float)__ldg(q + (P.c_mom + d) * B.st_n32);
+    }
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      v[5 + s] = (float)(__ldg(q + (P.c_spec + P.spec_perm[s]) * B.st_n32) / rho);
+    }
+#pragma unroll
+    for (int s = 5 + NS; s < 4 * R4; ++s) {
+      v[s] = 0.f;
+    }
+    float4* r = B.gr + (long long)c * R4;
+#pragma unroll
+    for (int m = 0; m < R4; ++m) {
+      r[m] = make_float4(v[4 * m], v[4 * m + 1], v[4 * m + 2], v[4 * m + 3]);
+    }
+  }
 }
 
 template <int NS, int NF, int BLOCK>
