@@ -180,6 +180,10 @@ int batch_enqueue_fp64(pmp_spray* h, const KParams& P, int nboxes, cudaStream_t 
   if (rc != PMP_OK) {
     return rc;
   }
+  rc = launch_gas_records64(h, P, 0, nboxes, st);
+  if (rc != PMP_OK) {
+    return rc;
+  }
   if (!m) {
     return dispatch_fp64_default(ns, nf, P, h->ncta, st);
   }

@@ -133,12 +133,34 @@ struct BoxEntry {
   // (k - state_lo[2]) * gr_k + (j - state_lo[1]) * gr_j + (i - state_lo[0])
   float4* gr;
   int gr_j, gr_k;
+  // FP64 gas records of the grown box (FP64 form; same cell order): per cell
+  // gas_rec2<NS>() double2 {rho, T}, {u, v}, {w, Y_0}, ... (mechanism order),
+  // holding exactly the per-cell terms the gather weights: rho, the cell's T
+  // (PeleC: from its energy), the velocity and Y = (rho Y) * (1 / rho); null
+  // when the FP64 kernel gathers the state planes itself (fallback list,
+  // allocation-free entry point)
+  double2* gr64;
 };
 
 // float4 records per cell of the FP32 gas records: rho, T, velocity, Y
 __host__ __device__ constexpr int gas_rec4(int ns) { return (8 + ns) / 4; }
+// double2 records per cell of the FP64 gas records
+__host__ __device__ constexpr int gas_rec2(int ns) { return (6 + ns) / 2; }
 
 #ifdef __CUDACC__
+// FP64 gas record of cell (i, j, k) of box B (inside its grown box), as 2 * R2 doubles.
+template <int R2>
+__device__ __forceinline__ void load_gas_rec64(const BoxEntry& B, int i, int j, int k, double* rec)
+{
+  const double2* r = B.gr64 + ((k - B.state_lo[2]) * B.gr_k + (j - B.state_lo[1]) * B.gr_j + (i - B.state_lo[0])) * R2;
+#pragma unroll
+  for (int m = 0; m < R2; ++m) {
+    const double2 v = __ldg(r + m);
+    rec[2 * m] = v.x;
+    rec[2 * m + 1] = v.y;
+  }
+}
+
 // Gas record of cell (i, j, k) of box B (inside its grown box), as 4 * R4 floats.
 template <int R4>
 __device__ __forceinline__ void load_gas_rec(const BoxEntry& B, int i, int j, int k, float* rec)

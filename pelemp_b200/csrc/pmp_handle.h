@@ -120,10 +120,11 @@ struct pmp_spray {
   int* d_box_map = nullptr;
   void* mesh_scratch = nullptr;
   size_t mesh_scratch_bytes = 0;
-  // FP32 gas records of the mixed and learned forms (BoxEntry::gr): capacity
-  // in float4, and the largest grown box (cells) of the last prepared update
-  float4* gas_rec = nullptr;
-  size_t gas_rec_cap = 0;
+  // gas records of the grown boxes (BoxEntry::gr, FP32, mixed and learned
+  // forms; BoxEntry::gr64, FP64 form): capacity in bytes, and the largest
+  // grown box (cells) of the last prepared update
+  void* gas_rec = nullptr;
+  size_t gas_rec_bytes = 0;
   int gas_rec_max_cells = 0;
   int nr() const { return PMP_PSTATE_NUM(nfuel); }
   int ncomp() const { return 3 + nr(); }
@@ -159,6 +160,9 @@ int install_packed(pmp_spray* h, double* soa, int* ids, const std::vector<long l
 void mesh_free(pmp_spray* h);
 // pmp_batch.cu
 int batch_enqueue_fp64(pmp_spray* h, const KParams& P, int nboxes, cudaStream_t st);
+// FP64 gas records (BoxEntry::gr64) of boxes [b0, b0 + nb), the handle's coupling;
+// a no-op when the update runs without them
+int launch_gas_records64(const pmp_spray* h, const KParams& P, int b0, int nb, cudaStream_t st);
 int graph_update(pmp_spray* h, const KParams& P, int nboxes, cudaStream_t st, int* graph_state);
 void batch_reset(pmp_spray* h);
 void batch_free(pmp_spray* h);

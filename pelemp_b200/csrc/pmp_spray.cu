@@ -580,30 +580,29 @@ int prepare_update_impl(
   const int need_state = 1 + std::max({c.rhoIndx, c.momIndx + 2, c.utempIndx, c.specIndx + NS - 1,
                                        h->pelec ? c.engIndx : 0});
   const int need_src = 1 + std::max({c.rhoSrcIndx, c.momSrcIndx + 2, c.engSrcIndx, c.specSrcIndx + NF - 1});
-  // FP32 gas records of the grown boxes for the mixed and learned forms
-  const bool records = h->mode == PMP_MODE_MIXED || h->mode == PMP_MODE_LEARNED;
-  const int R4 = pmp::gas_rec4(NS);
+  // gas records of the grown boxes: FP32 for the mixed and learned forms, FP64
+  // for the FP64 form (16-byte units per cell: R)
+  const bool rec32 = h->mode == PMP_MODE_MIXED || h->mode == PMP_MODE_LEARNED;
+  const int R = rec32 ? pmp::gas_rec4(NS) : pmp::gas_rec2(NS);
   size_t rec_total = 0;
   h->gas_rec_max_cells = 0;
-  if (records) {
-    for (int b = 0; b < nboxes; ++b) {
-      long long cells = 1;
-      for (int d = 0; d < 3; ++d) {
-        cells *= (long long)(h->boxes[b].hi[d] - h->boxes[b].lo[d] + 1 + 2 * state_ghosts);
-      }
-      if (cells * R4 >= (1LL << 31)) {
-        return set_err(h, PMP_ERR_INVALID, "a grown box holds 2^31 gas-record words or more", b);
-      }
-      h->gas_rec_max_cells = std::max(h->gas_rec_max_cells, (int)cells);
-      rec_total += (size_t)cells * R4;
+  for (int b = 0; b < nboxes; ++b) {
+    long long cells = 1;
+    for (int d = 0; d < 3; ++d) {
+      cells *= (long long)(h->boxes[b].hi[d] - h->boxes[b].lo[d] + 1 + 2 * state_ghosts);
     }
-    if (rec_total > h->gas_rec_cap) {
-      cudaFree(h->gas_rec);
-      h->gas_rec = nullptr;
-      h->gas_rec_cap = 0;
-      PMP_CUDA(h, cudaMalloc(&h->gas_rec, sizeof(float4) * rec_total));
-      h->gas_rec_cap = rec_total;
+    if (cells * R >= (1LL << 31)) {
+      return set_err(h, PMP_ERR_INVALID, "a grown box holds 2^31 gas-record words or more", b);
     }
+    h->gas_rec_max_cells = std::max(h->gas_rec_max_cells, (int)cells);
+    rec_total += (size_t)cells * R;
+  }
+  if (16 * rec_total > h->gas_rec_bytes) {
+    cudaFree(h->gas_rec);
+    h->gas_rec = nullptr;
+    h->gas_rec_bytes = 0;
+    PMP_CUDA(h, cudaMalloc(&h->gas_rec, 16 * rec_total));
+    h->gas_rec_bytes = 16 * rec_total;
   }
   size_t rec_off = 0;
   for (int b = 0; b < nboxes; ++b) {
@@ -661,14 +660,18 @@ int prepare_update_impl(
     e.sr_j32 = (int)source[b].jstride;
     e.sr_k32 = (int)source[b].kstride;
     e.sr_n32 = (int)source[b].nstride;
-    if (records) {
+    {
       const int nx = e.state_hi[0] - e.state_lo[0] + 1;
       const int ny = e.state_hi[1] - e.state_lo[1] + 1;
       const int nz = e.state_hi[2] - e.state_lo[2] + 1;
-      e.gr = h->gas_rec + rec_off;
+      if (rec32) {
+        e.gr = static_cast<float4*>(h->gas_rec) + rec_off;
+      } else {
+        e.gr64 = static_cast<double2*>(h->gas_rec) + rec_off;
+      }
       e.gr_j = nx;
       e.gr_k = nx * ny;
-      rec_off += (size_t)nx * ny * nz * R4;
+      rec_off += (size_t)nx * ny * nz * R;
     }
     e.at_bounds = tile_at_bndry(bx, h->geom);
     e.p_begin = h->box_begin[b];
@@ -852,11 +855,10 @@ int update_host_overlapped_impl(
     Q.list_box0 = b0;
     Q.list_nbox = b1 - b0;
     if (n > 0) {
-      if (h->mode != PMP_MODE_FP64) {
-        rc = pmp::launch_gas_records(NS, P, b0, b1 - b0, h->gas_rec_max_cells, st);
-        if (rc != PMP_OK) {
-          return set_err(h, rc, "no gas-record kernel for this species count");
-        }
+      rc = h->mode != PMP_MODE_FP64 ? pmp::launch_gas_records(NS, P, b0, b1 - b0, h->gas_rec_max_cells, st)
+                                    : pmp::launch_gas_records64(h, P, b0, b1 - b0, st);
+      if (rc != PMP_OK) {
+        return set_err(h, rc, "no gas-record kernel for this species count");
       }
       if (h->mode == PMP_MODE_LEARNED) {
         rc = pmp::launch_learned(h, P, st, c0, n);
@@ -1043,7 +1045,10 @@ int pmp::enqueue_update(pmp_spray* h, const KParams& P, int nboxes, cudaStream_t
         rc = dispatch_fp64_list(NS, NF, P, h->total, st);
       }
     } else if (P.pelec) {
-      rc = dispatch_fp64_pelec(NS, NF, P, h->ncta, st);
+      rc = pmp::launch_gas_records64(h, P, 0, nboxes, st);
+      if (rc == PMP_OK) {
+        rc = dispatch_fp64_pelec(NS, NF, P, h->ncta, st);
+      }
     } else {
       rc = pmp::batch_enqueue_fp64(h, P, nboxes, st);
     }
@@ -1067,6 +1072,29 @@ int pmp::run_update(
 {
   return do_update(h, state, source, nboxes, flow_dt, state_ghosts, source_ghosts, 0, is_ghost,
                    do_move, spray_cfl_lev, st);
+}
+
+int pmp::launch_gas_records64(const pmp_spray* h, const KParams& P, int b0, int nb, cudaStream_t st)
+{
+  const int max_cells = h->gas_rec_max_cells;
+  if (nb <= 0 || max_cells <= 0 || h->mode != PMP_MODE_FP64) {
+    return PMP_OK;
+  }
+  const dim3 grid((unsigned)std::min((max_cells + 255) / 256, 128), (unsigned)nb);
+#define PMP_REC_CASE(S)                                                  \
+  if (h->nspec == S) {                                                   \
+    if (h->pelec) {                                                      \
+      pmp::k_gas_records64<S, true><<<grid, 256, 0, st>>>(P, b0);        \
+    } else {                                                             \
+      pmp::k_gas_records64<S, false><<<grid, 256, 0, st>>>(P, b0);       \
+    }                                                                    \
+    return PMP_OK;                                                       \
+  }
+  PMP_REC_CASE(3)
+  PMP_REC_CASE(4)
+  PMP_REC_CASE(5)
+#undef PMP_REC_CASE
+  return PMP_ERR_UNSUPPORTED;
 }
 
 int pmp::dispatch_fp64_default(int ns, int nf, const KParams& P, int ncta, cudaStream_t st)

@@ -151,6 +151,22 @@ __device__ __forceinline__ void update_one(const KParams& P, const BoxEntry& B, 
               const int ck = ijk[2] + kk;
               if (!in_box(B.state_lo, B.state_hi, ci, cj, ck)) {
                 state_ok = false;
+              } else if (B.gr64) {
+                // the cell's record holds the same per-cell terms the plane
+                // gather below forms (k_gas_records64), so the sums are equal
+                constexpr int R2 = gas_rec2(NS);
+                double rec[2 * R2];
+                load_gas_rec64<R2>(B, ci, cj, ck, rec);
+                gpv.rho = __dadd_rn(gpv.rho, __dmul_rn(cw, rec[0]));
+#pragma unroll
+                for (int n = 0; n < NS; ++n) {
+                  gpv.Y[n] = __dadd_rn(gpv.Y[n], __dmul_rn(cw, rec[5 + n]));
+                }
+#pragma unroll
+                for (int dir = 0; dir < 3; ++dir) {
+                  gpv.vel[dir] = __dadd_rn(gpv.vel[dir], __dmul_rn(cw, rec[2 + dir]));
+                }
+                gpv.T = __dadd_rn(gpv.T, __dmul_rn(cw, rec[1]));
               } else {
                 const double* q = B.st + ((ci - B.st_lo[0]) + (cj - B.st_lo[1]) * B.st_j32 + (ck - B.st_lo[2]) * B.st_k32);
                 const double cur_rho = __ldg(q + P.c_rho * B.st_n32);
@@ -504,6 +520,66 @@ __global__ void __launch_bounds__(256) k_gas_records(const __grid_constant__ KPa
 #pragma unroll
     for (int m = 0; m < R4; ++m) {
       r[m] = make_float4(v[4 * m], v[4 * m + 1], v[4 * m + 2], v[4 * m + 3]);
+    }
+  }
+}
+
+// The FP64 gas records of boxes [b0, b0 + gridDim.y) (BoxEntry::gr64): per
+// cell of the grown box, rho, T, the velocity and the mass fractions formed
+// with exactly the operations of update_one's plane gather (PeleC: velocity
+// from momentum, T by EY2T from the cell's energy with its T as the guess),
+// so that the gathered sums are bit-identical.  Each cell is then converted
+// once per call instead of once per droplet and stencil corner (the PeleC
+// EOS inversion and the 1 / rho division included).
+template <int NS, bool PELEC>
+__global__ void __launch_bounds__(256) k_gas_records64(const __grid_constant__ KParams P, int b0)
+{
+  constexpr int R2 = gas_rec2(NS);
+  const BoxEntry& B = P.boxes[b0 + blockIdx.y];
+  const int nx = B.state_hi[0] - B.state_lo[0] + 1;
+  const int ny = B.state_hi[1] - B.state_lo[1] + 1;
+  const int nz = B.state_hi[2] - B.state_lo[2] + 1;
+  const int n = nx * ny * nz;
+  for (int c = blockIdx.x * 256 + threadIdx.x; c < n; c += gridDim.x * 256) {
+    const int i = c % nx;
+    const int t = c / nx;
+    const int j = t % ny;
+    const int k = t / ny;
+    const double* q = B.st + ((i + B.state_lo[0] - B.st_lo[0]) + (j + B.state_lo[1] - B.st_lo[1]) * B.st_j32 +
+                              (k + B.state_lo[2] - B.st_lo[2]) * B.st_k32);
+    const double cur_rho = __ldg(q + P.c_rho * B.st_n32);
+    const double inv_rho = 1. / cur_rho;
+    double v[2 * R2];
+    v[0] = cur_rho;
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      v[5 + s] = __dmul_rn(__ldg(q + (P.c_spec + s) * B.st_n32), inv_rho);
+    }
+    if (!PELEC) {
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        v[2 + d] = __ldg(q + (P.c_mom + d) * B.st_n32);
+      }
+      v[1] = __ldg(q + P.c_T * B.st_n32);
+    } else {
+      double ke = 0.;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const double vel = __dmul_rn(__ldg(q + (P.c_mom + d) * B.st_n32), inv_rho);
+        v[2 + d] = vel;
+        ke = __dadd_rn(ke, __dmul_rn(vel, vel) / 2.);
+      }
+      const double intEng = __dsub_rn(__dmul_rn(__ldg(q + P.c_eng * B.st_n32), inv_rho), ke);
+      v[1] = ey2t<NS>(P.m, intEng, v + 5, __ldg(q + P.c_T * B.st_n32));
+    }
+#pragma unroll
+    for (int s = 5 + NS; s < 2 * R2; ++s) {
+      v[s] = 0.;
+    }
+    double2* r = B.gr64 + (long long)c * R2;
+#pragma unroll
+    for (int m = 0; m < R2; ++m) {
+      r[m] = make_double2(v[2 * m], v[2 * m + 1]);
     }
   }
 }
