@@ -52,7 +52,8 @@ __device__ __forceinline__ void cell_of(const KParams& P, const double* pos, dou
 // works on one box (read at low latency, without re-deriving addresses), or
 // the global entry otherwise
 template <int NS, int NF, Form FORM, bool FF = false, bool PELEC = false>
-__device__ __forceinline__ void update_one(const KParams& P, const BoxEntry& B, int b, long long s, Counters& c)
+__device__ __forceinline__ void update_one(const KParams& P, const BoxEntry& B, int b, long long s, Counters& c,
+                                           double* sx = nullptr, int sxs = 0)
 {
   int id = P.parts.id[s];
   if (!(id > 0)) {
@@ -97,6 +98,15 @@ __device__ __forceinline__ void update_one(const KParams& P, const BoxEntry& B, 
     double lx[3];
     int ijk[3], ijkc[3];
     cell_of(P, pos, lx, ijk, ijkc);
+    if (FORM == Form::MIXED) {
+      // the mixed form keeps the position in shared memory across the
+      // droplet physics (sx: this thread's slots, stride sxs), which does
+      // not read it: fewer registers live there, fewer spills
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        sx[d * sxs] = pos[d];
+      }
+    }
     // trilinear_interp (SprayInterpolation.H:158-199)
     double ssv[2][3];
 #pragma unroll
@@ -312,7 +322,16 @@ __device__ __forceinline__ void update_one(const KParams& P, const BoxEntry& B, 
       for (int spf = 0; spf < NF; ++spf) {
         cBoilT[spf] = fminf(P.ff.critT[spf], fdiv(1.f, fmaf(lp, P.ff.hb[spf], P.ff.inv_boilT[spf])));
       }
-      nsub = spray_source_mixed<NS, NF, FF>(P, P.sub_dt, g, cBoilT, vel, T, dia, Y, num_ppp, id, src);
+      nsub = spray_source_mixed<NS, NF, FF>(P, P.sub_dt, g, cBoilT, vel, T, dia, Y, num_ppp, id, src, sx, sxs);
+      {
+        // the position and the cell it gives, back from shared memory
+        const volatile double* vx = sx;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          pos[d] = vx[d * sxs];
+        }
+        cell_of(P, pos, lx, ijk, ijkc);
+      }
     }
     c.sub += 1;
     c.inner += static_cast<unsigned>(nsub);
@@ -405,8 +424,8 @@ __device__ __forceinline__ void flush_counters(const KParams& P, Counters& c)
 #define PMP_FP64_MIN_BLOCKS 5  /* 96 registers: 5 CTAs of 128 per SM (measured best) */
 #endif
 #ifndef PMP_MIXED_MIN_BLOCKS
-#define PMP_MIXED_MIN_BLOCKS 8  /* 64 registers: 8 CTAs of 128 per SM; the spills cost less than the
-                                   latency the extra warps hide (measured against 4, 6, 7) */
+#define PMP_MIXED_MIN_BLOCKS 7  /* 72 registers: 7 CTAs of 128 per SM (measured best against 6 and 8
+                                   with the FP32 gas records and the shared-memory stash) */
 #endif
 
 // copy box b's entry into shared memory (all threads of the CTA call it)
@@ -458,8 +477,12 @@ __global__ void __launch_bounds__(BLOCK, PMP_MIXED_MIN_BLOCKS) spray_update_mixe
   stage_box(P, b, sB);
   const long long s = P.cta_start[blockIdx.x] + threadIdx.x;
   Counters c;
+  // per thread: position, parcel count, start mass, composition (update_one,
+  // spray_source_mixed)
+  __shared__ double stash[(5 + NF) * BLOCK];
+  double* sx = stash + threadIdx.x;
   if (s < sB.p_end) {
-    update_one<NS, NF, Form::MIXED, FF>(P, sB, b, s, c);
+    update_one<NS, NF, Form::MIXED, FF>(P, sB, b, s, c, sx, BLOCK);
   }
   flush_counters(P, c);
 }

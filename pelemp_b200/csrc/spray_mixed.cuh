@@ -247,7 +247,8 @@ struct SrcD {
 template <int NS, int NF, bool FF>
 __device__ __forceinline__ int spray_source_mixed(
   const KParams& P, double flow_dt, const GasF<NS>& g, const float* cBoilT, double* vel_io,
-  double& T_io, double& dia_io, double* Y_io, double num_ppp, int& id, SrcD<NF>& src)
+  double& T_io, double& dia_io, double* Y_io, double num_ppp, int& id, SrcD<NF>& src,
+  double* sx, int sxs)
 {
   const DevMechF& m = P.mf;
   const DevFuelF& ff = P.ff;
@@ -288,6 +289,15 @@ __device__ __forceinline__ int spray_source_mixed(
   int nsub = 1;
   double pmass = PMP_PI / 6. * rho_part * (dia_part * dia_part * dia_part);
   const double startmass = pmass;
+  {
+    // values needed only after the inner sub-steps: in shared memory across them
+    sx[3 * sxs] = num_ppp;
+    sx[4 * sxs] = startmass;
+#pragma unroll
+    for (int spf = 0; spf < NF; ++spf) {
+      sx[(5 + spf) * sxs] = Y_io[spf];
+    }
+  }
   // sums over the inner sub-steps in FP32; times the parcel count in FP64 at the end
   float eng_acc = 0.f;
   float mom_acc[3] = {0.f, 0.f, 0.f};
@@ -567,6 +577,15 @@ __device__ __forceinline__ int spray_source_mixed(
     }
     ++isub;
   }
+  // back from shared memory (volatile: read there, not kept in registers)
+  const volatile double* vx = sx;
+  num_ppp = vx[3 * sxs];
+  const double startmass_ = vx[4 * sxs];
+  double Y0[NF];
+#pragma unroll
+  for (int spf = 0; spf < NF; ++spf) {
+    Y0[spf] = vx[(5 + spf) * sxs];
+  }
   src.eng = num_ppp * (double)eng_acc;
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
@@ -580,7 +599,7 @@ __device__ __forceinline__ int spray_source_mixed(
     }
   }
   const double inv_dtf = 1. / (fdat.dtmod * flow_dt);
-  const double mdot_total = (pmass - startmass) * inv_dtf;
+  const double mdot_total = (pmass - startmass_) * inv_dtf;
   src.mass = num_ppp * mdot_total;
   if (fdat.mom_trans) {
 #pragma unroll
@@ -590,7 +609,7 @@ __device__ __forceinline__ int spray_source_mixed(
   }
 #pragma unroll
   for (int spf = 0; spf < NF; ++spf) {
-    const double midot = (Y_part[spf] * pmass - Y_io[spf] * startmass) * inv_dtf;
+    const double midot = (Y_part[spf] * pmass - Y0[spf] * startmass_) * inv_dtf;
     src.Ydot[spf] = num_ppp * midot;
     src.eng += num_ppp * midot * (double)hf(m, dep_sp<FF>(fdat, spf), T_h);
     Y_io[spf] = Y_part[spf];
