@@ -682,15 +682,20 @@ static void build_mlp(const std::vector<float>& p, MlpSmem& S)
 #define PMP_LEARNED_MIN_BLOCKS 2
 #endif
 constexpr int kLearnThreads = PMP_LEARNED_THREADS;  // threads per CTA, a multiple of kBlock
+constexpr int kLearnStash = 5 + PMP_MAX_FUEL;        // shared-memory doubles per thread
 
 template <int NS, int NF, int BLOCK, bool FF>
 __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
   spray_update_learned(const __grid_constant__ KParams P, const __grid_constant__ LearnParams L)
 {
-  // dynamic shared memory: the network's weights, then one scratch per warp
+  // dynamic shared memory: the network's weights, one scratch per warp, then
+  // per thread the values the droplet physics does not read (position,
+  // parcel count, start mass, composition: kLearnStash doubles, stride BLOCK)
   extern __shared__ __align__(16) unsigned char learn_smem[];
   MlpSmem& S = *reinterpret_cast<MlpSmem*>(learn_smem);
   MlpWarpScratch* WS = reinterpret_cast<MlpWarpScratch*>(learn_smem + sizeof(MlpSmem));
+  double* sx = reinterpret_cast<double*>(learn_smem + sizeof(MlpSmem) + sizeof(MlpWarpScratch) * (BLOCK / 32)) +
+               threadIdx.x;
   {
     const int4* src = reinterpret_cast<const int4*>(L.mlp);
     int4* dst = reinterpret_cast<int4*>(&S);
@@ -759,6 +764,13 @@ __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
       ok = false;
     }
   }
+  // a wall-film droplet stops the first sub-cycle (the film height never
+  // changes here, so the check is made once)
+  if (valid && ok && P.num_iter > 0 && id > 0 && film > 0.) {
+    set_error(P, PMP_ERR_UNSUPPORTED, b, s);
+    ok = false;
+  }
+  sx[3 * BLOCK] = num_ppp;
   const unsigned FULL = 0xffffffffu;
   for (int cur_iter = 0; cur_iter < P.num_iter; ++cur_iter) {
     // cell of the droplet (recomputed from the position each sub-cycle, so
@@ -767,10 +779,9 @@ __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
     int ijk[3], ijkc[3];
     cell_of(P, pos, lx, ijk, ijkc);
     bool active = valid && ok && id > 0;
-    if (active && film > 0.) {
-      set_error(P, PMP_ERR_UNSUPPORTED, b, s);
-      ok = false;
-      active = false;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      sx[d * BLOCK] = pos[d];
     }
     GasF<NS> g;
     float cBoilT[NF];
@@ -880,8 +891,13 @@ __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
     const double flow_dt = P.sub_dt;
     int isub = 1, nsub = 1;
     double pmass = PMP_PI / 6. * rho_part * (dia_part * dia_part * dia_part);
-    const double startmass = pmass;
-    double eng_acc = 0., mom_acc[3] = {0., 0., 0.};
+    sx[4 * BLOCK] = pmass;
+#pragma unroll
+    for (int spf = 0; spf < NF; ++spf) {
+      sx[(5 + spf) * BLOCK] = Y[spf];
+    }
+    // sums over the inner sub-steps in FP32; times the parcel count in FP64 at the end
+    float eng_acc = 0.f, mom_acc[3] = {0.f, 0.f, 0.f};
     float T_h = (float)T_part;
     bool pending = active;
     bool fell_back = false;
@@ -1005,16 +1021,15 @@ __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
           part_vel_src[d] = drag_force_p * diff_vel[d] + ff.body_force[d];
         }
         if (fdat.mom_trans) {
-          const double nd = num_ppp * (double)drag_force;
 #pragma unroll
           for (int d = 0; d < 3; ++d) {
-            mom_acc[d] += nd * (double)diff_vel[d];
+            mom_acc[d] = fmaf(drag_force, diff_vel[d], mom_acc[d]);
           }
           if (isub == 1) {
             nsub = min(max(nsub, static_cast<int>((float)flow_dt * drag_force_p) + 1), 100);
           }
         }
-        eng_acc += num_ppp * (double)conv_src;
+        eng_acc += conv_src;
         const float part_temp_src = fdiv((sumL + conv_src) * inv_pmass, cp_part);
         if (isub == 1 && delT > 1e-15f) {
           const float inv_tau_d = fdiv(-m_dot, 0.2f * (float)pmass);
@@ -1069,14 +1084,28 @@ __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
         pending = isub <= nsub;
       }
     }
+    // back from shared memory (volatile: read there, not kept in registers
+    // across the sub-steps), and the cell the position gives
+    const volatile double* vx = sx;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      pos[d] = vx[d * BLOCK];
+    }
+    num_ppp = vx[3 * BLOCK];
+    const double startmass = vx[4 * BLOCK];
+#pragma unroll
+    for (int spf = 0; spf < NF; ++spf) {
+      Y[spf] = vx[(5 + spf) * BLOCK];
+    }
+    cell_of(P, pos, lx, ijk, ijkc);
     if (fell_back) {
       continue;
     }
     if (active) {
-      src.eng = eng_acc;
+      src.eng = num_ppp * (double)eng_acc;
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
-        src.mom[d] = mom_acc[d];
+        src.mom[d] = num_ppp * (double)mom_acc[d];
       }
       if (nsub > 1) {
         src.eng /= static_cast<double>(nsub);
@@ -1288,7 +1317,8 @@ static int launch_learned_t(pmp_spray* h, const KParams& P, const LearnParams& L
   }
   constexpr int per = kLearnThreads / kBlock;
   const int grid = (LP.ncta + per - 1) / per;
-  constexpr size_t smem = sizeof(MlpSmem) + sizeof(MlpWarpScratch) * (kLearnThreads / 32);
+  constexpr size_t smem = sizeof(MlpSmem) + sizeof(MlpWarpScratch) * (kLearnThreads / 32) +
+                          sizeof(double) * kLearnStash * kLearnThreads;
   static_assert(sizeof(MlpSmem) % 16 == 0, "warp scratch must stay 16-byte aligned");
   auto kern = P.fuel_first ? spray_update_learned<NS, NF, kLearnThreads, true>
                            : spray_update_learned<NS, NF, kLearnThreads, false>;
