@@ -517,7 +517,10 @@ def main():
                  for s in prob.new_sources()]
         st_hv = views(st_h, [prob.grown(b, prob.state_ghosts)[0] for b in range(nboxes)])
         src_hv = views(src_h, [prob.grown(b, prob.source_ghosts)[0] for b in range(nboxes)])
-        h2d = 2 * sum(a.nbytes for a in st_h) + 2 * sum(a.nbytes for a in src_h)
+        # the state components the update reads (rho, velocity, T, species: all
+        # but rhoH) and every source component are copied, for MKD and MK
+        used = (5 + prob.nspec) / prob.n_state_comp
+        h2d = 2 * used * sum(a.nbytes for a in st_h) + 2 * sum(a.nbytes for a in src_h)
         d2h = 2 * sum(a.nbytes for a in src_h)
 
         # the deposits accumulate in the host source arrays over the timed

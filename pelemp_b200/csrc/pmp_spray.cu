@@ -462,6 +462,57 @@ size_t view_extent(const pmp_box_view& v)
   return (size_t)((v.ncomp - 1) * v.nstride + (nz - 1) * v.kstride + (ny - 1) * v.jstride + nx);
 }
 
+// The components an update reads of the state (rho, momentum or velocity,
+// T, species; PeleC: energy) or reads and writes of the source, as runs
+// [first, last) of consecutive components: the host-view update copies only
+// these.
+std::vector<std::pair<int, int>> comp_runs(const pmp_spray* h, bool state)
+{
+  const pmp_spray_comps& c = h->comps;
+  std::vector<int> need;
+  if (state) {
+    need = {c.rhoIndx, c.momIndx, c.momIndx + 1, c.momIndx + 2, c.utempIndx};
+    for (int n = 0; n < h->nspec; ++n) {
+      need.push_back(c.specIndx + n);
+    }
+    if (h->pelec) {
+      need.push_back(c.engIndx);
+    }
+  } else {
+    need = {c.rhoSrcIndx, c.momSrcIndx, c.momSrcIndx + 1, c.momSrcIndx + 2, c.engSrcIndx};
+    for (int n = 0; n < h->nfuel; ++n) {
+      need.push_back(c.specSrcIndx + n);
+    }
+  }
+  std::sort(need.begin(), need.end());
+  need.erase(std::unique(need.begin(), need.end()), need.end());
+  std::vector<std::pair<int, int>> runs;
+  for (int n : need) {
+    if (!runs.empty() && runs.back().second == n) {
+      runs.back().second = n + 1;
+    } else {
+      runs.push_back({n, n + 1});
+    }
+  }
+  return runs;
+}
+
+// Copies components runs of view v (same layout at dst and src).
+cudaError_t copy_runs(double* dst, const double* src, const pmp_box_view& v,
+                      const std::vector<std::pair<int, int>>& runs, cudaMemcpyKind kind, cudaStream_t st)
+{
+  const size_t one = view_extent(v) - (size_t)(v.ncomp - 1) * v.nstride;  // one component's extent
+  for (const auto& r : runs) {
+    const size_t off = (size_t)r.first * v.nstride;
+    const size_t n = (size_t)(r.second - 1 - r.first) * v.nstride + one;
+    const cudaError_t e = cudaMemcpyAsync(dst + off, src + off, sizeof(double) * n, kind, st);
+    if (e != cudaSuccess) {
+      return e;
+    }
+  }
+  return cudaSuccess;
+}
+
 // tile_at_bndry (Source/PP_Spray/WallFunctions.H:8-35)
 int tile_at_bndry(const pmp_box& b, const pmp_geometry& g)
 {
@@ -831,12 +882,12 @@ int update_host_overlapped_impl(
   PMP_CUDA(h, cudaEventRecord(h->hev_start, st));
   PMP_CUDA(h, cudaStreamWaitEvent(h->hs_in, h->hev_start, 0));
   PMP_CUDA(h, cudaStreamWaitEvent(h->hs_out, h->hev_start, 0));
+  const auto st_runs = comp_runs(h, true);
+  const auto sr_runs = comp_runs(h, false);
   auto copy_in = [&](int g) -> int {
     for (int b = gfirst[g]; b < gfirst[g + 1]; ++b) {
-      PMP_CUDA(h, cudaMemcpyAsync(dst[b].p, hst[b].p, sizeof(double) * view_extent(hst[b]),
-                                  cudaMemcpyHostToDevice, h->hs_in));
-      PMP_CUDA(h, cudaMemcpyAsync(dsr[b].p, hsr[b].p, sizeof(double) * view_extent(hsr[b]),
-                                  cudaMemcpyHostToDevice, h->hs_in));
+      PMP_CUDA(h, copy_runs(dst[b].p, hst[b].p, hst[b], st_runs, cudaMemcpyHostToDevice, h->hs_in));
+      PMP_CUDA(h, copy_runs(dsr[b].p, hsr[b].p, hsr[b], sr_runs, cudaMemcpyHostToDevice, h->hs_in));
     }
     PMP_CUDA(h, cudaEventRecord(h->hev_in[g], h->hs_in));
     return PMP_OK;
@@ -892,8 +943,7 @@ int update_host_overlapped_impl(
   for (int g = 0; g < ngroups; ++g) {
     PMP_CUDA(h, cudaStreamWaitEvent(h->hs_out, h->hev_done[g], 0));
     for (int b = gfirst[g]; b < gfirst[g + 1]; ++b) {
-      PMP_CUDA(h, cudaMemcpyAsync(hsr[b].p, dsr[b].p, sizeof(double) * view_extent(hsr[b]),
-                                  cudaMemcpyDeviceToHost, h->hs_out));
+      PMP_CUDA(h, copy_runs(hsr[b].p, dsr[b].p, hsr[b], sr_runs, cudaMemcpyDeviceToHost, h->hs_out));
     }
   }
   PMP_CUDA(h, cudaEventRecord(h->hev_out, h->hs_out));
@@ -1318,6 +1368,14 @@ int pmp_spray_set_comps(pmp_spray* h, const pmp_spray_comps* comps)
   if (!h || !comps) {
     return PMP_ERR_INVALID;
   }
+  const int idx[] = {comps->rhoIndx,    comps->momIndx,    comps->engIndx,
+                     comps->utempIndx,  comps->specIndx,   comps->rhoSrcIndx,
+                     comps->momSrcIndx, comps->engSrcIndx, comps->specSrcIndx};
+  for (int i : idx) {
+    if (i < 0) {
+      return set_err(h, PMP_ERR_INVALID, "negative component index");
+    }
+  }
   h->comps = *comps;
   h->have_comps = true;
   return PMP_OK;
@@ -1611,11 +1669,17 @@ int pmp_spray_update_host(
     return update_host_overlapped(h, state, source, dst.data(), dsr.data(), nboxes, flow_dt,
                                   state_ghosts, source_ghosts, is_ghost, do_move, spray_cfl_lev, st);
   }
+  const auto st_runs = comp_runs(h, true);
+  const auto sr_runs = comp_runs(h, false);
   for (int b = 0; b < nboxes; ++b) {
-    PMP_CUDA(h, cudaMemcpyAsync(dst[b].p, state[b].p, sizeof(double) * view_extent(state[b]),
-                                cudaMemcpyHostToDevice, st));
-    PMP_CUDA(h, cudaMemcpyAsync(dsr[b].p, source[b].p, sizeof(double) * view_extent(source[b]),
-                                cudaMemcpyHostToDevice, st));
+    if (st_runs.back().second > state[b].ncomp || sr_runs.back().second > source[b].ncomp ||
+        st_runs.front().first < 0 || sr_runs.front().first < 0) {
+      return set_err(h, PMP_ERR_INVALID, "a view has fewer components than the update reads", b);
+    }
+  }
+  for (int b = 0; b < nboxes; ++b) {
+    PMP_CUDA(h, copy_runs(dst[b].p, state[b].p, state[b], st_runs, cudaMemcpyHostToDevice, st));
+    PMP_CUDA(h, copy_runs(dsr[b].p, source[b].p, source[b], sr_runs, cudaMemcpyHostToDevice, st));
   }
   const int rc = do_update(h, dst.data(), dsr.data(), nboxes, flow_dt, state_ghosts, source_ghosts,
                            is_virt, is_ghost, do_move, spray_cfl_lev, st);
@@ -1623,8 +1687,7 @@ int pmp_spray_update_host(
     return rc;
   }
   for (int b = 0; b < nboxes; ++b) {
-    PMP_CUDA(h, cudaMemcpyAsync(source[b].p, h->stage_src[b], sizeof(double) * view_extent(source[b]),
-                                cudaMemcpyDeviceToHost, st));
+    PMP_CUDA(h, copy_runs(source[b].p, h->stage_src[b], source[b], sr_runs, cudaMemcpyDeviceToHost, st));
   }
   PMP_CUDA(h, cudaStreamSynchronize(st));
   return PMP_OK;

@@ -58,3 +58,38 @@ def test_host_views_sequential_launch_shape():
     def persistent(sp):
         sp.set_launch(kind=capi.PMP_LAUNCH_PERSISTENT, block=128, regs=96, chunk=512)
     compare(uneven(60_000), setup=persistent)
+
+
+def test_host_views_copy_only_the_components_used():
+    """The host-view update copies the state components the update reads and
+    the source components it deposits into: an unread state component may hold
+    NaN, and an extra source component keeps its host value."""
+    import torch
+    from pelemp_b200.spray import from_problem, views
+    prob = W.config1(n=20_000, steps=1)
+    pd, sd, _ = gpu_run(prob, 1)
+    ns = prob.nspec
+    st_h = []
+    for s in prob.state:
+        a = torch.from_numpy(s.copy()).pin_memory().numpy()
+        a[4 + ns] = np.nan  # rhoH: not read in the PeleLMeX coupling
+        st_h.append(a)
+    sp = from_problem(prob)
+    st_v = views(st_h, [prob.grown(b, prob.state_ghosts)[0] for b in range(len(prob.boxes))])
+    srcs = []
+    for do_move in (1, 0):
+        src = []
+        for s in prob.new_sources():
+            a = torch.zeros((s.shape[0] + 1,) + s.shape[1:], dtype=torch.float64).pin_memory().numpy()
+            a[-1] = 7.0
+            src.append(a)
+        src_v = views(src, [prob.grown(b, prob.source_ghosts)[0] for b in range(len(prob.boxes))])
+        sp.update_particles_host(st_v, src_v, prob.flow_dt, 0.0, prob.state_ghosts, prob.source_ghosts,
+                                 0, 0, do_move, prob.spray_cfl_lev, torch.cuda.current_stream().cuda_stream)
+        for a in src:
+            assert np.all(a[-1] == 7.0)
+        srcs.append([a[:-1].copy() for a in src])
+    ph = [sp.get_particles(b) for b in range(len(prob.boxes))]
+    assert_bitwise(pd, ph)
+    for a, b in zip(sd, srcs):
+        assert source_errors(b, a) <= 1e-12
