@@ -512,6 +512,10 @@ int pmp_learn_debug_grad(const float* params, const float* x, const float* y,
  * rows of normalised inputs xn[n][10] at params; outputs y[n][5]. */
 int pmp_learn_debug_infer(const float* params, const float* xn, int n,
                           float* y);
+/* The same with the CTA-level tcgen05 network (tensor-memory accumulators,
+ * 256 rows per CTA); PMP_ERR_TIMEOUT if an MMA completion wait timed out. */
+int pmp_learn_debug_infer_tc(const float* params, const float* xn, int n,
+                             float* y);
 int pmp_learn_param_count(void);
 
 #ifdef __cplusplus

@@ -20,6 +20,7 @@
 
 #include "learn/learn_common.cuh"
 #include "learn/mlp_mma.cuh"
+#include "learn/mlp_tc.cuh"
 #include "pmp_handle.h"
 #include "spray_kernels.cuh"
 
@@ -666,6 +667,31 @@ static void build_mlp(const std::vector<float>& p, MlpSmem& S)
       S.w4[o * kWStride + k] = host_bf16(o < kLearnOut ? p[kP_W4 + o * 64 + k] : 0.f);
     }
     S.b4[o] = o < kLearnOut ? p[kP_B4 + o] : 0.f;
+  }
+}
+
+// inference weights in the canonical tcgen05 operand layout of mlp_tc.cuh
+static void build_mlp_tc(const std::vector<float>& p, tc::TcMlp& S)
+{
+  memset(&S, 0, sizeof(S));  // bf16 zero is all-zero bits
+  for (int o = 0; o < 64; ++o) {
+    for (int k = 0; k < kLearnIn; ++k) {
+      S.w1[tc::tc_off(o, k, tc::kK1)] = host_bf16(0.5f * p[kP_W1 + o * 16 + k]);
+      S.w1[tc::tc_off(o, 16 + k, tc::kK1)] = host_bf16(0.5f * p[kP_W1 + o * 16 + k]);
+    }
+    for (int k = 0; k < 64; ++k) {
+      S.w2[tc::tc_off(o, k, tc::kHid)] = host_bf16(0.5f * p[kP_W2 + o * 64 + k]);
+      S.w3[tc::tc_off(o, k, tc::kHid)] = host_bf16(0.5f * p[kP_W3 + o * 64 + k]);
+    }
+    S.b1[o] = 0.5f * p[kP_B1 + o];
+    S.b2[o] = 0.5f * p[kP_B2 + o];
+    S.b3[o] = 0.5f * p[kP_B3 + o];
+  }
+  for (int o = 0; o < kLearnOut; ++o) {
+    for (int k = 0; k < 64; ++k) {
+      S.w4[tc::tc_off(o, k, tc::kHid)] = host_bf16(p[kP_W4 + o * 64 + k]);
+    }
+    S.b4[o] = p[kP_B4 + o];
   }
 }
 
@@ -1823,7 +1849,87 @@ __global__ void k_debug_infer(const MlpSmem* mlp, const float* xn, int n, float*
   }
 }
 
+// mlp_cta_tc over n rows of normalised inputs, TILES x 128 rows per CTA
+template <int TILES>
+__global__ void __launch_bounds__(TILES * tc::kTile) k_debug_infer_tc(const tc::TcMlp* mlp, const float* xn, int n,
+                                                                      float* y, int* status)
+{
+  extern __shared__ __align__(128) unsigned char tc_smem[];
+  tc::TcMlp& S = *reinterpret_cast<tc::TcMlp*>(tc_smem);
+  tc::TcTileA* A = reinterpret_cast<tc::TcTileA*>(tc_smem + sizeof(tc::TcMlp));
+  __shared__ uint32_t tmem_slot;
+  __shared__ unsigned long long mbar_slot;
+  {
+    const int4* src = reinterpret_cast<const int4*>(mlp);
+    int4* dst = reinterpret_cast<int4*>(&S);
+    for (int i = threadIdx.x; i < (int)(sizeof(tc::TcMlp) / 16); i += blockDim.x) {
+      dst[i] = src[i];
+    }
+  }
+  tc::TcCta c = tc::tc_setup(&tmem_slot, &mbar_slot, TILES * tc::kCols);
+  const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  float x[kLearnIn], o[kLearnOut];
+  for (int k = 0; k < kLearnIn; ++k) {
+    x[k] = r < n ? xn[r * kLearnIn + k] : 0.f;
+  }
+  const bool ok = tc::mlp_cta_tc<TILES>(S, A, c, x, o);
+  if (!ok) {
+    if (threadIdx.x == 0) {
+      atomicExch(status, 1);
+    }
+    tc::mbar_wait(c.mbar, c.phase ^ 1u);  // the MMAs the timed-out wait was for
+  } else if (r < n) {
+    for (int k = 0; k < kLearnOut; ++k) {
+      y[r * kLearnOut + k] = o[k];
+    }
+  }
+  tc::tc_teardown(c, TILES * tc::kCols);
+}
+
 }  // namespace
+
+extern "C" int pmp_learn_debug_infer_tc(const float* params, const float* xn, int n, float* y)
+{
+  if (!params || !xn || !y || n < 1) {
+    return PMP_ERR_INVALID;
+  }
+  std::vector<float> pw(params, params + kP_N);
+  tc::TcMlp S;
+  build_mlp_tc(pw, S);
+  tc::TcMlp* d_mlp = nullptr;
+  float *d_x = nullptr, *d_y = nullptr;
+  int* d_status = nullptr;
+  int rc = PMP_OK;
+  constexpr int kTiles = 2;
+  const size_t smem = sizeof(tc::TcMlp) + kTiles * sizeof(tc::TcTileA);
+  if (cudaMalloc(&d_mlp, sizeof(S)) != cudaSuccess ||
+      cudaMalloc(&d_x, sizeof(float) * (size_t)n * kLearnIn) != cudaSuccess ||
+      cudaMalloc(&d_y, sizeof(float) * (size_t)n * kLearnOut) != cudaSuccess ||
+      cudaMalloc(&d_status, sizeof(int)) != cudaSuccess ||
+      cudaFuncSetAttribute(k_debug_infer_tc<kTiles>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess) {
+    rc = PMP_ERR_CUDA;
+  } else {
+    cudaMemcpy(d_mlp, &S, sizeof(S), cudaMemcpyHostToDevice);
+    cudaMemcpy(d_x, xn, sizeof(float) * (size_t)n * kLearnIn, cudaMemcpyHostToDevice);
+    cudaMemset(d_status, 0, sizeof(int));
+    const int rows = kTiles * tc::kTile;
+    k_debug_infer_tc<kTiles><<<(n + rows - 1) / rows, rows, smem>>>(d_mlp, d_x, n, d_y, d_status);
+    int status = 0;
+    if (cudaDeviceSynchronize() != cudaSuccess) {
+      rc = PMP_ERR_CUDA;
+    } else {
+      cudaMemcpy(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost);
+      cudaMemcpy(y, d_y, sizeof(float) * (size_t)n * kLearnOut, cudaMemcpyDeviceToHost);
+      rc = status ? PMP_ERR_TIMEOUT : PMP_OK;
+    }
+  }
+  cudaFree(d_mlp);
+  cudaFree(d_x);
+  cudaFree(d_y);
+  cudaFree(d_status);
+  return rc;
+}
 
 // Inference check: the tensor-core network of the learned kernel on n rows of
 // normalised inputs xn[n][10] with the flat parameters params; y[n][5].

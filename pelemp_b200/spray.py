@@ -73,6 +73,7 @@ _SIGS = {
     "pmp_learn_debug_grad": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p,
                              C.POINTER(C.c_double)],
     "pmp_learn_debug_infer": [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p],
+    "pmp_learn_debug_infer_tc": [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p],
     "pmp_learn_param_count": [],
 }
 
@@ -436,13 +437,15 @@ def from_problem(prob, device=0, mode=capi.PMP_MODE_FP64, set_droplets=True):
     return sp
 
 
-def learn_debug_infer(params, xn):
-    """Outputs of the learned kernel's tensor-core network for normalised inputs."""
+def learn_debug_infer(params, xn, engine="mma"):
+    """Outputs of the tensor-core network for normalised inputs: engine "mma"
+    (warp-level mma.sync) or "tc" (CTA-level tcgen05, accumulators in TMEM)."""
     params = np.ascontiguousarray(params, np.float32)
     xn = np.ascontiguousarray(xn, np.float32)
     n = xn.shape[0]
     y = np.zeros((n, capi.LEARN_OUT), np.float32)
-    rc = lib().pmp_learn_debug_infer(params.ctypes.data, xn.ctypes.data, n, y.ctypes.data)
+    fn = lib().pmp_learn_debug_infer_tc if engine == "tc" else lib().pmp_learn_debug_infer
+    rc = fn(params.ctypes.data, xn.ctypes.data, n, y.ctypes.data)
     if rc != capi.PMP_OK:
         raise SprayError(rc)
     return y

@@ -75,6 +75,26 @@ def test_inference_matches_oracle():
     assert np.max(np.abs(yg - yo)) <= 6e-2 * scale
 
 
+def test_inference_tc_matches_oracle_and_mma():
+    """The CTA-level tcgen05 network (TMEM accumulators, 256 rows per CTA)
+    against the oracle with the same bound as the warp-level path, and against
+    that path (the same bf16 roundings; only the FP32 accumulation order
+    differs)."""
+    rng = np.random.default_rng(3)
+    p = M.random_params(17)
+    x = rng.standard_normal((1000, M.N_IN)).astype(np.float32)  # not a whole number of CTAs
+    yt = learn_debug_infer(p, x, engine="tc")
+    ym = learn_debug_infer(p, x, engine="mma")
+    yo = M.infer(p, x.astype(np.float64))
+    scale = np.sqrt(np.mean(yo ** 2))
+    rms = np.sqrt(np.mean((yt - yo) ** 2))
+    print("tc inference rms / scale", rms / scale, "max", np.max(np.abs(yt - yo)) / scale,
+          "vs mma rms", np.sqrt(np.mean((yt - ym) ** 2)) / scale)
+    assert rms <= 1e-2 * scale
+    assert np.max(np.abs(yt - yo)) <= 6e-2 * scale
+    assert np.sqrt(np.mean((yt - ym) ** 2)) <= 1e-2 * scale
+
+
 def _advance(sp, prob, st_v, stream):
     for do_move in (1, 0):
         _src, src_v = device_sources(prob)
