@@ -176,8 +176,8 @@ struct TcCta {
   uint32_t phase;   // parity of the next completion
 };
 
-// Warp 0 allocates ncols TMEM columns (a power of 2 >= 32) and the thread 0
-// initialises the mbarrier; every thread of the CTA calls it.
+// Warp 0 allocates ncols TMEM columns (a power of 2, 32 to 512) and the
+// thread 0 initialises the mbarrier; every thread of the CTA calls it.
 __device__ __forceinline__ TcCta tc_setup(uint32_t* tmem_slot, unsigned long long* mbar_slot, int ncols)
 {
   if (threadIdx.x < 32) {

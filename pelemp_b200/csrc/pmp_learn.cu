@@ -40,7 +40,8 @@ constexpr int kTupleW = 16;            // x[10], y[5], pad
 
 struct LearnParams {
   LearnNorm norm;
-  const MlpSmem* mlp;
+  const MlpSmem* mlp;        // warp-level layout (audit)
+  const tc::TcMlp* mlp_tc;   // tcgen05 operand layout (the update kernel)
   long long audit_stride;
   long long audit_offset;
   double* audit;  // [0] count, [1..5] sum of squared errors, [6..10] sum of squared targets
@@ -66,6 +67,7 @@ struct LearnState {
   double* d_loss = nullptr;
   // inference
   MlpSmem* d_mlp = nullptr;
+  tc::TcMlp* d_mlp_tc = nullptr;
   LearnNorm norm;
   bool trained = false;
   double gate_margin = 0.05;
@@ -605,6 +607,7 @@ static int ensure_params(LearnState* L)
   if (cudaMalloc(&L->d_stats, sizeof(double) * 64) != cudaSuccess ||
       cudaMalloc(&L->d_loss, sizeof(double)) != cudaSuccess ||
       cudaMalloc(&L->d_mlp, sizeof(MlpSmem)) != cudaSuccess ||
+      cudaMalloc(&L->d_mlp_tc, sizeof(tc::TcMlp)) != cudaSuccess ||
       cudaMalloc(&L->d_audit, sizeof(double) * 16) != cudaSuccess) {
     return -1;
   }
@@ -695,6 +698,14 @@ static void build_mlp_tc(const std::vector<float>& p, tc::TcMlp& S)
   }
 }
 
+static void upload_mlp_tc(LearnState* L, const std::vector<float>& p)
+{
+  tc::TcMlp* S = new tc::TcMlp;
+  build_mlp_tc(p, *S);
+  cudaMemcpy(L->d_mlp_tc, S, sizeof(tc::TcMlp), cudaMemcpyHostToDevice);
+  delete S;
+}
+
 // ---------------------------------------------------------------------------
 // the learned update kernel
 
@@ -702,44 +713,59 @@ static void build_mlp_tc(const std::vector<float>& p, tc::TcMlp& S)
 // shared memory serves 8 warps (measured against 128 threads x 4 CTAs and
 // 256 x 3 or 4 CTAs, whose register caps spill more than they gain)
 #ifndef PMP_LEARNED_THREADS
-#define PMP_LEARNED_THREADS 256
+#define PMP_LEARNED_THREADS 128  /* one M tile per CTA: 4 warps per barrier (measured against 256) */
 #endif
 #ifndef PMP_LEARNED_MIN_BLOCKS
-#define PMP_LEARNED_MIN_BLOCKS 2
+#define PMP_LEARNED_MIN_BLOCKS 4  /* 128 registers; 4 CTAs of 47 KB shared memory per SM */
 #endif
 constexpr int kLearnThreads = PMP_LEARNED_THREADS;  // threads per CTA, a multiple of kBlock
-constexpr int kLearnStash = 5 + PMP_MAX_FUEL;        // shared-memory doubles per thread
+// shared-memory doubles per thread (position, parcel count, start mass, composition)
+__host__ __device__ constexpr int learn_stash(int nf) { return 5 + nf; }
 
+// The CTA's droplets step together (a CTA-wide loop over the inner sub-steps)
+// so that every sub-step evaluates the network for all of them at once:
+// kBlock = 128 droplets per tcgen05 M tile, BLOCK / kBlock tiles per CTA.
 template <int NS, int NF, int BLOCK, bool FF>
 __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
   spray_update_learned(const __grid_constant__ KParams P, const __grid_constant__ LearnParams L)
 {
-  // dynamic shared memory: the network's weights, one scratch per warp, then
-  // per thread the values the droplet physics does not read (position,
-  // parcel count, start mass, composition: kLearnStash doubles, stride BLOCK)
-  extern __shared__ __align__(16) unsigned char learn_smem[];
-  MlpSmem& S = *reinterpret_cast<MlpSmem*>(learn_smem);
-  MlpWarpScratch* WS = reinterpret_cast<MlpWarpScratch*>(learn_smem + sizeof(MlpSmem));
-  double* sx = reinterpret_cast<double*>(learn_smem + sizeof(MlpSmem) + sizeof(MlpWarpScratch) * (BLOCK / 32)) +
+  constexpr int TILES = BLOCK / tc::kTile;
+  static_assert(BLOCK % tc::kTile == 0 && tc::kTile == kBlock, "one M tile per CTA-map item");
+  static_assert(TILES == 1 || TILES == 2 || TILES == 4, "TMEM is allocated in powers of 2 columns");
+  // dynamic shared memory: the network's weights (tcgen05 operand layout),
+  // one A operand per tile, then per thread the values the droplet physics
+  // does not read (learn_stash(NF) doubles, stride BLOCK)
+  extern __shared__ __align__(128) unsigned char learn_smem[];
+  tc::TcMlp& S = *reinterpret_cast<tc::TcMlp*>(learn_smem);
+  tc::TcTileA* A = reinterpret_cast<tc::TcTileA*>(learn_smem + sizeof(tc::TcMlp));
+  double* sx = reinterpret_cast<double*>(learn_smem + sizeof(tc::TcMlp) + sizeof(tc::TcTileA) * TILES) +
                threadIdx.x;
+  __shared__ uint32_t tmem_slot;
+  __shared__ unsigned long long mbar_slot;
   {
-    const int4* src = reinterpret_cast<const int4*>(L.mlp);
+    const int4* src = reinterpret_cast<const int4*>(L.mlp_tc);
     int4* dst = reinterpret_cast<int4*>(&S);
-    for (int i = threadIdx.x; i < (int)(sizeof(MlpSmem) / 16); i += BLOCK) {
+    for (int i = threadIdx.x; i < (int)(sizeof(tc::TcMlp) / 16); i += BLOCK) {
       dst[i] = src[i];
     }
   }
-  __syncthreads();
-  MlpWarpScratch& W = WS[threadIdx.x >> 5];
+  tc::TcCta tcs = tc::tc_setup(&tmem_slot, &mbar_slot, TILES * tc::kCols);
   const DevMechF& m = P.mf;
   const DevFuelF& ff = P.ff;
   const DevFuel& fdat = P.f;
-  // each group of kBlock threads takes one kBlock-slot item of the CTA map
-  const int item = blockIdx.x * (BLOCK / kBlock) + threadIdx.x / kBlock;
+  // each group of kBlock threads takes one kBlock-slot item of the CTA map;
+  // a CTA takes TILES items, and loops to the next TILES items gridDim.x
+  // apart when the grid is smaller than the map
+  __shared__ BoxEntry sB[TILES];
+  Counters c;
+  bool tc_dead = false;  // a timed-out MMA wait stops the CTA (uniform)
+  for (int it = blockIdx.x; it * TILES < L.ncta && !tc_dead; it += gridDim.x) {
+  const int item = it * TILES + threadIdx.x / kBlock;
   const bool item_ok = item < L.ncta;
   const int b = item_ok ? P.cta_box[item] : 0;
-  // this item's box entry, staged in shared memory
-  __shared__ BoxEntry sB[BLOCK / kBlock];
+  // this item's box entry, staged in shared memory (after the previous
+  // item's readers are done)
+  __syncthreads();
   {
     const int h = threadIdx.x / kBlock;
     const int* src = reinterpret_cast<const int*>(P.boxes + b);
@@ -751,7 +777,6 @@ __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
   __syncthreads();
   const BoxEntry& B = sB[threadIdx.x / kBlock];
   const long long s = item_ok ? P.cta_start[item] + threadIdx.x % kBlock : 0;
-  Counters c;
   bool valid = item_ok && s < B.p_end;
   int id = valid ? P.parts.id[s] : 0;
   valid = valid && id > 0;
@@ -797,7 +822,6 @@ __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
     ok = false;
   }
   sx[3 * BLOCK] = num_ppp;
-  const unsigned FULL = 0xffffffffu;
   for (int cur_iter = 0; cur_iter < P.num_iter; ++cur_iter) {
     // cell of the droplet (recomputed from the position each sub-cycle, so
     // the stencil indices are not live across the network evaluation)
@@ -927,7 +951,7 @@ __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
     float T_h = (float)T_part;
     bool pending = active;
     bool fell_back = false;
-    while (__any_sync(FULL, pending)) {
+    while (__syncthreads_or(pending)) {
       // closed-form vapor state, then the surrogate inputs
       float xin[kLearnIn];
       float xn[kLearnIn];
@@ -960,7 +984,19 @@ __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
         }
       }
       float yo[kLearnOut];
-      mlp_warp(S, W, xn, yo);
+      if (!tc::mlp_cta_tc<TILES>(S, A, tcs, xn, yo)) {
+        // an MMA completion wait timed out (uniformly over the CTA): stop, no
+        // further droplet of the CTA is written
+        tc_dead = true;
+        pending = false;
+        active = false;
+        valid = false;
+        if (threadIdx.x == 0) {
+          set_error(P, PMP_ERR_TIMEOUT, b, s);
+        }
+        tc::mbar_wait(tcs.mbar, tcs.phase ^ 1u);  // the MMAs the timed-out wait was for
+        continue;
+      }
       if (pending) {
         float yv[kLearnOut];
 #pragma unroll
@@ -1227,6 +1263,8 @@ __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
       c.killed += 1;
     }
   }
+  }  // items
+  tc::tc_teardown(tcs, TILES * tc::kCols);
   flush_counters(P, c);
 }
 
@@ -1343,9 +1381,8 @@ static int launch_learned_t(pmp_spray* h, const KParams& P, const LearnParams& L
   }
   constexpr int per = kLearnThreads / kBlock;
   const int grid = (LP.ncta + per - 1) / per;
-  constexpr size_t smem = sizeof(MlpSmem) + sizeof(MlpWarpScratch) * (kLearnThreads / 32) +
-                          sizeof(double) * kLearnStash * kLearnThreads;
-  static_assert(sizeof(MlpSmem) % 16 == 0, "warp scratch must stay 16-byte aligned");
+  constexpr size_t smem = sizeof(tc::TcMlp) + sizeof(tc::TcTileA) * (kLearnThreads / tc::kTile) +
+                          sizeof(double) * learn_stash(NF) * kLearnThreads;
   auto kern = P.fuel_first ? spray_update_learned<NS, NF, kLearnThreads, true>
                            : spray_update_learned<NS, NF, kLearnThreads, false>;
   if (smem > 48 * 1024) {
@@ -1354,6 +1391,9 @@ static int launch_learned_t(pmp_spray* h, const KParams& P, const LearnParams& L
       return PMP_ERR_CUDA;
     }
   }
+  // one CTA per TILES items (a grid capped at the resident CTAs, each looping
+  // over items, measured 2.8x slower: the CTA-wide steps of one item then
+  // leave the SM idle; nor does a shared-memory carveout preference help)
   kern<<<grid, kLearnThreads, smem, st>>>(P, LP);
   return PMP_OK;
 }
@@ -1381,6 +1421,7 @@ int launch_learned(pmp_spray* h, const KParams& P, cudaStream_t st, int first, i
   memset(&LP, 0, sizeof(LP));
   LP.norm = L->norm;
   LP.mlp = L->d_mlp;
+  LP.mlp_tc = L->d_mlp_tc;
   LP.audit = L->d_audit;
   LP.ncta = count;
   LP.audit_stride = 0;
@@ -1411,7 +1452,7 @@ static void free_state(LearnState* L)
 {
   void* bufs[] = {L->tuples, L->d_count, L->params, L->wq, L->grads, L->adam_m, L->adam_v, L->X, L->Yt,
                   L->H1, L->A1, L->H2, L->A2, L->H3, L->A3, L->Yp, L->dY, L->dA, L->dH, L->d_stats,
-                  L->d_loss, L->d_mlp, L->d_audit};
+                  L->d_loss, L->d_mlp, L->d_mlp_tc, L->d_audit};
   for (void* p : bufs) {
     cudaFree(p);
   }
@@ -1698,6 +1739,7 @@ extern "C" int pmp_spray_learn_train(pmp_spray* h, const pmp_learn_config* cfg, 
   MlpSmem S;
   build_mlp(pw, S);
   cudaMemcpy(L->d_mlp, &S, sizeof(S), cudaMemcpyHostToDevice);
+  upload_mlp_tc(L, pw);
   L->trained = true;
   const auto t1 = std::chrono::steady_clock::now();
   if (rep) {
@@ -1758,6 +1800,7 @@ extern "C" int pmp_spray_learn_weights(pmp_spray* h, int get, float* buf, long l
     MlpSmem S;
     build_mlp(pw, S);
     cudaMemcpy(L->d_mlp, &S, sizeof(S), cudaMemcpyHostToDevice);
+    upload_mlp_tc(L, pw);
     L->trained = true;
   }
   *count = total;
