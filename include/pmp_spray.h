@@ -508,12 +508,14 @@ int pmp_spray_learn_audit(const pmp_spray* h, long long* audited,
  * training forward pass does).  Runs on the current device. */
 int pmp_learn_debug_grad(const float* params, const float* x, const float* y,
                          int n, int quant, float* grads, double* loss);
-/* Check of the inference: the tensor-core network of the learned kernel on n
- * rows of normalised inputs xn[n][10] at params; outputs y[n][5]. */
+/* Check of the inference: the network evaluated with warp-level mma.sync
+ * tiles (the cross-check of the tcgen05 path) on n rows of normalised inputs
+ * xn[n][10] at params; outputs y[n][5]. */
 int pmp_learn_debug_infer(const float* params, const float* xn, int n,
                           float* y);
-/* The same with the CTA-level tcgen05 network (tensor-memory accumulators,
- * 256 rows per CTA); PMP_ERR_TIMEOUT if an MMA completion wait timed out. */
+/* The same with the CTA-level tcgen05 network of the learned update kernel
+ * (tensor-memory accumulators, 128-row tiles, 256 rows per CTA here);
+ * PMP_ERR_TIMEOUT if an MMA completion wait timed out. */
 int pmp_learn_debug_infer_tc(const float* params, const float* xn, int n,
                              float* y);
 int pmp_learn_param_count(void);
