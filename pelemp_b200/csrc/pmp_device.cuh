@@ -148,6 +148,13 @@ __host__ __device__ constexpr int gas_rec4(int ns) { return (8 + ns) / 4; }
 __host__ __device__ constexpr int gas_rec2(int ns) { return (6 + ns) / 2; }
 
 #ifdef __CUDACC__
+// Deposit into a source cell: a relaxed device-scope FP64 add with no return
+// value (red), so the issuing warp never waits for it.
+__device__ __forceinline__ void red_add(double* p, double v)
+{
+  asm volatile("red.relaxed.gpu.global.add.f64 [%0], %1;" ::"l"(p), "d"(v) : "memory");
+}
+
 // FP64 gas record of cell (i, j, k) of box B (inside its grown box), as 2 * R2 doubles.
 template <int R2>
 __device__ __forceinline__ void load_gas_rec64(const BoxEntry& B, int i, int j, int k, double* rec)

@@ -1212,15 +1212,15 @@ __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
         if (fdat.mom_trans) {
 #pragma unroll
           for (int dir = 0; dir < 3; ++dir) {
-            atomicAdd(q + (P.s_mom + dir) * B.sr_n32, cur_coef * src.mom[dir]);
+            red_add(q + (P.s_mom + dir) * B.sr_n32, cur_coef * src.mom[dir]);
           }
         }
-        atomicAdd(q + P.s_rho * B.sr_n32, cur_coef * src.mass);
+        red_add(q + P.s_rho * B.sr_n32, cur_coef * src.mass);
 #pragma unroll
         for (int spf = 0; spf < NF; ++spf) {
-          atomicAdd(q + (P.s_spec + spf) * B.sr_n32, cur_coef * src.Ydot[spf]);
+          red_add(q + (P.s_spec + spf) * B.sr_n32, cur_coef * src.Ydot[spf]);
         }
-        atomicAdd(q + P.s_eng * B.sr_n32, cur_coef * src.eng);
+        red_add(q + P.s_eng * B.sr_n32, cur_coef * src.eng);
         if (P.do_move && !fdat.fixed_parts && id > 0) {
 #pragma unroll
           for (int dir = 0; dir < 3; ++dir) {

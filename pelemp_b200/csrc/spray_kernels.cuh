@@ -348,17 +348,17 @@ __device__ __forceinline__ void update_one(const KParams& P, const BoxEntry& B, 
     if (P.f.mom_trans) {
 #pragma unroll
       for (int dir = 0; dir < 3; ++dir) {
-        atomicAdd(q + (P.s_mom + dir) * B.sr_n32, __dmul_rn(cur_coef, src.mom[dir]));
+        red_add(q + (P.s_mom + dir) * B.sr_n32, __dmul_rn(cur_coef, src.mom[dir]));
       }
     }
     if (P.f.mass_trans) {
-      atomicAdd(q + P.s_rho * B.sr_n32, __dmul_rn(cur_coef, src.mass));
+      red_add(q + P.s_rho * B.sr_n32, __dmul_rn(cur_coef, src.mass));
 #pragma unroll
       for (int spf = 0; spf < NF; ++spf) {
-        atomicAdd(q + (P.s_spec + spf) * B.sr_n32, __dmul_rn(cur_coef, src.Ydot[spf]));
+        red_add(q + (P.s_spec + spf) * B.sr_n32, __dmul_rn(cur_coef, src.Ydot[spf]));
       }
     }
-    atomicAdd(q + P.s_eng * B.sr_n32, __dmul_rn(cur_coef, src.eng));
+    red_add(q + P.s_eng * B.sr_n32, __dmul_rn(cur_coef, src.eng));
     // move (SprayParticles.cpp:444-476)
     if (P.do_move && !P.f.fixed_parts && id > 0) {
 #pragma unroll
