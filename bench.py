@@ -244,7 +244,7 @@ FORM_MODE = {"fp64": 0, "mixed": 1, "learned": 2}
 FORM_NAME = {"fp64": "plain FP64", "mixed": "mixed FP32 physics / FP64 state and deposits",
              "learned": "learned surrogate (bf16 MLP on tensor cores) + FP32 physics / FP64 state"}
 KERNEL = {"fp64": "spray_update_fp64<5,2,128>", "mixed": "spray_update_mixed<5,2,128,fuel_first>",
-          "learned": "spray_update_learned<5,2,256,fuel_first>"}
+          "learned": "spray_update_learned<5,2,128,fuel_first>"}
 # DRAM bytes per droplet of one config-2 MKD launch, measured by ncu on a
 # 2M-droplet launch (profiles/update_kernels_config2_2M.md): dram read + write
 # minus the mesh's algorithmic bytes (state read once, source read-modify-
@@ -254,7 +254,7 @@ KERNEL = {"fp64": "spray_update_fp64<5,2,128>", "mixed": "spray_update_mixed<5,2
 # for the FP64 kernel: its register spills reach DRAM; below it for the mixed
 # and learned kernels, whose gathers read the FP32 gas records (written by a
 # separate pass) instead of the FP64 state.
-DRAM_BYTES_PER_DROPLET = {"fp64": 278.4, "mixed": 143.2, "learned": 134.4}
+DRAM_BYTES_PER_DROPLET = {"fp64": 278.4, "mixed": 143.4, "learned": 133.2}
 
 
 def train_surrogate(sp, prob, st_v, stream, args):
