@@ -518,6 +518,10 @@ int pmp_learn_debug_infer(const float* params, const float* xn, int n,
  * PMP_ERR_TIMEOUT if an MMA completion wait timed out. */
 int pmp_learn_debug_infer_tc(const float* params, const float* xn, int n,
                              float* y);
+/* Check of the tcgen05 timeout path: one CTA waits on an mbarrier that
+ * nothing arrives on.  Returns PMP_ERR_TIMEOUT when the bounded wait gave up
+ * (as it must), with the cycles it waited; the device stays usable. */
+int pmp_learn_debug_wait_timeout(long long* cycles);
 int pmp_learn_param_count(void);
 
 #ifdef __cplusplus

@@ -1931,6 +1931,53 @@ __global__ void __launch_bounds__(TILES * tc::kTile) k_debug_infer_tc(const tc::
 
 }  // namespace
 
+namespace {
+
+// The timeout path of the tcgen05 waits: one CTA allocates its tensor memory
+// and waits on an mbarrier that nothing arrives on; the bounded wait must give
+// up, the CTA agree on it and free the tensor memory.
+__global__ void __launch_bounds__(tc::kTile) k_debug_wait_timeout(int* status, long long* cycles)
+{
+  __shared__ uint32_t tmem_slot;
+  __shared__ unsigned long long mbar_slot;
+  tc::TcCta c = tc::tc_setup(&tmem_slot, &mbar_slot, tc::kCols);
+  const long long t0 = clock64();
+  const bool ok = __syncthreads_and(tc::mbar_wait(c.mbar, c.phase)) != 0;
+  if (threadIdx.x == 0) {
+    *status = ok ? 0 : 1;
+    *cycles = clock64() - t0;
+  }
+  tc::tc_teardown(c, tc::kCols);
+}
+
+}  // namespace
+
+extern "C" int pmp_learn_debug_wait_timeout(long long* cycles)
+{
+  if (!cycles) {
+    return PMP_ERR_INVALID;
+  }
+  int* d_status = nullptr;
+  long long* d_cycles = nullptr;
+  int rc = PMP_OK;
+  if (cudaMalloc(&d_status, sizeof(int)) != cudaSuccess || cudaMalloc(&d_cycles, sizeof(long long)) != cudaSuccess) {
+    rc = PMP_ERR_CUDA;
+  } else {
+    k_debug_wait_timeout<<<1, tc::kTile>>>(d_status, d_cycles);
+    int status = 0;
+    if (cudaDeviceSynchronize() != cudaSuccess) {
+      rc = PMP_ERR_CUDA;
+    } else {
+      cudaMemcpy(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost);
+      cudaMemcpy(cycles, d_cycles, sizeof(long long), cudaMemcpyDeviceToHost);
+      rc = status ? PMP_ERR_TIMEOUT : PMP_OK;
+    }
+  }
+  cudaFree(d_status);
+  cudaFree(d_cycles);
+  return rc;
+}
+
 extern "C" int pmp_learn_debug_infer_tc(const float* params, const float* xn, int n, float* y)
 {
   if (!params || !xn || !y || n < 1) {

@@ -74,6 +74,7 @@ _SIGS = {
                              C.POINTER(C.c_double)],
     "pmp_learn_debug_infer": [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p],
     "pmp_learn_debug_infer_tc": [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p],
+    "pmp_learn_debug_wait_timeout": [C.POINTER(C.c_longlong)],
     "pmp_learn_param_count": [],
 }
 
@@ -449,3 +450,10 @@ def learn_debug_infer(params, xn, engine="mma"):
     if rc != capi.PMP_OK:
         raise SprayError(rc)
     return y
+
+
+def learn_debug_wait_timeout():
+    """(status, cycles) of a tcgen05 wait on an mbarrier nothing arrives on."""
+    cycles = C.c_longlong(0)
+    rc = lib().pmp_learn_debug_wait_timeout(C.byref(cycles))
+    return rc, cycles.value

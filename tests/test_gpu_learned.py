@@ -23,7 +23,7 @@ import pytest
 from oracle import mlp_oracle as M
 from pelemp_b200 import capi
 from pelemp_b200 import workloads as W
-from pelemp_b200.spray import from_problem, learn_debug_grad, learn_debug_infer
+from pelemp_b200.spray import from_problem, learn_debug_grad, learn_debug_infer, learn_debug_wait_timeout
 from tests.gpu_util import assert_bitwise, device_sources, device_state, gpu_run, host_run, oracle_run
 from tests.parity import source_errors
 from tests.parity import droplet_mass
@@ -93,6 +93,20 @@ def test_inference_tc_matches_oracle_and_mma():
     assert rms <= 1e-2 * scale
     assert np.max(np.abs(yt - yo)) <= 6e-2 * scale
     assert np.sqrt(np.mean((yt - ym) ** 2)) <= 1e-2 * scale
+
+
+def test_tcgen05_wait_times_out_and_recovers():
+    """A tcgen05 wait on an mbarrier that nothing arrives on gives up after its
+    bound (2^30 clock cycles, about half a second), the CTA frees its tensor
+    memory, the host reads PMP_ERR_TIMEOUT and the device keeps working."""
+    rc, cycles = learn_debug_wait_timeout()
+    assert rc == capi.PMP_ERR_TIMEOUT
+    assert (1 << 30) <= cycles < (1 << 32)
+    p = M.random_params(5)
+    x = np.random.default_rng(4).standard_normal((300, M.N_IN)).astype(np.float32)
+    yt = learn_debug_infer(p, x, engine="tc")
+    ym = learn_debug_infer(p, x, engine="mma")
+    assert np.sqrt(np.mean((yt - ym) ** 2)) <= 1e-2 * np.sqrt(np.mean(ym ** 2))
 
 
 def _advance(sp, prob, st_v, stream):
