@@ -229,6 +229,9 @@ struct KParams {
   // fallback-list kernel: when list_nbox > 0, only the entries of boxes
   // [list_box0, list_box0 + list_nbox) (one stage of the host-view pipeline)
   int list_box0, list_nbox;
+  // mixed form: the droplets below 2 um were listed before the launch
+  // (k_select_small); the mixed kernel skips them without listing them
+  int fb_pre;
   // mixed / learned forms: species k of DevMechF (and of their gas-state
   // gather) is mechanism species spec_perm[k]; fuel_first as in DevMechF
   int spec_perm[kMaxSpec];

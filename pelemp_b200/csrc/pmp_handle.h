@@ -98,6 +98,9 @@ struct pmp_spray {
   pmp::DevStatus* d_status = nullptr;
   pmp::DevStatus* h_status = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // the mixed form's FP64 list kernel runs on `side` beside the mixed kernel
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   pmp_error_info last_err;
   pmp_stats stats;
   // view pointers already checked to be device-accessible

@@ -34,6 +34,17 @@ int launch_mixed(int ns, int nf, const KParams& P, int ncta, int block, cudaStre
   return PMP_ERR_UNSUPPORTED;
 }
 
+int launch_select_small(const KParams& P, long long s0, long long s1, cudaStream_t st)
+{
+  const long long n = s1 - s0;
+  if (n <= 0) {
+    return PMP_OK;
+  }
+  const int grid = (int)std::min<long long>((n + 255) / 256, 148LL * 8);
+  k_select_small<<<grid, 256, 0, st>>>(P, s0, s1);
+  return PMP_OK;
+}
+
 int launch_gas_records(int ns, const KParams& P, int b0, int nb, int max_cells, cudaStream_t st)
 {
   if (nb <= 0 || max_cells <= 0) {

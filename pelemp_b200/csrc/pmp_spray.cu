@@ -23,6 +23,8 @@
 namespace pmp {
 // pmp_mixed.cu
 int launch_mixed(int ns, int nf, const KParams& P, int ncta, int block, cudaStream_t st);
+// the mixed form's droplets below 2 um of slots [s0, s1) onto the fallback list
+int launch_select_small(const KParams& P, long long s0, long long s1, cudaStream_t st);
 // FP32 gas records (BoxEntry::gr) of boxes [b0, b0 + nb); max_cells = the
 // largest grown box's cell count
 int launch_gas_records(int ns, const KParams& P, int b0, int nb, int max_cells, cudaStream_t st);
@@ -813,6 +815,36 @@ int do_update(
   return finish_update(h, graph_state);
 }
 
+// The mixed form over CTA-map items [c0, c0 + n) (Q's map already offset) and
+// droplet slots [s0, s1): the droplets it leaves to the FP64 kernel (d < 2 um)
+// are listed first, then the FP64 list kernel runs on the handle's
+// high-priority side stream beside the mixed kernel (which skips them), and
+// the caller's stream waits for both.  The list kernel is one thread per
+// listed droplet, so it costs the latency of one droplet's FP64 sub-cycles;
+// beside the mixed kernel that latency is hidden.
+int enqueue_mixed(pmp_spray* h, const KParams& Q, int n, long long s0, long long s1, cudaStream_t st)
+{
+  KParams R = Q;
+  R.fb_pre = 1;
+  int rc = pmp::launch_select_small(R, s0, s1, st);
+  if (rc != PMP_OK) {
+    return rc;
+  }
+  PMP_CUDA(h, cudaEventRecord(h->ev_fork, st));
+  PMP_CUDA(h, cudaStreamWaitEvent(h->side, h->ev_fork, 0));
+  rc = dispatch_fp64_list(h->nspec, h->nfuel, R, h->total, h->side);
+  if (rc != PMP_OK) {
+    return rc;
+  }
+  rc = pmp::launch_mixed(h->nspec, h->nfuel, R, n, kBlock, st);
+  if (rc != PMP_OK) {
+    return rc;
+  }
+  PMP_CUDA(h, cudaEventRecord(h->ev_join, h->side));
+  PMP_CUDA(h, cudaStreamWaitEvent(st, h->ev_join, 0));
+  return PMP_OK;
+}
+
 // The overlapped form of pmp_spray_update_host.  The boxes are split into up
 // to kHostStages consecutive groups of about equal bytes; group g's state and
 // source are copied in on one stream while the update of the groups before
@@ -914,13 +946,13 @@ int update_host_overlapped_impl(
       if (h->mode == PMP_MODE_LEARNED) {
         rc = pmp::launch_learned(h, P, st, c0, n);
       } else if (h->mode == PMP_MODE_MIXED) {
-        rc = pmp::launch_mixed(NS, NF, Q, n, kBlock, st);
+        rc = enqueue_mixed(h, Q, n, h->box_begin[b0], h->box_begin[b1], st);
       } else if (P.pelec) {
         rc = dispatch_fp64_pelec(NS, NF, Q, n, st);
       } else {
         rc = dispatch_fp64(NS, NF, Q, n, st);
       }
-      if (rc == PMP_OK && h->mode != PMP_MODE_FP64) {
+      if (rc == PMP_OK && h->mode == PMP_MODE_LEARNED) {
         PMP_CUDA(h, cudaGetLastError());
         rc = dispatch_fp64_list(NS, NF, Q, h->total, st);
       }
@@ -1088,11 +1120,7 @@ int pmp::enqueue_update(pmp_spray* h, const KParams& P, int nboxes, cudaStream_t
     } else if (h->mode == PMP_MODE_MIXED) {
       rc = pmp::launch_gas_records(NS, P, 0, nboxes, h->gas_rec_max_cells, st);
       if (rc == PMP_OK) {
-        rc = pmp::launch_mixed(NS, NF, P, h->ncta, kBlock, st);
-      }
-      if (rc == PMP_OK) {
-        PMP_CUDA(h, cudaGetLastError());
-        rc = dispatch_fp64_list(NS, NF, P, h->total, st);
+        rc = enqueue_mixed(h, P, h->ncta, 0, h->total, st);
       }
     } else if (P.pelec) {
       rc = pmp::launch_gas_records64(h, P, 0, nboxes, st);
@@ -1209,6 +1237,16 @@ int pmp_spray_create(const pmp_spray_config* cfg, pmp_spray** out)
     delete h;
     return PMP_ERR_CUDA;
   }
+  {
+    int lo = 0, hi = 0;
+    if (cudaDeviceGetStreamPriorityRange(&lo, &hi) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&h->side, cudaStreamNonBlocking, hi) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+      pmp_spray_destroy(h);
+      return PMP_ERR_CUDA;
+    }
+  }
   *out = h;
   return PMP_OK;
 }
@@ -1242,6 +1280,15 @@ int pmp_spray_destroy(pmp_spray* h)
   }
   if (h->ev1) {
     cudaEventDestroy(h->ev1);
+  }
+  if (h->side) {
+    cudaStreamDestroy(h->side);
+  }
+  if (h->ev_fork) {
+    cudaEventDestroy(h->ev_fork);
+  }
+  if (h->ev_join) {
+    cudaEventDestroy(h->ev_join);
   }
   if (h->hs_in) {
     cudaStreamDestroy(h->hs_in);

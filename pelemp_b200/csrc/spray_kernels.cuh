@@ -61,8 +61,10 @@ __device__ __forceinline__ void update_one(const KParams& P, const BoxEntry& B, 
   }
   double dia = P.parts.rd[PMP_PSTATE_DIA][s];
   if (FORM == Form::MIXED && dia < kMixedMinDia) {
-    const unsigned long long k = atomicAdd(&P.status->fallback, 1ULL);
-    P.fb_list[k] = s;
+    if (!P.fb_pre) {
+      const unsigned long long k = atomicAdd(&P.status->fallback, 1ULL);
+      P.fb_list[k] = s;
+    }
     return;
   }
   double pos[3], vel[3], Y[NF];
@@ -501,6 +503,19 @@ __device__ __forceinline__ int box_of_slot(const KParams& P, long long s)
     }
   }
   return lo;
+}
+
+// The droplets of slots [s0, s1) that the mixed kernel leaves to the FP64
+// kernel (alive, d < 2 um at the call's start), appended to the fallback list
+// before the mixed kernel runs, so that the FP64 list kernel can run beside it.
+static __global__ void __launch_bounds__(256) k_select_small(const __grid_constant__ KParams P, long long s0, long long s1)
+{
+  for (long long s = s0 + (long long)blockIdx.x * 256 + threadIdx.x; s < s1; s += (long long)gridDim.x * 256) {
+    if (P.parts.id[s] > 0 && P.parts.rd[PMP_PSTATE_DIA][s] < kMixedMinDia) {
+      const unsigned long long k = atomicAdd(&P.status->fallback, 1ULL);
+      P.fb_list[k] = s;
+    }
+  }
 }
 
 // The FP32 gas records of boxes [b0, b0 + gridDim.y) (BoxEntry::gr), one

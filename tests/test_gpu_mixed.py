@@ -87,3 +87,29 @@ def test_small_droplets_take_the_fp64_path(oracle):
     for k in ("pos", "rdata", "id"):
         a, b = pg[0][k], po[0][k]
         assert np.array_equal(a[..., small], b[..., small]), k
+
+
+def test_mixed_graph_and_side_stream_match_plain_launch(oracle):
+    """The mixed form's FP64 list kernel runs on a side stream beside the mixed
+    kernel; replayed from a CUDA graph (use_graph), the forked work gives the
+    same droplets bit for bit and the same deposits up to atomic order, and
+    the small droplets still match the FP64 oracle exactly."""
+    from tests.gpu_util import assert_bitwise
+    from tests.parity import source_errors
+    prob = W.config2(n=30_000, steps=2, ncells=(32, 32, 32), box=(16, 16, 16))
+    small = []
+    for p in prob.parts:
+        idx = np.arange(0, p["id"].shape[0], 11)
+        p["rdata"][capi.PSTATE_DIA, idx] = 1.5e-6
+        small.append(idx)
+    pa, sa, _ = gpu_run(prob, prob.steps, mode=capi.PMP_MODE_MIXED)
+    pb, sb, spb = gpu_run(prob, prob.steps, mode=capi.PMP_MODE_MIXED,
+                          setup=lambda sp: sp.set_launch(use_graph=True))
+    assert spb.stats().graph != 0
+    assert_bitwise(pa, pb)
+    for a, b in zip(sa, sb):
+        assert source_errors(b, a) <= 1e-12
+    po, _ = oracle_run(oracle, prob, prob.steps)
+    for b, idx in enumerate(small):
+        for k in ("pos", "rdata", "id"):
+            assert np.array_equal(pa[b][k][..., idx], po[b][k][..., idx]), (b, k)
