@@ -296,9 +296,9 @@ int pmp_spray_set_mode(pmp_spray* h, int mode);
  *                      energy the evaporated mass carries.
  * Call before pmp_spray_setup / pmp_spray_set_data (the latent heat is
  * shifted by the fuel enthalpy in the coupling's units there); PMP_ERR_INVALID
- * after.  The PeleC coupling runs the FP64 form with its default launch
- * (pmp_spray_set_launch does not apply); the other forms return
- * PMP_ERR_UNSUPPORTED in it, and pmp_spray_update_static couples to
+ * after.  The PeleC coupling runs the FP64 form (default launch:
+ * pmp_spray_set_launch does not apply) and the mixed form; the learned form
+ * returns PMP_ERR_UNSUPPORTED in it, and pmp_spray_update_static couples to
  * PeleLMeX only. */
 enum pmp_coupling { PMP_COUPLING_LMEX = 0, PMP_COUPLING_PELEC = 1 };
 int pmp_spray_set_coupling(pmp_spray* h, int coupling);

@@ -232,6 +232,9 @@ struct KParams {
   // mixed form: the droplets below 2 um were listed before the launch
   // (k_select_small); the mixed kernel skips them without listing them
   int fb_pre;
+  // mixed form: the diameter below which a droplet takes the FP64 path, 2 um
+  // in the coupling's length unit
+  double mixed_min_dia;
   // mixed / learned forms: species k of DevMechF (and of their gas-state
   // gather) is mechanism species spec_perm[k]; fuel_first as in DevMechF
   int spec_perm[kMaxSpec];

@@ -16,14 +16,20 @@ int launch_mixed(int ns, int nf, const KParams& P, int ncta, int block, cudaStre
   if (block != 128) {
     return PMP_ERR_INVALID;
   }
-#define PMP_MIXED_CASE(S, F)                                          \
-  if (ns == S && nf == F) {                                           \
-    if (P.fuel_first) {                                                \
-      spray_update_mixed<S, F, 128, true><<<ncta, 128, 0, st>>>(P);    \
-    } else {                                                           \
-      spray_update_mixed<S, F, 128, false><<<ncta, 128, 0, st>>>(P);   \
-    }                                                                  \
-    return PMP_OK;                                                    \
+#define PMP_MIXED_CASE(S, F)                                                  \
+  if (ns == S && nf == F) {                                                   \
+    if (P.pelec) {                                                            \
+      if (P.fuel_first) {                                                     \
+        spray_update_mixed<S, F, 128, true, true><<<ncta, 128, 0, st>>>(P);   \
+      } else {                                                                \
+        spray_update_mixed<S, F, 128, false, true><<<ncta, 128, 0, st>>>(P);  \
+      }                                                                       \
+    } else if (P.fuel_first) {                                                \
+      spray_update_mixed<S, F, 128, true><<<ncta, 128, 0, st>>>(P);           \
+    } else {                                                                  \
+      spray_update_mixed<S, F, 128, false><<<ncta, 128, 0, st>>>(P);          \
+    }                                                                         \
+    return PMP_OK;                                                            \
   }
   PMP_MIXED_CASE(3, 1)
   PMP_MIXED_CASE(5, 1)
@@ -53,7 +59,11 @@ int launch_gas_records(int ns, const KParams& P, int b0, int nb, int max_cells, 
   const dim3 grid((unsigned)std::min((max_cells + 255) / 256, 128), (unsigned)nb);
 #define PMP_REC_CASE(S)                                     \
   if (ns == S) {                                            \
-    k_gas_records<S><<<grid, 256, 0, st>>>(P, b0);          \
+    if (P.pelec) {                                          \
+      k_gas_records<S, true><<<grid, 256, 0, st>>>(P, b0);  \
+    } else {                                                \
+      k_gas_records<S><<<grid, 256, 0, st>>>(P, b0);        \
+    }                                                       \
     return PMP_OK;                                          \
   }
   PMP_REC_CASE(3)

@@ -291,7 +291,7 @@ int build_device_tables(pmp_spray* h)
     mf.inv_mw_kg[k] = (float)(1. / m.mw_kg[s]);
     mf.inv_mw_g[k] = (float)(1. / m.mw_g[s]);
     mf.mw_g[k] = (float)m.mw_g[s];
-    mf.ru_w_eng[k] = (float)(m.ru_w[s] * pmp::kEngConv);
+    mf.ru_w_eng[k] = (float)(m.ru_w[s] * (h->pelec ? 1. : pmp::kEngConv));
     for (int n = 0; n < 5; ++n) {
       mf.cp[k][n] = (float)m.cp[s][n];
     }
@@ -314,7 +314,7 @@ int build_device_tables(pmp_spray* h)
     ff.boilT[f] = (float)d.boilT[f];
     ff.inv_boilT[f] = (float)(1. / d.boilT[f]);
     ff.critT[f] = (float)d.critT[f];
-    ff.hb[f] = (float)(pmp::kRuCgs * pmp::kRuConv / (F.hboil_ref[f] * m.mw_kg[d.indx[f]]));
+    ff.hb[f] = (float)(pmp::kRuCgs * (h->pelec ? 1. : pmp::kRuConv) / (F.hboil_ref[f] * m.mw_kg[d.indx[f]]));
     ff.psat_a[f] = (float)d.psat_coef[4 * f];
     ff.psat_b[f] = (float)d.psat_coef[4 * f + 1];
     ff.psat_c[f] = (float)d.psat_coef[4 * f + 2];
@@ -583,7 +583,11 @@ int dispatch_fp64_list(int ns, int nf, const KParams& P, long long total, cudaSt
   const int grid = (int)std::max(1LL, std::min(need, 148LL * 4));
 #define PMP_CASE(S, F)                                                              \
   if (ns == S && nf == F) {                                                         \
-    pmp::spray_update_fp64_list<S, F, kBlock><<<grid, kBlock, 0, st>>>(P);          \
+    if (P.pelec) {                                                                  \
+      pmp::spray_update_fp64_list<S, F, kBlock, true><<<grid, kBlock, 0, st>>>(P);  \
+    } else {                                                                        \
+      pmp::spray_update_fp64_list<S, F, kBlock><<<grid, kBlock, 0, st>>>(P);        \
+    }                                                                               \
     return PMP_OK;                                                                  \
   }
   PMP_CASE(3, 1)
@@ -607,8 +611,8 @@ int prepare_update_impl(
   if (nboxes != (int)h->boxes.size()) {
     return set_err(h, PMP_ERR_INVALID, "nboxes differs from the grids given to set_grids");
   }
-  if (h->pelec && h->mode != PMP_MODE_FP64) {
-    return set_err(h, PMP_ERR_UNSUPPORTED, "the PeleC coupling runs the FP64 form only");
+  if (h->pelec && h->mode == PMP_MODE_LEARNED) {
+    return set_err(h, PMP_ERR_UNSUPPORTED, "the PeleC coupling runs the FP64 and mixed forms");
   }
   if (h->mode == PMP_MODE_LEARNED && !pmp::learn_ready(h)) {
     return set_err(h, PMP_ERR_INVALID, "the learned form needs a trained surrogate (pmp_spray_learn_train)");
@@ -764,6 +768,7 @@ int prepare_update_impl(
   P.c_T = c.utempIndx;
   P.c_eng = c.engIndx;
   P.pelec = h->pelec;
+  P.mixed_min_dia = h->pelec ? 100. * pmp::kMixedMinDia : pmp::kMixedMinDia;  // cm or m
   P.c_spec = c.specIndx;
   P.s_rho = c.rhoSrcIndx;
   P.s_mom = c.momSrcIndx;

@@ -60,7 +60,7 @@ __device__ __forceinline__ void update_one(const KParams& P, const BoxEntry& B, 
     return;
   }
   double dia = P.parts.rd[PMP_PSTATE_DIA][s];
-  if (FORM == Form::MIXED && dia < kMixedMinDia) {
+  if (FORM == Form::MIXED && dia < P.mixed_min_dia) {
     if (!P.fb_pre) {
       const unsigned long long k = atomicAdd(&P.status->fallback, 1ULL);
       P.fb_list[k] = s;
@@ -316,15 +316,15 @@ __device__ __forceinline__ void update_one(const KParams& P, const BoxEntry& B, 
         g.Y[n] = Yg[n];
         mwinv = fmaf(g.Y[n], P.mf.inv_mw_kg[n], mwinv);
       }
-      g.p = g.rho * (float)(kRuCgs * kRuConv) * mwinv * g.T;
+      g.p = g.rho * (float)(kRuCgs * Units<PELEC>::ru) * mwinv * g.T;
       g.mw_mix = fdiv(1.f, mwinv);
       float cBoilT[NF];
-      const float lp = flog(fdiv((float)(kPatmCgs * kPresConv), g.p));
+      const float lp = flog(fdiv((float)(kPatmCgs * Units<PELEC>::pres), g.p));
 #pragma unroll
       for (int spf = 0; spf < NF; ++spf) {
         cBoilT[spf] = fminf(P.ff.critT[spf], fdiv(1.f, fmaf(lp, P.ff.hb[spf], P.ff.inv_boilT[spf])));
       }
-      nsub = spray_source_mixed<NS, NF, FF>(P, P.sub_dt, g, cBoilT, vel, T, dia, Y, num_ppp, id, src, sx, sxs);
+      nsub = spray_source_mixed<NS, NF, FF, PELEC>(P, P.sub_dt, g, cBoilT, vel, T, dia, Y, num_ppp, id, src, sx, sxs);
       {
         // the position and the cell it gives, back from shared memory
         const volatile double* vx = sx;
@@ -471,7 +471,7 @@ __global__ void __launch_bounds__(BLOCK, PMP_FP64_MIN_BLOCKS) spray_update_fp64_
   flush_counters(P, c);
 }
 
-template <int NS, int NF, int BLOCK, bool FF>
+template <int NS, int NF, int BLOCK, bool FF, bool PELEC = false>
 __global__ void __launch_bounds__(BLOCK, PMP_MIXED_MIN_BLOCKS) spray_update_mixed(const __grid_constant__ KParams P)
 {
   __shared__ BoxEntry sB;
@@ -484,7 +484,7 @@ __global__ void __launch_bounds__(BLOCK, PMP_MIXED_MIN_BLOCKS) spray_update_mixe
   __shared__ double stash[(5 + NF) * BLOCK];
   double* sx = stash + threadIdx.x;
   if (s < sB.p_end) {
-    update_one<NS, NF, Form::MIXED, FF>(P, sB, b, s, c, sx, BLOCK);
+    update_one<NS, NF, Form::MIXED, FF, PELEC>(P, sB, b, s, c, sx, BLOCK);
   }
   flush_counters(P, c);
 }
@@ -511,7 +511,7 @@ __device__ __forceinline__ int box_of_slot(const KParams& P, long long s)
 static __global__ void __launch_bounds__(256) k_select_small(const __grid_constant__ KParams P, long long s0, long long s1)
 {
   for (long long s = s0 + (long long)blockIdx.x * 256 + threadIdx.x; s < s1; s += (long long)gridDim.x * 256) {
-    if (P.parts.id[s] > 0 && P.parts.rd[PMP_PSTATE_DIA][s] < kMixedMinDia) {
+    if (P.parts.id[s] > 0 && P.parts.rd[PMP_PSTATE_DIA][s] < P.mixed_min_dia) {
       const unsigned long long k = atomicAdd(&P.status->fallback, 1ULL);
       P.fb_list[k] = s;
     }
@@ -522,7 +522,7 @@ static __global__ void __launch_bounds__(256) k_select_small(const __grid_consta
 // thread per cell of the grown box, from the FP64 state: the mixed and
 // learned updates then gather 2-3 16-byte records per stencil cell instead of
 // 5 + NS FP64 planes, with rho*Y / rho divided once per cell.
-template <int NS>
+template <int NS, bool PELEC = false>
 __global__ void __launch_bounds__(256) k_gas_records(const __grid_constant__ KParams P, int b0)
 {
   constexpr int R4 = gas_rec4(NS);
@@ -541,14 +541,34 @@ __global__ void __launch_bounds__(256) k_gas_records(const __grid_constant__ KPa
     const double rho = __ldg(q + P.c_rho * B.st_n32);
     float v[4 * R4];
     v[0] = (float)rho;
-    v[1] = (float)__ldg(q + P.c_T * B.st_n32);
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      v[2 + d] = (float)__ldg(q + (P.c_mom + d) * B.st_n32);
-    }
 #pragma unroll
     for (int s = 0; s < NS; ++s) {
       v[5 + s] = (float)(__ldg(q + (P.c_spec + P.spec_perm[s]) * B.st_n32) / rho);
+    }
+    if (!PELEC) {
+      v[1] = (float)__ldg(q + P.c_T * B.st_n32);
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        v[2 + d] = (float)__ldg(q + (P.c_mom + d) * B.st_n32);
+      }
+    } else {
+      // velocity from momentum, T from the internal energy (FP64, as the
+      // FP64 records), mass fractions in mechanism order for the inversion
+      const double inv_rho = 1. / rho;
+      double Yc[NS];
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        Yc[s] = __ldg(q + (P.c_spec + s) * B.st_n32) * inv_rho;
+      }
+      double ke = 0.;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const double u = __ldg(q + (P.c_mom + d) * B.st_n32) * inv_rho;
+        v[2 + d] = (float)u;
+        ke += 0.5 * u * u;
+      }
+      const double e = __ldg(q + P.c_eng * B.st_n32) * inv_rho - ke;
+      v[1] = (float)ey2t<NS>(P.m, e, Yc, __ldg(q + P.c_T * B.st_n32));
     }
 #pragma unroll
     for (int s = 5 + NS; s < 4 * R4; ++s) {
@@ -622,7 +642,7 @@ __global__ void __launch_bounds__(256) k_gas_records64(const __grid_constant__ K
   }
 }
 
-template <int NS, int NF, int BLOCK>
+template <int NS, int NF, int BLOCK, bool PELEC = false>
 __global__ void __launch_bounds__(BLOCK, PMP_FP64_MIN_BLOCKS) spray_update_fp64_list(const __grid_constant__ KParams P)
 {
   const unsigned long long n = *reinterpret_cast<volatile unsigned long long*>(&P.status->fallback);
@@ -634,7 +654,7 @@ __global__ void __launch_bounds__(BLOCK, PMP_FP64_MIN_BLOCKS) spray_update_fp64_
     if (P.list_nbox > 0 && (b < P.list_box0 || b >= P.list_box0 + P.list_nbox)) {
       continue;
     }
-    update_one<NS, NF, Form::FP64>(P, P.boxes[b], b, s, c);
+    update_one<NS, NF, Form::FP64, false, PELEC>(P, P.boxes[b], b, s, c);
   }
   flush_counters(P, c);
 }

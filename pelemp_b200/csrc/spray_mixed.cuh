@@ -243,8 +243,10 @@ struct SrcD {
   double eng;
 };
 
-// calculateSpraySource with FP32 physics and FP64 state (see the file header).
-template <int NS, int NF, bool FF>
+// calculateSpraySource with FP32 physics and FP64 state (see the file header);
+// PELEC: CGS units and the drag-work and evaporated kinetic-energy terms of
+// the energy source (Drag.H:282-286, 418-421).
+template <int NS, int NF, bool FF, bool PELEC = false>
 __device__ __forceinline__ int spray_source_mixed(
   const KParams& P, double flow_dt, const GasF<NS>& g, const float* cBoilT, double* vel_io,
   double& T_io, double& dia_io, double* Y_io, double num_ppp, int& id, SrcD<NF>& src,
@@ -255,10 +257,10 @@ __device__ __forceinline__ int spray_source_mixed(
   const DevFuel& fdat = P.f;
   const float rule = 1.f / 3.f;
   const float C_eps = 1.E-15f;
-  const double min_mass = 1.E-13 * kMassConv;
+  const double min_mass = 1.E-13 * Units<PELEC>::mass;
   const int nSubMax = 100;
-  const float RU = (float)(kRuCgs * kRuConv);
-  const float PATM = (float)(kPatmCgs * kPresConv);
+  const float RU = (float)(kRuCgs * Units<PELEC>::ru);
+  const float PATM = (float)(kPatmCgs * Units<PELEC>::pres);
   float Y_skin[NS];
   float Ddiag[NF];
   float L_fuel[NF];
@@ -443,8 +445,8 @@ __device__ __forceinline__ int spray_source_mixed(
         }
       }
     }
-    mu_skin *= (float)kMuConv;
-    lambda_skin *= (float)kLambdaConv;
+    mu_skin *= (float)Units<PELEC>::mu;
+    lambda_skin *= (float)Units<PELEC>::lambda;
     float diff_vel[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
@@ -474,6 +476,15 @@ __device__ __forceinline__ int spray_source_mixed(
       for (int d = 0; d < 3; ++d) {
         mom_acc[d] = fmaf(drag_force, diff_vel[d], mom_acc[d]);
       }
+      if (PELEC) {
+        // drag work on the gas, (s_d,mu . u_d)
+        float S = 0.f;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          S = fmaf(diff_vel[d], (float)vel_part[d], S);
+        }
+        eng_acc = fmaf(drag_force, S, eng_acc);
+      }
       if (isub == 1) {
         nsub = min(max(nsub, static_cast<int>((float)flow_dt * drag_force_p) + 1), nSubMax);
       }
@@ -494,7 +505,7 @@ __device__ __forceinline__ int spray_source_mixed(
 #pragma unroll
         for (int spf = 0; spf < NF; ++spf) {
           const int fspec = fuel_sp<FF>(fdat, spf);
-          Ddiag[spf] *= mw_skin * m.inv_mw_kg[fspec] * (float)kRhodConv * (X_vapor[spf] * inv_sumX);
+          Ddiag[spf] *= mw_skin * m.inv_mw_kg[fspec] * (float)Units<PELEC>::rhod * (X_vapor[spf] * inv_sumX);
           rhoDtotal += Ddiag[spf];
           const float ysk = fsel(Y_skin, fspec);
           cp_fuel += ysk * cpf(m, fspec, T_skin);
@@ -601,6 +612,11 @@ __device__ __forceinline__ int spray_source_mixed(
   const double inv_dtf = 1. / (fdat.dtmod * flow_dt);
   const double mdot_total = (pmass - startmass_) * inv_dtf;
   src.mass = num_ppp * mdot_total;
+  if (PELEC) {
+    // kinetic energy carried by the evaporated mass
+    const double part_ke = 0.5 * (vel_part[0] * vel_part[0] + vel_part[1] * vel_part[1] + vel_part[2] * vel_part[2]);
+    src.eng += num_ppp * part_ke * mdot_total;
+  }
   if (fdat.mom_trans) {
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
