@@ -153,6 +153,18 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity)
   }
 }
 
+// One thread: a bulk (TMA, no tensor map) copy of `bytes` (a multiple of 16,
+// both addresses 16-byte aligned) from global to shared memory, completing
+// the mbarrier's current phase when the bytes have landed.
+__device__ __forceinline__ void bulk_load(void* smem_dst, const void* gsrc, uint32_t bytes, uint32_t mbar)
+{
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                 smem_u32(smem_dst)),
+               "l"(gsrc), "r"(bytes), "r"(mbar)
+               : "memory");
+}
+
 __device__ __forceinline__ unsigned silu2(float h0, float h1)
 {
   const __nv_bfloat162 p2 = __floats2bfloat162_rn(h0, h1);

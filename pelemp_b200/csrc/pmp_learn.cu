@@ -742,14 +742,17 @@ __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
                threadIdx.x;
   __shared__ uint32_t tmem_slot;
   __shared__ unsigned long long mbar_slot;
-  {
-    const int4* src = reinterpret_cast<const int4*>(L.mlp_tc);
-    int4* dst = reinterpret_cast<int4*>(&S);
-    for (int i = threadIdx.x; i < (int)(sizeof(tc::TcMlp) / 16); i += BLOCK) {
-      dst[i] = src[i];
-    }
+  __shared__ unsigned long long wbar_slot;
+  // the weights arrive by one bulk copy while the droplets are read and the
+  // first gather runs; the first network evaluation waits for them
+  static_assert(sizeof(tc::TcMlp) % 16 == 0, "bulk copies move multiples of 16 bytes");
+  const uint32_t wbar = tc::smem_u32(&wbar_slot);
+  if (threadIdx.x == 0) {
+    tc::mbar_init(wbar);
+    tc::bulk_load(&S, L.mlp_tc, (uint32_t)sizeof(tc::TcMlp), wbar);
   }
   tc::TcCta tcs = tc::tc_setup(&tmem_slot, &mbar_slot, TILES * tc::kCols);
+  bool weights_in = false;  // uniform over the CTA
   const DevMechF& m = P.mf;
   const DevFuelF& ff = P.ff;
   const DevFuel& fdat = P.f;
@@ -984,6 +987,22 @@ __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
         }
       }
       float yo[kLearnOut];
+      if (!weights_in) {
+        weights_in = true;
+        if (__syncthreads_and(tc::mbar_wait(wbar, 0)) == 0) {
+          // the weights never landed: stop the CTA (the copy is waited for
+          // once more before the exit)
+          tc_dead = true;
+          pending = false;
+          active = false;
+          valid = false;
+          weights_in = false;
+          if (threadIdx.x == 0) {
+            set_error(P, PMP_ERR_TIMEOUT, b, s);
+          }
+          continue;
+        }
+      }
       if (!tc::mlp_cta_tc<TILES>(S, A, tcs, xn, yo)) {
         // an MMA completion wait timed out (uniformly over the CTA): stop, no
         // further droplet of the CTA is written
@@ -1264,6 +1283,9 @@ __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
     }
   }
   }  // items
+  if (!weights_in) {
+    tc::mbar_wait(wbar, 0);  // no network evaluation waited for the weight copy: it must land before the exit
+  }
   tc::tc_teardown(tcs, TILES * tc::kCols);
   flush_counters(P, c);
 }
