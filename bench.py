@@ -241,6 +241,11 @@ WORKLOAD_TEXT = {
                "capped-Zipf counts, config-1 physics, MKD + MK per step, FP64",
 }
 FORM_MODE = {"fp64": 0, "mixed": 1, "learned": 2}
+# the library's kernels one update call launches (MKD and MK alike):
+# FP64: gas records + update; mixed: gas records + small-droplet selection +
+# update + FP64 list kernel (side stream); learned: gas records + update +
+# FP64 list kernel
+KERNELS_PER_CALL = {"fp64": 2, "mixed": 4, "learned": 3}
 FORM_NAME = {"fp64": "plain FP64", "mixed": "mixed FP32 physics / FP64 state and deposits",
              "learned": "learned surrogate (bf16 MLP on tensor cores) + FP32 physics / FP64 state"}
 KERNEL = {"fp64": "spray_update_fp64<5,2,128>", "mixed": "spray_update_mixed<5,2,128,fuel_first>",
@@ -368,6 +373,8 @@ def bench_batched(args, world, rank, local, pg):
                                      "what": "one launch per box, stream synchronised after each "
                                              "(SprayParticles.cpp:244-248,499)"},
                 "speedup_vs_per_box": v_tuned / v_box},
+            # the headline (autotuned) run: gas records + update per call
+            "gpu_launches": 2 * args.steps * KERNELS_PER_CALL["fp64"],
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
@@ -599,7 +606,7 @@ def main():
                          if peak_src == "measured" else "fallback 6650 GB/s"},
             "e2e": e2e,
             "cpu_baseline": cpu,
-            "gpu_launches": 2 * args.steps * (2 if head != "fp64" else 1),
+            "gpu_launches": 2 * args.steps * KERNELS_PER_CALL[head],
             "clocks": clocks,
             "substeps_per_step": results[head]["substeps"] / args.steps,
         }
