@@ -763,525 +763,525 @@ __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
   Counters c;
   bool tc_dead = false;  // a timed-out MMA wait stops the CTA (uniform)
   for (int it = blockIdx.x; it * TILES < L.ncta && !tc_dead; it += gridDim.x) {
-  const int item = it * TILES + threadIdx.x / kBlock;
-  const bool item_ok = item < L.ncta;
-  const int b = item_ok ? P.cta_box[item] : 0;
-  // this item's box entry, staged in shared memory (after the previous
-  // item's readers are done)
-  __syncthreads();
-  {
-    const int h = threadIdx.x / kBlock;
-    const int* src = reinterpret_cast<const int*>(P.boxes + b);
-    int* dst = reinterpret_cast<int*>(&sB[h]);
-    for (int i = threadIdx.x % kBlock; i < (int)(sizeof(BoxEntry) / 4); i += kBlock) {
-      dst[i] = src[i];
+    const int item = it * TILES + threadIdx.x / kBlock;
+    const bool item_ok = item < L.ncta;
+    const int b = item_ok ? P.cta_box[item] : 0;
+    // this item's box entry, staged in shared memory (after the previous
+    // item's readers are done)
+    __syncthreads();
+    {
+      const int h = threadIdx.x / kBlock;
+      const int* src = reinterpret_cast<const int*>(P.boxes + b);
+      int* dst = reinterpret_cast<int*>(&sB[h]);
+      for (int i = threadIdx.x % kBlock; i < (int)(sizeof(BoxEntry) / 4); i += kBlock) {
+        dst[i] = src[i];
+      }
     }
-  }
-  __syncthreads();
-  const BoxEntry& B = sB[threadIdx.x / kBlock];
-  const long long s = item_ok ? P.cta_start[item] + threadIdx.x % kBlock : 0;
-  bool valid = item_ok && s < B.p_end;
-  int id = valid ? P.parts.id[s] : 0;
-  valid = valid && id > 0;
-  double dia = valid ? P.parts.rd[PMP_PSTATE_DIA][s] : 1e-5;
-  if (valid && dia < kMixedMinDia) {
-    const unsigned long long k = atomicAdd(&P.status->fallback, 1ULL);
-    P.fb_list[k] = s;
-    valid = false;
-  }
-  double pos[3] = {0., 0., 0.}, vel[3] = {0., 0., 0.}, Y[NF];
-  double T = 300.;
-#pragma unroll
-  for (int f = 0; f < NF; ++f) {
-    Y[f] = 0.;
-  }
-  double num_ppp = 0., film = 0.;
-  if (valid) {
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      pos[d] = P.parts.pos[d][s];
-      vel[d] = P.parts.rd[PMP_PSTATE_VEL + d][s];
+    __syncthreads();
+    const BoxEntry& B = sB[threadIdx.x / kBlock];
+    const long long s = item_ok ? P.cta_start[item] + threadIdx.x % kBlock : 0;
+    bool valid = item_ok && s < B.p_end;
+    int id = valid ? P.parts.id[s] : 0;
+    valid = valid && id > 0;
+    double dia = valid ? P.parts.rd[PMP_PSTATE_DIA][s] : 1e-5;
+    if (valid && dia < kMixedMinDia) {
+      const unsigned long long k = atomicAdd(&P.status->fallback, 1ULL);
+      P.fb_list[k] = s;
+      valid = false;
     }
-    T = P.parts.rd[PMP_PSTATE_T][s];
+    double pos[3] = {0., 0., 0.}, vel[3] = {0., 0., 0.}, Y[NF];
+    double T = 300.;
 #pragma unroll
     for (int f = 0; f < NF; ++f) {
-      Y[f] = P.parts.rd[PMP_PSTATE_Y + f][s];
+      Y[f] = 0.;
     }
-    num_ppp = P.parts.rd[PMP_PSTATE_NUMDENS(NF)][s];
-    film = P.parts.rd[PMP_PSTATE_FILMHGHT(NF)][s];
-  }
-  int bflags[3] = {0, 0, 0};
-  bool ok = true;
-  if (valid && B.at_bounds) {
-    if (check_bounds(P, pos, bflags)) {
-      set_error(P, PMP_ERR_LEFT_DOMAIN, b, s);
+    double num_ppp = 0., film = 0.;
+    if (valid) {
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        pos[d] = P.parts.pos[d][s];
+        vel[d] = P.parts.rd[PMP_PSTATE_VEL + d][s];
+      }
+      T = P.parts.rd[PMP_PSTATE_T][s];
+#pragma unroll
+      for (int f = 0; f < NF; ++f) {
+        Y[f] = P.parts.rd[PMP_PSTATE_Y + f][s];
+      }
+      num_ppp = P.parts.rd[PMP_PSTATE_NUMDENS(NF)][s];
+      film = P.parts.rd[PMP_PSTATE_FILMHGHT(NF)][s];
+    }
+    int bflags[3] = {0, 0, 0};
+    bool ok = true;
+    if (valid && B.at_bounds) {
+      if (check_bounds(P, pos, bflags)) {
+        set_error(P, PMP_ERR_LEFT_DOMAIN, b, s);
+        ok = false;
+      }
+    }
+    // a wall-film droplet stops the first sub-cycle (the film height never
+    // changes here, so the check is made once)
+    if (valid && ok && P.num_iter > 0 && id > 0 && film > 0.) {
+      set_error(P, PMP_ERR_UNSUPPORTED, b, s);
       ok = false;
     }
-  }
-  // a wall-film droplet stops the first sub-cycle (the film height never
-  // changes here, so the check is made once)
-  if (valid && ok && P.num_iter > 0 && id > 0 && film > 0.) {
-    set_error(P, PMP_ERR_UNSUPPORTED, b, s);
-    ok = false;
-  }
-  sx[3 * BLOCK] = num_ppp;
-  for (int cur_iter = 0; cur_iter < P.num_iter; ++cur_iter) {
-    // cell of the droplet (recomputed from the position each sub-cycle, so
-    // the stencil indices are not live across the network evaluation)
-    double lx[3];
-    int ijk[3], ijkc[3];
-    cell_of(P, pos, lx, ijk, ijkc);
-    bool active = valid && ok && id > 0;
+    sx[3 * BLOCK] = num_ppp;
+    for (int cur_iter = 0; cur_iter < P.num_iter; ++cur_iter) {
+      // cell of the droplet (recomputed from the position each sub-cycle, so
+      // the stencil indices are not live across the network evaluation)
+      double lx[3];
+      int ijk[3], ijkc[3];
+      cell_of(P, pos, lx, ijk, ijkc);
+      bool active = valid && ok && id > 0;
 #pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      sx[d * BLOCK] = pos[d];
-    }
-    GasF<NS> g;
-    float cBoilT[NF];
-    g.T = 0.f;
-    g.rho = 1.f;
-    g.p = 1.f;
-    g.mw_mix = 1.f;
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      g.vel[d] = 0.f;
-    }
-#pragma unroll
-    for (int n = 0; n < NS; ++n) {
-      g.Y[n] = 0.f;
-    }
-#pragma unroll
-    for (int f = 0; f < NF; ++f) {
-      cBoilT[f] = 400.f;
-    }
-    if (active) {
-      double ssv[2][3];
-#pragma unroll
-      for (int dir = 0; dir < 3; ++dir) {
-        const double sx_hi = __dsub_rn(lx[dir], static_cast<double>(ijk[dir]));
-        const double sx_lo = __dsub_rn(1., sx_hi);
-        ssv[0][dir] = bflags[dir] > 1 ? 1. : (bflags[dir] < -1 ? 0. : sx_lo);
-        ssv[1][dir] = bflags[dir] > 1 ? 0. : (bflags[dir] < -1 ? 1. : sx_hi);
+      for (int d = 0; d < 3; ++d) {
+        sx[d * BLOCK] = pos[d];
       }
-      constexpr int R4 = gas_rec4(NS);
-      float rho = 0.f, Tg = 0.f, vg[3] = {0.f, 0.f, 0.f}, Yg[NS];
+      GasF<NS> g;
+      float cBoilT[NF];
+      g.T = 0.f;
+      g.rho = 1.f;
+      g.p = 1.f;
+      g.mw_mix = 1.f;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        g.vel[d] = 0.f;
+      }
 #pragma unroll
       for (int n = 0; n < NS; ++n) {
-        Yg[n] = 0.f;
+        g.Y[n] = 0.f;
       }
-      bool state_ok = true;
 #pragma unroll
-      for (int kk = -1; kk < 1; ++kk) {
+      for (int f = 0; f < NF; ++f) {
+        cBoilT[f] = 400.f;
+      }
+      if (active) {
+        double ssv[2][3];
 #pragma unroll
-        for (int jj = -1; jj < 1; ++jj) {
+        for (int dir = 0; dir < 3; ++dir) {
+          const double sx_hi = __dsub_rn(lx[dir], static_cast<double>(ijk[dir]));
+          const double sx_lo = __dsub_rn(1., sx_hi);
+          ssv[0][dir] = bflags[dir] > 1 ? 1. : (bflags[dir] < -1 ? 0. : sx_lo);
+          ssv[1][dir] = bflags[dir] > 1 ? 0. : (bflags[dir] < -1 ? 1. : sx_hi);
+        }
+        constexpr int R4 = gas_rec4(NS);
+        float rho = 0.f, Tg = 0.f, vg[3] = {0.f, 0.f, 0.f}, Yg[NS];
 #pragma unroll
-          for (int ii = -1; ii < 1; ++ii) {
-            const double cw = ssv[ii + 1][0] * ssv[jj + 1][1] * ssv[kk + 1][2];
-            if (cw > 0.) {
-              const int ci = ijk[0] + ii, cj = ijk[1] + jj, ck = ijk[2] + kk;
-              if (!in_box(B.state_lo, B.state_hi, ci, cj, ck)) {
-                state_ok = false;
-              } else {
-                float rec[4 * R4];
-                load_gas_rec<R4>(B, ci, cj, ck, rec);
-                const float w = (float)cw;
-                rho = fmaf(w, rec[0], rho);
-                Tg = fmaf(w, rec[1], Tg);
+        for (int n = 0; n < NS; ++n) {
+          Yg[n] = 0.f;
+        }
+        bool state_ok = true;
 #pragma unroll
-                for (int dir = 0; dir < 3; ++dir) {
-                  vg[dir] = fmaf(w, rec[2 + dir], vg[dir]);
-                }
+        for (int kk = -1; kk < 1; ++kk) {
 #pragma unroll
-                for (int n = 0; n < NS; ++n) {
-                  Yg[n] = fmaf(w, rec[5 + n], Yg[n]);
+          for (int jj = -1; jj < 1; ++jj) {
+#pragma unroll
+            for (int ii = -1; ii < 1; ++ii) {
+              const double cw = ssv[ii + 1][0] * ssv[jj + 1][1] * ssv[kk + 1][2];
+              if (cw > 0.) {
+                const int ci = ijk[0] + ii, cj = ijk[1] + jj, ck = ijk[2] + kk;
+                if (!in_box(B.state_lo, B.state_hi, ci, cj, ck)) {
+                  state_ok = false;
+                } else {
+                  float rec[4 * R4];
+                  load_gas_rec<R4>(B, ci, cj, ck, rec);
+                  const float w = (float)cw;
+                  rho = fmaf(w, rec[0], rho);
+                  Tg = fmaf(w, rec[1], Tg);
+#pragma unroll
+                  for (int dir = 0; dir < 3; ++dir) {
+                    vg[dir] = fmaf(w, rec[2 + dir], vg[dir]);
+                  }
+#pragma unroll
+                  for (int n = 0; n < NS; ++n) {
+                    Yg[n] = fmaf(w, rec[5 + n], Yg[n]);
+                  }
                 }
               }
             }
           }
         }
-      }
-      if (!state_ok) {
-        set_error(P, PMP_ERR_STATE_BOX, b, s);
-        ok = false;
-        active = false;
-      } else {
-        g.rho = rho;
-        g.T = Tg;
+        if (!state_ok) {
+          set_error(P, PMP_ERR_STATE_BOX, b, s);
+          ok = false;
+          active = false;
+        } else {
+          g.rho = rho;
+          g.T = Tg;
 #pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          g.vel[d] = vg[d];
-        }
-        float mwinv = 0.f;
+          for (int d = 0; d < 3; ++d) {
+            g.vel[d] = vg[d];
+          }
+          float mwinv = 0.f;
 #pragma unroll
-        for (int n = 0; n < NS; ++n) {
-          g.Y[n] = Yg[n];
-          mwinv = fmaf(g.Y[n], m.inv_mw_kg[n], mwinv);
-        }
-        g.p = g.rho * (float)(kRuCgs * kRuConv) * mwinv * g.T;
-        g.mw_mix = fdiv(1.f, mwinv);
-        const float lp = flog(fdiv((float)(kPatmCgs * kPresConv), g.p));
+          for (int n = 0; n < NS; ++n) {
+            g.Y[n] = Yg[n];
+            mwinv = fmaf(g.Y[n], m.inv_mw_kg[n], mwinv);
+          }
+          g.p = g.rho * (float)(kRuCgs * kRuConv) * mwinv * g.T;
+          g.mw_mix = fdiv(1.f, mwinv);
+          const float lp = flog(fdiv((float)(kPatmCgs * kPresConv), g.p));
 #pragma unroll
-        for (int spf = 0; spf < NF; ++spf) {
-          cBoilT[spf] = fminf(ff.critT[spf], fdiv(1.f, fmaf(lp, ff.hb[spf], ff.inv_boilT[spf])));
-        }
-      }
-    }
-    // calculateSpraySource with the surrogate for the evaporation sub-step
-    SrcD<NF> src;
-    double Y_part[NF];
-    double vel_part[3] = {vel[0], vel[1], vel[2]};
-    if (fdat.fixed_parts) {
-      vel_part[0] = vel_part[1] = vel_part[2] = 0.;
-    }
-    double T_part = T, dia_part = dia, rho_part = 0.;
-#pragma unroll
-    for (int spf = 0; spf < NF; ++spf) {
-      Y_part[spf] = Y[spf];
-      rho_part += Y_part[spf] / rhoL(fdat, dmin(T_part, (double)cBoilT[spf]), spf);
-    }
-    rho_part = 1. / rho_part;
-    double dt = P.sub_dt;
-    const double flow_dt = P.sub_dt;
-    int isub = 1, nsub = 1;
-    double pmass = PMP_PI / 6. * rho_part * (dia_part * dia_part * dia_part);
-    sx[4 * BLOCK] = pmass;
-#pragma unroll
-    for (int spf = 0; spf < NF; ++spf) {
-      sx[(5 + spf) * BLOCK] = Y[spf];
-    }
-    // sums over the inner sub-steps in FP32; times the parcel count in FP64 at the end
-    float eng_acc = 0.f, mom_acc[3] = {0.f, 0.f, 0.f};
-    float T_h = (float)T_part;
-    bool pending = active;
-    bool fell_back = false;
-    while (__syncthreads_or(pending)) {
-      // closed-form vapor state, then the surrogate inputs
-      float xin[kLearnIn];
-      float xn[kLearnIn];
-      float L_fuel[NF], X_vapor[NF], Yfv[NF];
-      float sumXVap, B_M;
-      bool in_range = true;
-      vapor_state_f<NS, NF, FF>(m, ff, fdat, g, cBoilT, (float)T_part, Y_part, L_fuel, X_vapor, Yfv, sumXVap, B_M);
-      {
-        double slip = 0.;
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          const double dv = (double)g.vel[d] - vel_part[d];
-          slip += dv * dv;
-        }
-        slip = sqrt(slip);
-        xin[0] = flog((float)dia_part);
-        xin[1] = (float)T_part;
-        xin[2] = g.T;
-        xin[3] = flog(g.p * (float)(1. / (kPatmCgs * kPresConv)));
-        xin[4] = fsel(g.Y, dep_sp<FF>(fdat, 0));
-        xin[5] = NF > 1 ? fsel(g.Y, dep_sp<FF>(fdat, NF > 1 ? 1 : 0)) : 0.f;
-        xin[6] = flog((float)(g.rho * slip * dia_part) + 1e-12f);
-        xin[7] = (float)Y_part[0];
-        xin[8] = Yfv[0];
-        xin[9] = NF > 1 ? Yfv[NF > 1 ? 1 : 0] : 0.f;
-#pragma unroll
-        for (int k = 0; k < kLearnIn; ++k) {
-          xn[k] = pending ? (xin[k] - L.norm.x_mean[k]) * L.norm.x_inv_std[k] : 0.f;
-          in_range = in_range && xin[k] >= L.norm.x_lo[k] && xin[k] <= L.norm.x_hi[k];
+          for (int spf = 0; spf < NF; ++spf) {
+            cBoilT[spf] = fminf(ff.critT[spf], fdiv(1.f, fmaf(lp, ff.hb[spf], ff.inv_boilT[spf])));
+          }
         }
       }
-      float yo[kLearnOut];
-      if (!weights_in) {
-        weights_in = true;
-        if (__syncthreads_and(tc::mbar_wait(wbar, 0)) == 0) {
-          // the weights never landed: stop the CTA (the copy is waited for
-          // once more before the exit)
+      // calculateSpraySource with the surrogate for the evaporation sub-step
+      SrcD<NF> src;
+      double Y_part[NF];
+      double vel_part[3] = {vel[0], vel[1], vel[2]};
+      if (fdat.fixed_parts) {
+        vel_part[0] = vel_part[1] = vel_part[2] = 0.;
+      }
+      double T_part = T, dia_part = dia, rho_part = 0.;
+#pragma unroll
+      for (int spf = 0; spf < NF; ++spf) {
+        Y_part[spf] = Y[spf];
+        rho_part += Y_part[spf] / rhoL(fdat, dmin(T_part, (double)cBoilT[spf]), spf);
+      }
+      rho_part = 1. / rho_part;
+      double dt = P.sub_dt;
+      const double flow_dt = P.sub_dt;
+      int isub = 1, nsub = 1;
+      double pmass = PMP_PI / 6. * rho_part * (dia_part * dia_part * dia_part);
+      sx[4 * BLOCK] = pmass;
+#pragma unroll
+      for (int spf = 0; spf < NF; ++spf) {
+        sx[(5 + spf) * BLOCK] = Y[spf];
+      }
+      // sums over the inner sub-steps in FP32; times the parcel count in FP64 at the end
+      float eng_acc = 0.f, mom_acc[3] = {0.f, 0.f, 0.f};
+      float T_h = (float)T_part;
+      bool pending = active;
+      bool fell_back = false;
+      while (__syncthreads_or(pending)) {
+        // closed-form vapor state, then the surrogate inputs
+        float xin[kLearnIn];
+        float xn[kLearnIn];
+        float L_fuel[NF], X_vapor[NF], Yfv[NF];
+        float sumXVap, B_M;
+        bool in_range = true;
+        vapor_state_f<NS, NF, FF>(m, ff, fdat, g, cBoilT, (float)T_part, Y_part, L_fuel, X_vapor, Yfv, sumXVap, B_M);
+        {
+          double slip = 0.;
+#pragma unroll
+          for (int d = 0; d < 3; ++d) {
+            const double dv = (double)g.vel[d] - vel_part[d];
+            slip += dv * dv;
+          }
+          slip = sqrt(slip);
+          xin[0] = flog((float)dia_part);
+          xin[1] = (float)T_part;
+          xin[2] = g.T;
+          xin[3] = flog(g.p * (float)(1. / (kPatmCgs * kPresConv)));
+          xin[4] = fsel(g.Y, dep_sp<FF>(fdat, 0));
+          xin[5] = NF > 1 ? fsel(g.Y, dep_sp<FF>(fdat, NF > 1 ? 1 : 0)) : 0.f;
+          xin[6] = flog((float)(g.rho * slip * dia_part) + 1e-12f);
+          xin[7] = (float)Y_part[0];
+          xin[8] = Yfv[0];
+          xin[9] = NF > 1 ? Yfv[NF > 1 ? 1 : 0] : 0.f;
+#pragma unroll
+          for (int k = 0; k < kLearnIn; ++k) {
+            xn[k] = pending ? (xin[k] - L.norm.x_mean[k]) * L.norm.x_inv_std[k] : 0.f;
+            in_range = in_range && xin[k] >= L.norm.x_lo[k] && xin[k] <= L.norm.x_hi[k];
+          }
+        }
+        float yo[kLearnOut];
+        if (!weights_in) {
+          weights_in = true;
+          if (__syncthreads_and(tc::mbar_wait(wbar, 0)) == 0) {
+            // the weights never landed: stop the CTA (the copy is waited for
+            // once more before the exit)
+            tc_dead = true;
+            pending = false;
+            active = false;
+            valid = false;
+            weights_in = false;
+            if (threadIdx.x == 0) {
+              set_error(P, PMP_ERR_TIMEOUT, b, s);
+            }
+            continue;
+          }
+        }
+        if (!tc::mlp_cta_tc<TILES>(S, A, tcs, xn, yo)) {
+          // an MMA completion wait timed out (uniformly over the CTA): stop, no
+          // further droplet of the CTA is written
           tc_dead = true;
           pending = false;
           active = false;
           valid = false;
-          weights_in = false;
           if (threadIdx.x == 0) {
             set_error(P, PMP_ERR_TIMEOUT, b, s);
           }
+          tc::mbar_wait(tcs.mbar, tcs.phase ^ 1u);  // the MMAs the timed-out wait was for
           continue;
         }
-      }
-      if (!tc::mlp_cta_tc<TILES>(S, A, tcs, xn, yo)) {
-        // an MMA completion wait timed out (uniformly over the CTA): stop, no
-        // further droplet of the CTA is written
-        tc_dead = true;
-        pending = false;
-        active = false;
-        valid = false;
-        if (threadIdx.x == 0) {
-          set_error(P, PMP_ERR_TIMEOUT, b, s);
-        }
-        tc::mbar_wait(tcs.mbar, tcs.phase ^ 1u);  // the MMAs the timed-out wait was for
-        continue;
-      }
-      if (pending) {
-        float yv[kLearnOut];
-#pragma unroll
-        for (int k = 0; k < kLearnOut; ++k) {
-          yv[k] = fmaf(yo[k], L.norm.y_std[k], L.norm.y_mean[k]);
-        }
-        if (cur_iter == 0 && isub == 1) {
-          // gate: some fuel evaporates, inputs inside the (widened)
-          // training range, outputs finite
-          bool in = sumXVap > 0.f && in_range;
+        if (pending) {
+          float yv[kLearnOut];
 #pragma unroll
           for (int k = 0; k < kLearnOut; ++k) {
-            in = in && isfinite(yv[k]);
+            yv[k] = fmaf(yo[k], L.norm.y_std[k], L.norm.y_mean[k]);
           }
-          if (!in) {
-            const unsigned long long k = atomicAdd(&P.status->fallback, 1ULL);
-            P.fb_list[k] = s;
-            fell_back = true;
-            valid = false;
-            active = false;
-            pending = false;
+          if (cur_iter == 0 && isub == 1) {
+            // gate: some fuel evaporates, inputs inside the (widened)
+            // training range, outputs finite
+            bool in = sumXVap > 0.f && in_range;
+#pragma unroll
+            for (int k = 0; k < kLearnOut; ++k) {
+              in = in && isfinite(yv[k]);
+            }
+            if (!in) {
+              const unsigned long long k = atomicAdd(&P.status->fallback, 1ULL);
+              P.fb_list[k] = s;
+              fell_back = true;
+              valid = false;
+              active = false;
+              pending = false;
+            }
           }
         }
-      }
-      if (pending) {
-        float yv[kLearnOut];
+        if (pending) {
+          float yv[kLearnOut];
 #pragma unroll
-        for (int k = 0; k < kLearnOut; ++k) {
-          yv[k] = fmaf(yo[k], L.norm.y_std[k], L.norm.y_mean[k]);
-        }
-        const float Tp_f = (float)T_part;
-        T_h = Tp_f;
-        const float dia_f = (float)dia_part;
-        float cp_part = 0.f;
-        double Tboil = 0.;
-#pragma unroll
-        for (int spf = 0; spf < NF; ++spf) {
-          Tboil += Y_part[spf] * (double)cBoilT[spf];
-          cp_part += (float)Y_part[spf] * ff.cp[spf];
-        }
-        const float delT = fmaxf(g.T - Tp_f, 0.f);
-        float mi_dot[NF];
-        float m_dot = 0.f, sumL = 0.f;
-        if (sumXVap > 0.f) {
-          // mdot_f = -pi d (rhoD_f Sh*) (X_v,f / sum X_v) ln(1 + B_M), clipped at 0
-          const float coef = (float)PMP_PI * dia_f * flog1p(B_M) * fdiv(1.f, sumXVap);
+          for (int k = 0; k < kLearnOut; ++k) {
+            yv[k] = fmaf(yo[k], L.norm.y_std[k], L.norm.y_mean[k]);
+          }
+          const float Tp_f = (float)T_part;
+          T_h = Tp_f;
+          const float dia_f = (float)dia_part;
+          float cp_part = 0.f;
+          double Tboil = 0.;
 #pragma unroll
           for (int spf = 0; spf < NF; ++spf) {
-            mi_dot[spf] = -fmaxf(fexp(yv[spf < 2 ? spf : 0]) * X_vapor[spf] * coef, 0.f);
-            m_dot += mi_dot[spf];
-            sumL += mi_dot[spf] * L_fuel[spf];
+            Tboil += Y_part[spf] * (double)cBoilT[spf];
+            cp_part += (float)Y_part[spf] * ff.cp[spf];
           }
-        } else {
+          const float delT = fmaxf(g.T - Tp_f, 0.f);
+          float mi_dot[NF];
+          float m_dot = 0.f, sumL = 0.f;
+          if (sumXVap > 0.f) {
+            // mdot_f = -pi d (rhoD_f Sh*) (X_v,f / sum X_v) ln(1 + B_M), clipped at 0
+            const float coef = (float)PMP_PI * dia_f * flog1p(B_M) * fdiv(1.f, sumXVap);
 #pragma unroll
-          for (int spf = 0; spf < NF; ++spf) {
-            mi_dot[spf] = 0.f;
+            for (int spf = 0; spf < NF; ++spf) {
+              mi_dot[spf] = -fmaxf(fexp(yv[spf < 2 ? spf : 0]) * X_vapor[spf] * coef, 0.f);
+              m_dot += mi_dot[spf];
+              sumL += mi_dot[spf] * L_fuel[spf];
+            }
+          } else {
+#pragma unroll
+            for (int spf = 0; spf < NF; ++spf) {
+              mi_dot[spf] = 0.f;
+            }
           }
-        }
-        const float conv_src = (float)PMP_PI * dia_f * delT * fexp(yv[2]);
-        const float mu_skin = fexp(yv[3]);
-        const float rho_skin = fexp(yv[4]);
-        float diff_vel[3];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          diff_vel[d] = g.vel[d] - (float)vel_part[d];
-        }
-        const float diff_vel_mag =
-          sqrtf(diff_vel[0] * diff_vel[0] + diff_vel[1] * diff_vel[1] + diff_vel[2] * diff_vel[2]);
-        const float Reyn = fdiv(rho_skin * diff_vel_mag * dia_f, mu_skin);
-        const float inv_pmass = (float)(1. / pmass);
-        float drag_coef = 0.f;
-        if (Reyn > 1000.f) {
-          drag_coef = 0.424f;
-        } else if (Reyn > 1.f) {
-          drag_coef = fdiv(24.f, Reyn) * (1.f + fcbrt(Reyn * Reyn) * (1.f / 6.f));
-        } else if (Reyn > 0.f) {
-          drag_coef = fdiv(24.f, Reyn);
-        }
-        const float drag_force = 0.125f * rho_skin * drag_coef * (float)PMP_PI * dia_f * dia_f * diff_vel_mag;
-        const float drag_force_p = fdiv(0.75f * rho_skin * drag_coef * diff_vel_mag, dia_f * (float)rho_part);
-        float part_vel_src[3];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          part_vel_src[d] = drag_force_p * diff_vel[d] + ff.body_force[d];
-        }
-        if (fdat.mom_trans) {
+          const float conv_src = (float)PMP_PI * dia_f * delT * fexp(yv[2]);
+          const float mu_skin = fexp(yv[3]);
+          const float rho_skin = fexp(yv[4]);
+          float diff_vel[3];
 #pragma unroll
           for (int d = 0; d < 3; ++d) {
-            mom_acc[d] = fmaf(drag_force, diff_vel[d], mom_acc[d]);
+            diff_vel[d] = g.vel[d] - (float)vel_part[d];
+          }
+          const float diff_vel_mag =
+            sqrtf(diff_vel[0] * diff_vel[0] + diff_vel[1] * diff_vel[1] + diff_vel[2] * diff_vel[2]);
+          const float Reyn = fdiv(rho_skin * diff_vel_mag * dia_f, mu_skin);
+          const float inv_pmass = (float)(1. / pmass);
+          float drag_coef = 0.f;
+          if (Reyn > 1000.f) {
+            drag_coef = 0.424f;
+          } else if (Reyn > 1.f) {
+            drag_coef = fdiv(24.f, Reyn) * (1.f + fcbrt(Reyn * Reyn) * (1.f / 6.f));
+          } else if (Reyn > 0.f) {
+            drag_coef = fdiv(24.f, Reyn);
+          }
+          const float drag_force = 0.125f * rho_skin * drag_coef * (float)PMP_PI * dia_f * dia_f * diff_vel_mag;
+          const float drag_force_p = fdiv(0.75f * rho_skin * drag_coef * diff_vel_mag, dia_f * (float)rho_part);
+          float part_vel_src[3];
+#pragma unroll
+          for (int d = 0; d < 3; ++d) {
+            part_vel_src[d] = drag_force_p * diff_vel[d] + ff.body_force[d];
+          }
+          if (fdat.mom_trans) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+              mom_acc[d] = fmaf(drag_force, diff_vel[d], mom_acc[d]);
+            }
+            if (isub == 1) {
+              nsub = min(max(nsub, static_cast<int>((float)flow_dt * drag_force_p) + 1), 100);
+            }
+          }
+          eng_acc += conv_src;
+          const float part_temp_src = fdiv((sumL + conv_src) * inv_pmass, cp_part);
+          if (isub == 1 && delT > 1e-15f) {
+            const float inv_tau_d = fdiv(-m_dot, 0.2f * (float)pmass);
+            const float inv_tau_T = fdiv(conv_src * inv_pmass, cp_part * delT);
+            nsub = min(max(nsub, max(static_cast<int>((float)flow_dt * inv_tau_d),
+                                     static_cast<int>((float)flow_dt * inv_tau_T)) + 1),
+                       100);
           }
           if (isub == 1) {
-            nsub = min(max(nsub, static_cast<int>((float)flow_dt * drag_force_p) + 1), 100);
+            dt = flow_dt / static_cast<double>(nsub);
           }
-        }
-        eng_acc += conv_src;
-        const float part_temp_src = fdiv((sumL + conv_src) * inv_pmass, cp_part);
-        if (isub == 1 && delT > 1e-15f) {
-          const float inv_tau_d = fdiv(-m_dot, 0.2f * (float)pmass);
-          const float inv_tau_T = fdiv(conv_src * inv_pmass, cp_part * delT);
-          nsub = min(max(nsub, max(static_cast<int>((float)flow_dt * inv_tau_d),
-                                   static_cast<int>((float)flow_dt * inv_tau_T)) + 1),
-                     100);
-        }
-        if (isub == 1) {
-          dt = flow_dt / static_cast<double>(nsub);
-        }
-        const double part_dt = fdat.dtmod * dt;
-        if (!fdat.fixed_parts) {
+          const double part_dt = fdat.dtmod * dt;
+          if (!fdat.fixed_parts) {
 #pragma unroll
-          for (int d = 0; d < 3; ++d) {
-            vel_part[d] += part_dt * (double)part_vel_src[d];
+            for (int d = 0; d < 3; ++d) {
+              vel_part[d] += part_dt * (double)part_vel_src[d];
+            }
           }
-        }
-        const double newT = T_part + part_dt * (double)part_temp_src;
-        const double new_mass = pmass + (double)m_dot * part_dt;
-        if (new_mass > 1.E-13 * kMassConv && newT < Tboil) {
-          T_part = newT;
-          if (NF > 1) {
-            rho_part = 0.;
-            double sumY = 0.;
+          const double newT = T_part + part_dt * (double)part_temp_src;
+          const double new_mass = pmass + (double)m_dot * part_dt;
+          if (new_mass > 1.E-13 * kMassConv && newT < Tboil) {
+            T_part = newT;
+            if (NF > 1) {
+              rho_part = 0.;
+              double sumY = 0.;
 #pragma unroll
-            for (int spf = 0; spf < NF; ++spf) {
-              Y_part[spf] = dmin(1., dmax(0., (Y_part[spf] * pmass + (double)mi_dot[spf] * part_dt) / new_mass));
-              if (Y_part[spf] <= 1.E-12) {
-                Y_part[spf] = 0.;
+              for (int spf = 0; spf < NF; ++spf) {
+                Y_part[spf] = dmin(1., dmax(0., (Y_part[spf] * pmass + (double)mi_dot[spf] * part_dt) / new_mass));
+                if (Y_part[spf] <= 1.E-12) {
+                  Y_part[spf] = 0.;
+                }
+                sumY += Y_part[spf];
               }
-              sumY += Y_part[spf];
-            }
 #pragma unroll
-            for (int spf = 0; spf < NF; ++spf) {
-              Y_part[spf] /= sumY;
-              rho_part += Y_part[spf] / rhoL(fdat, dmin(T_part, (double)cBoilT[spf]), spf);
+              for (int spf = 0; spf < NF; ++spf) {
+                Y_part[spf] /= sumY;
+                rho_part += Y_part[spf] / rhoL(fdat, dmin(T_part, (double)cBoilT[spf]), spf);
+              }
+              rho_part = 1. / rho_part;
+            } else {
+              rho_part = rhoL(fdat, dmin(T_part, (double)cBoilT[0]), 0);
             }
-            rho_part = 1. / rho_part;
+            pmass = new_mass;
+            dia_part = dcbrt_from_f(6. * pmass / (PMP_PI * rho_part));
           } else {
-            rho_part = rhoL(fdat, dmin(T_part, (double)cBoilT[0]), 0);
+            pmass = 0.;
+            id = -1;
+            nsub = isub;
+            isub = nsub + 1;
           }
-          pmass = new_mass;
-          dia_part = dcbrt_from_f(6. * pmass / (PMP_PI * rho_part));
-        } else {
-          pmass = 0.;
-          id = -1;
-          nsub = isub;
-          isub = nsub + 1;
+          ++isub;
+          pending = isub <= nsub;
         }
-        ++isub;
-        pending = isub <= nsub;
       }
-    }
-    // back from shared memory (volatile: read there, not kept in registers
-    // across the sub-steps), and the cell the position gives
-    const volatile double* vx = sx;
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      pos[d] = vx[d * BLOCK];
-    }
-    num_ppp = vx[3 * BLOCK];
-    const double startmass = vx[4 * BLOCK];
-#pragma unroll
-    for (int spf = 0; spf < NF; ++spf) {
-      Y[spf] = vx[(5 + spf) * BLOCK];
-    }
-    cell_of(P, pos, lx, ijk, ijkc);
-    if (fell_back) {
-      continue;
-    }
-    if (active) {
-      src.eng = num_ppp * (double)eng_acc;
+      // back from shared memory (volatile: read there, not kept in registers
+      // across the sub-steps), and the cell the position gives
+      const volatile double* vx = sx;
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
-        src.mom[d] = num_ppp * (double)mom_acc[d];
+        pos[d] = vx[d * BLOCK];
       }
-      if (nsub > 1) {
-        src.eng /= static_cast<double>(nsub);
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          src.mom[d] /= static_cast<double>(nsub);
-        }
-      }
-      const double inv_dtf = 1. / (fdat.dtmod * flow_dt);
-      const double mdot_total = (pmass - startmass) * inv_dtf;
-      src.mass = num_ppp * mdot_total;
-      if (fdat.mom_trans) {
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          src.mom[d] += num_ppp * vel_part[d] * mdot_total;
-        }
-      }
+      num_ppp = vx[3 * BLOCK];
+      const double startmass = vx[4 * BLOCK];
 #pragma unroll
       for (int spf = 0; spf < NF; ++spf) {
-        const double midot = (Y_part[spf] * pmass - Y[spf] * startmass) * inv_dtf;
-        src.Ydot[spf] = num_ppp * midot;
-        src.eng += num_ppp * midot * (double)hf(m, dep_sp<FF>(fdat, spf), T_h);
-        Y[spf] = Y_part[spf];
+        Y[spf] = vx[(5 + spf) * BLOCK];
       }
+      cell_of(P, pos, lx, ijk, ijkc);
+      if (fell_back) {
+        continue;
+      }
+      if (active) {
+        src.eng = num_ppp * (double)eng_acc;
 #pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        vel[d] = vel_part[d];
-      }
-      T = T_part;
-      dia = dia_part;
-      c.sub += 1;
-      c.inner += static_cast<unsigned>(nsub);
-      // deposit into the cell holding the droplet (SprayParticles.cpp:419-441)
-      const double cur_coef = __dmul_rn(-P.inv_vol, P.sub_dt) / P.flow_dt;
-      bool src_ok = in_box(B.src_lo, B.src_hi, ijkc[0], ijkc[1], ijkc[2]) ||
-                    (P.is_ghost && in_box(B.sr_alo, B.sr_ahi, ijkc[0], ijkc[1], ijkc[2]));
-      if (!src_ok) {
-        set_error(P, PMP_ERR_SOURCE_BOX, b, s);
-        ok = false;
-      } else {
-        double* q = B.sr + ((ijkc[0] - B.sr_lo[0]) + (ijkc[1] - B.sr_lo[1]) * B.sr_j32 + (ijkc[2] - B.sr_lo[2]) * B.sr_k32);
+        for (int d = 0; d < 3; ++d) {
+          src.mom[d] = num_ppp * (double)mom_acc[d];
+        }
+        if (nsub > 1) {
+          src.eng /= static_cast<double>(nsub);
+#pragma unroll
+          for (int d = 0; d < 3; ++d) {
+            src.mom[d] /= static_cast<double>(nsub);
+          }
+        }
+        const double inv_dtf = 1. / (fdat.dtmod * flow_dt);
+        const double mdot_total = (pmass - startmass) * inv_dtf;
+        src.mass = num_ppp * mdot_total;
         if (fdat.mom_trans) {
 #pragma unroll
-          for (int dir = 0; dir < 3; ++dir) {
-            red_add(q + (P.s_mom + dir) * B.sr_n32, cur_coef * src.mom[dir]);
+          for (int d = 0; d < 3; ++d) {
+            src.mom[d] += num_ppp * vel_part[d] * mdot_total;
           }
         }
-        red_add(q + P.s_rho * B.sr_n32, cur_coef * src.mass);
 #pragma unroll
         for (int spf = 0; spf < NF; ++spf) {
-          red_add(q + (P.s_spec + spf) * B.sr_n32, cur_coef * src.Ydot[spf]);
+          const double midot = (Y_part[spf] * pmass - Y[spf] * startmass) * inv_dtf;
+          src.Ydot[spf] = num_ppp * midot;
+          src.eng += num_ppp * midot * (double)hf(m, dep_sp<FF>(fdat, spf), T_h);
+          Y[spf] = Y_part[spf];
         }
-        red_add(q + P.s_eng * B.sr_n32, cur_coef * src.eng);
-        if (P.do_move && !fdat.fixed_parts && id > 0) {
 #pragma unroll
-          for (int dir = 0; dir < 3; ++dir) {
-            pos[dir] = __dadd_rn(pos[dir], __dmul_rn(P.sub_dt, vel[dir]));
-          }
-          if (B.at_bounds) {
-            if (check_bounds(P, pos, bflags)) {
-              id = -1;
-            } else {
-              impose_wall(P, pos, vel, bflags);
+        for (int d = 0; d < 3; ++d) {
+          vel[d] = vel_part[d];
+        }
+        T = T_part;
+        dia = dia_part;
+        c.sub += 1;
+        c.inner += static_cast<unsigned>(nsub);
+        // deposit into the cell holding the droplet (SprayParticles.cpp:419-441)
+        const double cur_coef = __dmul_rn(-P.inv_vol, P.sub_dt) / P.flow_dt;
+        bool src_ok = in_box(B.src_lo, B.src_hi, ijkc[0], ijkc[1], ijkc[2]) ||
+                      (P.is_ghost && in_box(B.sr_alo, B.sr_ahi, ijkc[0], ijkc[1], ijkc[2]));
+        if (!src_ok) {
+          set_error(P, PMP_ERR_SOURCE_BOX, b, s);
+          ok = false;
+        } else {
+          double* q = B.sr + ((ijkc[0] - B.sr_lo[0]) + (ijkc[1] - B.sr_lo[1]) * B.sr_j32 + (ijkc[2] - B.sr_lo[2]) * B.sr_k32);
+          if (fdat.mom_trans) {
+#pragma unroll
+            for (int dir = 0; dir < 3; ++dir) {
+              red_add(q + (P.s_mom + dir) * B.sr_n32, cur_coef * src.mom[dir]);
             }
           }
-          cell_of(P, pos, lx, ijk, ijkc);
-        }
-        if (P.is_ghost && !in_box(B.src_lo, B.src_hi, ijkc[0], ijkc[1], ijkc[2])) {
-          id = -1;
+          red_add(q + P.s_rho * B.sr_n32, cur_coef * src.mass);
+#pragma unroll
+          for (int spf = 0; spf < NF; ++spf) {
+            red_add(q + (P.s_spec + spf) * B.sr_n32, cur_coef * src.Ydot[spf]);
+          }
+          red_add(q + P.s_eng * B.sr_n32, cur_coef * src.eng);
+          if (P.do_move && !fdat.fixed_parts && id > 0) {
+#pragma unroll
+            for (int dir = 0; dir < 3; ++dir) {
+              pos[dir] = __dadd_rn(pos[dir], __dmul_rn(P.sub_dt, vel[dir]));
+            }
+            if (B.at_bounds) {
+              if (check_bounds(P, pos, bflags)) {
+                id = -1;
+              } else {
+                impose_wall(P, pos, vel, bflags);
+              }
+            }
+            cell_of(P, pos, lx, ijk, ijkc);
+          }
+          if (P.is_ghost && !in_box(B.src_lo, B.src_hi, ijkc[0], ijkc[1], ijkc[2])) {
+            id = -1;
+          }
         }
       }
     }
-  }
-  if (valid && ok) {
-    if (P.do_move) {
+    if (valid && ok) {
+      if (P.do_move) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          P.parts.pos[d][s] = pos[d];
+        }
+      }
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
-        P.parts.pos[d][s] = pos[d];
+        P.parts.rd[PMP_PSTATE_VEL + d][s] = vel[d];
+      }
+      P.parts.rd[PMP_PSTATE_T][s] = T;
+      P.parts.rd[PMP_PSTATE_DIA][s] = dia;
+#pragma unroll
+      for (int f = 0; f < NF; ++f) {
+        P.parts.rd[PMP_PSTATE_Y + f][s] = Y[f];
+      }
+      if (id <= 0) {
+        P.parts.id[s] = id;
+        c.killed += 1;
       }
     }
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      P.parts.rd[PMP_PSTATE_VEL + d][s] = vel[d];
-    }
-    P.parts.rd[PMP_PSTATE_T][s] = T;
-    P.parts.rd[PMP_PSTATE_DIA][s] = dia;
-#pragma unroll
-    for (int f = 0; f < NF; ++f) {
-      P.parts.rd[PMP_PSTATE_Y + f][s] = Y[f];
-    }
-    if (id <= 0) {
-      P.parts.id[s] = id;
-      c.killed += 1;
-    }
-  }
   }  // items
   if (!weights_in) {
     tc::mbar_wait(wbar, 0);  // no network evaluation waited for the weight copy: it must land before the exit
