@@ -312,9 +312,9 @@ const char* pmp_spray_version(void);
 
 /* Allocation-free update.  No counterpart in the reference: PeleMP relies on
  * AMReX allocating as it goes.  For hosts that cannot call cudaMalloc when the
- * update runs -- every byte of device memory already handed to their own
- * pre-sized pool, or work being issued into a CUDA stream capture, where
- * allocation is not allowed.  The caller passes everything: the gas species
+ * update runs: every byte of device memory is already handed to their own
+ * pre-sized pool (an arena sized at start-up), or their solver forbids device
+ * allocations after initialisation.  The caller passes everything: the gas species
  * (cfg; cfg->device is ignored, the current device is used), a built SprayData,
  * the component indices, geometry and boxes, the droplets of each box as
  * DEVICE SoA arrays (updated in place, caller's order, not sorted), and

@@ -2,9 +2,9 @@
 // device allocation at all.
 //
 // Who needs it: hosts that hand every byte of device memory to their own
-// pre-sized pool (an AMReX arena sized at start-up, a solver that forbids
-// allocations after initialisation) and code that issues work while a CUDA
-// stream is being captured, where cudaMalloc/cudaFree are not allowed.  Such
+// pre-sized pool (an AMReX arena sized at start-up) or run a solver that
+// forbids device allocations after initialisation, so that a cudaMalloc
+// during the step would fail or is not allowed.  Such
 // callers own the droplet arrays and the mesh views; this entry point runs
 // the update on them in place and keeps its own working data (the per-box
 // table, the CTA-to-box prefix and the status/counter block) in one

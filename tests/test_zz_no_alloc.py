@@ -1,7 +1,7 @@
 """pmp_spray_update_static: the update for callers that cannot allocate device
 memory while it runs (their device memory is all in their own pre-sized pool,
-or they issue the update inside a CUDA stream capture, where cudaMalloc is
-not allowed).  The entry point takes the caller's own device arrays and keeps
+or their solver forbids device allocations after initialisation).  The entry
+point takes the caller's own device arrays and keeps
 its working data in a fixed array inside the library.
 
 Checked here through the C ABI against pmp_spray_update on the same inputs,
