@@ -138,96 +138,110 @@ def dist_setup():
     return world, rank, local
 
 
-def run_reference(args, world, rank):
-    """PeleMP's spray physics (oracle/_ref) on the host cores, bounded sample."""
-    if rank != 0:
-        return None
-    from pelemp_b200 import workloads as W
+def _reference_lib(nspec, nfuel):
+    """The reference's CPU path (oracle/_ref, PeleMP's spray physics headers
+    compiled from the reference sources) or, without it, the C oracle."""
     from oracle.pyoracle import Oracle, Reference
+    if Reference.available(nspec, nfuel):
+        return Reference(nspec, nfuel), "reference", (
+            "PeleMP Drag.H/SprayFuelData.H/SprayInterpolation.H/WallFunctions.H compiled from the "
+            "reference sources (oracle/_ref), project thermo/transport, OpenMP over droplets with "
+            "atomic deposits")
+    return Oracle(libm=True), "port", "CPU oracle (C restatement of the reference path, C library math), OpenMP"
 
+
+def cpu_sample_size(seconds):
+    """Droplets of the config-2 workload whose MKD+MK step takes about `seconds`
+    of the reference's CPU path on this host (all cores), at most 4M."""
+    from pelemp_b200 import workloads as W
+    from oracle.pyoracle import Oracle
     cores = os.cpu_count() or 1
-    prob = W.config2(n=args.cpu_sample, steps=1)
-    kind = "reference"
-    if Reference.available(prob.nspec, prob.nfuel):
-        lib = Reference(prob.nspec, prob.nfuel)
-        desc = ("PeleMP Drag.H/SprayFuelData.H/SprayInterpolation.H/WallFunctions.H compiled "
-                "from the reference sources (oracle/_ref), project thermo/transport, OpenMP "
-                "over droplets with atomic deposits")
-    else:
-        lib = Oracle(libm=True)
-        kind = "port"
-        desc = "CPU oracle (C restatement of the reference path, C library math), OpenMP"
+    probe = W.config2(n=20_000, steps=1)
+    lib, _, _ = _reference_lib(probe.nspec, probe.nfuel)
+    orc = Oracle(libm=True)
+    mech = orc.mech(probe.species)
+    _, fdat = orc.setup(probe, mech)
+    src = probe.new_sources()
+    parts = probe.copy_parts()
+    t0 = time.perf_counter()
+    for do_move in (1, 0):
+        for a in src:
+            a.fill(0.0)
+        rc, err, _ = lib.update(probe, mech, fdat, parts, src, do_move, nthreads=cores)
+        assert rc == 0, err.message
+    dt = time.perf_counter() - t0
+    return int(min(4_000_000, max(20_000, 20_000 * seconds / max(dt, 1e-3))))
+
+
+def time_reference_steps(n, steps, warmup):
+    """The reference's CPU path on n droplets of the config-2 workload: warmup
+    + steps MKD+MK steps from the same initial droplets, the source arrays
+    allocated (and faulted in) before the timed region and zeroed inside it,
+    as the GPU step zeroes its sources.  Returns (substeps/s, seconds per
+    timed step, cores, kind, description)."""
+    from pelemp_b200 import workloads as W
+    from oracle.pyoracle import Oracle
+    cores = os.cpu_count() or 1
+    prob = W.config2(n=n, steps=1)
+    lib, kind, desc = _reference_lib(prob.nspec, prob.nfuel)
     orc = Oracle(libm=True)
     mech = orc.mech(prob.species)
     _, fdat = orc.setup(prob, mech)
-    total_sub = 0
-    t_total = 0.0
-    for step in range(args.warmup + args.steps):
+    src = prob.new_sources()
+    for a in src:
+        a.fill(1.0)  # fault the pages in outside the timed region
+    total_sub, t_total = 0, 0.0
+    for step in range(warmup + steps):
         parts = prob.copy_parts()
         t0 = time.perf_counter()
         nsub = 0
         for do_move in (1, 0):
-            src = prob.new_sources()
+            for a in src:
+                a.fill(0.0)
             rc, err, ns = lib.update(prob, mech, fdat, parts, src, do_move, nthreads=cores)
             assert rc == 0, err.message
             nsub += ns
         dt = time.perf_counter() - t0
-        if step >= args.warmup:
+        if step >= warmup:
             total_sub += nsub
             t_total += dt
-    value = total_sub / t_total
+    return total_sub / t_total, t_total / max(steps, 1), cores, kind, desc
+
+
+def run_reference(args, world, rank):
+    """PeleMP's spray physics (oracle/_ref) on the host cores, bounded sample."""
+    if rank != 0:
+        return None
+    n = args.cpu_sample or cpu_sample_size(args.cpu_seconds)
+    value, s_per_step, cores, kind, desc = time_reference_steps(n, args.steps, args.warmup)
     line = {
         "metric": "droplet-substeps/s", "value": value, "unit": "droplet-substeps/s",
         "impl": "reference", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * t_total / args.steps, "higher_is_better": True,
+        "ms_per_step": 1e3 * s_per_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded config-2 sample)",
         "config": {"workload": "config2 sample: two-fuel droplets on 128^3 (8 boxes of 64^3), "
                                "5 species, dt=5e-7 s, MKD (4 sub-cycles) + MK",
-                   "droplets_per_step": args.cpu_sample},
+                   "droplets_per_step": n},
         "cpu_baseline": {"value": value, "unit": "droplet-substeps/s", "cores": cores,
                          "kind": kind,
-                         "sample": f"{args.cpu_sample} droplets of the 16M workload per step; {desc}"},
+                         "sample": f"{n} droplets of the 16M config-2 workload per step "
+                                   f"(the same sample size as the GPU arm's cpu_baseline), "
+                                   f"{args.warmup} + {args.steps} steps; {desc}"},
         "e2e": {"value": value, "unit": "droplet-substeps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
     return line
 
 
-def cpu_baseline(seconds=12.0):
-    """The reference's CPU path on a bounded sample, for rank 0 at N=1."""
-    from pelemp_b200 import workloads as W
-    from oracle.pyoracle import Oracle, Reference
-
-    cores = os.cpu_count() or 1
-    orc = Oracle(libm=True)
-    probe = W.config2(n=20_000, steps=1)
-    have_ref = Reference.available(probe.nspec, probe.nfuel)
-    lib = Reference(probe.nspec, probe.nfuel) if have_ref else orc
-    mech = orc.mech(probe.species)
-    _, fdat = orc.setup(probe, mech)
-
-    def one(prob):
-        parts = prob.copy_parts()
-        t0 = time.perf_counter()
-        nsub = 0
-        for do_move in (1, 0):
-            rc, err, ns = lib.update(prob, mech, fdat, parts, prob.new_sources(), do_move,
-                                     nthreads=cores)
-            assert rc == 0, err.message
-            nsub += ns
-        return nsub, time.perf_counter() - t0
-
-    ns, dt = one(probe)
-    n = int(min(4_000_000, max(20_000, 20_000 * seconds / max(dt, 1e-3))))
-    prob = W.config2(n=n, steps=1)
-    ns, dt = one(prob)
-    return {"value": ns / dt, "unit": "droplet-substeps/s", "cores": cores,
-            "kind": "reference" if have_ref else "port",
-            "sample": (f"{n} droplets of the config-2 workload, one MKD+MK step ({ns} droplet-substeps, "
-                       f"{dt:.1f} s); " + ("PeleMP's spray physics headers compiled from the reference "
-                                           "sources (oracle/_ref), OpenMP over droplets"
-                                           if have_ref else "CPU oracle, OpenMP"))}
+def cpu_baseline(args):
+    """The reference's CPU path on a bounded sample, for rank 0 at N=1: one
+    MKD+MK step (after one untimed step) of the sample the reference arm uses."""
+    n = args.cpu_sample or cpu_sample_size(args.cpu_seconds)
+    value, s_per_step, cores, kind, desc = time_reference_steps(n, 1, 1)
+    return {"value": value, "unit": "droplet-substeps/s", "cores": cores, "kind": kind,
+            "sample": (f"{n} droplets of the config-2 workload, one timed MKD+MK step "
+                       f"({s_per_step:.1f} s) after one untimed; {desc}")}
 
 
 WORKLOAD_TEXT = {
@@ -251,7 +265,7 @@ FORM_NAME = {"fp64": "plain FP64", "mixed": "mixed FP32 physics / FP64 state and
 KERNEL = {"fp64": "spray_update_fp64<5,2,128>", "mixed": "spray_update_mixed<5,2,128,fuel_first>",
           "learned": "spray_update_learned<5,2,128,fuel_first>"}
 # DRAM bytes per droplet of one config-2 MKD launch, measured by ncu on a
-# 2M-droplet launch (profiles/update_kernels_config2_2M.md): dram read + write
+# 2M-droplet launch of the same kernel (one-launch capture): dram read + write
 # minus the mesh's algorithmic bytes (state read once, source read-modify-
 # write), divided by the droplets.  The droplet part grows with the droplet
 # count, the mesh part does not, so a full launch's traffic is estimated as
@@ -309,26 +323,38 @@ def bench_batched(args, world, rank, local, pg):
     src = [torch.zeros(s.shape, dtype=torch.float64, device="cuda") for s in prob.new_sources()]
     src_v = views(src, [prob.grown(b, prob.source_ghosts)[0] for b in range(nboxes)])
 
-    def timed(sp, steps):
-        def step():
-            for s in src:
-                s.zero_()
-            n = 0
-            for do_move in (1, 0):
-                sp.update_particles(st_v, src_v, prob.flow_dt, 0.0, prob.state_ghosts, prob.source_ghosts,
-                                    0, 0, do_move, prob.spray_cfl_lev, stream.cuda_stream)
-                n += sp.stats().substeps
-            return n
+    def step(sp, st_handle):
+        for s in src:
+            s.zero_()
+        for do_move in (1, 0):
+            sp.update_particles(st_v, src_v, prob.flow_dt, 0.0, prob.state_ghosts, prob.source_ghosts,
+                                0, 0, do_move, prob.spray_cfl_lev, st_handle, sync=False)
+
+    def timed(sp, steps, whole_graph=False):
+        """Eager steps, or replays of one CUDA graph of a whole step; returns
+        (droplet-substeps/s, ms per step)."""
         for _ in range(args.warmup):
-            step()
+            step(sp, stream.cuda_stream)
+        sp.sync()
+        run = lambda: step(sp, stream.cuda_stream)  # noqa: E731
+        g = None
+        if whole_graph:
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                step(sp, torch.cuda.current_stream().cuda_stream)
+            run = g.replay
         if pg:
             pg.barrier()
         torch.cuda.synchronize()
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ev0.record(stream)
-        n = sum(step() for _ in range(steps))
+        for _ in range(steps):
+            run()
         ev1.record(stream)
         torch.cuda.synchronize()
+        sp.sync()
+        n = sp.stats().substeps
+        del g
         t, n = reduce_over_ranks(pg, ev0.elapsed_time(ev1), n)
         return n / (t * 1e-3), t / steps
 
@@ -338,15 +364,27 @@ def bench_batched(args, world, rank, local, pg):
     v_default, ms_default = timed(sp, args.steps)
     sp.close()
     sp = from_problem(prob, device=local)
+    v_default_g, ms_default_g = timed(sp, args.steps, whole_graph=True)
+    sp.close()
+    sp = from_problem(prob, device=local)
     rep = sp.autotune(st_v, src_v, prob.flow_dt, prob.state_ghosts, prob.source_ghosts, 0, 1,
                       prob.spray_cfl_lev, stream=stream.cuda_stream)
     best = rep.best
+    sp.close()
+    # the tuned shape, each call replaying the library's graph of its device work
+    sp = from_problem(prob, device=local)
     sp.set_launch(kind=best.kind, block=best.block, regs=best.regs, chunk=best.chunk,
                   ctas_per_sm=best.ctas_per_sm, use_graph=True)
+    v_call_g, ms_call_g = timed(sp, args.steps)
+    sp.close()
+    # the tuned shape inside one CUDA graph of the whole step (the headline)
+    sp = from_problem(prob, device=local)
+    sp.set_launch(kind=best.kind, block=best.block, regs=best.regs, chunk=best.chunk,
+                  ctas_per_sm=best.ctas_per_sm, use_graph=False)
     sampler = ClockSampler(local)
     sampler.start()
     time.sleep(0.3)
-    v_tuned, ms_tuned = timed(sp, args.steps)
+    v_tuned, ms_tuned = timed(sp, args.steps, whole_graph=True)
     clocks = sampler.stop()
     sp.close()
     sp = from_problem(prob, device=local)
@@ -363,12 +401,20 @@ def bench_batched(args, world, rank, local, pg):
                        "largest_box": int(max(prob.meta["counts"])), "smallest_box": int(min(prob.meta["counts"])),
                        "parallelism": f"replicas x{world}"},
             "launches": {
-                "autotuned_graph": {"value": v_tuned, "ms_per_step": ms_tuned,
-                                    "shape": {"kind": best.kind, "block": best.block, "regs": best.regs,
-                                              "chunk": best.chunk},
-                                    "tuner": {"candidates": rep.ncandidates, "best_ms": rep.best_ms,
-                                              "default_ms": rep.default_ms, "per_box_ms": rep.per_box_ms}},
-                "default_one_launch": {"value": v_default, "ms_per_step": ms_default},
+                "autotuned_step_graph": {"value": v_tuned, "ms_per_step": ms_tuned,
+                                         "what": "tuned shape, one CUDA graph of the whole step replayed",
+                                         "shape": {"kind": best.kind, "block": best.block, "regs": best.regs,
+                                                   "chunk": best.chunk},
+                                         "tuner": {"candidates": rep.ncandidates, "best_ms": rep.best_ms,
+                                                   "default_ms": rep.default_ms,
+                                                   "per_box_ms": rep.per_box_ms}},
+                "autotuned_call_graphs": {"value": v_call_g, "ms_per_step": ms_call_g,
+                                          "what": "tuned shape, eager steps, each call replaying the "
+                                                  "library's graph of its device work"},
+                "default_one_launch": {"value": v_default, "ms_per_step": ms_default,
+                                       "what": "default shape, eager steps"},
+                "default_step_graph": {"value": v_default_g, "ms_per_step": ms_default_g,
+                                       "what": "default shape, one CUDA graph of the whole step"},
                 "per_box_baseline": {"value": v_box, "ms_per_step": ms_box,
                                      "what": "one launch per box, stream synchronised after each "
                                              "(SprayParticles.cpp:244-248,499)"},
@@ -395,7 +441,12 @@ def main():
                     help="config2 (default): the headline; config3: batched FP64 launch shapes; "
                          "config4 / config5: config-1 distributions at 32M / 16M droplets")
     ap.add_argument("--e2e-steps", type=int, default=6)
-    ap.add_argument("--cpu-sample", type=int, default=100_000)
+    ap.add_argument("--cpu-sample", type=int, default=0,
+                    help="droplets per CPU step (0: sized for --cpu-seconds per step)")
+    ap.add_argument("--cpu-seconds", type=float, default=8.0)
+    ap.add_argument("--no-graph", action="store_true",
+                    help="time eager steps only (default: the timed steps replay one CUDA graph of a "
+                         "whole step -- source zeroing, MKD and MK -- and eager steps are timed beside)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--forms", default="fp64,mixed,learned",
@@ -440,18 +491,35 @@ def main():
     src = [torch.zeros(s.shape, dtype=torch.float64, device="cuda") for s in prob.new_sources()]
     src_v = views(src, [prob.grown(b, prob.source_ghosts)[0] for b in range(nboxes)])
     peak, peak_src = measured_peaks()
+    graphs = {}
 
-    def step(sp):
+    def step(sp, st_handle):
+        """One step, stream-ordered: zero the sources, MKD, MK (no host wait)."""
         for s in src:
             s.zero_()
-        out = []
         for do_move in (1, 0):
             sp.update_particles(st_v, src_v, prob.flow_dt, 0.0, prob.state_ghosts,
                                 prob.source_ghosts, 0, 0, do_move, prob.spray_cfl_lev,
-                                stream.cuda_stream)
-            s_ = sp.stats()
-            out.append((s_.substeps, s_.kernel_ms, s_.fallback))
-        return out
+                                st_handle, sync=False)
+
+    def timed_steps(sp, run, steps):
+        """Device time of `steps` calls of run() on the stream, max over ranks,
+        and the droplet-substeps and fallback count they executed."""
+        sp.sync()  # clears the accumulated counters
+        if pg:
+            pg.barrier()
+        torch.cuda.synchronize()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(steps):
+            run()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        sp.sync()
+        st_ = sp.stats()
+        t_max, sub_total = reduce_over_ranks(pg, ev0.elapsed_time(ev1), st_.substeps)
+        return t_max, sub_total, st_.substeps, st_.fallback
 
     results = {}
     containers = {}
@@ -464,32 +532,43 @@ def main():
             info["train"] = {"seconds": t_train, "tuples": rep.tuples, "adam_steps": rep.steps,
                              "val_rel_rms": list(rep.val_rel_rms), "epochs": args.learn_epochs,
                              "sample_stride": args.learn_stride}
-        for _ in range(args.warmup):
-            step(sp)
+        # warm-up steps; the MKD call of each is waited for, for its kernel time
+        # (the library's events around the call's kernels: the roofline's launch)
+        mkd_ms = []
+        for w in range(args.warmup):
+            for s_ in src:
+                s_.zero_()
+            for do_move in (1, 0):
+                sp.update_particles(st_v, src_v, prob.flow_dt, 0.0, prob.state_ghosts,
+                                    prob.source_ghosts, 0, 0, do_move, prob.spray_cfl_lev,
+                                    stream.cuda_stream, sync=True)
+                if do_move and w > 0:
+                    mkd_ms.append(sp.stats().kernel_ms)
+        # eager steps (a launch per kernel, the host never waits inside)
+        t_eager, _, _, _ = timed_steps(sp, lambda: step(sp, stream.cuda_stream), args.steps)
+        graph = None
         sampler = ClockSampler(local)
-        if pg:
-            pg.barrier()
-        torch.cuda.synchronize()
-        sampler.start()
-        time.sleep(0.3)
-        ev0 = torch.cuda.Event(enable_timing=True)
-        ev1 = torch.cuda.Event(enable_timing=True)
-        ev0.record(stream)
-        substeps, fallback, mkd_ms = 0, 0, []
-        for _ in range(args.steps):
-            rec = step(sp)
-            substeps += rec[0][0] + rec[1][0]
-            fallback += rec[0][2] + rec[1][2]
-            mkd_ms.append(rec[0][1])
-        ev1.record(stream)
-        torch.cuda.synchronize()
-        if pg:
-            pg.barrier()
+        if not args.no_graph:
+            # one CUDA graph of a whole step, captured on torch's capture
+            # stream (the library's calls are capturable once run outside)
+            graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(graph):
+                step(sp, torch.cuda.current_stream().cuda_stream)
+            sampler.start()
+            time.sleep(0.3)
+            t_max, sub_total, sub_local, fb = timed_steps(sp, graph.replay, args.steps)
+        else:
+            sampler.start()
+            time.sleep(0.3)
+            t_max, sub_total, sub_local, fb = timed_steps(sp, lambda: step(sp, stream.cuda_stream),
+                                                          args.steps)
         c = sampler.stop()
-        t_max, sub_total = reduce_over_ranks(pg, ev0.elapsed_time(ev1), substeps)
+        graphs[form] = graph
         info.update({"value": sub_total / (t_max * 1e-3), "ms_per_step": t_max / args.steps,
+                     "ms_per_step_eager": t_eager / args.steps,
+                     "timed": "whole-step CUDA graph replays" if graph is not None else "eager steps",
                      "mkd_launch_ms": float(np.mean(mkd_ms)), "substeps": sub_total,
-                     "fallback_frac": fallback / max(substeps, 1), "clocks": c})
+                     "fallback_frac": fb / max(sub_local, 1), "clocks": c})
         results[form] = info
 
     fast = [f for f in forms if f != "fp64"]
@@ -505,7 +584,7 @@ def main():
         ref = [containers["fp64"].get_particles(0)]
         for f in fast:
             accuracy[f] = droplet_errors([containers[f].get_particles(0)], ref, prob)
-        accuracy["steps"] = args.warmup + args.steps
+        accuracy["steps"] = args.warmup + args.steps * (1 if args.no_graph else 2)
 
     # roofline of the headline form's MKD launch (algorithmic bytes / launch time)
     mkd_bytes = algorithmic_bytes(prob.n_droplets, prob.nfuel, prob.nspec, ncells, True)
@@ -534,15 +613,13 @@ def main():
         # steps (zeroing them is the caller's host work, and the droplets do
         # not read them); every call still copies them in and back
         def host_step():
-            n = 0
             for do_move in (1, 0):
                 sp.update_particles_host(st_hv, src_hv, prob.flow_dt, 0.0, prob.state_ghosts,
                                          prob.source_ghosts, 0, 0, do_move, prob.spray_cfl_lev,
-                                         stream.cuda_stream)
-                n += sp.stats().substeps
-            return n
+                                         stream.cuda_stream, sync=False)
 
         host_step()
+        sp.sync()
         if pg:
             pg.barrier()
         torch.cuda.synchronize()
@@ -550,28 +627,30 @@ def main():
         e_ev0 = torch.cuda.Event(enable_timing=True)
         e_ev1 = torch.cuda.Event(enable_timing=True)
         e_ev0.record(stream)
-        ns = 0
         for _ in range(args.e2e_steps):
-            ns += host_step()
+            host_step()
         e_ev1.record(stream)
         torch.cuda.synchronize()
         te = max(e_ev0.elapsed_time(e_ev1), 1e3 * (time.perf_counter() - t0))
-        te, ns = reduce_over_ranks(pg, te, ns)
+        sp.sync()
+        te, ns = reduce_over_ranks(pg, te, sp.stats().substeps)
         e2e = {"value": ns / (te * 1e-3), "unit": "droplet-substeps/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                "steps": args.e2e_steps, "form": head,
                "path": "pmp_spray_update_host: pinned host state/source, H2D+D2H inside, "
-                       "copies overlapped with the update in box groups"}
+                       "copies overlapped with the update in box groups, calls stream-ordered "
+                       "(the host waits once, after the last step)"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_baseline()
+        cpu = cpu_baseline(args)
 
     if rank == 0:
         forms_out = {}
         for f in forms:
             r = results[f]
             forms_out[f] = {"value": r["value"], "ms_per_step": r["ms_per_step"],
+                            "ms_per_step_eager": r["ms_per_step_eager"], "timed": r["timed"],
                             "mkd_launch_ms": r["mkd_launch_ms"], "fallback_frac": r["fallback_frac"],
                             "speedup_vs_fp64": (r["value"] / results["fp64"]["value"]
                                                 if "fp64" in results else None)}
@@ -596,8 +675,8 @@ def main():
             "forms": forms_out,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
-                         "traffic_source": "ncu dram bytes of a 2M-droplet MKD launch scaled by droplet "
-                                           "count (mesh part fixed); profiles/update_kernels_config2_2M.md"
+                         "traffic_source": "ncu dram bytes of a 2M-droplet MKD launch of the same kernel "
+                                           "scaled by droplet count (mesh part fixed)"
                          if traffic else None,
                          "kernel": KERNEL[head] + " (MKD launch)",
                          "launch_ms": results[head]["mkd_launch_ms"],
@@ -611,6 +690,7 @@ def main():
             "substeps_per_step": results[head]["substeps"] / args.steps,
         }
         print(json.dumps(line), flush=True)
+    graphs.clear()  # release the graphs before their containers
     for sp in containers.values():
         sp.close()
     if pg:

@@ -18,7 +18,23 @@
  *    SprayParticles.cpp:350,422 and SprayInterpolation.H:122).
  *  - One handle must not be used from two host threads at once; separate
  *    handles are independent.  Kernels run on the stream passed in (NULL =
- *    the legacy default stream) and the call returns once they completed.
+ *    the legacy default stream).
+ *  - The update entry points (pmp_spray_update, _update_host, _move_kick,
+ *    _move_kick_drift) are stream-ordered: they check their arguments,
+ *    enqueue the device work on the stream and return without waiting for
+ *    it (the reference instead synchronises after every box,
+ *    SprayParticles.cpp:499).  Their return value reports argument and
+ *    host-side errors, and a device error of an earlier call that the host
+ *    can already see.  Device errors (the reference's amrex::Abort sites)
+ *    are reported by pmp_spray_sync; after one, later calls leave the
+ *    droplets untouched until pmp_spray_sync has reported it.  A handle's
+ *    calls go on one stream, or the caller orders its streams.  The other
+ *    entry points (droplet hand-over and read-back, the operations around
+ *    the update, learning, tuning) first wait for the handle's enqueued
+ *    updates.  Update calls may be captured into a CUDA graph by the caller
+ *    once the same call has run outside the capture (so that its buffers
+ *    exist); a captured call's box table stays in the handle (up to 8
+ *    distinct tables captured per handle).
  */
 #ifndef PMP_SPRAY_H
 #define PMP_SPRAY_H
@@ -200,17 +216,19 @@ typedef struct pmp_error_info {
   char message[160];
 } pmp_error_info;
 
-/* Counters of the last update call. */
+/* Counters of the update calls between the last two pmp_spray_sync calls
+ * (summed over those calls), as of the last pmp_spray_sync. */
 typedef struct pmp_stats {
   long long substeps;        /* droplet-substeps executed (live droplets x sub-cycles) */
   long long killed;          /* droplets that evaporated or left the domain */
   long long inner_steps;     /* sum over droplet-substeps of the inner nsub */
   long long fallback;        /* mixed / learned forms: droplets handed to the
                                 plain FP64 kernel (small, out of range) */
-  double kernel_ms;          /* device time of the update kernels (host views:
-                                from the first copy in to the last copy out) */
-  int graph;                 /* 1: the update replayed a captured CUDA graph,
-                                2: it captured a new one, 0: direct launches */
+  double kernel_ms;          /* device time of the last call's update kernels
+                                (host views: from the first copy in to the
+                                last copy out) */
+  int graph;                 /* last call: 1 replayed the batched form's
+                                CUDA graph, 2 captured a new one, 0 direct launches */
 } pmp_stats;
 
 typedef struct pmp_spray pmp_spray;
@@ -245,10 +263,11 @@ int pmp_spray_get_particles(pmp_spray* h, int box, pmp_particles* out);
 int pmp_spray_num_particles(const pmp_spray* h, int box, long long* n);
 
 /* SprayParticleContainer::updateParticles (SprayParticles.cpp:142-502) for
- * all boxes in one call.  state[b] / source[b] are DEVICE views of box b's
- * state and source fabs; deposits are added to source (callers zero it, as
- * transferSource does at SprayParticles.H:294).  ltransparm is not needed:
- * the transport model is built into the handle. */
+ * all boxes in one call, stream-ordered (see the conventions above).
+ * state[b] / source[b] are DEVICE views of box b's state and source fabs;
+ * deposits are added to source (callers zero it, as transferSource does at
+ * SprayParticles.H:294).  ltransparm is not needed: the transport model is
+ * built into the handle. */
 int pmp_spray_update(
   pmp_spray* h, const pmp_box_view* state, const pmp_box_view* source,
   int nboxes, double flow_dt, double time, int state_ghosts,
@@ -262,7 +281,10 @@ int pmp_spray_update(
  * back while later groups run (page-locked host memory lets all three
  * proceed at once).  The FP64 form with a non-default launch shape or CUDA
  * graph, and the learned form with its audit on, copy, update and copy back
- * in sequence.  Returns after the sources are back in host memory. */
+ * in sequence.  Stream-ordered like pmp_spray_update: with page-locked host
+ * views the call returns before the copies run, so the caller synchronises
+ * the stream (or calls pmp_spray_sync) before it reads the host source or
+ * writes the host state. */
 int pmp_spray_update_host(
   pmp_spray* h, const pmp_box_view* state, const pmp_box_view* source,
   int nboxes, double flow_dt, double time, int state_ghosts,
@@ -304,6 +326,15 @@ enum pmp_coupling { PMP_COUPLING_LMEX = 0, PMP_COUPLING_PELEC = 1 };
 int pmp_spray_set_coupling(pmp_spray* h, int coupling);
 int pmp_spray_get_coupling(const pmp_spray* h, int* coupling);
 
+/* Wait for the device work of the handle's update calls (the stream of the
+ * last call), report and clear their status: returns the first device error
+ * of the calls since the previous pmp_spray_sync (PMP_OK if none), with the
+ * box, the droplet (caller's index) and its position in pmp_spray_last_error,
+ * and sets pmp_spray_get_stats to those calls' summed counters.  The
+ * synchronising point of the update, where the reference's device code would
+ * have aborted (SprayParticles.cpp:350,422, SprayInterpolation.H:122).
+ * After graph replays on another stream, synchronise that stream first. */
+int pmp_spray_sync(pmp_spray* h);
 int pmp_spray_last_error(const pmp_spray* h, pmp_error_info* info);
 int pmp_spray_get_stats(const pmp_spray* h, pmp_stats* stats);
 
@@ -323,10 +354,19 @@ const char* pmp_spray_version(void);
  * held until the process exits); nothing is allocated or freed.
  *  - nboxes <= PMP_STATIC_MAX_BOXES, else PMP_ERR_INVALID;
  *  - the first call on a device looks up that array's address (with the
- *    device current): make it before any stream capture;
+ *    device current) and loads this entry point's kernels.  Under CUDA's
+ *    default lazy module loading that is when the array and the kernels'
+ *    code take device memory: make the first call at initialisation, before
+ *    the pool reserves the device's memory, or run with
+ *    CUDA_MODULE_LOADING=EAGER;
+ *  - synchronous: the call waits for its kernel and reads the status back,
+ *    so it cannot be captured into a CUDA graph (PMP_ERR_INVALID under an
+ *    active capture);
  *  - all calls share the array: calls whose GPU work overlaps race, so
  *    serialise them;
- *  - err (may be NULL) receives the status, box and droplet index. */
+ *  - err (may be NULL) receives the status, box and droplet index; on a
+ *    nonzero return the droplet arrays and the sources may be partly updated
+ *    (restore or discard them). */
 #define PMP_STATIC_MAX_BOXES 256
 int pmp_spray_update_static(
   const pmp_spray_config* cfg, const pmp_spray_data* data,

@@ -24,11 +24,17 @@ SOURCES = [("pmp_spray.cu", "-fmad=false"), ("pmp_static.cu", "-fmad=false"),
            ("pmp_batch.cu", "-fmad=false"), ("batch/pmp_batch_b64.cu", "-fmad=false"),
            ("batch/pmp_batch_b128.cu", "-fmad=false"), ("batch/pmp_batch_b256.cu", "-fmad=false"),
            ("pmp_mesh.cu", "-fmad=false")]
-HEADERS = ["pmp_device.cuh", "pmp_handle.h", "spray_fp64.cuh", "spray_mixed.cuh",
-           "spray_kernels.cuh", "learn/learn_common.cuh", "learn/mlp_mma.cuh",
-           "batch/batch_kernels.cuh",
-           "phys/pmp_math.h", "phys/pmp_math_tables.h", "phys/pmp_thermo.h",
-           "phys/pmp_thermo_data.h"]
+def _headers():
+    """Every header under csrc/ (a change to any of them rebuilds the library)."""
+    out = []
+    for d, _, files in os.walk(CSRC):
+        for f in files:
+            if f.endswith((".h", ".cuh", ".H")):
+                out.append(os.path.relpath(os.path.join(d, f), CSRC))
+    return sorted(out)
+
+
+HEADERS = _headers()
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 OBJDIR = os.path.join(ROOT, "_build")

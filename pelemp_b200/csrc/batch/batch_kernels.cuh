@@ -33,7 +33,9 @@ __global__ void __launch_bounds__(BLOCK, MINB)
   __shared__ BoxEntry sB;
   const int item = blockIdx.x;
   const int b = W.box[item];
-  stage_box(P, b, sB);
+  if (stage_box(P, b, sB)) {
+    return;
+  }
   const long long s = W.start[item] + threadIdx.x;
   Counters c;
   if (s < sB.p_end) {
@@ -48,6 +50,9 @@ __global__ void __launch_bounds__(BLOCK, MINB)
 {
   __shared__ int s_item;
   Counters c;
+  if (cta_call_failed(P)) {
+    return;
+  }
   for (;;) {
     if (threadIdx.x == 0) {
       s_item = atomicAdd(W.counter, 1);

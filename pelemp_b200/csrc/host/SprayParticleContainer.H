@@ -11,6 +11,12 @@
 // Mesh data are passed as one pmp_box_view per box (the Array4 of the box's
 // fab: data pointer, allocated bounds, strides), in ParIter order, on the
 // device (pmp_spray_update) or on the host (updateParticlesHost).
+//
+// The update methods are stream-ordered, as the C ABI is: they return once
+// the work is enqueued.  synchronize() is where a device-side error of the
+// enqueued updates surfaces as SprayAbort (the reference's device abort
+// surfaces at its stream synchronisation, SprayParticles.cpp:499); call it
+// before reading host-view sources or the stats.
 #pragma once
 
 #include <stdexcept>
@@ -152,6 +158,11 @@ public:
       state_ghosts, source_ghosts, isVirt, isGhost, do_move, spray_cfl_lev, stream));
   }
 
+  /// Wait for the enqueued updates; throws SprayAbort with the reference's
+  /// abort message if one of them failed on the device.
+  void synchronize() { check(pmp_spray_sync(h_)); }
+
+  /// counters of the updates between the last two synchronize() calls
   pmp_stats stats() const
   {
     pmp_stats s{};

@@ -168,6 +168,9 @@ int main(int argc, char** argv)
           spc.moveKick(st_views, sr_views, 0, flow_dt, 0.0, false, false, state_ghosts,
                        source_ghosts, nullptr, cfl);
         }
+        // the host sources are read next: wait for the call (device errors
+        // surface here)
+        spc.synchronize();
         substeps += spc.stats().substeps;
         for (int b = 0; b < nboxes; ++b) {
           for (size_t i = 0; i < src[b].size(); ++i) {

@@ -130,8 +130,12 @@ constexpr size_t kMaxGraphs = 4;
 
 void destroy_graphs(pmp_spray* h)
 {
+  if (!h->batch.graphs.empty()) {
+    quiesce(h);  // a replay may still be running
+  }
   for (BatchState::Graph& g : h->batch.graphs) {
     cudaGraphExecDestroy(g.exec);
+    release_table(h, g.table_slot);
   }
   h->batch.graphs.clear();
 }
@@ -271,13 +275,20 @@ int graph_update(pmp_spray* h, const KParams& P, int nboxes, cudaStream_t st, in
                                   [](const BatchState::Graph& a, const BatchState::Graph& b) {
                                     return a.last_use < b.last_use;
                                   });
+      quiesce(h);
       cudaGraphExecDestroy(lru->exec);
+      release_table(h, lru->table_slot);
       B.graphs.erase(lru);
     }
     B.graphs.push_back(BatchState::Graph{});
     G = &B.graphs.back();
     G->key.swap(key);
     G->exec = exec;
+    // the graph reads the call's box table: keep that slot in place
+    G->table_slot = h->cur_table;
+    if (G->table_slot >= 0) {
+      h->tables[G->table_slot].holds += 1;
+    }
     *graph_state = 2;
   }
   G->last_use = ++B.use_clock;
@@ -403,6 +414,7 @@ extern "C" int pmp_spray_autotune(
     return set_err(h, PMP_ERR_INVALID, "the autotuner tunes the FP64 form (set PMP_MODE_FP64)");
   }
   cudaSetDevice(h->device);
+  pmp::quiesce(h);
   cudaStream_t st = (cudaStream_t)stream;
   memset(rep, 0, sizeof(*rep));
   // validation, packing and the sub-cycle count

@@ -184,7 +184,11 @@ __device__ __forceinline__ void load_gas_rec(const BoxEntry& B, int i, int j, in
 }
 #endif
 
-// Device status word block, zeroed before each update.
+// Device status block of a handle.  Update calls are stream-ordered and do
+// not wait for one another: code/box/slot (the first error, sticky) and the
+// counters accumulate over every call since the host last read and cleared
+// the block (pmp_spray_sync); fb_count alone is per call (the length of the
+// call's FP64 fallback list, reset by each call before its kernels).
 struct DevStatus {
   int code;
   int box;
@@ -193,6 +197,7 @@ struct DevStatus {
   unsigned long long killed;
   unsigned long long inner;
   unsigned long long fallback;
+  unsigned long long fb_count;
 };
 
 // SoA droplet store: ncomp double arrays of length cap, then ids.
@@ -224,6 +229,9 @@ struct KParams {
   const long long* box_begin;  // nboxes + 1 slot offsets
   long long* fb_list;          // slots handed to the FP64 fallback kernel
   DevStatus* status;
+  // page-locked, device-mapped host word: the first error code is also
+  // written here, so the host sees a failed call without synchronising
+  int* err_host;
   // PeleC coupling (FP64 form only): energy component of the state
   int pelec, c_eng;
   // fallback-list kernel: when list_nbox > 0, only the entries of boxes

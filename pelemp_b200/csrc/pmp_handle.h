@@ -23,6 +23,23 @@ struct BoxStore {
 
 struct LearnState;  // learned form (pmp_learn.cu)
 
+// A device copy of one update call's box table (a BoxEntry per box).  Calls
+// reuse the slot whose content they repeat, so the steady state uploads
+// nothing; a new table is uploaded from the slot's page-locked staging on the
+// call's stream.  A slot read by a captured CUDA graph is held (never
+// rewritten) while that graph exists.
+struct TableSlot {
+  std::vector<BoxEntry> host;      // the table's content
+  BoxEntry* d = nullptr;           // device copy
+  BoxEntry* stage = nullptr;       // page-locked staging of the upload
+  int cap = 0;
+  cudaEvent_t uploaded = nullptr;  // completion of the last upload
+  cudaStream_t stream = nullptr;   // the stream that upload was issued on
+  unsigned long long last_use = 0;
+  int holds = 0;                   // captured graphs that read this slot
+};
+constexpr int kTableSlots = 8;
+
 // (box, first slot) work items of `chunk` slots (batched form, pmp_batch.cu)
 struct WorkMap {
   int chunk = 0;
@@ -47,6 +64,7 @@ struct BatchState {
     std::vector<unsigned char> key;
     cudaGraphExec_t exec = nullptr;
     unsigned long long last_use = 0;
+    int table_slot = -1;  // the box-table slot the graph reads (held)
   };
   std::vector<Graph> graphs;
   unsigned long long use_clock = 0;
@@ -92,12 +110,23 @@ struct pmp_spray {
   long long* d_cta_start = nullptr;
   long long* d_box_begin = nullptr;
   long long* fb_list = nullptr;  // fallback slots (mixed / learned forms)
-  pmp::BoxEntry* d_boxes = nullptr;
-  pmp::BoxEntry* h_boxes = nullptr;
+  pmp::BoxEntry* h_boxes = nullptr;  // the box table of the call being prepared
   int boxes_cap = 0;
+  pmp::TableSlot tables[pmp::kTableSlots];
+  unsigned long long table_clock = 0;
+  int cur_table = -1;  // slot of the last prepared call's table
   pmp::DevStatus* d_status = nullptr;
   pmp::DevStatus* h_status = nullptr;
+  // the first device error code, written by the kernels into page-locked
+  // host memory mapped into the device (err_dev: its device address)
+  int* err_host = nullptr;
+  int* err_dev = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // stream-ordered updates: the stream of the last call and an event after
+  // its device work; pending = work enqueued since the last pmp_spray_sync
+  cudaStream_t last_stream = nullptr;
+  cudaEvent_t ev_done = nullptr;
+  bool pending = false;
   // the mixed form's FP64 list kernel runs on `side` beside the mixed kernel
   cudaStream_t side = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
@@ -137,6 +166,15 @@ namespace pmp {
 
 // pmp_spray.cu
 int set_err(pmp_spray* h, int code, const char* msg, int box = -1, long long particle = -1);
+// wait for the handle's enqueued update work (entry points that read or
+// replace the droplets, or free buffers the kernels use, call it first)
+void quiesce(pmp_spray* h);
+// read, report and clear the device status after the handle's last call
+// (pmp_spray_sync): the first device error of the calls since the previous
+// sync, or PMP_OK; fills stats and the error record
+int sync_status(pmp_spray* h);
+// release a box-table slot held by a captured graph
+void release_table(pmp_spray* h, int slot);
 // validate views, pack droplets, upload the box table, reset the status
 // block and fill the kernel parameters of one update call
 int prepare_update(
@@ -145,10 +183,10 @@ int prepare_update(
   double spray_cfl_lev, cudaStream_t st, KParams& P);
 int run_fp64_list(int ns, int nf, const KParams& P, long long total, cudaStream_t st);
 int dispatch_fp64_default(int ns, int nf, const KParams& P, int ncta, cudaStream_t st);
-// the device work of one update after prepare: box table upload, status
-// reset, timing events, kernels, status read-back (no synchronisation)
+// the device work of one update after prepare: the per-call fallback count
+// reset, timing events, kernels (no synchronisation, no status read-back)
 int enqueue_update(pmp_spray* h, const KParams& P, int nboxes, cudaStream_t st);
-// a whole update call (prepare, launch, synchronise, status)
+// a whole update call, synchronous (prepare, launch, sync_status)
 int run_update(
   pmp_spray* h, const pmp_box_view* state, const pmp_box_view* source, int nboxes,
   double flow_dt, int state_ghosts, int source_ghosts, int is_ghost, int do_move,

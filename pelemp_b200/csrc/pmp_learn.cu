@@ -746,6 +746,11 @@ __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
   // the weights arrive by one bulk copy while the droplets are read and the
   // first gather runs; the first network evaluation waits for them
   static_assert(sizeof(tc::TcMlp) % 16 == 0, "bulk copies move multiples of 16 bytes");
+  // a failed call since the last status read: leave the droplets (before any
+  // copy is issued or tensor memory allocated)
+  if (cta_call_failed(P)) {
+    return;
+  }
   const uint32_t wbar = tc::smem_u32(&wbar_slot);
   if (threadIdx.x == 0) {
     tc::mbar_init(wbar);
@@ -785,8 +790,7 @@ __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
     valid = valid && id > 0;
     double dia = valid ? P.parts.rd[PMP_PSTATE_DIA][s] : 1e-5;
     if (valid && dia < kMixedMinDia) {
-      const unsigned long long k = atomicAdd(&P.status->fallback, 1ULL);
-      P.fb_list[k] = s;
+      push_fallback(P, s);
       valid = false;
     }
     double pos[3] = {0., 0., 0.}, vel[3] = {0., 0., 0.}, Y[NF];
@@ -1031,8 +1035,7 @@ __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
               in = in && isfinite(yv[k]);
             }
             if (!in) {
-              const unsigned long long k = atomicAdd(&P.status->fallback, 1ULL);
-              P.fb_list[k] = s;
+              push_fallback(P, s);
               fell_back = true;
               valid = false;
               active = false;
@@ -1538,6 +1541,7 @@ extern "C" int pmp_spray_learn_generate(
     return PMP_ERR_INVALID;
   }
   cudaSetDevice(h->device);
+  pmp::quiesce(h);
   cudaStream_t st = (cudaStream_t)stream;
   // prepare_update validates source views too: pass the state views, which
   // cover the boxes and are never written here.  The teacher needs no trained
@@ -1642,6 +1646,7 @@ extern "C" int pmp_spray_learn_train(pmp_spray* h, const pmp_learn_config* cfg, 
     return PMP_ERR_INVALID;
   }
   cudaSetDevice(h->device);
+  pmp::quiesce(h);
   LearnState* L = learn_state(h);
   long long n = 0;
   pmp_spray_learn_count(h, &n);
@@ -1793,6 +1798,7 @@ extern "C" int pmp_spray_learn_weights(pmp_spray* h, int get, float* buf, long l
     return PMP_ERR_INVALID;
   }
   cudaSetDevice(h->device);
+  pmp::quiesce(h);
   LearnState* L = learn_state(h);
   if (ensure_params(L) != 0) {
     return PMP_ERR_CUDA;

@@ -552,6 +552,7 @@ extern "C" int pmp_spray_est_timestep(pmp_spray* h, double cfl, double max_jet_v
     return set_err(h, PMP_ERR_INVALID, "setup and geometry must be set first");
   }
   cudaSetDevice(h->device);
+  pmp::quiesce(h);
   cudaStream_t st = (cudaStream_t)stream;
   if (h->data.fixed_parts) {
     *dt = -1.;
@@ -599,6 +600,7 @@ extern "C" int pmp_spray_derive(pmp_spray* h, const pmp_box_view* vars, int nbox
     return set_err(h, PMP_ERR_INVALID, "setup and geometry must be set first");
   }
   cudaSetDevice(h->device);
+  pmp::quiesce(h);
   cudaStream_t st = (cudaStream_t)stream;
   int rc = ensure_packed(h);
   if (rc != PMP_OK) {
@@ -689,6 +691,7 @@ extern "C" int pmp_spray_transfer_source(pmp_spray* h, const pmp_box_view* tmp_s
     return set_err(h, PMP_ERR_INVALID, "setup, comps and geometry must be set first");
   }
   cudaSetDevice(h->device);
+  pmp::quiesce(h);
   cudaStream_t st = (cudaStream_t)stream;
   int rc = ensure_box_map(h, st);
   if (rc != PMP_OK) {
@@ -798,6 +801,7 @@ extern "C" int pmp_spray_redistribute(pmp_spray* h, long long* removed, void* st
     return set_err(h, PMP_ERR_INVALID, "geometry must be set first");
   }
   cudaSetDevice(h->device);
+  pmp::quiesce(h);
   cudaStream_t st = (cudaStream_t)stream;
   int rc = ensure_packed(h);
   if (rc == PMP_OK) {

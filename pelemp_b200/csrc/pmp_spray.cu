@@ -332,13 +332,83 @@ int ensure_boxes_cap(pmp_spray* h, int n)
   if (n <= h->boxes_cap) {
     return PMP_OK;
   }
-  cudaFree(h->d_boxes);
-  cudaFreeHost(h->h_boxes);
-  h->d_boxes = nullptr;
-  h->h_boxes = nullptr;
-  PMP_CUDA(h, cudaMalloc(&h->d_boxes, sizeof(BoxEntry) * n));
-  PMP_CUDA(h, cudaMallocHost(&h->h_boxes, sizeof(BoxEntry) * n));
+  delete[] h->h_boxes;
+  h->h_boxes = new BoxEntry[n];
   h->boxes_cap = n;
+  return PMP_OK;
+}
+
+// The device box table of the call being prepared (h->h_boxes[0, nboxes)):
+// the slot already holding that content, or else the least recently used
+// slot that no captured graph holds, uploaded on st.  Under stream capture
+// the slot is held from then on: the graph reads it (and, if the capture
+// uploaded it, copies from its staging) at every replay.
+int acquire_table(pmp_spray* h, int nboxes, cudaStream_t st, const BoxEntry** out)
+{
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  PMP_CUDA(h, cudaStreamIsCapturing(st, &cap));
+  const bool capturing = cap == cudaStreamCaptureStatusActive;
+  const size_t bytes = sizeof(BoxEntry) * (size_t)nboxes;
+  int pick = -1;
+  for (int i = 0; i < pmp::kTableSlots; ++i) {
+    pmp::TableSlot& t = h->tables[i];
+    if (t.d && (int)t.host.size() == nboxes && memcmp(t.host.data(), h->h_boxes, bytes) == 0) {
+      if (!capturing && t.stream != st) {
+        PMP_CUDA(h, cudaStreamWaitEvent(st, t.uploaded, 0));
+      }
+      pick = i;
+      break;
+    }
+  }
+  if (pick < 0) {
+    for (int i = 0; i < pmp::kTableSlots; ++i) {
+      const pmp::TableSlot& t = h->tables[i];
+      if (t.holds == 0 && (pick < 0 || t.last_use < h->tables[pick].last_use)) {
+        pick = i;
+      }
+    }
+    if (pick < 0) {
+      return set_err(h, PMP_ERR_INVALID, "every box-table slot is held by a captured CUDA graph");
+    }
+    pmp::TableSlot& t = h->tables[pick];
+    const int need = std::max(nboxes, 1);
+    if (t.cap < need) {
+      // kernels of earlier calls may still read the slot's table
+      pmp::quiesce(h);
+      cudaFree(t.d);
+      cudaFreeHost(t.stage);
+      t.d = nullptr;
+      t.stage = nullptr;
+      t.cap = 0;
+      t.host.clear();
+      const int n = std::max(need, 8);
+      PMP_CUDA(h, cudaMalloc(&t.d, sizeof(BoxEntry) * n));
+      PMP_CUDA(h, cudaMallocHost(&t.stage, sizeof(BoxEntry) * n));
+      t.cap = n;
+    }
+    if (!t.uploaded) {
+      PMP_CUDA(h, cudaEventCreateWithFlags(&t.uploaded, cudaEventDisableTiming));
+    } else {
+      // the slot's previous upload has read its staging
+      PMP_CUDA(h, cudaEventSynchronize(t.uploaded));
+    }
+    memcpy(t.stage, h->h_boxes, bytes);
+    t.host.assign(h->h_boxes, h->h_boxes + nboxes);
+    if (nboxes > 0) {
+      PMP_CUDA(h, cudaMemcpyAsync(t.d, t.stage, bytes, cudaMemcpyHostToDevice, st));
+    }
+    if (!capturing) {
+      PMP_CUDA(h, cudaEventRecord(t.uploaded, st));
+      t.stream = st;
+    }
+  }
+  pmp::TableSlot& t = h->tables[pick];
+  t.last_use = ++h->table_clock;
+  if (capturing) {
+    t.holds += 1;
+  }
+  h->cur_table = pick;
+  *out = t.d;
   return PMP_OK;
 }
 
@@ -604,7 +674,6 @@ int prepare_update_impl(
   double flow_dt, int state_ghosts, int source_ghosts, int is_ghost, int do_move,
   double spray_cfl_lev, cudaStream_t st, KParams& P)
 {
-  memset(&h->stats, 0, sizeof(h->stats));
   if (!h->have_data || !h->have_comps || !h->have_geom) {
     return set_err(h, PMP_ERR_INVALID, "setup, comps and geometry must be set before update");
   }
@@ -655,6 +724,7 @@ int prepare_update_impl(
     rec_total += (size_t)cells * R;
   }
   if (16 * rec_total > h->gas_rec_bytes) {
+    pmp::quiesce(h);  // kernels of earlier calls may still read the records
     cudaFree(h->gas_rec);
     h->gas_rec = nullptr;
     h->gas_rec_bytes = 0;
@@ -734,7 +804,11 @@ int prepare_update_impl(
     e.p_begin = h->box_begin[b];
     e.p_end = h->box_begin[b + 1];
   }
-  (void)st;
+  const BoxEntry* dtab = nullptr;
+  rc = acquire_table(h, nboxes, st, &dtab);
+  if (rc != PMP_OK) {
+    return rc;
+  }
   memset(&P, 0, sizeof(P));
   P.m = h->dmech;
   P.f = h->dfuel;
@@ -786,38 +860,68 @@ int prepare_update_impl(
   P.do_move = do_move;
   P.is_ghost = is_ghost;
   P.nboxes = nboxes;
-  P.boxes = h->d_boxes;
+  P.boxes = dtab;
   P.cta_box = h->d_cta_box;
   P.cta_start = h->d_cta_start;
   P.status = h->d_status;
+  P.err_host = h->err_dev;
   P.box_begin = h->d_box_begin;
   P.fb_list = h->fb_list;
   return PMP_OK;
 }
 
-int finish_update(pmp_spray* h, int graph_state);
+// After a call's device work is enqueued on st: remember the stream and mark
+// the point (nothing is recorded while st is being captured into a graph;
+// the caller then orders the replays).
+int mark_enqueued(pmp_spray* h, cudaStream_t st)
+{
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  PMP_CUDA(h, cudaStreamIsCapturing(st, &cap));
+  if (cap != cudaStreamCaptureStatusNone) {
+    return PMP_OK;
+  }
+  PMP_CUDA(h, cudaEventRecord(h->ev_done, st));
+  h->last_stream = st;
+  h->pending = true;
+  return PMP_OK;
+}
 
+// A device error of an earlier call that the host can already see (the
+// kernels also write the code into mapped host memory): report it at once.
+bool earlier_call_failed(const pmp_spray* h)
+{
+  return h->err_host && *reinterpret_cast<volatile const int*>(h->err_host) != 0;
+}
+
+// updateParticles for all boxes, stream-ordered: validates, enqueues the
+// device work on st and returns without waiting for it.
 int do_update(
   pmp_spray* h, const pmp_box_view* state, const pmp_box_view* source, int nboxes,
   double flow_dt, int state_ghosts, int source_ghosts, int is_virt, int is_ghost, int do_move,
   double spray_cfl_lev, cudaStream_t st)
 {
   (void)is_virt;
+  if (earlier_call_failed(h)) {
+    return pmp::sync_status(h);
+  }
   KParams P;
   int rc = prepare_update_impl(h, state, source, nboxes, flow_dt, state_ghosts, source_ghosts,
                                is_ghost, do_move, spray_cfl_lev, st, P);
   if (rc != PMP_OK) {
     return rc;
   }
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  PMP_CUDA(h, cudaStreamIsCapturing(st, &cap));
+  // the internal graph of the batched form is not nested in a caller's capture
   const bool graph = h->batch.cfg.use_graph && h->mode != PMP_MODE_LEARNED &&
-                     h->batch.cfg.kind != PMP_LAUNCH_PER_BOX;
+                     h->batch.cfg.kind != PMP_LAUNCH_PER_BOX && cap == cudaStreamCaptureStatusNone;
   int graph_state = 0;
   rc = graph ? pmp::graph_update(h, P, nboxes, st, &graph_state) : pmp::enqueue_update(h, P, nboxes, st);
   if (rc != PMP_OK) {
     return rc;
   }
-  PMP_CUDA(h, cudaStreamSynchronize(st));
-  return finish_update(h, graph_state);
+  h->stats.graph = graph_state;
+  return mark_enqueued(h, st);
 }
 
 // The mixed form over CTA-map items [c0, c0 + n) (Q's map already offset) and
@@ -838,15 +942,18 @@ int enqueue_mixed(pmp_spray* h, const KParams& Q, int n, long long s0, long long
   PMP_CUDA(h, cudaEventRecord(h->ev_fork, st));
   PMP_CUDA(h, cudaStreamWaitEvent(h->side, h->ev_fork, 0));
   rc = dispatch_fp64_list(h->nspec, h->nfuel, R, h->total, h->side);
+  if (rc == PMP_OK) {
+    rc = pmp::launch_mixed(h->nspec, h->nfuel, R, n, kBlock, st);
+  }
+  // join the side stream whatever happened (a capture must not end with
+  // unjoined work, and a failing launch keeps its own code)
+  const cudaError_t e1 = cudaEventRecord(h->ev_join, h->side);
+  const cudaError_t e2 = cudaStreamWaitEvent(st, h->ev_join, 0);
   if (rc != PMP_OK) {
     return rc;
   }
-  rc = pmp::launch_mixed(h->nspec, h->nfuel, R, n, kBlock, st);
-  if (rc != PMP_OK) {
-    return rc;
-  }
-  PMP_CUDA(h, cudaEventRecord(h->ev_join, h->side));
-  PMP_CUDA(h, cudaStreamWaitEvent(st, h->ev_join, 0));
+  PMP_CUDA(h, e1);
+  PMP_CUDA(h, e2);
   return PMP_OK;
 }
 
@@ -912,9 +1019,7 @@ int update_host_overlapped_impl(
   }
   const int NS = h->nspec;
   const int NF = h->nfuel;
-  PMP_CUDA(h, cudaMemcpyAsync(h->d_boxes, h->h_boxes, sizeof(BoxEntry) * nboxes,
-                              cudaMemcpyHostToDevice, st));
-  PMP_CUDA(h, cudaMemsetAsync(h->d_status, 0, sizeof(DevStatus), st));
+  PMP_CUDA(h, cudaMemsetAsync(&h->d_status->fb_count, 0, sizeof(unsigned long long), st));
   PMP_CUDA(h, cudaEventRecord(h->ev0, st));
   PMP_CUDA(h, cudaEventRecord(h->hev_start, st));
   PMP_CUDA(h, cudaStreamWaitEvent(h->hs_in, h->hev_start, 0));
@@ -986,9 +1091,8 @@ int update_host_overlapped_impl(
   PMP_CUDA(h, cudaEventRecord(h->hev_out, h->hs_out));
   PMP_CUDA(h, cudaStreamWaitEvent(st, h->hev_out, 0));
   PMP_CUDA(h, cudaEventRecord(h->ev1, st));
-  PMP_CUDA(h, cudaMemcpyAsync(h->h_status, h->d_status, sizeof(DevStatus), cudaMemcpyDeviceToHost, st));
-  PMP_CUDA(h, cudaStreamSynchronize(st));
-  return finish_update(h, 0);
+  h->stats.graph = 0;
+  return mark_enqueued(h, st);
 }
 
 int update_host_overlapped(
@@ -996,6 +1100,9 @@ int update_host_overlapped(
   const pmp_box_view* dsr, int nboxes, double flow_dt, int state_ghosts, int source_ghosts,
   int is_ghost, int do_move, double spray_cfl_lev, cudaStream_t st)
 {
+  if (earlier_call_failed(h)) {
+    return pmp::sync_status(h);
+  }
   const int rc = update_host_overlapped_impl(h, hst, hsr, dst, dsr, nboxes, flow_dt, state_ghosts,
                                              source_ghosts, is_ghost, do_move, spray_cfl_lev, st);
   if (rc != PMP_OK && h->hs_in) {
@@ -1007,10 +1114,31 @@ int update_host_overlapped(
   return rc;
 }
 
-// Stats and the error record from the status an update copied back (its
-// stream synchronised).
-int finish_update(pmp_spray* h, int graph_state)
+}  // namespace
+
+void pmp::quiesce(pmp_spray* h)
 {
+  if (h->pending && h->ev_done) {
+    cudaEventSynchronize(h->ev_done);
+  }
+}
+
+void pmp::release_table(pmp_spray* h, int slot)
+{
+  if (slot >= 0 && slot < pmp::kTableSlots && h->tables[slot].holds > 0) {
+    h->tables[slot].holds -= 1;
+  }
+}
+
+// The status the handle's calls accumulated since the last read: copied back
+// after the last call's work on its stream, reported (stats, error record)
+// and cleared.
+int pmp::sync_status(pmp_spray* h)
+{
+  cudaStream_t st = h->last_stream;
+  PMP_CUDA(h, cudaMemcpyAsync(h->h_status, h->d_status, sizeof(DevStatus), cudaMemcpyDeviceToHost, st));
+  PMP_CUDA(h, cudaStreamSynchronize(st));
+  h->pending = false;
   const long long T = h->total;
   float ms = 0.f;
   if (cudaEventElapsedTime(&ms, h->ev0, h->ev1) == cudaSuccess) {
@@ -1019,7 +1147,6 @@ int finish_update(pmp_spray* h, int graph_state)
     h->stats.kernel_ms = -1.;
     cudaGetLastError();  // not sticky: clear it so that the next call does not report it
   }
-  h->stats.graph = graph_state;
   h->stats.substeps = (long long)h->h_status->substeps;
   h->stats.killed = (long long)h->h_status->killed;
   h->stats.inner_steps = (long long)h->h_status->inner;
@@ -1038,18 +1165,22 @@ int finish_update(pmp_spray* h, int graph_state)
     static const char* names[] = {"ok", "droplet left the domain", "state box too small",
                                   "source box too small", "unsupported droplet state", "timeout"};
     const int code = h->h_status->code;
+    // clear the status (the error is reported once; later calls run again)
+    PMP_CUDA(h, cudaMemsetAsync(h->d_status, 0, sizeof(DevStatus), st));
+    PMP_CUDA(h, cudaStreamSynchronize(st));
+    *reinterpret_cast<volatile int*>(h->err_host) = 0;
     set_err(h, code, code < 6 ? names[code] : "error", b, caller);
     for (int d = 0; d < 3; ++d) {
       h->last_err.pos[d] = pos[d];
     }
     return code;
   }
+  PMP_CUDA(h, cudaMemsetAsync(h->d_status, 0, sizeof(DevStatus), st));
+  PMP_CUDA(h, cudaStreamSynchronize(st));
   memset(&h->last_err, 0, sizeof(h->last_err));
   h->last_err.particle = -1;
   return PMP_OK;
 }
-
-}  // namespace
 
 int pmp::prepare_update(
   pmp_spray* h, const pmp_box_view* state, const pmp_box_view* source, int nboxes,
@@ -1061,9 +1192,7 @@ int pmp::prepare_update(
   if (rc != PMP_OK) {
     return rc;
   }
-  PMP_CUDA(h, cudaMemcpyAsync(h->d_boxes, h->h_boxes, sizeof(BoxEntry) * nboxes,
-                              cudaMemcpyHostToDevice, st));
-  PMP_CUDA(h, cudaMemsetAsync(h->d_status, 0, sizeof(DevStatus), st));
+  PMP_CUDA(h, cudaMemsetAsync(&h->d_status->fb_count, 0, sizeof(unsigned long long), st));
   return PMP_OK;
 }
 
@@ -1105,9 +1234,7 @@ int pmp::enqueue_update(pmp_spray* h, const KParams& P, int nboxes, cudaStream_t
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   PMP_CUDA(h, cudaStreamIsCapturing(st, &cap));
   const unsigned ev_flags = cap == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : 0u;
-  PMP_CUDA(h, cudaMemcpyAsync(h->d_boxes, h->h_boxes, sizeof(BoxEntry) * nboxes,
-                              cudaMemcpyHostToDevice, st));
-  PMP_CUDA(h, cudaMemsetAsync(h->d_status, 0, sizeof(DevStatus), st));
+  PMP_CUDA(h, cudaMemsetAsync(&h->d_status->fb_count, 0, sizeof(unsigned long long), st));
   PMP_CUDA(h, cudaEventRecordWithFlags(h->ev0, st, ev_flags));
   if (h->ncta > 0) {
     const int NS = h->nspec;
@@ -1144,7 +1271,6 @@ int pmp::enqueue_update(pmp_spray* h, const KParams& P, int nboxes, cudaStream_t
     PMP_CUDA(h, cudaGetLastError());
   }
   PMP_CUDA(h, cudaEventRecordWithFlags(h->ev1, st, ev_flags));
-  PMP_CUDA(h, cudaMemcpyAsync(h->h_status, h->d_status, sizeof(DevStatus), cudaMemcpyDeviceToHost, st));
   return PMP_OK;
 }
 
@@ -1153,8 +1279,12 @@ int pmp::run_update(
   double flow_dt, int state_ghosts, int source_ghosts, int is_ghost, int do_move,
   double spray_cfl_lev, cudaStream_t st)
 {
-  return do_update(h, state, source, nboxes, flow_dt, state_ghosts, source_ghosts, 0, is_ghost,
-                   do_move, spray_cfl_lev, st);
+  const int rc = do_update(h, state, source, nboxes, flow_dt, state_ghosts, source_ghosts, 0, is_ghost,
+                           do_move, spray_cfl_lev, st);
+  if (rc != PMP_OK) {
+    return rc;
+  }
+  return sync_status(h);
 }
 
 int pmp::launch_gas_records64(const pmp_spray* h, const KParams& P, int b0, int nb, cudaStream_t st)
@@ -1237,11 +1367,16 @@ int pmp_spray_create(const pmp_spray_config* cfg, pmp_spray** out)
   memset(&h->stats, 0, sizeof(h->stats));
   if (cudaSetDevice(h->device) != cudaSuccess ||
       cudaMalloc(&h->d_status, sizeof(DevStatus)) != cudaSuccess ||
+      cudaMemset(h->d_status, 0, sizeof(DevStatus)) != cudaSuccess ||
       cudaMallocHost(&h->h_status, sizeof(DevStatus)) != cudaSuccess ||
-      cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess) {
-    delete h;
+      cudaHostAlloc(&h->err_host, sizeof(int), cudaHostAllocMapped) != cudaSuccess ||
+      cudaHostGetDevicePointer(&h->err_dev, h->err_host, 0) != cudaSuccess ||
+      cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->ev_done, cudaEventDisableTiming) != cudaSuccess) {
+    pmp_spray_destroy(h);
     return PMP_ERR_CUDA;
   }
+  *h->err_host = 0;
   {
     int lo = 0, hi = 0;
     if (cudaDeviceGetStreamPriorityRange(&lo, &hi) != cudaSuccess ||
@@ -1262,6 +1397,7 @@ int pmp_spray_destroy(pmp_spray* h)
     return PMP_OK;
   }
   cudaSetDevice(h->device);
+  pmp::quiesce(h);
   for (auto& s : h->staged) {
     free_store(s);
   }
@@ -1276,10 +1412,20 @@ int pmp_spray_destroy(pmp_spray* h)
     cudaFree(p);
   }
   cudaFree(h->gas_rec);
-  cudaFree(h->d_boxes);
-  cudaFreeHost(h->h_boxes);
+  delete[] h->h_boxes;
+  for (pmp::TableSlot& t : h->tables) {
+    cudaFree(t.d);
+    cudaFreeHost(t.stage);
+    if (t.uploaded) {
+      cudaEventDestroy(t.uploaded);
+    }
+  }
   cudaFree(h->d_status);
   cudaFreeHost(h->h_status);
+  cudaFreeHost(h->err_host);
+  if (h->ev_done) {
+    cudaEventDestroy(h->ev_done);
+  }
   if (h->ev0) {
     cudaEventDestroy(h->ev0);
   }
@@ -1460,6 +1606,7 @@ int pmp_spray_set_grids(pmp_spray* h, int nboxes, const pmp_box* boxes)
     return PMP_ERR_INVALID;
   }
   cudaSetDevice(h->device);
+  pmp::quiesce(h);
   for (auto& s : h->staged) {
     free_store(s);
   }
@@ -1480,6 +1627,7 @@ int pmp_spray_set_particles(pmp_spray* h, int box, const pmp_particles* p)
     return set_err(h, PMP_ERR_INVALID, "set_geometry must precede set_particles");
   }
   cudaSetDevice(h->device);
+  pmp::quiesce(h);
   // unpack the other boxes first if the layout changes
   if (h->packed) {
     const int nb = (int)h->boxes.size();
@@ -1608,6 +1756,7 @@ int pmp_spray_get_particles(pmp_spray* h, int box, pmp_particles* out)
     return PMP_ERR_INVALID;
   }
   cudaSetDevice(h->device);
+  pmp::quiesce(h);
   long long n = 0;
   pmp_spray_num_particles(h, box, &n);
   if (out->n != n) {
@@ -1680,6 +1829,9 @@ int pmp_spray_update_host(
   }
   cudaSetDevice(h->device);
   cudaStream_t st = (cudaStream_t)stream;
+  if (earlier_call_failed(h)) {
+    return pmp::sync_status(h);
+  }
   if ((int)h->stage_state.size() < nboxes) {
     h->stage_state.resize(nboxes, nullptr);
     h->stage_src.resize(nboxes, nullptr);
@@ -1693,6 +1845,9 @@ int pmp_spray_update_host(
     }
     const size_t ns = view_extent(state[b]);
     const size_t nsr = view_extent(source[b]);
+    if (h->stage_state_n[b] < ns || h->stage_src_n[b] < nsr) {
+      pmp::quiesce(h);  // earlier calls' kernels may still read the staged views
+    }
     if (h->stage_state_n[b] < ns) {
       cudaFree(h->stage_state[b]);
       h->stage_state[b] = nullptr;
@@ -1736,13 +1891,13 @@ int pmp_spray_update_host(
   const int rc = do_update(h, dst.data(), dsr.data(), nboxes, flow_dt, state_ghosts, source_ghosts,
                            is_virt, is_ghost, do_move, spray_cfl_lev, st);
   if (rc != PMP_OK) {
+    cudaStreamSynchronize(st);  // no copy of the caller's memory in flight on return
     return rc;
   }
   for (int b = 0; b < nboxes; ++b) {
     PMP_CUDA(h, copy_runs(source[b].p, h->stage_src[b], source[b], sr_runs, cudaMemcpyDeviceToHost, st));
   }
-  PMP_CUDA(h, cudaStreamSynchronize(st));
-  return PMP_OK;
+  return mark_enqueued(h, st);
 }
 
 int pmp_spray_move_kick_drift(
@@ -1791,6 +1946,15 @@ int pmp_spray_get_coupling(const pmp_spray* h, int* coupling)
   }
   *coupling = h->pelec;
   return PMP_OK;
+}
+
+int pmp_spray_sync(pmp_spray* h)
+{
+  if (!h) {
+    return PMP_ERR_INVALID;
+  }
+  cudaSetDevice(h->device);
+  return pmp::sync_status(h);
 }
 
 int pmp_spray_last_error(const pmp_spray* h, pmp_error_info* info)

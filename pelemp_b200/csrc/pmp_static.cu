@@ -16,8 +16,17 @@
 //    (about 90 KB) and stays resident on every device that loads the
 //    library until the process exits;
 //  - the first call on a device looks up the array's device address
-//    (cudaGetSymbolAddress) with that device current; make that first call
-//    before any stream capture starts;
+//    (cudaGetSymbolAddress) with that device current and loads every kernel
+//    of this entry point: with CUDA's lazy module loading (the default) that
+//    first call is when the array and the kernels' code take device memory,
+//    so make it at initialisation, before the host's pool reserves the
+//    device's memory (or run with CUDA_MODULE_LOADING=EAGER);
+//  - the call is synchronous (it waits for its kernel and reads the status
+//    back) and cannot be captured into a CUDA graph: under an active stream
+//    capture it returns PMP_ERR_INVALID;
+//  - on a nonzero return the droplet arrays and the sources may be partly
+//    updated (every droplet whose thread ran to the end was): restore or
+//    discard them;
 //  - every call reuses the same array: calls whose GPU work overlaps (two
 //    streams, two host threads) race on it and must be serialised by the
 //    caller;
@@ -33,7 +42,7 @@
 
 #include "phys/pmp_thermo.h"
 #include "pmp_device.cuh"
-#include "spray_fp64.cuh"
+#include "spray_kernels.cuh"
 
 namespace {
 
@@ -72,255 +81,75 @@ int fail(pmp_error_info* err, int code, const char* msg, int box = -1, long long
   return code;
 }
 
-// The droplet loop of spray_update_fp64 (spray_fp64.cuh) for per-box caller
-// arrays: CTA -> box by a search of the prefix table in the scratch array.
+// The FP64 update over per-box caller arrays: CTA -> box by a search of the
+// prefix table in the scratch array, the box's entry and array pointers
+// staged in shared memory, then the droplet body every FP64 launch of the
+// library runs (update_one), so each droplet's result is the same bits as
+// pmp_spray_update's.
 template <int NS, int NF>
-__global__ void __launch_bounds__(kStaticBlock)
-  spray_update_fp64_static(const __grid_constant__ pmp::KParams P, StaticScratch* scr)
+__global__ void __launch_bounds__(kStaticBlock, PMP_FP64_MIN_BLOCKS)
+  spray_update_fp64_static(const __grid_constant__ pmp::KParams P, const StaticScratch* scr)
 {
   using namespace pmp;
-  int lo = 0;
-  int hi = P.nboxes;  // cta_prefix[lo] <= blockIdx.x < cta_prefix[hi]
-  while (hi - lo > 1) {
-    const int mid = (lo + hi) / 2;
-    if (scr->cta_prefix[mid] <= (int)blockIdx.x) {
-      lo = mid;
-    } else {
-      hi = mid;
+  __shared__ BoxEntry sB;
+  __shared__ DevParts sD;
+  __shared__ int s_box;
+  __shared__ long long s_n;
+  if (threadIdx.x == 0) {
+    int lo = 0;
+    int hi = P.nboxes;  // cta_prefix[lo] <= blockIdx.x < cta_prefix[hi]
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) / 2;
+      if (scr->cta_prefix[mid] <= (int)blockIdx.x) {
+        lo = mid;
+      } else {
+        hi = mid;
+      }
+    }
+    s_box = lo;
+    s_n = scr->boxes[lo].n;
+  }
+  __syncthreads();
+  const int b = s_box;
+  {
+    static_assert(sizeof(BoxEntry) % 4 == 0 && sizeof(DevParts) % 4 == 0, "copied as words");
+    const int* src_e = reinterpret_cast<const int*>(&scr->boxes[b].e);
+    const int* src_d = reinterpret_cast<const int*>(&scr->boxes[b].parts);
+    int* dst_e = reinterpret_cast<int*>(&sB);
+    int* dst_d = reinterpret_cast<int*>(&sD);
+    for (int i = threadIdx.x; i < (int)(sizeof(BoxEntry) / 4); i += kStaticBlock) {
+      dst_e[i] = src_e[i];
+    }
+    for (int i = threadIdx.x; i < (int)(sizeof(DevParts) / 4); i += kStaticBlock) {
+      dst_d[i] = src_d[i];
     }
   }
-  const int b = lo;
-  const StaticBox& SB = scr->boxes[b];
-  const BoxEntry& B = SB.e;
-  const DevParts& parts = SB.parts;
+  __syncthreads();
   const long long s = (long long)(blockIdx.x - scr->cta_prefix[b]) * kStaticBlock + threadIdx.x;
-  unsigned long long my_sub = 0, my_killed = 0, my_inner = 0;
-  DevStatus* status = &scr->status;
-  auto set_err = [&](int code) {
-    if (atomicCAS(&status->code, 0, code) == 0) {
-      status->box = b;
-      status->slot = s;
-    }
-  };
-  if (s < SB.n) {
-    int id = parts.id[s];
-    if (id > 0) {
-      double pos[3], vel[3], Y[NF];
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        pos[d] = parts.pos[d][s];
-        vel[d] = parts.rd[PMP_PSTATE_VEL + d][s];
-      }
-      double T = parts.rd[PMP_PSTATE_T][s];
-      double dia = parts.rd[PMP_PSTATE_DIA][s];
-#pragma unroll
-      for (int spf = 0; spf < NF; ++spf) {
-        Y[spf] = parts.rd[PMP_PSTATE_Y + spf][s];
-      }
-      const double num_ppp = parts.rd[PMP_PSTATE_NUMDENS(NF)][s];
-      const double film = parts.rd[PMP_PSTATE_FILMHGHT(NF)][s];
-      double lx[3];
-      int ijk[3], ijkc[3];
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        lx[d] = (pos[d] - P.plo[d]) * P.dxi[d] + 0.5;
-        ijk[d] = static_cast<int>(floor(lx[d]));
-        ijkc[d] = static_cast<int>(floor((pos[d] - P.plo[d]) * P.dxi[d]));
-      }
-      int bflags[3] = {0, 0, 0};
-      bool ok = true;
-      if (B.at_bounds) {
-        if (check_bounds(P, pos, bflags)) {
-          set_err(PMP_ERR_LEFT_DOMAIN);
-          ok = false;
-        }
-      }
-      for (int cur_iter = 0; ok && cur_iter < P.num_iter && id > 0; ++cur_iter) {
-        if (film > 0.) {
-          set_err(PMP_ERR_UNSUPPORTED);
-          ok = false;
-          break;
-        }
-        double ssv[2][3];
-#pragma unroll
-        for (int dir = 0; dir < 3; ++dir) {
-          const double sx_hi = lx[dir] - static_cast<double>(ijk[dir]);
-          const double sx_lo = 1. - sx_hi;
-          if (bflags[dir] > 1) {
-            ssv[0][dir] = 1.;
-            ssv[1][dir] = 0.;
-          } else if (bflags[dir] < -1) {
-            ssv[0][dir] = 0.;
-            ssv[1][dir] = 1.;
-          } else {
-            ssv[0][dir] = sx_lo;
-            ssv[1][dir] = sx_hi;
-          }
-        }
-        GasVals<NS, NF> gpv;
-        gpv.rho = 0.;
-        gpv.T = 0.;
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          gpv.vel[d] = 0.;
-          gpv.mom_src[d] = 0.;
-        }
-#pragma unroll
-        for (int n = 0; n < NS; ++n) {
-          gpv.Y[n] = 0.;
-        }
-#pragma unroll
-        for (int spf = 0; spf < NF; ++spf) {
-          gpv.Ydot[spf] = 0.;
-        }
-        gpv.eng_src = 0.;
-        gpv.mass_src = 0.;
-        bool state_ok = true;
-#pragma unroll
-        for (int kk = -1; kk < 1; ++kk) {
-#pragma unroll
-          for (int jj = -1; jj < 1; ++jj) {
-#pragma unroll
-            for (int ii = -1; ii < 1; ++ii) {
-              const double cw = ssv[ii + 1][0] * ssv[jj + 1][1] * ssv[kk + 1][2];
-              if (cw > 0.) {
-                const int ci = ijk[0] + ii;
-                const int cj = ijk[1] + jj;
-                const int ck = ijk[2] + kk;
-                if (!in_box(B.state_lo, B.state_hi, ci, cj, ck)) {
-                  state_ok = false;
-                } else {
-                  const double* q = B.st + (long long)(ci - B.st_lo[0]) +
-                                    (long long)(cj - B.st_lo[1]) * B.st_js +
-                                    (long long)(ck - B.st_lo[2]) * B.st_ks;
-                  const double cur_rho = __ldg(q + (long long)P.c_rho * B.st_ns);
-                  gpv.rho += cw * cur_rho;
-                  const double inv_rho = 1. / cur_rho;
-#pragma unroll
-                  for (int n = 0; n < NS; ++n) {
-                    const double cur_mf = __ldg(q + (long long)(P.c_spec + n) * B.st_ns) * inv_rho;
-                    gpv.Y[n] += cw * cur_mf;
-                  }
-#pragma unroll
-                  for (int dir = 0; dir < 3; ++dir) {
-                    gpv.vel[dir] += cw * __ldg(q + (long long)(P.c_mom + dir) * B.st_ns);
-                  }
-                  gpv.T += cw * __ldg(q + (long long)P.c_T * B.st_ns);
-                }
-              }
-            }
-          }
-        }
-        if (!state_ok) {
-          set_err(PMP_ERR_STATE_BOX);
-          ok = false;
-          break;
-        }
-        double mw_mix = 0.;
-#pragma unroll
-        for (int n = 0; n < NS; ++n) {
-          mw_mix += gpv.Y[n] / P.m.mw_kg[n];
-        }
-        gpv.p = gpv.rho * kRuCgs * mw_mix * gpv.T * kRuConv;
-        gpv.mw_mix = 1. / mw_mix;
-        double cBoilT[NF];
-        {
-          const double RU = kRuCgs * kRuConv;
-          const double PATM = kPatmCgs * kPresConv;
-          const double lp = pmp_log(PATM / gpv.p);
-#pragma unroll
-          for (int spf = 0; spf < NF; ++spf) {
-            const double mw_fuel = P.m.mw_kg[P.f.indx[spf]];
-            const double c = 1. / (lp * RU / (P.f.hboil_ref[spf] * mw_fuel) + 1. / P.f.boilT[spf]);
-            cBoilT[spf] = dmin(P.f.critT[spf], c);
-          }
-        }
-        const int nsub = spray_source_fp64<NS, NF>(P, P.sub_dt, gpv, vel, T, dia, Y, num_ppp, id, cBoilT);
-        my_sub += 1;
-        my_inner += static_cast<unsigned long long>(nsub);
-        const double cur_coef = -P.inv_vol * P.sub_dt / P.flow_dt;
-        if (!in_box(B.src_lo, B.src_hi, ijkc[0], ijkc[1], ijkc[2])) {
-          if (!P.is_ghost || !in_box(B.sr_alo, B.sr_ahi, ijkc[0], ijkc[1], ijkc[2])) {
-            set_err(PMP_ERR_SOURCE_BOX);
-            ok = false;
-            break;
-          }
-        }
-        double* q = B.sr + (long long)(ijkc[0] - B.sr_lo[0]) + (long long)(ijkc[1] - B.sr_lo[1]) * B.sr_js +
-                    (long long)(ijkc[2] - B.sr_lo[2]) * B.sr_ks;
-        if (P.f.mom_trans) {
-#pragma unroll
-          for (int dir = 0; dir < 3; ++dir) {
-            atomicAdd(q + (long long)(P.s_mom + dir) * B.sr_ns, cur_coef * gpv.mom_src[dir]);
-          }
-        }
-        if (P.f.mass_trans) {
-          atomicAdd(q + (long long)P.s_rho * B.sr_ns, cur_coef * gpv.mass_src);
-#pragma unroll
-          for (int spf = 0; spf < NF; ++spf) {
-            atomicAdd(q + (long long)(P.s_spec + spf) * B.sr_ns, cur_coef * gpv.Ydot[spf]);
-          }
-        }
-        atomicAdd(q + (long long)P.s_eng * B.sr_ns, cur_coef * gpv.eng_src);
-        if (P.do_move && !P.f.fixed_parts && id > 0) {
-#pragma unroll
-          for (int dir = 0; dir < 3; ++dir) {
-            pos[dir] += P.sub_dt * vel[dir];
-          }
-          if (B.at_bounds) {
-            if (check_bounds(P, pos, bflags)) {
-              id = -1;
-            } else {
-              impose_wall(P, pos, vel, bflags);
-            }
-          }
-#pragma unroll
-          for (int d = 0; d < 3; ++d) {
-            lx[d] = (pos[d] - P.plo[d]) * P.dxi[d] + 0.5;
-            ijk[d] = static_cast<int>(floor(lx[d]));
-            ijkc[d] = static_cast<int>(floor((pos[d] - P.plo[d]) * P.dxi[d]));
-          }
-        }
-        if (P.is_ghost && !in_box(B.src_lo, B.src_hi, ijkc[0], ijkc[1], ijkc[2])) {
-          id = -1;
-        }
-      }
-      if (ok) {
-        if (P.do_move) {
-#pragma unroll
-          for (int d = 0; d < 3; ++d) {
-            parts.pos[d][s] = pos[d];
-          }
-        }
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          parts.rd[PMP_PSTATE_VEL + d][s] = vel[d];
-        }
-        parts.rd[PMP_PSTATE_T][s] = T;
-        parts.rd[PMP_PSTATE_DIA][s] = dia;
-#pragma unroll
-        for (int spf = 0; spf < NF; ++spf) {
-          parts.rd[PMP_PSTATE_Y + spf][s] = Y[spf];
-        }
-        if (id <= 0) {
-          parts.id[s] = id;
-          my_killed = 1;
-        }
-      }
-    }
+  Counters c;
+  if (s < s_n) {
+    update_one<NS, NF, Form::FP64>(P, sD, sB, b, s, c);
   }
-  const unsigned mask = 0xffffffffu;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    my_sub += __shfl_down_sync(mask, my_sub, o);
-    my_killed += __shfl_down_sync(mask, my_killed, o);
-    my_inner += __shfl_down_sync(mask, my_inner, o);
-  }
-  if ((threadIdx.x & 31) == 0 && (my_sub | my_killed | my_inner)) {
-    atomicAdd(&status->substeps, my_sub);
-    atomicAdd(&status->killed, my_killed);
-    atomicAdd(&status->inner, my_inner);
-  }
+  flush_counters(P, c);
+}
+
+// Loads every instantiation of the kernel (CUDA loads a kernel's code on its
+// first use when modules load lazily, and that load allocates device memory).
+bool load_static_kernels()
+{
+  cudaFuncAttributes a;
+  return cudaFuncGetAttributes(&a, spray_update_fp64_static<3, 1>) == cudaSuccess &&
+         cudaFuncGetAttributes(&a, spray_update_fp64_static<5, 1>) == cudaSuccess &&
+         cudaFuncGetAttributes(&a, spray_update_fp64_static<5, 2>) == cudaSuccess &&
+         cudaFuncGetAttributes(&a, spray_update_fp64_static<4, 1>) == cudaSuccess &&
+         cudaFuncGetAttributes(&a, spray_update_fp64_static<4, 2>) == cudaSuccess;
+}
+
+// elements a view spans, first to last
+long long extent(const pmp_box_view& v)
+{
+  return (long long)(v.hi[0] - v.lo[0]) + (long long)(v.hi[1] - v.lo[1]) * v.jstride +
+         (long long)(v.hi[2] - v.lo[2]) * v.kstride + (long long)(v.ncomp - 1) * v.nstride + 1;
 }
 
 bool covers(const pmp_box_view& v, const int* lo, const int* hi, int need)
@@ -391,12 +220,25 @@ extern "C" int pmp_spray_update_static(
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
     return fail(err, PMP_ERR_NO_DEVICE, "no current CUDA device");
   }
-  // one-time set-up on this device: the array's device address
+  cudaStream_t st = (cudaStream_t)stream;
+  {
+    // synchronous (the status is read back before returning): not capturable
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone) {
+      return fail(err, PMP_ERR_INVALID, "pmp_spray_update_static is synchronous and cannot be captured");
+    }
+  }
+  // one-time set-up on this device: the array's device address, and every
+  // kernel instantiation loaded now (with lazy module loading both would
+  // otherwise allocate device memory at their first use)
   if (!g_scratch_ptr[dev]) {
     void* p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
     if (e != cudaSuccess || !p) {
       return fail(err, PMP_ERR_CUDA, "cudaGetSymbolAddress of the static scratch array failed");
+    }
+    if (!load_static_kernels()) {
+      return fail(err, PMP_ERR_CUDA, "loading the allocation-free kernels failed");
     }
     g_scratch_ptr[dev] = static_cast<StaticScratch*>(p);
   }
@@ -498,6 +340,7 @@ extern "C" int pmp_spray_update_static(
   P.do_move = do_move;
   P.is_ghost = is_ghost;
   P.nboxes = nboxes;
+  P.status = &scr->status;  // device address inside the scratch array
   // per-box table, built on the host stack and copied into the array
   const int need_state = 1 + std::max(std::max(comps->rhoIndx, comps->momIndx + 2),
                                       std::max(comps->utempIndx, comps->specIndx + NS - 1));
@@ -555,6 +398,15 @@ extern "C" int pmp_spray_update_static(
     e.sr_js = source[b].jstride;
     e.sr_ks = source[b].kstride;
     e.sr_ns = source[b].nstride;
+    if (extent(state[b]) >= (1LL << 31) || extent(source[b]) >= (1LL << 31)) {
+      return fail(err, PMP_ERR_INVALID, "a state or source view spans 2^31 elements or more", b);
+    }
+    e.st_j32 = (int)state[b].jstride;
+    e.st_k32 = (int)state[b].kstride;
+    e.st_n32 = (int)state[b].nstride;
+    e.sr_j32 = (int)source[b].jstride;
+    e.sr_k32 = (int)source[b].kstride;
+    e.sr_n32 = (int)source[b].nstride;
     e.at_bounds = at_boundary(boxes[b], *geom);
     for (int d = 0; d < 3; ++d) {
       sb.parts.pos[d] = pp.pos[d];
@@ -572,7 +424,6 @@ extern "C" int pmp_spray_update_static(
     ncta += (int)nb;
   }
   h_prefix[nboxes] = ncta;
-  cudaStream_t st = (cudaStream_t)stream;
   if (cudaMemcpyAsync(scr->boxes, h_boxes, sizeof(StaticBox) * nboxes, cudaMemcpyHostToDevice, st) != cudaSuccess ||
       cudaMemcpyAsync(scr->cta_prefix, h_prefix, sizeof(int) * (nboxes + 1), cudaMemcpyHostToDevice, st) !=
         cudaSuccess ||

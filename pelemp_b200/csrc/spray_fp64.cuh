@@ -628,7 +628,32 @@ __device__ __forceinline__ void set_error(const KParams& P, int code, int box, l
   if (atomicCAS(&P.status->code, 0, code) == 0) {
     P.status->box = box;
     P.status->slot = slot;
+    if (P.err_host) {
+      *reinterpret_cast<volatile int*>(P.err_host) = code;
+    }
   }
+}
+
+// True when a call of the handle failed since the host last cleared the
+// status: the CTA then leaves the droplets as they are, so that the state the
+// host reads after pmp_spray_sync is the failing call's.  CTA-uniform (read
+// once, shared), as the callers end in CTA- or warp-wide operations.
+__device__ __forceinline__ bool cta_call_failed(const KParams& P)
+{
+  __shared__ int s_failed;
+  if (threadIdx.x == 0) {
+    s_failed = *reinterpret_cast<volatile const int*>(&P.status->code);
+  }
+  __syncthreads();
+  return s_failed != 0;
+}
+
+// Append slot s to the call's FP64 fallback list.
+__device__ __forceinline__ void push_fallback(const KParams& P, long long s)
+{
+  const unsigned long long k = atomicAdd(&P.status->fb_count, 1ULL);
+  P.fb_list[k] = s;
+  atomicAdd(&P.status->fallback, 1ULL);
 }
 
 __device__ __forceinline__ bool in_box(const int* lo, const int* hi, int i, int j, int k)

@@ -47,39 +47,40 @@ __device__ __forceinline__ void cell_of(const KParams& P, const double* pos, dou
   }
 }
 
-// Returns false if the droplet was handed to the fallback list (MIXED only).
-// B is box b's entry: the kernel passes a copy in shared memory when the CTA
-// works on one box (read at low latency, without re-deriving addresses), or
-// the global entry otherwise
+// One droplet slot s of box b through the whole call.  D holds the droplet
+// arrays (the library's packed SoA, or a caller's per-box arrays in the
+// allocation-free entry point).  B is box b's entry: the kernel passes a copy
+// in shared memory when the CTA works on one box (read at low latency,
+// without re-deriving addresses), or the global entry otherwise.  A mixed-form
+// droplet below 2 um is left to the fallback list.
 template <int NS, int NF, Form FORM, bool FF = false, bool PELEC = false>
-__device__ __forceinline__ void update_one(const KParams& P, const BoxEntry& B, int b, long long s, Counters& c,
-                                           double* sx = nullptr, int sxs = 0)
+__device__ __forceinline__ void update_one(const KParams& P, const DevParts& D, const BoxEntry& B, int b,
+                                           long long s, Counters& c, double* sx = nullptr, int sxs = 0)
 {
-  int id = P.parts.id[s];
+  int id = D.id[s];
   if (!(id > 0)) {
     return;
   }
-  double dia = P.parts.rd[PMP_PSTATE_DIA][s];
+  double dia = D.rd[PMP_PSTATE_DIA][s];
   if (FORM == Form::MIXED && dia < P.mixed_min_dia) {
     if (!P.fb_pre) {
-      const unsigned long long k = atomicAdd(&P.status->fallback, 1ULL);
-      P.fb_list[k] = s;
+      push_fallback(P, s);
     }
     return;
   }
   double pos[3], vel[3], Y[NF];
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
-    pos[d] = P.parts.pos[d][s];
-    vel[d] = P.parts.rd[PMP_PSTATE_VEL + d][s];
+    pos[d] = D.pos[d][s];
+    vel[d] = D.rd[PMP_PSTATE_VEL + d][s];
   }
-  double T = P.parts.rd[PMP_PSTATE_T][s];
+  double T = D.rd[PMP_PSTATE_T][s];
 #pragma unroll
   for (int spf = 0; spf < NF; ++spf) {
-    Y[spf] = P.parts.rd[PMP_PSTATE_Y + spf][s];
+    Y[spf] = D.rd[PMP_PSTATE_Y + spf][s];
   }
-  const double num_ppp = P.parts.rd[PMP_PSTATE_NUMDENS(NF)][s];
-  const double film = P.parts.rd[PMP_PSTATE_FILMHGHT(NF)][s];
+  const double num_ppp = D.rd[PMP_PSTATE_NUMDENS(NF)][s];
+  const double film = D.rd[PMP_PSTATE_FILMHGHT(NF)][s];
   int bflags[3] = {0, 0, 0};
   bool ok = true;
   if (B.at_bounds) {
@@ -386,24 +387,32 @@ __device__ __forceinline__ void update_one(const KParams& P, const BoxEntry& B, 
     if (P.do_move) {
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
-        P.parts.pos[d][s] = pos[d];
+        D.pos[d][s] = pos[d];
       }
     }
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      P.parts.rd[PMP_PSTATE_VEL + d][s] = vel[d];
+      D.rd[PMP_PSTATE_VEL + d][s] = vel[d];
     }
-    P.parts.rd[PMP_PSTATE_T][s] = T;
-    P.parts.rd[PMP_PSTATE_DIA][s] = dia;
+    D.rd[PMP_PSTATE_T][s] = T;
+    D.rd[PMP_PSTATE_DIA][s] = dia;
 #pragma unroll
     for (int spf = 0; spf < NF; ++spf) {
-      P.parts.rd[PMP_PSTATE_Y + spf][s] = Y[spf];
+      D.rd[PMP_PSTATE_Y + spf][s] = Y[spf];
     }
     if (id <= 0) {
-      P.parts.id[s] = id;
+      D.id[s] = id;
       c.killed += 1;
     }
   }
+}
+
+// update_one over the library's packed droplet arrays
+template <int NS, int NF, Form FORM, bool FF = false, bool PELEC = false>
+__device__ __forceinline__ void update_one(const KParams& P, const BoxEntry& B, int b, long long s, Counters& c,
+                                           double* sx = nullptr, int sxs = 0)
+{
+  update_one<NS, NF, FORM, FF, PELEC>(P, P.parts, B, b, s, c, sx, sxs);
 }
 
 __device__ __forceinline__ void flush_counters(const KParams& P, Counters& c)
@@ -430,16 +439,23 @@ __device__ __forceinline__ void flush_counters(const KParams& P, Counters& c)
                                    with the FP32 gas records and the shared-memory stash) */
 #endif
 
-// copy box b's entry into shared memory (all threads of the CTA call it)
-__device__ __forceinline__ void stage_box(const KParams& P, int b, BoxEntry& sB)
+// Copy box b's entry into shared memory (all threads of the CTA call it).
+// Returns true, for the whole CTA, when a call of the handle failed since the
+// host last cleared the status (cta_call_failed): the CTA then does nothing.
+__device__ __forceinline__ bool stage_box(const KParams& P, int b, BoxEntry& sB)
 {
   static_assert(sizeof(BoxEntry) % 4 == 0, "box entry copied as words");
+  __shared__ int s_failed;
+  if (threadIdx.x == 0) {
+    s_failed = *reinterpret_cast<volatile const int*>(&P.status->code);
+  }
   const int* src = reinterpret_cast<const int*>(P.boxes + b);
   int* dst = reinterpret_cast<int*>(&sB);
   for (int i = threadIdx.x; i < (int)(sizeof(BoxEntry) / 4); i += blockDim.x) {
     dst[i] = src[i];
   }
   __syncthreads();
+  return s_failed != 0;
 }
 
 template <int NS, int NF, int BLOCK>
@@ -447,7 +463,9 @@ __global__ void __launch_bounds__(BLOCK, PMP_FP64_MIN_BLOCKS) spray_update_fp64(
 {
   __shared__ BoxEntry sB;
   const int b = P.cta_box[blockIdx.x];
-  stage_box(P, b, sB);
+  if (stage_box(P, b, sB)) {
+    return;
+  }
   const long long s = P.cta_start[blockIdx.x] + threadIdx.x;
   Counters c;
   if (s < sB.p_end) {
@@ -462,7 +480,9 @@ __global__ void __launch_bounds__(BLOCK, PMP_FP64_MIN_BLOCKS) spray_update_fp64_
 {
   __shared__ BoxEntry sB;
   const int b = P.cta_box[blockIdx.x];
-  stage_box(P, b, sB);
+  if (stage_box(P, b, sB)) {
+    return;
+  }
   const long long s = P.cta_start[blockIdx.x] + threadIdx.x;
   Counters c;
   if (s < sB.p_end) {
@@ -476,7 +496,9 @@ __global__ void __launch_bounds__(BLOCK, PMP_MIXED_MIN_BLOCKS) spray_update_mixe
 {
   __shared__ BoxEntry sB;
   const int b = P.cta_box[blockIdx.x];
-  stage_box(P, b, sB);
+  if (stage_box(P, b, sB)) {
+    return;
+  }
   const long long s = P.cta_start[blockIdx.x] + threadIdx.x;
   Counters c;
   // per thread: position, parcel count, start mass, composition (update_one,
@@ -512,8 +534,7 @@ static __global__ void __launch_bounds__(256) k_select_small(const __grid_consta
 {
   for (long long s = s0 + (long long)blockIdx.x * 256 + threadIdx.x; s < s1; s += (long long)gridDim.x * 256) {
     if (P.parts.id[s] > 0 && P.parts.rd[PMP_PSTATE_DIA][s] < P.mixed_min_dia) {
-      const unsigned long long k = atomicAdd(&P.status->fallback, 1ULL);
-      P.fb_list[k] = s;
+      push_fallback(P, s);
     }
   }
 }
@@ -645,7 +666,10 @@ __global__ void __launch_bounds__(256) k_gas_records64(const __grid_constant__ K
 template <int NS, int NF, int BLOCK, bool PELEC = false>
 __global__ void __launch_bounds__(BLOCK, PMP_FP64_MIN_BLOCKS) spray_update_fp64_list(const __grid_constant__ KParams P)
 {
-  const unsigned long long n = *reinterpret_cast<volatile unsigned long long*>(&P.status->fallback);
+  if (cta_call_failed(P)) {
+    return;
+  }
+  const unsigned long long n = *reinterpret_cast<volatile unsigned long long*>(&P.status->fb_count);
   Counters c;
   for (unsigned long long i = blockIdx.x * (unsigned long long)BLOCK + threadIdx.x; i < n;
        i += (unsigned long long)gridDim.x * BLOCK) {

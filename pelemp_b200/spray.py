@@ -48,6 +48,7 @@ _SIGS = {
     "pmp_spray_set_mode": [C.c_void_p, C.c_int],
     "pmp_spray_set_coupling": [C.c_void_p, C.c_int],
     "pmp_spray_get_coupling": [C.c_void_p, C.POINTER(C.c_int)],
+    "pmp_spray_sync": [C.c_void_p],
     "pmp_spray_last_error": [C.c_void_p, C.POINTER(capi.ErrorInfo)],
     "pmp_spray_get_stats": [C.c_void_p, C.POINTER(capi.Stats)],
     "pmp_spray_version": [],
@@ -270,31 +271,48 @@ class SprayParticleContainer:
         return buf
 
     # --- the update (SprayParticles.cpp:37-87,142-502) --------------------
+    # The C ABI's update calls are stream-ordered (they enqueue and return);
+    # with sync=True (the default here) the mirror then waits for the call
+    # and raises its device error, as the reference's per-box synchronisation
+    # (SprayParticles.cpp:499) would abort.  sync=False leaves the call in
+    # flight: errors and stats come from sync().
     def update_particles(self, state, source, flow_dt, time, state_ghosts, source_ghosts,
-                         is_virt, is_ghost, do_move, spray_cfl_lev, stream=0):
+                         is_virt, is_ghost, do_move, spray_cfl_lev, stream=0, sync=True):
         """state/source: pmp_box_view arrays (device memory)."""
         self._check(lib().pmp_spray_update(
             self._h, state, source, len(state), flow_dt, time, state_ghosts, source_ghosts,
             int(is_virt), int(is_ghost), int(do_move), spray_cfl_lev, C.c_void_p(stream)))
+        if sync:
+            self.sync()
 
     def update_particles_host(self, state, source, flow_dt, time, state_ghosts, source_ghosts,
-                              is_virt, is_ghost, do_move, spray_cfl_lev, stream=0):
+                              is_virt, is_ghost, do_move, spray_cfl_lev, stream=0, sync=True):
         """Same call with host-memory views (copies inside)."""
         self._check(lib().pmp_spray_update_host(
             self._h, state, source, len(state), flow_dt, time, state_ghosts, source_ghosts,
             int(is_virt), int(is_ghost), int(do_move), spray_cfl_lev, C.c_void_p(stream)))
+        if sync:
+            self.sync()
 
     def move_kick_drift(self, state, source, dt, time, is_virt, is_ghost, state_ghosts,
-                        source_ghosts, do_move=True, spray_cfl_lev=-1.0, stream=0):
+                        source_ghosts, do_move=True, spray_cfl_lev=-1.0, stream=0, sync=True):
         self._check(lib().pmp_spray_move_kick_drift(
             self._h, state, source, len(state), dt, time, int(is_virt), int(is_ghost),
             state_ghosts, source_ghosts, int(do_move), spray_cfl_lev, C.c_void_p(stream)))
+        if sync:
+            self.sync()
 
     def move_kick(self, state, source, dt, time, is_virt, is_ghost, state_ghosts, source_ghosts,
-                  spray_cfl_lev=-1.0, stream=0):
+                  spray_cfl_lev=-1.0, stream=0, sync=True):
         self._check(lib().pmp_spray_move_kick(
             self._h, state, source, len(state), dt, time, int(is_virt), int(is_ghost),
             state_ghosts, source_ghosts, spray_cfl_lev, C.c_void_p(stream)))
+        if sync:
+            self.sync()
+
+    def sync(self):
+        """Wait for the enqueued updates; raise SprayError for a device error."""
+        self._check(lib().pmp_spray_sync(self._h))
 
     def last_error(self):
         info = capi.ErrorInfo()

@@ -18,7 +18,7 @@ from tests.parity import droplet_mass, source_errors
 pytestmark = pytest.mark.gpu
 
 CASES = {
-    "config1": dict(n=100_000, steps=3),
+    "config1": dict(n=100_000, steps=10),
     "config2": dict(n=40_000, steps=3, ncells=(32, 32, 32), box=(16, 16, 16)),
     "walls": dict(n=8000),
 }
