@@ -122,6 +122,18 @@ class Oracle(_Base):
     def _couple(self):
         self.lib.pmp_oracle_set_coupling(1 if self.pelec else 0)
 
+    def update_energy(self, prob, mech, fdat, parts, sources, do_move, residual, **kw):
+        """update() that also adds each parcel's energy-identity residual of the
+        call to residual[b][i] (float64 arrays, one per box; PeleLMeX coupling)."""
+        ptrs = (C.c_void_p * len(residual))(*[r.ctypes.data for r in residual])
+        self.lib.pmp_oracle_set_energy_out.restype = None
+        self.lib.pmp_oracle_set_energy_out.argtypes = [C.c_void_p]
+        self.lib.pmp_oracle_set_energy_out(C.cast(ptrs, C.c_void_p))
+        try:
+            return self.update(prob, mech, fdat, parts, sources, do_move, **kw)
+        finally:
+            self.lib.pmp_oracle_set_energy_out(None)
+
     def math(self, fn, x, y=None):
         """fn in ('exp','log','log1p','pow','cbrt') over float64 arrays."""
         code = ("exp", "log", "log1p", "pow", "cbrt").index(fn)

@@ -229,9 +229,30 @@ static void calcVaporState(
 
 /* calculateSpraySource (Drag.H:138-441), PeleLMeX branch (no KE terms).
  * rdata = droplet real components; returns the Reynolds number. */
+/* calculateSpraySource (Drag.H:138-441).
+ *
+ * eres (may be NULL) accumulates the droplet's term of the energy identity of
+ * the explicit scheme (PeleLMeX coupling): the liquid enthalpy change plus the
+ * enthalpy the gas receives equals, per parcel of num_ppp droplets,
+ *   sum_i sum_f [ dM_fi cp_f (T_{i+1} - T_i)                 explicit update
+ *               + (p mdot_fi - dM_fi) L_fi                   composition clip
+ *               + p mdot_fi (L'_fi - L_fi)                   latent heat below boiling
+ *               + dM_fi (h_f(T_i) - h_dep(f)(T_last)) ]      vapour enthalpy at T_last
+ *   + sum_f M_fk L_fk - p conv_k                             kill at step k
+ *   - (nsub / k - 1) sum_{i<=k} p conv_i                     average over k steps
+ * with i the inner sub-steps (part_dt p, droplet temperature T_i, fuel masses
+ * M_fi = m Y_f, their change dM_fi, the evaporation rates mdot_fi that enter
+ * the temperature update, convective heat conv_i), the liquid enthalpy
+ * h_L,f(T) = cp_f (T - ref_T) - latent_f and the latent heat it implies
+ * L_fi = h_f(T_i) - h_L,f(T_i); the temperature update uses L'_fi, the same
+ * expression at min(T_i, 0.99 cBoilT) (Drag.H:79-83); the vapour enthalpy the
+ * gas receives is taken at the last sub-step's droplet temperature T_last
+ * (Drag.H:425-434), the convective heat averaged over nsub (Drag.H:410-413),
+ * and when the droplet dies at sub-step k (Drag.H:401-406) its remaining
+ * mass passes to the gas as vapour with the heat of that sub-step unabsorbed. */
 static double calculateSpraySource(
   const pmp_mech* mech, double flow_dt, gpv_t* gpv, const pmp_spray_data* fdat,
-  double* rdata, int* id, double* cBoilT)
+  double* rdata, int* id, double* cBoilT, double* eres)
 {
   const int NF = fdat->nfuel;
   const int NS = mech->nspec;
@@ -279,6 +300,10 @@ static double calculateSpraySource(
   const double startmass = pmass;
   double Reyn = 0.;
   double part_vel_src[3];
+  /* energy identity terms (eres) */
+  double e_expl = 0., e_clip = 0., e_lat = 0., e_vap = 0., e_kill = 0., e_conv = 0.;
+  double dM_tot[PMP_MAX_FUEL] = {0.0};
+  int nsub_first = 1, k_kill = 0;
   while (isub <= nsub) {
     double cp_part = 0.;
     double Tboil = 0.;
@@ -372,6 +397,8 @@ static double calculateSpraySource(
 
     double part_temp_src = 0.;
     double m_dot = 0.;
+    double conv_i = 0.;                    /* this sub-step's convective heat */
+    double mL[PMP_MAX_FUEL] = {0.0};      /* the rates in its temperature update */
     if (fdat->mass_trans) {
       const double Pr_skin = mu_skin * cp_skin / lambda_skin;
       const double powR = dmax(PMP_POW(dmin(400., Reyn), 0.077), 1.);
@@ -406,12 +433,14 @@ static double calculateSpraySource(
             mi_dot[spf] = -dmax(Ddiag[fspec] * mdotcoeff, 0.);
             m_dot += mi_dot[spf];
             sumL += mi_dot[spf] * L_fuel[spf];
+            mL[spf] = mi_dot[spf];
           }
         }
       } else {
         Nu_num = Nu_0;
       }
       const double conv_src = PMP_PI * lambda_skin * dia_part * delT * Nu_num;
+      conv_i = conv_src;
       gpv->fluid_eng_src += num_ppp * conv_src;
       part_temp_src = (sumL + conv_src) * inv_pmass / cp_part;
       if (isub == 1 && delT > C_eps) {
@@ -424,6 +453,7 @@ static double calculateSpraySource(
     }
     if (isub == 1) {
       dt = flow_dt / (double)nsub;
+      nsub_first = nsub;
     }
     const double part_dt = fdat->dtmod * dt;
     if (!fdat->fixed_parts) {
@@ -431,9 +461,17 @@ static double calculateSpraySource(
         vel_part[d] += part_dt * part_vel_src[d];
       }
     }
+    /* the sub-step's start state, for the energy identity */
+    const double T_i = T_part;
+    const double pm_i = pmass;
+    double Y_i[PMP_MAX_FUEL];
+    for (int spf = 0; spf < NF; ++spf) {
+      Y_i[spf] = Y_part[spf];
+    }
     if (fdat->mass_trans) {
       const double newT = T_part + part_dt * part_temp_src;
       const double new_mass = pmass + m_dot * part_dt;
+      e_conv += part_dt * conv_i;
       if (new_mass > min_mass && newT < Tboil) {
         T_part = newT;
         if (NF > 1) {
@@ -457,7 +495,29 @@ static double calculateSpraySource(
         }
         pmass = new_mass;
         dia_part = PMP_CBRT(6. * pmass / (PMP_PI * rho_part));
+        if (eres) {
+          for (int spf = 0; spf < NF; ++spf) {
+            const double dM = pmass * Y_part[spf] - pm_i * Y_i[spf];
+            const double L = h_part[fdat->indx[spf]] + fdat->latent[spf] - fdat->cp[spf] * (T_i - fdat->ref_T);
+            e_expl += dM * fdat->cp[spf] * (T_part - T_i);
+            e_clip += (part_dt * mL[spf] - dM) * L;
+            e_lat += part_dt * mL[spf] * (L_fuel[spf] - L);
+            e_vap += dM * h_part[fdat->indx[spf]];
+            dM_tot[spf] += dM;
+          }
+        }
       } else {
+        if (eres) {
+          for (int spf = 0; spf < NF; ++spf) {
+            const double M = pm_i * Y_i[spf];
+            const double L = h_part[fdat->indx[spf]] + fdat->latent[spf] - fdat->cp[spf] * (T_i - fdat->ref_T);
+            e_vap -= M * h_part[fdat->indx[spf]];
+            dM_tot[spf] -= M;
+            e_kill += M * L;
+          }
+          e_kill -= part_dt * conv_i;
+          k_kill = isub;
+        }
         pmass = 0.;
         *id = -1;
         nsub = isub;
@@ -465,6 +525,14 @@ static double calculateSpraySource(
       }
     }
     ++isub;
+  }
+  if (eres && fdat->mass_trans) {
+    /* the gas receives the vapour at the last sub-step's enthalpies */
+    for (int spf = 0; spf < NF; ++spf) {
+      e_vap -= dM_tot[spf] * h_part[fdat->dep_indx[spf]];
+    }
+    const double avg = k_kill > 0 ? -((double)nsub_first / (double)k_kill - 1.) * e_conv : 0.;
+    *eres += num_ppp * (e_expl + e_clip + e_lat + e_vap + e_kill + avg);
   }
   if (nsub > 1) {
     gpv->fluid_eng_src /= (double)nsub;
@@ -663,7 +731,8 @@ static inline void dep(const ctx_t* c, double* p, double v)
 
 /* The per-droplet body of updateParticles (SprayParticles.cpp:324-481).
  * Returns 0 or an error code. */
-static int update_droplet(const ctx_t* c, double* pos, double* rdata, int* id, long long* nsubsteps)
+static int update_droplet(const ctx_t* c, double* pos, double* rdata, int* id, long long* nsubsteps,
+                          double* eres)
 {
   const pmp_spray_data* fdat = c->fdat;
   const pmp_geometry* g = c->geom;
@@ -739,7 +808,7 @@ static int update_droplet(const ctx_t* c, double* pos, double* rdata, int* id, l
     }
     gpv_define(&gpv, NS);
     calcBoilT(fdat, &gpv, cBoilT);
-    calculateSpraySource(c->mech, c->sub_dt, &gpv, fdat, rdata, id, cBoilT);
+    calculateSpraySource(c->mech, c->sub_dt, &gpv, fdat, rdata, id, cBoilT, eres);
     if (nsubsteps) {
       *nsubsteps += 1;
     }
@@ -793,6 +862,10 @@ static int update_droplet(const ctx_t* c, double* pos, double* rdata, int* id, l
   }
   return 0;
 }
+
+static double** eres_box = NULL;
+
+void pmp_oracle_set_energy_out(double** per_box) { eres_box = per_box; }
 
 int pmp_oracle_update(
   const pmp_mech* mech, const pmp_spray_data* fdat,
@@ -872,7 +945,7 @@ int pmp_oracle_update(
       }
       int id = P->id[i];
       long long ns = 0;
-      const int rc = update_droplet(&c, pos, rd, &id, &ns);
+      const int rc = update_droplet(&c, pos, rd, &id, &ns, eres_box ? eres_box[b] + i : NULL);
       nsubs += ns;
       if (rc != 0) {
 #ifdef _OPENMP
@@ -937,7 +1010,7 @@ double pmp_oracle_droplet_source(
   }
   gpv_define(&gpv, NS);
   calcBoilT(fdat, &gpv, cBoilT);
-  const double re = calculateSpraySource(mech, flow_dt, &gpv, fdat, rdata, id, cBoilT);
+  const double re = calculateSpraySource(mech, flow_dt, &gpv, fdat, rdata, id, cBoilT, NULL);
   for (int d = 0; d < 3; ++d) {
     src[d] = gpv.fluid_mom_src[d];
   }

@@ -64,6 +64,17 @@ int pmp_oracle_update(
   double spray_cfl_lev, int nthreads, pmp_error_info* err,
   long long* substeps);
 
+/* Energy identity of the explicit scheme (PeleLMeX coupling): when per_box
+ * is not NULL, every following pmp_oracle_update adds to per_box[b][i] the
+ * parcel's residual of  (liquid enthalpy change) + (enthalpy received by the
+ * gas)  for droplet i of box b, summed over the call's sub-cycles, as the
+ * named terms of calculateSpraySource's comment in spray_oracle.c (the
+ * explicit update, the composition clip, the latent heat taken below the
+ * boiling temperature, the vapour enthalpy taken at the last sub-step, a
+ * droplet's death, the average over the sub-steps).  NULL
+ * switches it off. */
+void pmp_oracle_set_energy_out(double** per_box);
+
 /* One evaluation of calculateSpraySource for a single droplet against a
  * given interpolated gas state (unit-level hook for the tests).
  * rdata: the droplet's real components (updated in place); gas: rho, T,

@@ -90,8 +90,17 @@ def build_driver(force=False):
     return DRIVER
 
 
+# The reference's spray sources, for the reference build under oracle/_ref
+# (test infrastructure): PMP_REFERENCE_SRC, else the read-only checkout this
+# build recipe compiles them from when it is present.
+REFERENCE_SRC = os.environ.get("PMP_REFERENCE_SRC", "/root/reference/Source/PP_Spray")
+
+
 def build_oracle():
-    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
+    cmd = ["make", "-s", "-C", os.path.join(ROOT, "oracle")]
+    if os.path.exists(os.path.join(REFERENCE_SRC, "Drag.H")):
+        cmd.append("REF_DIR=" + REFERENCE_SRC)
+    subprocess.run(cmd, check=True)
 
 
 def main(argv):

@@ -87,3 +87,21 @@ def assert_bitwise(pa, pb):
             if not np.array_equal(a[k], b[k]):
                 diff = np.nonzero(~np.all(a[k] == b[k], axis=0) if a[k].ndim > 1 else a[k] != b[k])[0]
                 raise AssertionError(f"{k} differs at {diff[:10]} (of {diff.size})")
+
+
+def oracle_energy_residual(oracle, prob, steps):
+    """The oracle's run with the energy-identity residual of every parcel:
+    returns (fdat, parts, sources per call, residual per box)."""
+    mech = oracle.mech(prob.species)
+    rc, fdat = oracle.setup(prob, mech)
+    assert rc == 0
+    parts = prob.copy_parts()
+    res = [np.zeros(p["id"].size) for p in parts]
+    srcs = []
+    for _ in range(steps):
+        for do_move in (1, 0):
+            src = prob.new_sources()
+            rc, err, _ = oracle.update_energy(prob, mech, fdat, parts, src, do_move, res)
+            assert rc == 0, (rc, err.message)
+            srcs.append(src)
+    return fdat, parts, srcs, res

@@ -75,3 +75,42 @@ def droplet_mass(prob, parts, rho_l):
         m = np.where(p["id"] > 0, m, 0.0)
         out.append(m * p["rdata"][capi.pstate_numdens(nf)])
     return out
+
+
+def liquid_enthalpy(prob, fdat, parts, rho_l):
+    """Sum over live droplets of N m h_L, h_L = sum_f Y_f (cp_f (T - ref_T) - latent_f)
+    (the liquid enthalpy the scheme's latent heat implies: L_f = h_f - h_L,f)."""
+    nf = prob.nfuel
+    masses = droplet_mass(prob, parts, rho_l)  # N m, zero for dead droplets
+    total = 0.0
+    for p, m in zip(parts, masses):
+        Y = p["rdata"][capi.PSTATE_Y:capi.PSTATE_Y + nf]
+        T = p["rdata"][capi.PSTATE_T]
+        hL = np.zeros_like(T)
+        for f in range(nf):
+            hL += Y[f] * (fdat.cp[f] * (T - fdat.ref_T) - fdat.latent[f])
+        total += float(np.sum(m * hL))
+    return total
+
+
+def gas_enthalpy_gain(prob, fdat, calls):
+    """Enthalpy the gas receives from the energy deposits of the given calls
+    (each call's source times cell volume times dtmod * flow_dt), and the same
+    sum of magnitudes (the scale of the exchange)."""
+    vol = float(np.prod(prob.dx))
+    c = prob.comps().engSrcIndx
+    gain, scale = 0.0, 0.0
+    for call in calls:
+        for s in call:
+            gain += float(np.sum(s[c])) * vol * fdat.dtmod * prob.flow_dt
+            scale += float(np.sum(np.abs(s[c]))) * vol * fdat.dtmod * prob.flow_dt
+    return gain, scale
+
+
+def energy_identity(prob, fdat, parts0, parts1, calls, residual, rho_l):
+    """(liquid enthalpy change + gas enthalpy gain - sum of the scheme's
+    residual terms) / exchange scale, and the residual / scale."""
+    dH = liquid_enthalpy(prob, fdat, parts1, rho_l) - liquid_enthalpy(prob, fdat, parts0, rho_l)
+    G, scale = gas_enthalpy_gain(prob, fdat, calls)
+    R = float(sum(np.sum(r) for r in residual))
+    return (dH + G - R) / scale, R / scale

@@ -274,3 +274,21 @@ def test_learned_faster_than_fp64(trained):
     print("MK of 2M droplets: FP64 %.3f ms, learned %.3f ms, speed-up %.2f" % (
         times[0], times[2], times[0] / times[2]))
     assert times[2] < times[0]
+
+
+def test_learned_energy_identity(trained, oracle):
+    """Global energy drift of the learned form against the FP64 scheme's
+    energy residual: within 5e-3 of the enthalpy exchanged (the surrogate's
+    heat and mass transfer errors enter the exchange itself)."""
+    from tests.gpu_util import oracle_energy_residual
+    from tests.parity import energy_identity
+    w, _ = trained
+    prob = W.config2(n=40_000, seed=0, **SMALL)
+    rho_l = [W.LIQUIDS[f]["rho"] for f in prob.fuels]
+    fdat, _, _, res = oracle_energy_residual(oracle, prob, prob.steps)
+    pg, sg, sp = gpu_run(prob, prob.steps, mode=capi.PMP_MODE_LEARNED,
+                         setup=lambda s: s.set_learn_weights(w))
+    err, rel = energy_identity(prob, fdat, prob.parts, pg, sg, res, rho_l)
+    print(f"learned energy drift {err:.2e} of the exchange (FP64 scheme residual {rel:.2e})")
+    assert abs(err) <= 5e-3
+    sp.close()

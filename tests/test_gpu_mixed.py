@@ -113,3 +113,20 @@ def test_mixed_graph_and_side_stream_match_plain_launch(oracle):
     for b, idx in enumerate(small):
         for k in ("pos", "rdata", "id"):
             assert np.array_equal(pa[b][k][..., idx], po[b][k][..., idx]), (b, k)
+
+
+def test_mixed_energy_identity(oracle):
+    """Global energy drift of the mixed form: its liquid enthalpy change plus
+    the enthalpy its deposits give the gas, against the FP64 scheme's residual
+    (the oracle's): within 1e-5 of the enthalpy exchanged (the FP64 form closes
+    it to round-off)."""
+    from tests.gpu_util import oracle_energy_residual
+    from tests.parity import energy_identity
+    prob = W.config2(n=40_000, steps=3, ncells=(32, 32, 32), box=(16, 16, 16))
+    rho_l = [W.LIQUIDS[f]["rho"] for f in prob.fuels]
+    fdat, _, _, res = oracle_energy_residual(oracle, prob, prob.steps)
+    pg, sg, sp = gpu_run(prob, prob.steps, mode=capi.PMP_MODE_MIXED)
+    err, rel = energy_identity(prob, fdat, prob.parts, pg, sg, res, rho_l)
+    print(f"mixed energy drift {err:.2e} of the exchange (FP64 scheme residual {rel:.2e})")
+    assert abs(err) <= 1e-5
+    sp.close()

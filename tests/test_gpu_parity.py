@@ -13,7 +13,7 @@ from pelemp_b200 import capi
 from pelemp_b200 import workloads as W
 from pelemp_b200.spray import SprayError, from_problem, views
 from tests.gpu_util import assert_bitwise, device_sources, device_state, gpu_run, oracle_run
-from tests.parity import droplet_mass, source_errors
+from tests.parity import assert_parts_close, droplet_mass, source_errors
 
 pytestmark = pytest.mark.gpu
 
@@ -180,3 +180,54 @@ def test_full_size_config2_sampled_parity_and_mass(oracle):
     for b, sel in enumerate(picks):
         for k in ("pos", "rdata", "id"):
             assert np.array_equal(pg[b][k][..., sel], po[b][k]), (b, k)
+
+
+@pytest.mark.parametrize("case", ["config1_n400", "config2_n400", "walls_n400"])
+def test_fp64_vs_reference_golden(case):
+    """The FP64 kernel against the reference build's committed outputs
+    (tests/golden): the kernel runs the project math library, the reference
+    the C library's, so droplets agree within the FP64 tolerances of
+    tests/parity.py and deposits, (m_new - m_old)/dt differences, within 1e-9
+    of the largest."""
+    import os
+    from oracle.pyoracle import Oracle
+    from tests.golden import make_golden as G
+    g = np.load(os.path.join(os.path.dirname(G.__file__), case + ".npz"))
+    prob, _ = G.problem(case, Oracle(libm=True).mech)
+    assert str(g["input_sha256"]) == G.input_digest(prob)
+    pg, sg, sp = gpu_run(prob, prob.steps)
+    gold_parts = [{k: g[f"b{b}_{k}"] for k in ("pos", "rdata", "id")} for b in range(len(prob.boxes))]
+    assert_parts_close(pg, gold_parts, prob.nfuel, prob.dx)
+    gold = G.unpack_sources(g, prob, int(g["ncalls"]))
+    for a, b in zip(sg, gold):
+        assert source_errors(b, a) <= 1e-9
+    sp.close()
+
+
+@pytest.mark.parametrize("name", ["config1", "config2", "kills"])
+def test_fp64_energy_identity(name, oracle):
+    """Global liquid + gas energy: the GPU's liquid enthalpy change plus the
+    enthalpy its deposits give the gas equals the explicit scheme's residual
+    (summed over the droplets by the oracle, Drag.H:345-434) to round-off;
+    the mass balance closes exactly (liquid loss == gas gain)."""
+    from tests.gpu_util import oracle_energy_residual
+    from tests.parity import energy_identity
+    if name == "kills":
+        prob = W.config1(n=20_000, steps=2)
+        prob.parts[0]["rdata"][capi.PSTATE_DIA, ::5] = 0.75e-6
+    elif name == "config1":
+        prob = W.config1(n=100_000, steps=3)
+    else:
+        prob = W.config2(n=40_000, steps=3, ncells=(32, 32, 32), box=(16, 16, 16))
+    rho_l = [W.LIQUIDS[f]["rho"] for f in prob.fuels]
+    fdat, _, _, res = oracle_energy_residual(oracle, prob, prob.steps)
+    pg, sg, sp = gpu_run(prob, prob.steps)
+    err, rel = energy_identity(prob, fdat, prob.parts, pg, sg, res, rho_l)
+    print(f"{name}: FP64 energy identity {err:.2e} of the exchange (scheme residual {rel:.2e})")
+    assert abs(err) <= 1e-10
+    m0 = sum(float(np.sum(m)) for m in droplet_mass(prob, prob.parts, rho_l))
+    m1 = sum(float(np.sum(m)) for m in droplet_mass(prob, pg, rho_l))
+    vol = float(np.prod(prob.dx))
+    gas = sum(float(np.sum(s[prob.comps().rhoSrcIndx])) for call in sg for s in call) * vol * fdat.dtmod * prob.flow_dt
+    assert abs(gas + (m1 - m0)) <= 1e-10 * abs(m1 - m0)
+    sp.close()

@@ -4,7 +4,9 @@
   SprayInterpolation.H / WallFunctions.H compiled here (oracle/_ref), bit for
   bit, on the configured workloads and on the error paths;
 * oracle with the project math library within the FP64 tolerance of it;
-* oracle against the committed golden vectors (tests/golden);
+* oracle built with the C library's math == the committed golden vectors
+  (tests/golden, made by the reference build with tests/golden/make_golden.py),
+  bit for bit, so the pin holds where the reference sources are absent;
 * known answers: Stokes drag, saturated gas, kill below min_mass, boiling
   temperature at 1 atm, latent-heat adjustment of spraySetup;
 * mass conservation of the deposits.
@@ -265,3 +267,67 @@ def test_mass_conservation_identity(oracle):
         # species: the fuel deposit equals the mass deposit (single-species liquid pieces)
         fuel = sum(float(np.sum(s[4] + s[5])) for s in src)
         assert abs(fuel - sum(float(np.sum(s[3])) for s in src)) <= 1e-9 * abs(fuel)
+
+
+@pytest.mark.parametrize("case", ["config1_n400", "config2_n400", "walls_n400", "pelec_config1_n400"])
+def test_oracle_libm_matches_golden(case):
+    """The libm oracle reproduces the reference build's committed outputs bit for bit."""
+    import os
+    from oracle.pyoracle import Oracle
+    from tests.golden import make_golden as G
+    g = np.load(os.path.join(os.path.dirname(G.__file__), case + ".npz"))
+    pelec = G.CASES[case][2]
+    orc = Oracle(libm=True, pelec=pelec)
+    prob, _ = G.problem(case, orc.mech)
+    assert str(g["input_sha256"]) == G.input_digest(prob), "workload generator changed"
+    mech = orc.mech(prob.species)
+    rc, fdat = orc.setup(prob, mech)
+    assert rc == 0
+    parts, calls = G.run(orc, prob, mech, fdat)
+    for b, p in enumerate(parts):
+        for k in ("pos", "rdata", "id"):
+            assert np.array_equal(p[k], g[f"b{b}_{k}"]), (b, k)
+    gold = G.unpack_sources(g, prob, int(g["ncalls"]))
+    assert len(gold) == len(calls)
+    for a, b in zip(calls, gold):
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y)
+
+
+def _energy_run(orc, prob, steps):
+    mech = orc.mech(prob.species)
+    rc, fdat = orc.setup(prob, mech)
+    assert rc == 0
+    parts = prob.copy_parts()
+    res = [np.zeros(p["id"].size) for p in parts]
+    calls = []
+    for _ in range(steps):
+        for do_move in (1, 0):
+            src = prob.new_sources()
+            rc, err, _ = orc.update_energy(prob, mech, fdat, parts, src, do_move, res)
+            assert rc == 0, err.message
+            calls.append(src)
+    return fdat, parts, calls, res
+
+
+@pytest.mark.parametrize("name", ["config1", "config2", "kills"])
+def test_energy_identity_of_the_explicit_scheme(name, oracle):
+    """Liquid enthalpy change + gas enthalpy gain == the sum of the scheme's
+    named residual terms (explicit update, composition clip, vapour enthalpy at
+    the last sub-step, droplet death, average over the sub-steps), to
+    round-off of the exchanged enthalpy; PeleLMeX coupling, periodic domain."""
+    from tests.parity import energy_identity
+    if name == "kills":
+        prob = W.config1(n=3000, steps=2)
+        # a fifth of the droplets near min_mass (1e-16 kg): they die in the call
+        p = prob.parts[0]
+        p["rdata"][capi.PSTATE_DIA, ::5] = 0.75e-6
+    else:
+        prob = W.CONFIGS[name](**SMALL[name])
+    rho_l = [W.LIQUIDS[f]["rho"] for f in prob.fuels]
+    fdat, parts, calls, res = _energy_run(oracle, prob, prob.steps)
+    err, rel_res = energy_identity(prob, fdat, prob.parts, parts, calls, res, rho_l)
+    print(f"{name}: energy identity closes to {err:.2e} of the exchange; scheme residual {rel_res:.2e}")
+    assert abs(err) <= 1e-10
+    if name == "kills":
+        assert sum(int(np.sum(q["id"] <= 0)) for q in parts) > 0
