@@ -274,6 +274,29 @@ KERNEL = {"fp64": "spray_update_fp64<5,2,128>", "mixed": "spray_update_mixed<5,2
 # and learned kernels, whose gathers read the FP32 gas records (written by a
 # separate pass) instead of the FP64 state.
 DRAM_BYTES_PER_DROPLET = {"fp64": 278.4, "mixed": 143.4, "learned": 133.2}
+# Thread-level instructions per droplet-substep on the FP64, FMA (FP32) and
+# XU (transcendental) pipes of one config-2 MKD launch of each form, from the
+# ncu instruction counts of a 2M-droplet launch (sm__inst_executed_pipe_*,
+# warp instructions x 32 / droplet-substeps); with the live throughput and
+# the measured pipe peaks they give the compute roofline.
+PIPE_INSTR_PER_SUBSTEP = {}
+
+
+def compute_roofline(form, substeps_per_s, peaks):
+    """Achieved instruction rate of each pipe / its measured peak for the
+    form's update kernel (None where the instruction counts are not known)."""
+    if peaks is None:
+        return None
+    out = {"peaks": peaks, "peaks_source": "pmp_measure_peaks: loop kernels of independent DFMA, FFMA and "
+                                            "ex2.approx on this GPU, best of three launches"}
+    counts = PIPE_INSTR_PER_SUBSTEP.get(form)
+    if counts:
+        rates = {"fp64": 0.5e12 * peaks["fp64_tflops"], "fma": 0.5e12 * peaks["fp32_tflops"],
+                 "xu": 1e9 * peaks["sfu_gops"]}
+        out["pipes"] = {k: {"instr_per_substep": counts[k], "achieved_per_s": counts[k] * substeps_per_s,
+                            "peak_per_s": rates[k], "frac": counts[k] * substeps_per_s / rates[k]}
+                        for k in rates if k in counts}
+    return out
 
 
 def train_surrogate(sp, prob, st_v, stream, args):
@@ -287,25 +310,72 @@ def train_surrogate(sp, prob, st_v, stream, args):
 
 
 def droplet_errors(pa, pb, prob):
-    """Per-droplet relative errors of T and liquid mass (d^3 / sum(Y/rho_l)) of pa vs pb."""
+    """Per-droplet relative errors of pa vs pb: temperature, diameter, liquid mass
+    (d^3 / sum(Y/rho_l)) and velocity (|du| / max(|u|, 1 m/s))."""
     from pelemp_b200 import workloads as W
     nfuel = prob.nfuel
     rho = np.array([W.LIQUIDS[f]["rho"] for f in prob.fuels])
-    eT, em = [], []
+    e = {"T": [], "dia": [], "mass": [], "vel": []}
     for a, b in zip(pa, pb):
         al = (a["id"] > 0) & (b["id"] > 0)
         ra, rb = a["rdata"][:, al], b["rdata"][:, al]
-        eT.append(np.abs(ra[3] / rb[3] - 1))
+        e["T"].append(np.abs(ra[3] / rb[3] - 1))
+        e["dia"].append(np.abs(ra[4] / rb[4] - 1))
 
         def mass(r):
             return r[4] ** 3 / np.sum(r[5:5 + nfuel] / rho[:, None], axis=0)
-        em.append(np.abs(mass(ra) / mass(rb) - 1))
-    eT, em = np.concatenate(eT), np.concatenate(em)
+        e["mass"].append(np.abs(mass(ra) / mass(rb) - 1))
+        speed = np.maximum(np.sqrt(np.sum(rb[0:3] ** 2, axis=0)), 1.0)
+        e["vel"].append(np.sqrt(np.sum((ra[0:3] - rb[0:3]) ** 2, axis=0)) / speed)
 
-    def q(e):
-        return {"rms": float(np.sqrt(np.mean(e ** 2))), "p99_9": float(np.quantile(e, 0.999)),
-                "max": float(e.max())}
-    return {"T": q(eT), "mass": q(em), "droplets": int(eT.size)}
+    def q(v):
+        v = np.concatenate(v)
+        return {"rms": float(np.sqrt(np.mean(v ** 2))), "p99_9": float(np.quantile(v, 0.999)),
+                "max": float(v.max())}
+    out = {k: q(v) for k, v in e.items()}
+    out["droplets"] = int(sum(x.size for x in e["T"]))
+    return out
+
+
+def deposit_errors(sa, sb, prob):
+    """Per source component (momentum, density, fuel species, energy): the
+    largest |sa - sb| over the cells as a fraction of the largest |sb|."""
+    c = prob.comps()
+    names = {c.momSrcIndx + d: "mom_" + "xyz"[d] for d in range(3)}
+    names[c.rhoSrcIndx] = "mass"
+    names[c.engSrcIndx] = "energy"
+    for f in range(prob.nfuel):
+        names[c.specSrcIndx + f] = "species_" + prob.fuels[f]
+    out = {}
+    for k, name in names.items():
+        scale = float(np.max(np.abs(sb[k])))
+        out[name] = float(np.max(np.abs(sa[k] - sb[k]))) / scale if scale > 0 else 0.0
+    return out
+
+
+def step_balance(prob, fdat, p0, p1, src, rho_l):
+    """Liquid + gas balances of one step of the droplets of one box (p0 -> p1,
+    deposits src): mass (gas gain + liquid change) / |liquid change|, and the
+    liquid enthalpy change plus the enthalpy the gas receives, over the sum of
+    the exchanged magnitudes (the explicit scheme's own energy residual: not
+    zero by construction, the FP64 form's value is the reference)."""
+    nf = prob.nfuel
+    c = prob.comps()
+    vol = float(np.prod(prob.dx))
+    tau = fdat.dtmod * prob.flow_dt
+
+    def liquid(p):
+        Y = p["rdata"][5:5 + nf]
+        m = np.pi / 6 * p["rdata"][4] ** 3 / np.sum(Y / np.asarray(rho_l)[:, None], axis=0)
+        m = np.where(p["id"] > 0, m, 0.0) * p["rdata"][5 + nf]
+        hL = sum(Y[f] * (fdat.cp[f] * (p["rdata"][3] - fdat.ref_T) - fdat.latent[f]) for f in range(nf))
+        return float(np.sum(m)), float(np.sum(m * hL))
+    m0, h0 = liquid(p0)
+    m1, h1 = liquid(p1)
+    gas_m = float(np.sum(src[c.rhoSrcIndx])) * vol * tau
+    gas_e = float(np.sum(src[c.engSrcIndx])) * vol * tau
+    scale_e = float(np.sum(np.abs(src[c.engSrcIndx]))) * vol * tau
+    return {"mass": (gas_m + m1 - m0) / abs(m1 - m0), "energy": (gas_e + h1 - h0) / scale_e}
 
 
 def bench_batched(args, world, rank, local, pg):
@@ -440,6 +510,9 @@ def main():
     ap.add_argument("--workload", default="config2", choices=["config2", "config3", "config4", "config5"],
                     help="config2 (default): the headline; config3: batched FP64 launch shapes; "
                          "config4 / config5: config-1 distributions at 32M / 16M droplets")
+    ap.add_argument("--mesh", type=int, default=0,
+                    help="config2 only: cells per side of a smaller cubic mesh (boxes of half that), "
+                         "keeping droplets per cell at a given --droplets (profiling captures)")
     ap.add_argument("--e2e-steps", type=int, default=6)
     ap.add_argument("--cpu-sample", type=int, default=0,
                     help="droplets per CPU step (0: sized for --cpu-seconds per step)")
@@ -482,7 +555,11 @@ def main():
     forms = [f for f in args.forms.split(",") if f]
     ndrop = args.droplets or {"config2": 16_000_000, "config4": 32_000_000,
                               "config5": 16_000_000}[args.workload]
-    prob = W.CONFIGS[args.workload](n=ndrop, seed=rank, steps=args.steps)
+    if args.mesh and args.workload == "config2":
+        m = args.mesh
+        prob = W.config2(n=ndrop, seed=rank, steps=args.steps, ncells=(m, m, m), box=(m // 2, m // 2, m // 2))
+    else:
+        prob = W.CONFIGS[args.workload](n=ndrop, seed=rank, steps=args.steps)
     nboxes = len(prob.boxes)
     ncells = int(np.prod([prob.domain_hi[d] - prob.domain_lo[d] + 1 for d in range(3)]))
     stream = torch.cuda.current_stream()
@@ -492,6 +569,7 @@ def main():
     src_v = views(src, [prob.grown(b, prob.source_ghosts)[0] for b in range(nboxes)])
     peak, peak_src = measured_peaks()
     graphs = {}
+    balance = {}
 
     def step(sp, st_handle):
         """One step, stream-ordered: zero the sources, MKD, MK (no host wait)."""
@@ -564,6 +642,14 @@ def main():
                                                           args.steps)
         c = sampler.stop()
         graphs[form] = graph
+        # one more step, waited for, on which the balances and deposits are
+        # compared (the droplets of box 0; every form takes the same steps)
+        sp.sync()
+        b0_before = sp.get_particles(0) if rank == 0 else None
+        step(sp, stream.cuda_stream)
+        sp.sync()
+        if rank == 0:
+            balance[form] = (b0_before, sp.get_particles(0), src[0].cpu().numpy())
         info.update({"value": sub_total / (t_max * 1e-3), "ms_per_step": t_max / args.steps,
                      "ms_per_step_eager": t_eager / args.steps,
                      "timed": "whole-step CUDA graph replays" if graph is not None else "eager steps",
@@ -581,11 +667,27 @@ def main():
     # oracle): every form advanced the same initial droplets by warmup + steps steps
     accuracy = {}
     if "fp64" in containers and rank == 0:
-        ref = [containers["fp64"].get_particles(0)]
+        ref = [balance["fp64"][1]]
+        fd = containers["fp64"].spray_data()
+        rho_l = [W.LIQUIDS[f]["rho"] for f in prob.fuels]
+        bal = {f: step_balance(prob, fd, balance[f][0], balance[f][1], balance[f][2], rho_l) for f in forms}
         for f in fast:
-            accuracy[f] = droplet_errors([containers[f].get_particles(0)], ref, prob)
-        accuracy["steps"] = args.warmup + args.steps * (1 if args.no_graph else 2)
+            accuracy[f] = droplet_errors([balance[f][1]], ref, prob)
+            accuracy[f]["deposits_last_step"] = deposit_errors(balance[f][2], balance["fp64"][2], prob)
+            accuracy[f]["mass_balance_last_step"] = bal[f]["mass"]
+            accuracy[f]["energy_drift_vs_fp64"] = bal[f]["energy"] - bal["fp64"]["energy"]
+        accuracy["fp64_balance_last_step"] = bal["fp64"]
+        accuracy["steps"] = args.warmup + args.steps * (1 if args.no_graph else 2) + 1
+        accuracy["what"] = ("box 0's droplets after all steps against the FP64 form (bit-identical to the FP64 "
+                            "oracle); deposits and balances of the last step; energy drift: the form's "
+                            "(liquid enthalpy change + gas gain) / exchanged enthalpy minus the FP64 form's")
 
+    peaks_c = None
+    try:
+        from pelemp_b200.spray import measure_peaks
+        peaks_c = measure_peaks(local)
+    except Exception as e:  # noqa: BLE001 -- reported, not fatal
+        print("measure_peaks:", e, file=sys.stderr)
     # roofline of the headline form's MKD launch (algorithmic bytes / launch time)
     mkd_bytes = algorithmic_bytes(prob.n_droplets, prob.nfuel, prob.nspec, ncells, True)
     achieved = mkd_bytes / (results[head]["mkd_launch_ms"] * 1e-3) / 1e9
@@ -666,7 +768,10 @@ def main():
             "dtype": {"fp64": "f64", "mixed": "f32 physics, f64 state/deposits",
                       "learned": "bf16 MLP (f32 accumulate), f32 physics, f64 state/deposits"}[head],
             "data": "synthetic (seeded, numpy PCG64)",
-            "config": {"workload": WORKLOAD_TEXT[args.workload].format(n=prob.n_droplets / 1e6),
+            "config": {"workload": (WORKLOAD_TEXT[args.workload].format(n=prob.n_droplets / 1e6) if not args.mesh
+                                    else WORKLOAD_TEXT[args.workload].format(n=prob.n_droplets / 1e6).replace(
+                                        "128^3 mesh as 8 boxes of 64^3",
+                                        f"{args.mesh}^3 mesh as 8 boxes of {args.mesh // 2}^3")),
                        "droplets_per_gpu": prob.n_droplets, "boxes": nboxes, "form": head,
                        "form_name": FORM_NAME[head],
                        "l2": "inputs larger than L2 (droplet SoA %.1f GB per GPU)" % (
@@ -682,7 +787,8 @@ def main():
                          "launch_ms": results[head]["mkd_launch_ms"],
                          "algorithmic_bytes_per_launch": mkd_bytes,
                          "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)"
-                         if peak_src == "measured" else "fallback 6650 GB/s"},
+                         if peak_src == "measured" else "fallback 6650 GB/s",
+                         "compute": compute_roofline(head, results[head]["value"] / world, peaks_c)},
             "e2e": e2e,
             "cpu_baseline": cpu,
             "gpu_launches": 2 * args.steps * KERNELS_PER_CALL[head],

@@ -255,7 +255,8 @@ int pmp_spray_set_geometry(pmp_spray* h, const pmp_geometry* geom);
 int pmp_spray_set_grids(pmp_spray* h, int nboxes, const pmp_box* boxes);
 
 /* Hand the droplets of box `box` to the library (copied; the library keeps
- * them on the device, sorted by cell, and remembers the caller's order). */
+ * them on the device, sorted by cell in 2 x 2 x 2 bricks, and remembers the
+ * caller's order). */
 int pmp_spray_set_particles(pmp_spray* h, int box, const pmp_particles* p);
 /* Copy the droplets of box `box` back in the caller's order; out->n must be
  * the count given to set_particles and out's arrays sized for it. */
@@ -421,7 +422,8 @@ int pmp_spray_transfer_source(pmp_spray* h, const pmp_box_view* tmp_source,
  * x < plo: x += L), each droplet goes to the box whose valid region holds its
  * cell floor((x - plo)/dx), and droplets with id <= 0 or in no box are
  * dropped (*removed, may be NULL, receives their count).  Afterwards every
- * box's droplets are in cell order and that order is the box's caller order
+ * box's droplets are in cell order (2 x 2 x 2 bricks, x fastest, cells x
+ * fastest within a brick) and that order is the box's caller order
  * for pmp_spray_get_particles. */
 int pmp_spray_redistribute(pmp_spray* h, long long* removed, void* stream);
 
@@ -563,6 +565,16 @@ int pmp_learn_debug_infer_tc(const float* params, const float* xn, int n,
  * (as it must), with the cycles it waited; the device stays usable. */
 int pmp_learn_debug_wait_timeout(long long* cycles);
 int pmp_learn_param_count(void);
+
+/* ---------------------------------------------------------------------------
+ * Measured compute peaks of a device (no counterpart in the reference): the
+ * rates of loop kernels of independent FP64 FMAs, FP32 FMAs and SFU base-2
+ * exponentials over the whole GPU, best of three timed launches, at the
+ * clocks the device runs at (no setting is changed).  The denominators of
+ * the update kernels' compute roofline: fp64 and fp32 in TFLOP/s (an FMA is
+ * 2 FLOP), sfu in G operations/s. */
+int pmp_measure_peaks(int device, double* fp64_tflops, double* fp32_tflops,
+                      double* sfu_gops);
 
 #ifdef __cplusplus
 }

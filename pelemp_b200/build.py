@@ -23,7 +23,7 @@ SOURCES = [("pmp_spray.cu", "-fmad=false"), ("pmp_static.cu", "-fmad=false"),
            ("pmp_mixed.cu", "-fmad=true"), ("pmp_learn.cu", "-fmad=true"),
            ("pmp_batch.cu", "-fmad=false"), ("batch/pmp_batch_b64.cu", "-fmad=false"),
            ("batch/pmp_batch_b128.cu", "-fmad=false"), ("batch/pmp_batch_b256.cu", "-fmad=false"),
-           ("pmp_mesh.cu", "-fmad=false")]
+           ("pmp_mesh.cu", "-fmad=false"), ("pmp_peaks.cu", "-fmad=true")]
 def _headers():
     """Every header under csrc/ (a change to any of them rebuilds the library)."""
     out = []

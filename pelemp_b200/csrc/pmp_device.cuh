@@ -142,6 +142,28 @@ struct BoxEntry {
   double2* gr64;
 };
 
+// Place of cell (c0, c1, c2) (>= 0, relative to a corner of a region ex x ey
+// x .. cells wide) in the droplets' sort order: bricks of 2 x 2 x 2 cells,
+// bricks x fastest, cells within a brick x fastest.  The 128 consecutive
+// droplets a CTA takes (about 17 cells at 7-8 droplets per cell) then cover a
+// compact block of cells, whose 8-cell stencils fit the shared-memory gather
+// tile; a plain x-fastest order spreads them along a row (and a quarter of
+// the CTAs over two rows).
+__host__ __device__ inline unsigned long long brick_key(int c0, int c1, int c2, int ex, int ey)
+{
+  const unsigned long long nbx = (unsigned long long)((ex + 1) >> 1);
+  const unsigned long long nby = (unsigned long long)((ey + 1) >> 1);
+  const unsigned long long brick = ((unsigned long long)(c2 >> 1) * nby + (unsigned long long)(c1 >> 1)) * nbx +
+                                   (unsigned long long)(c0 >> 1);
+  return brick * 8ULL + (unsigned long long)(((c2 & 1) * 2 + (c1 & 1)) * 2 + (c0 & 1));
+}
+// keys brick_key can return for a region of ex x ey x ez cells
+__host__ __device__ inline unsigned long long brick_key_count(int ex, int ey, int ez)
+{
+  return (unsigned long long)((ex + 1) >> 1) * (unsigned long long)((ey + 1) >> 1) *
+         (unsigned long long)((ez + 1) >> 1) * 8ULL;
+}
+
 // float4 records per cell of the FP32 gas records: rho, T, velocity, Y
 __host__ __device__ constexpr int gas_rec4(int ns) { return (8 + ns) / 4; }
 // double2 records per cell of the FP64 gas records

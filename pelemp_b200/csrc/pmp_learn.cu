@@ -1231,18 +1231,7 @@ __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
           ok = false;
         } else {
           double* q = B.sr + ((ijkc[0] - B.sr_lo[0]) + (ijkc[1] - B.sr_lo[1]) * B.sr_j32 + (ijkc[2] - B.sr_lo[2]) * B.sr_k32);
-          if (fdat.mom_trans) {
-#pragma unroll
-            for (int dir = 0; dir < 3; ++dir) {
-              red_add(q + (P.s_mom + dir) * B.sr_n32, cur_coef * src.mom[dir]);
-            }
-          }
-          red_add(q + P.s_rho * B.sr_n32, cur_coef * src.mass);
-#pragma unroll
-          for (int spf = 0; spf < NF; ++spf) {
-            red_add(q + (P.s_spec + spf) * B.sr_n32, cur_coef * src.Ydot[spf]);
-          }
-          red_add(q + P.s_eng * B.sr_n32, cur_coef * src.eng);
+          deposit<NF>(P, q, B.sr_n32, cur_coef, src.mom, src.mass, src.Ydot, src.eng);
           if (P.do_move && !fdat.fixed_parts && id > 0) {
 #pragma unroll
             for (int dir = 0; dir < 3; ++dir) {

@@ -489,9 +489,9 @@ __global__ void k_rebin_keys(double* px, double* py, double* pz, const int* id, 
     return;
   }
   const pmp_box& bx = boxes[o];
-  const long long ex = bx.hi[0] - bx.lo[0] + 1, ey = bx.hi[1] - bx.lo[1] + 1;
-  const long long local = ((long long)(c[2] - bx.lo[2]) * ey + (c[1] - bx.lo[1])) * ex + (c[0] - bx.lo[0]);
-  keys[s] = ((unsigned long long)o << kKeyShift) | (unsigned long long)local;
+  const int ex = bx.hi[0] - bx.lo[0] + 1, ey = bx.hi[1] - bx.lo[1] + 1;
+  const unsigned long long local = pmp::brick_key(c[0] - bx.lo[0], c[1] - bx.lo[1], c[2] - bx.lo[2], ex, ey);
+  keys[s] = ((unsigned long long)o << kKeyShift) | local;
 }
 
 __global__ void k_box_bounds(const unsigned long long* keys, long long n, int nb, long long* begin)
@@ -814,8 +814,9 @@ extern "C" int pmp_spray_redistribute(pmp_spray* h, long long* removed, void* st
   const long long n = h->total;
   const int nc = h->ncomp();
   for (const pmp_box& bx : h->boxes) {
-    const long long cells = (long long)(bx.hi[0] - bx.lo[0] + 1) * (bx.hi[1] - bx.lo[1] + 1) * (bx.hi[2] - bx.lo[2] + 1);
-    if (cells >= (1LL << kKeyShift) || nb >= (1 << 22)) {
+    const unsigned long long cells =
+      pmp::brick_key_count(bx.hi[0] - bx.lo[0] + 1, bx.hi[1] - bx.lo[1] + 1, bx.hi[2] - bx.lo[2] + 1);
+    if (cells >= (1ULL << kKeyShift) || nb >= (1 << 22)) {
       return set_err(h, PMP_ERR_INVALID, "box too large for the re-binning key");
     }
   }

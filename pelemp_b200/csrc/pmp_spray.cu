@@ -120,7 +120,7 @@ __global__ void k_cell_keys(
     v = v < 0 ? 0 : (v >= ext[d] ? ext[d] - 1 : v);
     c[d] = v;
   }
-  keys[i] = (unsigned)((c[2] * (long long)ext[1] + c[1]) * ext[0] + c[0]);
+  keys[i] = (unsigned)pmp::brick_key(c[0], c[1], c[2], ext[0], ext[1]);
   idx[i] = i;
 }
 
@@ -1702,7 +1702,8 @@ int pmp_spray_set_particles(pmp_spray* h, int box, const pmp_particles* p)
     cudaFree(rid);
     return set_err(h, PMP_ERR_INVALID, "unknown particle layout");
   }
-  // sort by the cell holding the droplet (margin kSortPad around the box)
+  // sort by the cell holding the droplet, in brick order (margin kSortPad
+  // around the box)
   const pmp_box& bx = h->boxes[box];
   const int ext[3] = {bx.hi[0] - bx.lo[0] + 1 + 2 * kSortPad, bx.hi[1] - bx.lo[1] + 1 + 2 * kSortPad,
                       bx.hi[2] - bx.lo[2] + 1 + 2 * kSortPad};
@@ -1718,7 +1719,15 @@ int pmp_spray_set_particles(pmp_spray* h, int box, const pmp_particles* p)
                                 bx.lo[2], ext[0], ext[1], ext[2], keys, idx);
   PMP_CUDA(h, cudaGetLastError());
   size_t tbytes = 0;
-  const long long maxkey = (long long)ext[0] * ext[1] * ext[2];
+  const long long maxkey = (long long)pmp::brick_key_count(ext[0], ext[1], ext[2]);
+  if (maxkey >= (1LL << 32)) {
+    cudaFree(raw);
+    cudaFree(rid);
+    cudaFree(keys);
+    cudaFree(keys2);
+    cudaFree(idx);
+    return set_err(h, PMP_ERR_INVALID, "box too large for the droplet sort key", box);
+  }
   int end_bit = 1;
   while ((1LL << end_bit) < maxkey && end_bit < 32) {
     ++end_bit;

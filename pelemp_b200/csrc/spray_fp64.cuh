@@ -656,6 +656,75 @@ __device__ __forceinline__ void push_fallback(const KParams& P, long long s)
   atomicAdd(&P.status->fallback, 1ULL);
 }
 
+#ifndef PMP_WARP_AGG_DEPOSITS
+#define PMP_WARP_AGG_DEPOSITS 1
+#endif
+
+// One droplet's source increments of a sub-cycle, coef * {momentum (with
+// mom_trans), density and the fuels' species (with mass_trans), energy},
+// added into its source cell q (SprayParticles.cpp:419-441; nstride: the
+// view's component stride).  Warp-aggregated: the lanes of the warp that
+// deposit at the same time match on the cell; when every such group is a run
+// of consecutive lanes (the droplets are sorted by cell, so they usually
+// are), a segmented shuffle reduction sums each group's increments into its
+// first lane, which alone issues the FP64 reductions -- one per cell and
+// component instead of one per droplet.  Otherwise every lane issues its own.
+// The sum order differs from lane-by-lane atomics only in rounding, as
+// atomics are unordered anyway.
+template <int NF>
+__device__ __forceinline__ void deposit(const KParams& P, double* q, int nstride, double coef,
+                                        const double* mom, double mass, const double* Ydot, double eng)
+{
+  constexpr int NC = 5 + NF;
+  double v[NC];
+  int off[NC];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    v[d] = coef * mom[d];
+    off[d] = (P.s_mom + d) * nstride;
+  }
+  v[3] = coef * mass;
+  off[3] = P.s_rho * nstride;
+#pragma unroll
+  for (int f = 0; f < NF; ++f) {
+    v[4 + f] = coef * Ydot[f];
+    off[4 + f] = (P.s_spec + f) * nstride;
+  }
+  v[4 + NF] = coef * eng;
+  off[4 + NF] = P.s_eng * nstride;
+  const bool mom_on = P.f.mom_trans != 0;
+  const bool mass_on = P.f.mass_trans != 0;
+#if PMP_WARP_AGG_DEPOSITS
+  const unsigned act = __activemask();
+  const unsigned peers = __match_any_sync(act, reinterpret_cast<unsigned long long>(q));
+  const int lane = threadIdx.x & 31;
+  const int first = __ffs(peers) - 1;
+  const int last = 31 - __clz(peers);
+  const bool run = __popc(peers) == last - first + 1;
+  if (__all_sync(act, run)) {
+    const int width = (int)__reduce_max_sync(act, (unsigned)(last - first + 1));
+    for (int o = 1; o < width; o <<= 1) {
+      const bool take = lane + o <= last;
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        const double t = __shfl_down_sync(act, v[c], o);
+        v[c] = take ? v[c] + t : v[c];
+      }
+    }
+    if (lane != first) {
+      return;
+    }
+  }
+#endif
+#pragma unroll
+  for (int c = 0; c < NC; ++c) {
+    const bool on = c < 3 ? mom_on : (c < 4 + NF ? mass_on : true);
+    if (on) {
+      red_add(q + off[c], v[c]);
+    }
+  }
+}
+
 __device__ __forceinline__ bool in_box(const int* lo, const int* hi, int i, int j, int k)
 {
   return i >= lo[0] && i <= hi[0] && j >= lo[1] && j <= hi[1] && k >= lo[2] && k <= hi[2];

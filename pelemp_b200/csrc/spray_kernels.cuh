@@ -36,6 +36,117 @@ struct Counters {
   unsigned inner = 0;
 };
 
+#ifndef PMP_GATHER_TILE
+#define PMP_GATHER_TILE 1
+#endif
+
+// The gas records (BoxEntry::gr or gr64, R 16-byte words per cell) of the
+// cells that a CTA's 8-cell stencils cover when the call starts, copied into
+// shared memory once per call: the state does not change during a call, so
+// every sub-cycle's gather whose stencil lies inside the tile reads it there
+// (cell-sorted droplets share their stencils) instead of through L1/L2.
+// Stencils that leave it (a droplet that moved across a cell face) read the
+// records in global memory as before.
+template <typename Rec>
+struct CellTile {
+  int lo[3], hi[3];  // cells covered, inclusive (state index space)
+  int nx, nxy;
+  int on;            // 0: the CTA's stencils span more than the tile's capacity
+  Rec* rec;          // R records per cell, x fastest
+};
+
+// Stage the tile: every thread of the CTA calls it (BLOCK threads), with its
+// droplet slot s when it holds one.  CAP: capacity in cells.
+template <int R, int CAP, int BLOCK, typename Rec>
+__device__ __forceinline__ void stage_tile(const KParams& P, const DevParts& D, const BoxEntry& B, long long s,
+                                           bool holds, const Rec* grec, CellTile<Rec>& T, Rec* buf)
+{
+  __shared__ int wred[6][BLOCK / 32];
+  int v[6];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    v[d] = 0x7fffffff;
+    v[3 + d] = 0x7fffffff;
+  }
+  if (holds && D.id[s] > 0) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double l = __dadd_rn(__dmul_rn(__dsub_rn(D.pos[d][s], P.plo[d]), P.dxi[d]), 0.5);
+      // stencil cells ijk - 1 and ijk (upper cell centre); clamped so that
+      // a droplet far outside cannot overflow the arithmetic
+      const int ijk = max(-(1 << 24), min(1 << 24, static_cast<int>(floor(l))));
+      v[d] = ijk - 1;
+      v[3 + d] = -ijk;
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 6; ++i) {
+    v[i] = __reduce_min_sync(0xffffffffu, v[i]);
+  }
+  const int warp = threadIdx.x / 32;
+  if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+      wred[i][warp] = v[i];
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int m[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+      m[i] = wred[i][0];
+      for (int w = 1; w < BLOCK / 32; ++w) {
+        m[i] = min(m[i], wred[i][w]);
+      }
+    }
+    long long vol = 1;
+    for (int d = 0; d < 3; ++d) {
+      T.lo[d] = max(m[d], B.state_lo[d]);
+      T.hi[d] = m[3 + d] == 0x7fffffff ? T.lo[d] - 1 : min(-m[3 + d], B.state_hi[d]);
+      vol *= (long long)max(T.hi[d] - T.lo[d] + 1, 0);
+    }
+    T.nx = T.hi[0] - T.lo[0] + 1;
+    T.nxy = T.nx * (T.hi[1] - T.lo[1] + 1);
+    T.on = vol > 0 && vol <= CAP;
+    T.rec = buf;
+  }
+  __syncthreads();
+  if (T.on) {
+    const int nx = T.nx;
+    const int ny = T.nxy / nx;
+    const int n = T.nxy * (T.hi[2] - T.lo[2] + 1) * R;
+    for (int c = threadIdx.x; c < n; c += BLOCK) {
+      const int cell = c / R;
+      const int w = c - cell * R;
+      const int i = cell % nx;
+      const int t = cell / nx;
+      const int j = t % ny;
+      const int k = t / ny;
+      const int g = (k + T.lo[2] - B.state_lo[2]) * B.gr_k + (j + T.lo[1] - B.state_lo[1]) * B.gr_j +
+                    (i + T.lo[0] - B.state_lo[0]);
+      buf[c] = grec[g * R + w];
+    }
+  }
+  __syncthreads();
+}
+
+// Index in the tile of stencil corner (ijk - 1), or -1 when the stencil
+// ijk - 1 .. ijk is not inside it.
+template <typename Rec>
+__device__ __forceinline__ int tile_base(const CellTile<Rec>* T, const int* ijk)
+{
+  if (!T || !T->on) {
+    return -1;
+  }
+  bool in = true;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    in = in && ijk[d] - 1 >= T->lo[d] && ijk[d] <= T->hi[d];
+  }
+  return in ? (ijk[2] - 1 - T->lo[2]) * T->nxy + (ijk[1] - 1 - T->lo[1]) * T->nx + (ijk[0] - 1 - T->lo[0]) : -1;
+}
+
 __device__ __forceinline__ void cell_of(const KParams& P, const double* pos, double* lx, int* ijk, int* ijkc)
 {
 #pragma unroll
@@ -55,7 +166,9 @@ __device__ __forceinline__ void cell_of(const KParams& P, const double* pos, dou
 // droplet below 2 um is left to the fallback list.
 template <int NS, int NF, Form FORM, bool FF = false, bool PELEC = false>
 __device__ __forceinline__ void update_one(const KParams& P, const DevParts& D, const BoxEntry& B, int b,
-                                           long long s, Counters& c, double* sx = nullptr, int sxs = 0)
+                                           long long s, Counters& c, double* sx = nullptr, int sxs = 0,
+                                           const CellTile<double2>* tile64 = nullptr,
+                                           const CellTile<float4>* tile32 = nullptr)
 {
   int id = D.id[s];
   if (!(id > 0)) {
@@ -151,6 +264,7 @@ __device__ __forceinline__ void update_one(const KParams& P, const DevParts& D, 
       }
       gpv.eng_src = 0.;
       gpv.mass_src = 0.;
+      const int tb = tile_base(tile64, ijk);
 #pragma unroll
       for (int kk = -1; kk < 1; ++kk) {
 #pragma unroll
@@ -169,7 +283,17 @@ __device__ __forceinline__ void update_one(const KParams& P, const DevParts& D, 
                 // gather below forms (k_gas_records64), so the sums are equal
                 constexpr int R2 = gas_rec2(NS);
                 double rec[2 * R2];
-                load_gas_rec64<R2>(B, ci, cj, ck, rec);
+                if (tb >= 0) {
+                  const double2* r = tile64->rec + (tb + (kk + 1) * tile64->nxy + (jj + 1) * tile64->nx + (ii + 1)) * R2;
+#pragma unroll
+                  for (int m = 0; m < R2; ++m) {
+                    const double2 v = r[m];
+                    rec[2 * m] = v.x;
+                    rec[2 * m + 1] = v.y;
+                  }
+                } else {
+                  load_gas_rec64<R2>(B, ci, cj, ck, rec);
+                }
                 gpv.rho = __dadd_rn(gpv.rho, __dmul_rn(cw, rec[0]));
 #pragma unroll
                 for (int n = 0; n < NS; ++n) {
@@ -267,6 +391,7 @@ __device__ __forceinline__ void update_one(const KParams& P, const DevParts& D, 
       for (int n = 0; n < NS; ++n) {
         Yg[n] = 0.f;
       }
+      const int tb = tile_base(tile32, ijk);
 #pragma unroll
       for (int kk = -1; kk < 1; ++kk) {
 #pragma unroll
@@ -282,7 +407,19 @@ __device__ __forceinline__ void update_one(const KParams& P, const DevParts& D, 
                 state_ok = false;
               } else {
                 float rec[4 * R4];
-                load_gas_rec<R4>(B, ci, cj, ck, rec);
+                if (tb >= 0) {
+                  const float4* r = tile32->rec + (tb + (kk + 1) * tile32->nxy + (jj + 1) * tile32->nx + (ii + 1)) * R4;
+#pragma unroll
+                  for (int m = 0; m < R4; ++m) {
+                    const float4 v = r[m];
+                    rec[4 * m] = v.x;
+                    rec[4 * m + 1] = v.y;
+                    rec[4 * m + 2] = v.z;
+                    rec[4 * m + 3] = v.w;
+                  }
+                } else {
+                  load_gas_rec<R4>(B, ci, cj, ck, rec);
+                }
                 const float w = (float)cw;
                 rho = fmaf(w, rec[0], rho);
                 Tg = fmaf(w, rec[1], Tg);
@@ -348,20 +485,7 @@ __device__ __forceinline__ void update_one(const KParams& P, const DevParts& D, 
       }
     }
     double* q = B.sr + ((ijkc[0] - B.sr_lo[0]) + (ijkc[1] - B.sr_lo[1]) * B.sr_j32 + (ijkc[2] - B.sr_lo[2]) * B.sr_k32);
-    if (P.f.mom_trans) {
-#pragma unroll
-      for (int dir = 0; dir < 3; ++dir) {
-        red_add(q + (P.s_mom + dir) * B.sr_n32, __dmul_rn(cur_coef, src.mom[dir]));
-      }
-    }
-    if (P.f.mass_trans) {
-      red_add(q + P.s_rho * B.sr_n32, __dmul_rn(cur_coef, src.mass));
-#pragma unroll
-      for (int spf = 0; spf < NF; ++spf) {
-        red_add(q + (P.s_spec + spf) * B.sr_n32, __dmul_rn(cur_coef, src.Ydot[spf]));
-      }
-    }
-    red_add(q + P.s_eng * B.sr_n32, __dmul_rn(cur_coef, src.eng));
+    deposit<NF>(P, q, B.sr_n32, cur_coef, src.mom, src.mass, src.Ydot, src.eng);
     // move (SprayParticles.cpp:444-476)
     if (P.do_move && !P.f.fixed_parts && id > 0) {
 #pragma unroll
@@ -410,9 +534,11 @@ __device__ __forceinline__ void update_one(const KParams& P, const DevParts& D, 
 // update_one over the library's packed droplet arrays
 template <int NS, int NF, Form FORM, bool FF = false, bool PELEC = false>
 __device__ __forceinline__ void update_one(const KParams& P, const BoxEntry& B, int b, long long s, Counters& c,
-                                           double* sx = nullptr, int sxs = 0)
+                                           double* sx = nullptr, int sxs = 0,
+                                           const CellTile<double2>* tile64 = nullptr,
+                                           const CellTile<float4>* tile32 = nullptr)
 {
-  update_one<NS, NF, FORM, FF, PELEC>(P, P.parts, B, b, s, c, sx, sxs);
+  update_one<NS, NF, FORM, FF, PELEC>(P, P.parts, B, b, s, c, sx, sxs, tile64, tile32);
 }
 
 __device__ __forceinline__ void flush_counters(const KParams& P, Counters& c)
@@ -458,8 +584,17 @@ __device__ __forceinline__ bool stage_box(const KParams& P, int b, BoxEntry& sB)
   return s_failed != 0;
 }
 
-template <int NS, int NF, int BLOCK>
-__global__ void __launch_bounds__(BLOCK, PMP_FP64_MIN_BLOCKS) spray_update_fp64(const __grid_constant__ KParams P)
+// capacities of the gather tiles, in cells: FP64 records (the FP64 forms,
+// 5 CTAs per SM) and FP32 records (the mixed form, 7 CTAs per SM)
+#ifndef PMP_TILE64_CELLS
+#define PMP_TILE64_CELLS 192
+#endif
+#ifndef PMP_TILE32_CELLS
+#define PMP_TILE32_CELLS 192
+#endif
+
+template <int NS, int NF, int BLOCK, bool PELEC>
+__device__ __forceinline__ void fp64_cta(const KParams& P)
 {
   __shared__ BoxEntry sB;
   const int b = P.cta_box[blockIdx.x];
@@ -468,27 +603,36 @@ __global__ void __launch_bounds__(BLOCK, PMP_FP64_MIN_BLOCKS) spray_update_fp64(
   }
   const long long s = P.cta_start[blockIdx.x] + threadIdx.x;
   Counters c;
-  if (s < sB.p_end) {
-    update_one<NS, NF, Form::FP64>(P, sB, b, s, c);
+#if PMP_GATHER_TILE
+  constexpr int R2 = gas_rec2(NS);
+  __shared__ CellTile<double2> tile;
+  __shared__ double2 tile_rec[PMP_TILE64_CELLS * R2];
+  const bool tiled = sB.gr64 != nullptr;
+  if (tiled) {
+    stage_tile<R2, PMP_TILE64_CELLS, BLOCK>(P, P.parts, sB, s, s < sB.p_end, sB.gr64, tile, tile_rec);
   }
+  if (s < sB.p_end) {
+    update_one<NS, NF, Form::FP64, false, PELEC>(P, sB, b, s, c, nullptr, 0, tiled ? &tile : nullptr);
+  }
+#else
+  if (s < sB.p_end) {
+    update_one<NS, NF, Form::FP64, false, PELEC>(P, sB, b, s, c);
+  }
+#endif
   flush_counters(P, c);
+}
+
+template <int NS, int NF, int BLOCK>
+__global__ void __launch_bounds__(BLOCK, PMP_FP64_MIN_BLOCKS) spray_update_fp64(const __grid_constant__ KParams P)
+{
+  fp64_cta<NS, NF, BLOCK, false>(P);
 }
 
 // the PeleC coupling of the FP64 form
 template <int NS, int NF, int BLOCK>
 __global__ void __launch_bounds__(BLOCK, PMP_FP64_MIN_BLOCKS) spray_update_fp64_pelec(const __grid_constant__ KParams P)
 {
-  __shared__ BoxEntry sB;
-  const int b = P.cta_box[blockIdx.x];
-  if (stage_box(P, b, sB)) {
-    return;
-  }
-  const long long s = P.cta_start[blockIdx.x] + threadIdx.x;
-  Counters c;
-  if (s < sB.p_end) {
-    update_one<NS, NF, Form::FP64, false, true>(P, sB, b, s, c);
-  }
-  flush_counters(P, c);
+  fp64_cta<NS, NF, BLOCK, true>(P);
 }
 
 template <int NS, int NF, int BLOCK, bool FF, bool PELEC = false>
@@ -505,9 +649,19 @@ __global__ void __launch_bounds__(BLOCK, PMP_MIXED_MIN_BLOCKS) spray_update_mixe
   // spray_source_mixed)
   __shared__ double stash[(5 + NF) * BLOCK];
   double* sx = stash + threadIdx.x;
+#if PMP_GATHER_TILE
+  constexpr int R4 = gas_rec4(NS);
+  __shared__ CellTile<float4> tile;
+  __shared__ float4 tile_rec[PMP_TILE32_CELLS * R4];
+  stage_tile<R4, PMP_TILE32_CELLS, BLOCK>(P, P.parts, sB, s, s < sB.p_end, sB.gr, tile, tile_rec);
+  if (s < sB.p_end) {
+    update_one<NS, NF, Form::MIXED, FF, PELEC>(P, sB, b, s, c, sx, BLOCK, nullptr, &tile);
+  }
+#else
   if (s < sB.p_end) {
     update_one<NS, NF, Form::MIXED, FF, PELEC>(P, sB, b, s, c, sx, BLOCK);
   }
+#endif
   flush_counters(P, c);
 }
 

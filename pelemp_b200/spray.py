@@ -77,6 +77,7 @@ _SIGS = {
     "pmp_learn_debug_infer_tc": [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p],
     "pmp_learn_debug_wait_timeout": [C.POINTER(C.c_longlong)],
     "pmp_learn_param_count": [],
+    "pmp_measure_peaks": [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)],
 }
 
 
@@ -475,3 +476,12 @@ def learn_debug_wait_timeout():
     cycles = C.c_longlong(0)
     rc = lib().pmp_learn_debug_wait_timeout(C.byref(cycles))
     return rc, cycles.value
+
+
+def measure_peaks(device=0):
+    """Measured FP64 / FP32 FMA (TFLOP/s) and SFU ex2 (G op/s) rates of the device."""
+    a, b, c = C.c_double(), C.c_double(), C.c_double()
+    rc = lib().pmp_measure_peaks(device, C.byref(a), C.byref(b), C.byref(c))
+    if rc != 0:
+        raise SprayError(rc, capi.ErrorInfo())
+    return {"fp64_tflops": a.value, "fp32_tflops": b.value, "sfu_gops": c.value}

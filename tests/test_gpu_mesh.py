@@ -133,8 +133,12 @@ def test_redistribute_then_update():
         c = MO.cells_of(got["pos"], prob.plo, prob.dx)
         lo, hi = prob.boxes[b]
         assert np.all((c >= np.asarray(lo)[:, None]) & (c <= np.asarray(hi)[:, None]))
-        key = (c[2] * 1_000_000 + c[1]) * 1000 + c[0]
-        assert np.all(np.diff(key) >= 0)  # cell order
+        # cell order in 2x2x2 bricks (bricks x fastest, cells x fastest in a brick)
+        r = c - np.asarray(lo)[:, None]
+        ex, ey = hi[0] - lo[0] + 1, hi[1] - lo[1] + 1
+        brick = ((r[2] // 2) * ((ey + 1) // 2) + r[1] // 2) * ((ex + 1) // 2) + r[0] // 2
+        key = brick * 8 + ((r[2] % 2) * 2 + r[1] % 2) * 2 + r[0] % 2
+        assert np.all(np.diff(key) >= 0)
     # the re-binned droplets go through an update (stencils inside their boxes)
     st_keep, st_v = device_state(prob)
     _src, src_v = device_sources(prob)
