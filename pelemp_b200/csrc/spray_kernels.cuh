@@ -214,10 +214,10 @@ __device__ __forceinline__ void update_one(const KParams& P, const DevParts& D, 
     double lx[3];
     int ijk[3], ijkc[3];
     cell_of(P, pos, lx, ijk, ijkc);
-    if (FORM == Form::MIXED) {
-      // the mixed form keeps the position in shared memory across the
-      // droplet physics (sx: this thread's slots, stride sxs), which does
-      // not read it: fewer registers live there, fewer spills
+    if (sx) {
+      // the position waits in shared memory across the droplet physics (sx:
+      // this thread's slots, stride sxs), which does not read it: fewer
+      // registers live there, fewer spills
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
         sx[d * sxs] = pos[d];
@@ -372,7 +372,16 @@ __device__ __forceinline__ void update_one(const KParams& P, const DevParts& D, 
           cBoilT[spf] = dmin(P.f.critT[spf], cc);
         }
       }
-      nsub = spray_source_fp64<NS, NF, PELEC>(P, P.sub_dt, gpv, vel, T, dia, Y, num_ppp, id, cBoilT);
+      nsub = spray_source_fp64<NS, NF, PELEC>(P, P.sub_dt, gpv, vel, T, dia, Y, num_ppp, id, cBoilT, sx, sxs);
+      if (sx) {
+        // the position and the cell it gives, back from shared memory
+        const volatile double* vx = sx;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          pos[d] = vx[d * sxs];
+        }
+        cell_of(P, pos, lx, ijk, ijkc);
+      }
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
         src.mom[d] = gpv.mom_src[d];
@@ -603,6 +612,10 @@ __device__ __forceinline__ void fp64_cta(const KParams& P)
   }
   const long long s = P.cta_start[blockIdx.x] + threadIdx.x;
   Counters c;
+  // per thread: position, parcel count, start mass, composition, across the
+  // droplet physics (update_one, spray_source_fp64)
+  __shared__ double stash[(5 + NF) * BLOCK];
+  double* sx = stash + threadIdx.x;
 #if PMP_GATHER_TILE
   constexpr int R2 = gas_rec2(NS);
   __shared__ CellTile<double2> tile;
@@ -612,11 +625,11 @@ __device__ __forceinline__ void fp64_cta(const KParams& P)
     stage_tile<R2, PMP_TILE64_CELLS, BLOCK>(P, P.parts, sB, s, s < sB.p_end, sB.gr64, tile, tile_rec);
   }
   if (s < sB.p_end) {
-    update_one<NS, NF, Form::FP64, false, PELEC>(P, sB, b, s, c, nullptr, 0, tiled ? &tile : nullptr);
+    update_one<NS, NF, Form::FP64, false, PELEC>(P, sB, b, s, c, sx, BLOCK, tiled ? &tile : nullptr);
   }
 #else
   if (s < sB.p_end) {
-    update_one<NS, NF, Form::FP64, false, PELEC>(P, sB, b, s, c);
+    update_one<NS, NF, Form::FP64, false, PELEC>(P, sB, b, s, c, sx, BLOCK);
   }
 #endif
   flush_counters(P, c);
