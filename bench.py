@@ -257,9 +257,9 @@ WORKLOAD_TEXT = {
 FORM_MODE = {"fp64": 0, "mixed": 1, "learned": 2}
 # the library's kernels one update call launches (MKD and MK alike):
 # FP64: gas records + update; mixed: gas records + small-droplet selection +
-# update + FP64 list kernel (side stream); learned: gas records + update +
-# FP64 list kernel
-KERNELS_PER_CALL = {"fp64": 2, "mixed": 4, "learned": 3}
+# update + FP64 list kernel (side stream); learned: the same + the FP64 kernel
+# over the droplets its gate rejected
+KERNELS_PER_CALL = {"fp64": 2, "mixed": 4, "learned": 5}
 FORM_NAME = {"fp64": "plain FP64", "mixed": "mixed FP32 physics / FP64 state and deposits",
              "learned": "learned surrogate (bf16 MLP on tensor cores) + FP32 physics / FP64 state"}
 KERNEL = {"fp64": "spray_update_fp64<5,2,128>", "mixed": "spray_update_mixed<5,2,128,fuel_first>",
@@ -299,14 +299,31 @@ def compute_roofline(form, substeps_per_s, peaks):
     return out
 
 
-def train_surrogate(sp, prob, st_v, stream, args):
-    """Tuples from the plain FP64 teacher on a sample of the workload's droplets,
-    then GPU training; returns (seconds, report)."""
+def train_surrogate(sp, prob, st_v, src_v, stream, args):
+    """Tuples labelled by the plain FP64 teacher along the workload's own
+    trajectory: every learn_gap steps (advanced by the FP64 form) for
+    learn_gens states, a sample of the droplets (every learn_stride-th, plus 3
+    perturbed copies of each); then GPU training, and the initial droplets
+    put back.  Returns (seconds, report, tuples)."""
+    from pelemp_b200 import capi
     t0 = time.perf_counter()
-    sp.learn_generate(st_v, prob.flow_dt, prob.state_ghosts, True, prob.spray_cfl_lev,
-                      sample_stride=args.learn_stride, augment=3, seed=7, stream=stream)
-    rep = sp.learn_train(epochs=args.learn_epochs, batch=2048, audit_fraction=0.0)
-    return time.perf_counter() - t0, rep
+    sp.set_mode(capi.PMP_MODE_FP64)
+    for g in range(args.learn_gens):
+        sp.learn_generate(st_v, prob.flow_dt, prob.state_ghosts, True, prob.spray_cfl_lev,
+                          sample_stride=args.learn_stride, augment=3, seed=7 + g, stream=stream)
+        if g + 1 < args.learn_gens:
+            for _ in range(args.learn_gap):
+                for do_move in (1, 0):
+                    sp.update_particles(st_v, src_v, prob.flow_dt, 0.0, prob.state_ghosts,
+                                        prob.source_ghosts, 0, 0, do_move, prob.spray_cfl_lev, stream,
+                                        sync=False)
+    sp.sync()
+    tuples = sp.learn_count()
+    rep = sp.learn_train(epochs=args.learn_epochs, batch=4096, audit_fraction=0.0)
+    for b, p in enumerate(prob.parts):
+        sp.set_particles(b, p["pos"], p["rdata"], p["id"])
+    sp.set_mode(capi.PMP_MODE_LEARNED)
+    return time.perf_counter() - t0, rep, tuples
 
 
 def droplet_errors(pa, pb, prob):
@@ -524,8 +541,11 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--forms", default="fp64,mixed,learned",
                     help="forms to time; the fastest non-FP64 one is the headline value")
-    ap.add_argument("--learn-stride", type=int, default=64)
-    ap.add_argument("--learn-epochs", type=int, default=40)
+    ap.add_argument("--learn-stride", type=int, default=16,
+                    help="label every n-th droplet (x4 with the perturbed copies) at each state")
+    ap.add_argument("--learn-gens", type=int, default=12, help="states along the trajectory labelled")
+    ap.add_argument("--learn-gap", type=int, default=2, help="FP64 steps between labelled states")
+    ap.add_argument("--learn-epochs", type=int, default=4)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -606,10 +626,14 @@ def main():
         containers[form] = sp
         info = {}
         if form == "learned":
-            t_train, rep = train_surrogate(sp, prob, st_v, stream.cuda_stream, args)
+            t_train, rep, ntup = train_surrogate(sp, prob, st_v, src_v, stream.cuda_stream, args)
             info["train"] = {"seconds": t_train, "tuples": rep.tuples, "adam_steps": rep.steps,
                              "val_rel_rms": list(rep.val_rel_rms), "epochs": args.learn_epochs,
-                             "sample_stride": args.learn_stride}
+                             "sample_stride": args.learn_stride, "states": args.learn_gens,
+                             "steps_between_states": args.learn_gap,
+                             "what": "tuples labelled by the FP64 teacher along the workload's "
+                                     "trajectory (FP64 steps), untimed; the timed steps start from "
+                                     "the initial droplets"}
         # warm-up steps; the MKD call of each is waited for, for its kernel time
         # (the library's events around the call's kernels: the roofline's launch)
         mkd_ms = []

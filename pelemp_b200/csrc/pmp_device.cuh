@@ -220,6 +220,9 @@ struct DevStatus {
   unsigned long long inner;
   unsigned long long fallback;
   unsigned long long fb_count;
+  // learned form: droplets its gate rejects, listed from the end of the
+  // fallback list (per call, reset with fb_count)
+  unsigned long long fb_gate;
 };
 
 // SoA droplet store: ncomp double arrays of length cap, then ids.
@@ -259,9 +262,14 @@ struct KParams {
   // fallback-list kernel: when list_nbox > 0, only the entries of boxes
   // [list_box0, list_box0 + list_nbox) (one stage of the host-view pipeline)
   int list_box0, list_nbox;
-  // mixed form: the droplets below 2 um were listed before the launch
-  // (k_select_small); the mixed kernel skips them without listing them
+  // mixed and learned forms: the droplets below 2 um were listed before the
+  // launch (k_select_small); the update kernel skips them without listing them
   int fb_pre;
+  // fallback-list kernel: list_back = 1 runs the learned form's gate
+  // rejections, fb_list[fb_cap - 1 - i] for i < fb_gate, instead of
+  // fb_list[i] for i < fb_count
+  int list_back;
+  long long fb_cap;
   // mixed form: the diameter below which a droplet takes the FP64 path, 2 um
   // in the coupling's length unit
   double mixed_min_dia;

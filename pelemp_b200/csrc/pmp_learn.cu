@@ -790,7 +790,9 @@ __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
     valid = valid && id > 0;
     double dia = valid ? P.parts.rd[PMP_PSTATE_DIA][s] : 1e-5;
     if (valid && dia < kMixedMinDia) {
-      push_fallback(P, s);
+      if (!P.fb_pre) {
+        push_fallback(P, s);
+      }
       valid = false;
     }
     double pos[3] = {0., 0., 0.}, vel[3] = {0., 0., 0.}, Y[NF];
@@ -1035,7 +1037,7 @@ __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
               in = in && isfinite(yv[k]);
             }
             if (!in) {
-              push_fallback(P, s);
+              push_fallback_back(P, s);
               fell_back = true;
               valid = false;
               active = false;

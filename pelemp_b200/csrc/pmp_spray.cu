@@ -867,6 +867,7 @@ int prepare_update_impl(
   P.err_host = h->err_dev;
   P.box_begin = h->d_box_begin;
   P.fb_list = h->fb_list;
+  P.fb_cap = h->total > 0 ? h->total : 1;
   return PMP_OK;
 }
 
@@ -957,6 +958,41 @@ int enqueue_mixed(pmp_spray* h, const KParams& Q, int n, long long s0, long long
   return PMP_OK;
 }
 
+// The learned form over CTA-map items [c0, c0 + n) and droplet slots
+// [s0, s1), arranged as the mixed form's: the droplets below 2 um are listed
+// first and their FP64 kernel runs on the side stream beside the learned
+// kernel; the droplets the learned kernel's gate rejects (listed from the end
+// of the fallback list) are updated by the FP64 kernel after it.  Q's box
+// filter (list_box0 / list_nbox) applies to both lists.
+int enqueue_learned(pmp_spray* h, const KParams& Q, int c0, int n, long long s0, long long s1, cudaStream_t st)
+{
+  KParams R = Q;
+  R.fb_pre = 1;
+  int rc = pmp::launch_select_small(R, s0, s1, st);
+  if (rc != PMP_OK) {
+    return rc;
+  }
+  PMP_CUDA(h, cudaEventRecord(h->ev_fork, st));
+  PMP_CUDA(h, cudaStreamWaitEvent(h->side, h->ev_fork, 0));
+  rc = dispatch_fp64_list(h->nspec, h->nfuel, R, h->total, h->side);
+  if (rc == PMP_OK) {
+    rc = pmp::launch_learned(h, R, st, c0, n);
+  }
+  if (rc == PMP_OK) {
+    KParams G = R;
+    G.list_back = 1;
+    rc = dispatch_fp64_list(h->nspec, h->nfuel, G, h->total, st);
+  }
+  const cudaError_t e1 = cudaEventRecord(h->ev_join, h->side);
+  const cudaError_t e2 = cudaStreamWaitEvent(st, h->ev_join, 0);
+  if (rc != PMP_OK) {
+    return rc;
+  }
+  PMP_CUDA(h, e1);
+  PMP_CUDA(h, e2);
+  return PMP_OK;
+}
+
 // The overlapped form of pmp_spray_update_host.  The boxes are split into up
 // to kHostStages consecutive groups of about equal bytes; group g's state and
 // source are copied in on one stream while the update of the groups before
@@ -1019,7 +1055,7 @@ int update_host_overlapped_impl(
   }
   const int NS = h->nspec;
   const int NF = h->nfuel;
-  PMP_CUDA(h, cudaMemsetAsync(&h->d_status->fb_count, 0, sizeof(unsigned long long), st));
+  PMP_CUDA(h, cudaMemsetAsync(&h->d_status->fb_count, 0, 2 * sizeof(unsigned long long), st));
   PMP_CUDA(h, cudaEventRecord(h->ev0, st));
   PMP_CUDA(h, cudaEventRecord(h->hev_start, st));
   PMP_CUDA(h, cudaStreamWaitEvent(h->hs_in, h->hev_start, 0));
@@ -1054,17 +1090,18 @@ int update_host_overlapped_impl(
         return set_err(h, rc, "no gas-record kernel for this species count");
       }
       if (h->mode == PMP_MODE_LEARNED) {
-        rc = pmp::launch_learned(h, P, st, c0, n);
+        // the learned kernel takes the whole map and an item range; the
+        // fallback lists are filtered to the group's boxes
+        KParams Lq = P;
+        Lq.list_box0 = b0;
+        Lq.list_nbox = b1 - b0;
+        rc = enqueue_learned(h, Lq, c0, n, h->box_begin[b0], h->box_begin[b1], st);
       } else if (h->mode == PMP_MODE_MIXED) {
         rc = enqueue_mixed(h, Q, n, h->box_begin[b0], h->box_begin[b1], st);
       } else if (P.pelec) {
         rc = dispatch_fp64_pelec(NS, NF, Q, n, st);
       } else {
         rc = dispatch_fp64(NS, NF, Q, n, st);
-      }
-      if (rc == PMP_OK && h->mode == PMP_MODE_LEARNED) {
-        PMP_CUDA(h, cudaGetLastError());
-        rc = dispatch_fp64_list(NS, NF, Q, h->total, st);
       }
       if (rc == PMP_ERR_UNSUPPORTED) {
         return set_err(h, rc, "no kernel for this species / fuel count");
@@ -1192,7 +1229,7 @@ int pmp::prepare_update(
   if (rc != PMP_OK) {
     return rc;
   }
-  PMP_CUDA(h, cudaMemsetAsync(&h->d_status->fb_count, 0, sizeof(unsigned long long), st));
+  PMP_CUDA(h, cudaMemsetAsync(&h->d_status->fb_count, 0, 2 * sizeof(unsigned long long), st));
   return PMP_OK;
 }
 
@@ -1234,7 +1271,7 @@ int pmp::enqueue_update(pmp_spray* h, const KParams& P, int nboxes, cudaStream_t
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   PMP_CUDA(h, cudaStreamIsCapturing(st, &cap));
   const unsigned ev_flags = cap == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : 0u;
-  PMP_CUDA(h, cudaMemsetAsync(&h->d_status->fb_count, 0, sizeof(unsigned long long), st));
+  PMP_CUDA(h, cudaMemsetAsync(&h->d_status->fb_count, 0, 2 * sizeof(unsigned long long), st));
   PMP_CUDA(h, cudaEventRecordWithFlags(h->ev0, st, ev_flags));
   if (h->ncta > 0) {
     const int NS = h->nspec;
@@ -1243,11 +1280,7 @@ int pmp::enqueue_update(pmp_spray* h, const KParams& P, int nboxes, cudaStream_t
     if (h->mode == PMP_MODE_LEARNED) {
       rc = pmp::launch_gas_records(NS, P, 0, nboxes, h->gas_rec_max_cells, st);
       if (rc == PMP_OK) {
-        rc = pmp::launch_learned(h, P, st);
-      }
-      if (rc == PMP_OK) {
-        PMP_CUDA(h, cudaGetLastError());
-        rc = dispatch_fp64_list(NS, NF, P, h->total, st);
+        rc = enqueue_learned(h, P, 0, h->ncta, 0, h->total, st);
       }
     } else if (h->mode == PMP_MODE_MIXED) {
       rc = pmp::launch_gas_records(NS, P, 0, nboxes, h->gas_rec_max_cells, st);

@@ -680,8 +680,21 @@ __device__ __forceinline__ void push_fallback(const KParams& P, long long s)
   atomicAdd(&P.status->fallback, 1ULL);
 }
 
+// Append slot s to the learned form's list of gate rejections, which grows
+// from the end of the fallback list (a droplet is on one of the two lists at
+// most, so they never meet).
+__device__ __forceinline__ void push_fallback_back(const KParams& P, long long s)
+{
+  const unsigned long long k = atomicAdd(&P.status->fb_gate, 1ULL);
+  P.fb_list[P.fb_cap - 1 - (long long)k] = s;
+  atomicAdd(&P.status->fallback, 1ULL);
+}
+
+// Off by default: on config 2 (16M droplets, 7-8 per cell, cell-sorted) the
+// aggregation's shuffles cost more issue slots than the reductions it saves
+// (mixed form 7.40e9 -> 7.18e9 droplet-substeps/s, FP64 2.26e9 -> 2.24e9).
 #ifndef PMP_WARP_AGG_DEPOSITS
-#define PMP_WARP_AGG_DEPOSITS 1
+#define PMP_WARP_AGG_DEPOSITS 0
 #endif
 
 // One droplet's source increments of a sub-cycle, coef * {momentum (with

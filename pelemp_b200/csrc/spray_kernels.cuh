@@ -36,8 +36,12 @@ struct Counters {
   unsigned inner = 0;
 };
 
+// Off by default: on config 2 the staging (the CTA's stencil box, about 9x
+// the cells its droplets hold) and its barriers add more instructions than
+// the L1/L2 gather latency it removes in these issue-bound kernels (mixed
+// form 7.40e9 -> 7.05e9 droplet-substeps/s, FP64 2.26e9 -> 2.13e9).
 #ifndef PMP_GATHER_TILE
-#define PMP_GATHER_TILE 1
+#define PMP_GATHER_TILE 0
 #endif
 
 // The gas records (BoxEntry::gr or gr64, R 16-byte words per cell) of the
@@ -836,11 +840,12 @@ __global__ void __launch_bounds__(BLOCK, PMP_FP64_MIN_BLOCKS) spray_update_fp64_
   if (cta_call_failed(P)) {
     return;
   }
-  const unsigned long long n = *reinterpret_cast<volatile unsigned long long*>(&P.status->fb_count);
+  const unsigned long long n =
+    *reinterpret_cast<volatile unsigned long long*>(P.list_back ? &P.status->fb_gate : &P.status->fb_count);
   Counters c;
   for (unsigned long long i = blockIdx.x * (unsigned long long)BLOCK + threadIdx.x; i < n;
        i += (unsigned long long)gridDim.x * BLOCK) {
-    const long long s = P.fb_list[i];
+    const long long s = P.list_back ? P.fb_list[P.fb_cap - 1 - (long long)i] : P.fb_list[i];
     const int b = box_of_slot(P, s);
     if (P.list_nbox > 0 && (b < P.list_box0 || b >= P.list_box0 + P.list_nbox)) {
       continue;

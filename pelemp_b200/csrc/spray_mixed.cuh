@@ -191,17 +191,28 @@ __device__ __forceinline__ float hf(const DevMechF& m, int n, float T)
   return fmaf(hp, T, c[5]) * m.ru_w_eng[n];
 }
 
-__device__ __forceinline__ float heat_coeff_f(float ratio, float B_M, float Nu_0)
+// log1p(x) and (1 + x)^0.7 from one base-2 logarithm of 1 + x: the values
+// flog1p(x) and fpow(1 + x, 0.7f) give, with one SFU logarithm fewer
+__device__ __forceinline__ void flog1p_pow07(float x, float& l1p, float& p07)
+{
+  const float u = 1.f + x;
+  const float l2 = flog2(u);
+  l1p = fabsf(x) < 1e-2f ? flog1p(x) : l2 * 0.693147181f;
+  p07 = (u == 0.f) ? 0.f : fexp2(0.7f * l2);
+}
+
+// calcHeatCoeff (Drag.H:6-45) in FP32; lnBM1 = ln(1 + B_M)
+__device__ __forceinline__ float heat_coeff_f(float ratio, float B_M, float Nu_0, float lnBM1)
 {
   if (B_M <= 1e-15f) {
     return 0.f;
   }
   const float NU2 = Nu_0 - 2.f;
-  const float lnBM1 = flog(1.f + B_M);
   float phi = fdiv(ratio, Nu_0);
   float B_T_old = fexp(phi * lnBM1) - 1.f;
-  float logB = flog1p(B_T_old);
-  float invFT = fdiv(B_T_old, logB * fpow(1.f + B_T_old, 0.7f));
+  float logB, p07;
+  flog1p_pow07(B_T_old, logB, p07);
+  float invFT = fdiv(B_T_old, logB * p07);
   float Nu_num = 2.f + NU2 * invFT;
   phi = fdiv(ratio, Nu_num);
   float B_T = fexp(phi * lnBM1) - 1.f;
@@ -209,18 +220,23 @@ __device__ __forceinline__ float heat_coeff_f(float ratio, float B_M, float Nu_0
   int k = 0;
   while (k < 100 && error > fmaxf(1e-7f, 8.f * 1.1920929e-7f * fabsf(B_T))) {
     B_T_old = B_T;
-    logB = flog1p(B_T);
-    invFT = fdiv(B_T, logB * fpow(1.f + B_T, 0.7f));
+    flog1p_pow07(B_T, logB, p07);
+    invFT = fdiv(B_T, logB * p07);
     Nu_num = 2.f + NU2 * invFT;
     phi = fdiv(ratio, Nu_num);
     B_T = fexp(phi * lnBM1) - 1.f;
     error = fabsf(B_T - B_T_old);
     k++;
   }
-  logB = flog1p(B_T);
-  invFT = fdiv(B_T, logB * fpow(1.f + B_T, 0.7f));
+  flog1p_pow07(B_T, logB, p07);
+  invFT = fdiv(B_T, logB * p07);
   Nu_num = 2.f + NU2 * invFT;
   return fdiv(Nu_num * logB, B_T);
+}
+
+__device__ __forceinline__ float heat_coeff_f(float ratio, float B_M, float Nu_0)
+{
+  return heat_coeff_f(ratio, B_M, Nu_0, flog(1.f + B_M));
 }
 
 // interpolated gas state in FP32
@@ -513,13 +529,15 @@ __device__ __forceinline__ int spray_source_mixed(
         }
         cp_fuel = fdiv(cp_fuel, sumYSkin);
         const float Sc_skin = fdiv(mu_skin, rhoDtotal);
-        const float logB = flog1p(B_M);
-        const float invFM = fdiv(B_M, logB * fpow(1.f + B_M, 0.7f));
+        float logB, pBM07;
+        flog1p_pow07(B_M, logB, pBM07);
+        const float invFM = fdiv(B_M, logB * pBM07);
         const float Sh_0 = 1.f + powR * fcbrt(1.f + Reyn * Sc_skin);
         const float Sh_num = 2.f + (Sh_0 - 2.f) * invFM;
         const float mdotcoeff = (float)PMP_PI * dia_f * Sh_num * logB;
         const float ratio = fdiv(cp_fuel * Sh_num * rhoDtotal, lambda_skin);
-        Nu_num = heat_coeff_f(ratio, B_M, Nu_0);
+        // ln(1 + B_M): the logarithm above where it was taken from lg2, else again
+        Nu_num = heat_coeff_f(ratio, B_M, Nu_0, fabsf(B_M) < 1e-2f ? flog(1.f + B_M) : logB);
 #pragma unroll
         for (int spf = 0; spf < NF; ++spf) {
           if (X_vapor[spf] > 0.f) {

@@ -116,7 +116,6 @@ def test_device_error_reported_by_sync_and_next_call():
     # enqueued: no error yet
     sp.update_particles(*args, sync=False)
     torch.cuda.synchronize()
-    before = [sp.get_particles(b) for b in range(len(prob.boxes))]
     # the failing call has finished: the next call reports its error at once
     with pytest.raises(SprayError) as e:
         sp.update_particles(*args, sync=False)
@@ -125,20 +124,33 @@ def test_device_error_reported_by_sync_and_next_call():
     # reported once: the next sync is clean
     sp.sync()
 
-    # a failing call A with a call B enqueued behind it before A runs (the GPU
-    # is held busy first): B leaves the droplets as A left them, and sync
-    # reports A's error
+    # a failing call A with a call B enqueued behind it before A runs: B
+    # leaves the droplets as A left them, and sync reports A's error.  Both
+    # handles first take one reported failing call (a handle's first call
+    # allocates its buffers, which waits for the device); then the GPU is
+    # held busy so that A and B are both enqueued before A runs.
+    def failed_once(h):
+        with pytest.raises(SprayError):
+            h.update_particles(*args)
+
+    ref = from_problem(prob)
+    failed_once(ref)
+    with pytest.raises(SprayError):
+        ref.update_particles(*args)  # A alone
+    want = [ref.get_particles(b) for b in range(len(prob.boxes))]
     sp2 = from_problem(prob)
+    failed_once(sp2)
     torch.cuda._sleep(200_000_000)
-    sp2.update_particles(*args, sync=False)
-    sp2.update_particles(*args, sync=False)
+    sp2.update_particles(*args, sync=False)  # A
+    sp2.update_particles(*args, sync=False)  # B
     with pytest.raises(SprayError) as e2:
         sp2.sync()
     assert e2.value.code == capi.PMP_ERR_LEFT_DOMAIN
     assert e2.value.info.box == 0 and e2.value.info.particle == 7
     after = [sp2.get_particles(b) for b in range(len(prob.boxes))]
-    assert_bitwise(after, before)
+    assert_bitwise(after, want)
     sp.close()
+    ref.close()
     sp2.close()
     del st_keep
 
