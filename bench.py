@@ -265,37 +265,41 @@ FORM_NAME = {"fp64": "plain FP64", "mixed": "mixed FP32 physics / FP64 state and
 KERNEL = {"fp64": "spray_update_fp64<5,2,128>", "mixed": "spray_update_mixed<5,2,128,fuel_first>",
           "learned": "spray_update_learned<5,2,128,fuel_first>"}
 # DRAM bytes per droplet of one config-2 MKD launch, measured by ncu on a
-# 2M-droplet launch of the same kernel (one-launch capture): dram read + write
-# minus the mesh's algorithmic bytes (state read once, source read-modify-
-# write), divided by the droplets.  The droplet part grows with the droplet
-# count, the mesh part does not, so a full launch's traffic is estimated as
-# mesh bytes + droplets x this.  Above the 184 algorithmic bytes per droplet
-# for the FP64 kernel: its register spills reach DRAM; below it for the mixed
-# and learned kernels, whose gathers read the FP32 gas records (written by a
+# 2M-droplet launch of the same kernel at config-2 density (64^3 mesh, 7-8
+# droplets per cell; one-launch capture): dram read + write minus the mesh's
+# algorithmic bytes (state read once, source read-modify-write), divided by
+# the droplets.  The droplet part grows with the droplet count, the mesh part
+# does not, so a full launch's traffic is estimated as mesh bytes + droplets
+# x this.  The mixed and learned kernels move less than the 184 algorithmic
+# bytes per droplet: their gathers read the FP32 gas records (written by a
 # separate pass) instead of the FP64 state.
-DRAM_BYTES_PER_DROPLET = {"fp64": 278.4, "mixed": 143.4, "learned": 133.2}
-# Thread-level instructions per droplet-substep on the FP64, FMA (FP32) and
-# XU (transcendental) pipes of one config-2 MKD launch of each form, from the
-# ncu instruction counts of a 2M-droplet launch (sm__inst_executed_pipe_*,
-# warp instructions x 32 / droplet-substeps); with the live throughput and
-# the measured pipe peaks they give the compute roofline.
-PIPE_INSTR_PER_SUBSTEP = {}
+DRAM_BYTES_PER_DROPLET = {"fp64": 184.6, "mixed": 160.1, "learned": 153.4}
+# Pipe utilisation of each form's update kernel in the same captures (% of
+# the pipe's peak while the SM is active: sm__inst_executed_pipe_*; issue:
+# smsp__issue_active), and its measured pipe peaks: the compute side of the
+# roofline.  The kernels are bound by instruction issue and latency, not by
+# one pipe.
+PIPE_PCT = {
+    "mixed": {"issue": 58.97, "xu": 39.06, "fma": 22.14, "alu": 25.42, "fp64": 11.97, "lsu": 15.89,
+              "tensor": 0.0},
+    "fp64": {"issue": 46.61, "xu": 13.34, "fma": 6.21, "alu": 15.90, "fp64": 32.02, "lsu": 9.69,
+             "tensor": 0.0},
+    "learned": {"issue": 45.55, "xu": 41.07, "fma": 13.91, "alu": 22.27, "fp64": 8.65, "lsu": 12.16,
+                "tensor": 5.84},
+}
 
 
-def compute_roofline(form, substeps_per_s, peaks):
-    """Achieved instruction rate of each pipe / its measured peak for the
-    form's update kernel (None where the instruction counts are not known)."""
-    if peaks is None:
-        return None
-    out = {"peaks": peaks, "peaks_source": "pmp_measure_peaks: loop kernels of independent DFMA, FFMA and "
-                                            "ex2.approx on this GPU, best of three launches"}
-    counts = PIPE_INSTR_PER_SUBSTEP.get(form)
-    if counts:
-        rates = {"fp64": 0.5e12 * peaks["fp64_tflops"], "fma": 0.5e12 * peaks["fp32_tflops"],
-                 "xu": 1e9 * peaks["sfu_gops"]}
-        out["pipes"] = {k: {"instr_per_substep": counts[k], "achieved_per_s": counts[k] * substeps_per_s,
-                            "peak_per_s": rates[k], "frac": counts[k] * substeps_per_s / rates[k]}
-                        for k in rates if k in counts}
+def compute_roofline(form, peaks):
+    """The compute side of the roofline of the form's update kernel: the
+    measured pipe peaks of this GPU and the kernel's pipe utilisation."""
+    out = {"pipes_pct_of_peak": PIPE_PCT.get(form),
+           "pipes_source": "ncu capture of the same kernel: one MKD launch of 2M droplets at config-2 density "
+                           "(sm__inst_executed_pipe_*.avg.pct_of_peak_sustained_active, "
+                           "smsp__issue_active, sm__pipe_tensor_cycles_active)"}
+    if peaks is not None:
+        out["peaks"] = peaks
+        out["peaks_source"] = ("pmp_measure_peaks on this GPU: loop kernels of independent DFMA, FFMA and "
+                               "ex2.approx, best of three launches")
     return out
 
 
@@ -531,6 +535,9 @@ def main():
                     help="config2 only: cells per side of a smaller cubic mesh (boxes of half that), "
                          "keeping droplets per cell at a given --droplets (profiling captures)")
     ap.add_argument("--e2e-steps", type=int, default=6)
+    ap.add_argument("--eager-steps", type=int, default=2,
+                    help="eager steps timed beside the graph replays (the droplets' drift over all "
+                         "steps must stay inside the ghost cells)")
     ap.add_argument("--cpu-sample", type=int, default=0,
                     help="droplets per CPU step (0: sized for --cpu-seconds per step)")
     ap.add_argument("--cpu-seconds", type=float, default=8.0)
@@ -647,7 +654,7 @@ def main():
                 if do_move and w > 0:
                     mkd_ms.append(sp.stats().kernel_ms)
         # eager steps (a launch per kernel, the host never waits inside)
-        t_eager, _, _, _ = timed_steps(sp, lambda: step(sp, stream.cuda_stream), args.steps)
+        t_eager, _, _, _ = timed_steps(sp, lambda: step(sp, stream.cuda_stream), args.eager_steps)
         graph = None
         sampler = ClockSampler(local)
         if not args.no_graph:
@@ -675,7 +682,7 @@ def main():
         if rank == 0:
             balance[form] = (b0_before, sp.get_particles(0), src[0].cpu().numpy())
         info.update({"value": sub_total / (t_max * 1e-3), "ms_per_step": t_max / args.steps,
-                     "ms_per_step_eager": t_eager / args.steps,
+                     "ms_per_step_eager": t_eager / args.eager_steps,
                      "timed": "whole-step CUDA graph replays" if graph is not None else "eager steps",
                      "mkd_launch_ms": float(np.mean(mkd_ms)), "substeps": sub_total,
                      "fallback_frac": fb / max(sub_local, 1), "clocks": c})
@@ -701,7 +708,7 @@ def main():
             accuracy[f]["mass_balance_last_step"] = bal[f]["mass"]
             accuracy[f]["energy_drift_vs_fp64"] = bal[f]["energy"] - bal["fp64"]["energy"]
         accuracy["fp64_balance_last_step"] = bal["fp64"]
-        accuracy["steps"] = args.warmup + args.steps * (1 if args.no_graph else 2) + 1
+        accuracy["steps"] = args.warmup + args.eager_steps + (0 if args.no_graph else args.steps) + 1
         accuracy["what"] = ("box 0's droplets after all steps against the FP64 form (bit-identical to the FP64 "
                             "oracle); deposits and balances of the last step; energy drift: the form's "
                             "(liquid enthalpy change + gas gain) / exchanged enthalpy minus the FP64 form's")
@@ -724,6 +731,9 @@ def main():
     e2e = None
     if not args.no_e2e:
         sp = containers[head]
+        # from the initial droplets again (their drift stays inside the ghost cells)
+        for b, p in enumerate(prob.parts):
+            sp.set_particles(b, p["pos"], p["rdata"], p["id"])
         st_h = [torch.from_numpy(s).pin_memory().numpy() for s in prob.state]
         src_h = [torch.zeros(s.shape, dtype=torch.float64).pin_memory().numpy()
                  for s in prob.new_sources()]
@@ -804,15 +814,15 @@ def main():
             "forms": forms_out,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
-                         "traffic_source": "ncu dram bytes of a 2M-droplet MKD launch of the same kernel "
-                                           "scaled by droplet count (mesh part fixed)"
+                         "traffic_source": "ncu dram bytes of a 2M-droplet MKD launch of the same kernel at "
+                                           "config-2 density, scaled by droplet count (mesh part fixed)"
                          if traffic else None,
                          "kernel": KERNEL[head] + " (MKD launch)",
                          "launch_ms": results[head]["mkd_launch_ms"],
                          "algorithmic_bytes_per_launch": mkd_bytes,
                          "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)"
                          if peak_src == "measured" else "fallback 6650 GB/s",
-                         "compute": compute_roofline(head, results[head]["value"] / world, peaks_c)},
+                         "compute": compute_roofline(head, peaks_c)},
             "e2e": e2e,
             "cpu_baseline": cpu,
             "gpu_launches": 2 * args.steps * KERNELS_PER_CALL[head],

@@ -5,7 +5,7 @@
 * oracle/ (test infrastructure) -- `make -C oracle` builds the CPU oracle and,
   when the PeleMP sources are present, the reference build under oracle/_ref.
 
-Usage: python -m pelemp_b200.build [--verbose-ptxas]
+Usage: python -m pelemp_b200.build [--force] [--verbose-ptxas] [--define NAME=VALUE ...]
 """
 import os
 import subprocess
@@ -47,11 +47,16 @@ def _newer(target, deps):
     return any(os.path.getmtime(d) > t for d in deps)
 
 
+STAMP = LIB + ".flags"  # the extra flags the library was last built with
+
+
 def build_lib(force=False, ptxas_verbose=False, extra=()):
     deps = [os.path.join(CSRC, s) for s, _ in SOURCES] + [os.path.join(CSRC, h) for h in HEADERS]
     deps.append(os.path.join(ROOT, "include", "pmp_spray.h"))
     deps.append(os.path.abspath(__file__))
-    if not (force or ptxas_verbose or extra or _newer(LIB, deps)):
+    flags = " ".join(extra)
+    built_with = open(STAMP).read() if os.path.exists(STAMP) else ""
+    if not (force or ptxas_verbose or flags != built_with or _newer(LIB, deps)):
         return LIB
     os.makedirs(OBJDIR, exist_ok=True)
     procs = []
@@ -70,6 +75,8 @@ def build_lib(force=False, ptxas_verbose=False, extra=()):
             raise subprocess.CalledProcessError(p.returncode, "nvcc")
     subprocess.run([NVCC, *ARCH, "-shared", "-o", LIB + ".tmp", *objs], check=True)
     os.replace(LIB + ".tmp", LIB)
+    with open(STAMP, "w") as f:
+        f.write(flags)
     return LIB
 
 
@@ -104,7 +111,11 @@ def build_oracle():
 
 
 def main(argv):
-    build_lib(force="--force" in argv, ptxas_verbose="--verbose-ptxas" in argv)
+    # --define NAME=VALUE (repeatable): a build option of the kernels, e.g.
+    # PMP_GATHER_TILE=1, PMP_WARP_AGG_DEPOSITS=1, PMP_FP64_MIN_BLOCKS=4
+    defines = ["-D" + argv[i + 1] for i, a in enumerate(argv) if a == "--define" and i + 1 < len(argv)]
+    build_lib(force="--force" in argv or bool(defines), ptxas_verbose="--verbose-ptxas" in argv,
+              extra=defines)
     build_driver(force="--force" in argv)
     if "--no-oracle" not in argv:
         build_oracle()

@@ -789,7 +789,7 @@ __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
     int id = valid ? P.parts.id[s] : 0;
     valid = valid && id > 0;
     double dia = valid ? P.parts.rd[PMP_PSTATE_DIA][s] : 1e-5;
-    if (valid && dia < kMixedMinDia) {
+    if (valid && dia < P.mixed_min_dia) {
       if (!P.fb_pre) {
         push_fallback(P, s);
       }
@@ -1337,7 +1337,7 @@ __global__ void k_learn_audit(const __grid_constant__ KParams P, const __grid_co
     return;
   }
   const double dia = P.parts.rd[PMP_PSTATE_DIA][s];
-  if (dia < kMixedMinDia) {
+  if (dia < P.mixed_min_dia) {  // the droplets the FP64 kernel updates
     return;
   }
   const BoxEntry& B = P.boxes[box_of_slot(P, s)];

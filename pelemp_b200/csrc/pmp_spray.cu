@@ -843,6 +843,9 @@ int prepare_update_impl(
   P.c_eng = c.engIndx;
   P.pelec = h->pelec;
   P.mixed_min_dia = h->pelec ? 100. * pmp::kMixedMinDia : pmp::kMixedMinDia;  // cm or m
+  if (h->mode == PMP_MODE_LEARNED) {
+    P.mixed_min_dia = pmp::kLearnMinDia;  // PeleLMeX only
+  }
   P.c_spec = c.specIndx;
   P.s_rho = c.rhoSrcIndx;
   P.s_mom = c.momSrcIndx;

@@ -29,6 +29,10 @@
 namespace pmp {
 
 constexpr double kMixedMinDia = 2e-6;  // below: FP64 path
+// The learned form's threshold (PeleLMeX units): the surrogate's errors are
+// largest for the small droplets that heat and evaporate fastest, and below
+// 4 um (0.05% of config-2 droplets) the FP64 kernel updates them instead.
+constexpr double kLearnMinDia = 4e-6;
 
 #ifndef PMP_MIXED_FULL_RANGE_SFU
 #define PMP_MIXED_FULL_RANGE_SFU 1

@@ -170,7 +170,7 @@ def test_handle_runs_after_reported_error(oracle):
         sp.update_particles(st_v, src_v, prob.flow_dt, 0.0, prob.state_ghosts, prob.source_ghosts,
                             0, 0, 1, prob.spray_cfl_lev, stream)
     for b, p in enumerate(prob.parts):
-        sp.set_particles(b, p)
+        sp.set_particles(b, p["pos"], p["rdata"], p["id"])
     for do_move in (1, 0):
         for s in src:
             s.zero_()

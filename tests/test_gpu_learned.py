@@ -9,13 +9,18 @@ update against the FP64 oracle.
 * update after several MKD+MK steps with a surrogate trained on another
   sample of the same workload: droplet temperature, diameter and mass within
   1e-4 relative of the FP64 oracle in RMS over the droplets (99.9% of the
-  droplets within 1e-3; the rest are droplets whose sub-step count, an
-  integer the reference derives from the rates, lands one off), total liquid
-  mass within 1e-6, liquid + gas mass balance closed to FP64 round-off,
-  deposits within 5e-2 of the component's largest deposit;
+  droplets within 1e-3; the tail is the surrogate's own error on the
+  transfer rates, largest for small droplets that heat and evaporate fast --
+  every droplet-substep of these workloads takes one inner sub-step, so no
+  sub-step count flips), total liquid mass within 1e-6, liquid + gas mass
+  balance closed to FP64 round-off, deposits within 5e-2 of the component's
+  largest deposit;
 * droplets outside the training range go to the FP64 kernel: bit-identical
   to the oracle;
-* the learned update is faster than the plain FP64 update.
+* the learned update against the plain FP64 update and against the method
+  without the network (the mixed form, the same FP32 physics with the
+  transport, B_T fixed point and Nusselt/Sherwood numbers evaluated
+  exactly): what the network gains is measured and printed.
 """
 import numpy as np
 import pytest
@@ -249,31 +254,43 @@ def test_gate_sends_out_of_range_droplets_to_fp64(trained, oracle):
             assert np.array_equal(pg[b][k][..., idx], po[b][k][..., idx]), (b, k)
 
 
-def test_learned_faster_than_fp64(trained):
+def test_learned_gain_over_fp64_and_over_the_method_without_it():
+    """MKD calls (4 sub-cycles) on the same 2M droplets at config-2 density
+    (7-8 per cell), with a surrogate trained on this workload: the learned
+    form against the plain FP64 form and against the mixed form, which is the
+    same FP32 method without the network.  Measured on B200: the network
+    costs more issue slots than the FP32 physics it replaces, so the gain
+    over the mixed form is below 1 (printed); the bounds are regression
+    guards: faster than FP64, at least half the mixed form's speed."""
     import torch
-    w, _ = trained
     prob = W.config2(n=2_000_000, seed=2, steps=1, ncells=(64, 64, 64), box=(32, 32, 32))
-    times = {}
-    for mode in (capi.PMP_MODE_FP64, capi.PMP_MODE_LEARNED):
+    st_keep, st_v = device_state(prob)
+    stream = torch.cuda.current_stream().cuda_stream
+    times, fallback = {}, 0
+    for mode in (capi.PMP_MODE_FP64, capi.PMP_MODE_MIXED, capi.PMP_MODE_LEARNED):
         sp = from_problem(prob, mode=mode)
         if mode == capi.PMP_MODE_LEARNED:
-            sp.set_learn_weights(w)
-        st_keep, st_v = device_state(prob)
-        stream = torch.cuda.current_stream().cuda_stream
+            sp.learn_generate(st_v, prob.flow_dt, prob.state_ghosts, True, prob.spray_cfl_lev,
+                              sample_stride=4, augment=3, seed=11, stream=stream)
+            sp.learn_train(epochs=8, batch=4096)
         ms = []
         for _ in range(3):
             _src, src_v = device_sources(prob)
             sp.update_particles(st_v, src_v, prob.flow_dt, 0.0, prob.state_ghosts, prob.source_ghosts,
-                                0, 0, 0, prob.spray_cfl_lev, stream)
+                                0, 0, 1, prob.spray_cfl_lev, stream)
             ms.append(sp.stats().kernel_ms)
+            if mode == capi.PMP_MODE_LEARNED:
+                fallback = sp.stats().fallback
         times[mode] = min(ms)
-        if mode == capi.PMP_MODE_LEARNED:
-            print("learned fallback", sp.stats().fallback, "of", sp.stats().substeps)
-        del st_keep
         sp.close()
-    print("MK of 2M droplets: FP64 %.3f ms, learned %.3f ms, speed-up %.2f" % (
-        times[0], times[2], times[0] / times[2]))
-    assert times[2] < times[0]
+    del st_keep
+    fp64, mixed, learned = (times[capi.PMP_MODE_FP64], times[capi.PMP_MODE_MIXED],
+                            times[capi.PMP_MODE_LEARNED])
+    print("MKD of 2M droplets: FP64 %.3f ms, mixed %.3f ms, learned %.3f ms (fallback %d); "
+          "learned vs FP64 %.2fx, gain over the method without the network %.2fx" % (
+              fp64, mixed, learned, fallback, fp64 / learned, mixed / learned))
+    assert learned < fp64
+    assert learned < 2.0 * mixed
 
 
 def test_learned_energy_identity(trained, oracle):
