@@ -321,6 +321,10 @@ def train_surrogate(sp, prob, st_v, src_v, stream, args):
                     sp.update_particles(st_v, src_v, prob.flow_dt, 0.0, prob.state_ghosts,
                                         prob.source_ghosts, 0, 0, do_move, prob.spray_cfl_lev, stream,
                                         sync=False)
+            # re-bin the moved droplets to their boxes (periodic wrap), as the
+            # flow solver's step does, so the trajectory can run any length
+            sp.sync()
+            sp.redistribute(stream)
     sp.sync()
     tuples = sp.learn_count()
     rep = sp.learn_train(epochs=args.learn_epochs, batch=4096, audit_fraction=0.0)

@@ -149,8 +149,16 @@ struct BoxEntry {
 // compact block of cells, whose 8-cell stencils fit the shared-memory gather
 // tile; a plain x-fastest order spreads them along a row (and a quarter of
 // the CTAs over two rows).
+#ifndef PMP_SORT_BRICKS
+#define PMP_SORT_BRICKS 1
+#endif
 __host__ __device__ inline unsigned long long brick_key(int c0, int c1, int c2, int ex, int ey)
 {
+#if !PMP_SORT_BRICKS
+  // the plain x-fastest cell order (build option)
+  return ((unsigned long long)c2 * (unsigned long long)ey + (unsigned long long)c1) * (unsigned long long)ex +
+         (unsigned long long)c0;
+#endif
   const unsigned long long nbx = (unsigned long long)((ex + 1) >> 1);
   const unsigned long long nby = (unsigned long long)((ey + 1) >> 1);
   const unsigned long long brick = ((unsigned long long)(c2 >> 1) * nby + (unsigned long long)(c1 >> 1)) * nbx +
