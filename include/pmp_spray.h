@@ -255,8 +255,7 @@ int pmp_spray_set_geometry(pmp_spray* h, const pmp_geometry* geom);
 int pmp_spray_set_grids(pmp_spray* h, int nboxes, const pmp_box* boxes);
 
 /* Hand the droplets of box `box` to the library (copied; the library keeps
- * them on the device, sorted by cell in 2 x 2 x 2 bricks, and remembers the
- * caller's order). */
+ * them on the device, sorted by cell, and remembers the caller's order). */
 int pmp_spray_set_particles(pmp_spray* h, int box, const pmp_particles* p);
 /* Copy the droplets of box `box` back in the caller's order; out->n must be
  * the count given to set_particles and out's arrays sized for it. */
@@ -422,8 +421,8 @@ int pmp_spray_transfer_source(pmp_spray* h, const pmp_box_view* tmp_source,
  * x < plo: x += L), each droplet goes to the box whose valid region holds its
  * cell floor((x - plo)/dx), and droplets with id <= 0 or in no box are
  * dropped (*removed, may be NULL, receives their count).  Afterwards every
- * box's droplets are in cell order (2 x 2 x 2 bricks, x fastest, cells x
- * fastest within a brick) and that order is the box's caller order
+ * box's droplets are in cell order (x fastest) and that order is the box's
+ * caller order
  * for pmp_spray_get_particles. */
 int pmp_spray_redistribute(pmp_spray* h, long long* removed, void* stream);
 

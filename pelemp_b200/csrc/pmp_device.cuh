@@ -143,14 +143,18 @@ struct BoxEntry {
 };
 
 // Place of cell (c0, c1, c2) (>= 0, relative to a corner of a region ex x ey
-// x .. cells wide) in the droplets' sort order: bricks of 2 x 2 x 2 cells,
-// bricks x fastest, cells within a brick x fastest.  The 128 consecutive
-// droplets a CTA takes (about 17 cells at 7-8 droplets per cell) then cover a
-// compact block of cells, whose 8-cell stencils fit the shared-memory gather
-// tile; a plain x-fastest order spreads them along a row (and a quarter of
-// the CTAs over two rows).
+// x .. cells wide) in the droplets' sort order: x-fastest cells by default;
+// with PMP_SORT_BRICKS, bricks of 2 x 2 x 2 cells, bricks x fastest, cells
+// within a brick x fastest.  In the brick order the 128 consecutive droplets
+// a CTA takes (about 17 cells at 7-8 droplets per cell) cover a compact
+// block of cells whose 8-cell stencils fit the shared-memory gather tile;
+// the row order spreads them along a row (and a quarter of the CTAs over two
+// rows).
+// The brick order goes with the gather tile (a build option): measured alone,
+// the row order is 2 % faster for the mixed form on config 2 (7.49e9 vs
+// 7.34e9 droplet-substeps/s), its gathers hitting L1 more often.
 #ifndef PMP_SORT_BRICKS
-#define PMP_SORT_BRICKS 1
+#define PMP_SORT_BRICKS PMP_GATHER_TILE
 #endif
 __host__ __device__ inline unsigned long long brick_key(int c0, int c1, int c2, int ex, int ey)
 {
