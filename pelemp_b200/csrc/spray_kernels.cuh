@@ -405,18 +405,29 @@ __device__ __forceinline__ void update_one(const KParams& P, const DevParts& D, 
         Yg[n] = 0.f;
       }
       const int tb = tile_base(tile32, ijk);
+      // FP32 weights from the FP64 factors; a corner is gathered when all
+      // three factors are positive (the FP64 product's test, which FP32
+      // products could underflow); one bounds check for the whole stencil,
+      // per corner only when the stencil crosses the grown state box
+      float wf[2][3];
+#pragma unroll
+      for (int dir = 0; dir < 3; ++dir) {
+        wf[0][dir] = (float)ssv[0][dir];
+        wf[1][dir] = (float)ssv[1][dir];
+      }
+      const bool stencil_in = in_box(B.state_lo, B.state_hi, ijk[0] - 1, ijk[1] - 1, ijk[2] - 1) &&
+                              in_box(B.state_lo, B.state_hi, ijk[0], ijk[1], ijk[2]);
 #pragma unroll
       for (int kk = -1; kk < 1; ++kk) {
 #pragma unroll
         for (int jj = -1; jj < 1; ++jj) {
 #pragma unroll
           for (int ii = -1; ii < 1; ++ii) {
-            const double cw = ssv[ii + 1][0] * ssv[jj + 1][1] * ssv[kk + 1][2];
-            if (cw > 0.) {
+            if (ssv[ii + 1][0] > 0. && ssv[jj + 1][1] > 0. && ssv[kk + 1][2] > 0.) {
               const int ci = ijk[0] + ii;
               const int cj = ijk[1] + jj;
               const int ck = ijk[2] + kk;
-              if (!in_box(B.state_lo, B.state_hi, ci, cj, ck)) {
+              if (!stencil_in && !in_box(B.state_lo, B.state_hi, ci, cj, ck)) {
                 state_ok = false;
               } else {
                 float rec[4 * R4];
@@ -433,7 +444,7 @@ __device__ __forceinline__ void update_one(const KParams& P, const DevParts& D, 
                 } else {
                   load_gas_rec<R4>(B, ci, cj, ck, rec);
                 }
-                const float w = (float)cw;
+                const float w = wf[ii + 1][0] * wf[jj + 1][1] * wf[kk + 1][2];
                 rho = fmaf(w, rec[0], rho);
                 Tg = fmaf(w, rec[1], Tg);
 #pragma unroll
