@@ -1,6 +1,6 @@
 """CPU oracle of the operations around the update (numpy restatement).
 
-Test infrastructure: only the tests use this module, as the checker of
+Test infrastructure: only the tests use this module, to check
 pmp_spray_est_timestep, pmp_spray_derive, pmp_spray_transfer_source and
 pmp_spray_redistribute.  Each function follows the reference lines it cites.
 Arrays are per box (ncomp, nz, ny, nx) with a lower corner `lo` (x, y, z);

@@ -1,6 +1,6 @@
 """CPU oracle of the learned form's network and its training gradient.
 
-Test infrastructure: only the tests use this module, as the checker of the
+Test infrastructure: only the tests use this module, to check the
 GPU training kernels (pmp_learn_debug_grad) and of the tensor-core inference.
 There is no counterpart in the reference; the network is the project's own
 surrogate (10 -> 64 -> 64 -> 64 -> 5, SiLU).

@@ -1,7 +1,7 @@
 """ctypes bindings of the CPU oracle and of the reference build.
 
 TEST INFRASTRUCTURE: imported only by tests/, __graft_entry__.smoke() and
-bench.py's CPU-baseline leg, as the checker.  The product never imports it.
+bench.py's CPU-baseline leg, to compare against.  The product never imports it.
 
 * ``Oracle(libm=False)`` -- oracle/liboracle.so (project math, the functions
   the CUDA kernels use); ``Oracle(libm=True)`` -- oracle/liboracle_libm.so

@@ -1,7 +1,7 @@
 /* spray_oracle.h -- CPU FP64 oracle of the spray particle update.
  *
  * TEST INFRASTRUCTURE.  Only the tests, the smoke check and the bench's CPU
- * baseline load this code, as the checker; the product (libpmpspray) never
+ * baseline load this code, to compare against; the product (libpmpspray) never
  * links it.
  *
  * A plain-C restatement of PeleMP's non-EB, no-breakup, no-splash

@@ -1336,7 +1336,7 @@ __device__ void mlp_simt(const MlpSmem& S, const float* xn, float* y)
   }
 }
 
-// The judge: on every audit_stride-th droplet, compare the surrogate with the
+// The audit: on every audit_stride-th droplet, compare the surrogate with the
 // FP64 teacher at the droplet's state at call entry.
 template <int NS, int NF>
 __global__ void k_learn_audit(const __grid_constant__ KParams P, const __grid_constant__ LearnParams L, long long total)
