@@ -17,7 +17,9 @@ Arms
   its per-droplet error against the FP64 form (bit-identical to the FP64
   oracle) after all steps.  ``e2e``: the headline form's steps through
   pmp_spray_update_host with the mesh state and source in pinned host memory
-  (copies inside the timed region).
+  (copies inside the timed region).  ``other_workloads`` (N=1, default
+  sizes): the figures of configs 3, 4 and 5, each from a run of this script
+  in its own process.
 * --impl reference: PeleMP's own spray physics headers (oracle/_ref, built
   from the reference sources) on the host cores, OpenMP over droplets, on a
   bounded random sample of the same workload.
@@ -524,6 +526,45 @@ def bench_batched(args, world, rank, local, pg):
         pg.destroy_process_group()
 
 
+def other_workloads(args):
+    """The other workloads' lines, each from its own process (`--workload W
+    --steps S --no-cpu --no-e2e`), reduced to their figures: config 3 the
+    batched FP64 launches against one launch per box, configs 4 and 5 the
+    three forms at 32M / 16M droplets of config 1's distributions."""
+    out = {}
+    for w in [x for x in args.also.split(",") if x and x != "none"]:
+        cmd = [sys.executable, os.path.abspath(__file__), "--workload", w, "--steps", str(args.also_steps),
+               "--warmup", "3", "--no-cpu", "--no-e2e", "--also", "none"]
+        if w == "config4":
+            cmd += ["--learn-stride", "32"]
+        t0 = time.perf_counter()
+        try:
+            r = subprocess.run(cmd, capture_output=True, text=True, timeout=900)
+        except subprocess.TimeoutExpired:
+            out[w] = {"error": "no line within 900 s"}
+            continue
+        lines = [x for x in r.stdout.splitlines() if x.startswith("{")]
+        if r.returncode != 0 or not lines:
+            out[w] = {"error": "exit %d: %s" % (r.returncode, r.stderr.strip().splitlines()[-1:] or "")}
+            continue
+        d = json.loads(lines[-1])
+        o = {"workload": d["config"]["workload"], "value": d["value"], "ms_per_step": d["ms_per_step"],
+             "steps": d["steps"], "clocks": d.get("clocks"), "wall_s": round(time.perf_counter() - t0, 1)}
+        if "launches" in d:
+            o["launches"] = {k: (v if k == "speedup_vs_per_box" else
+                                 {"value": v["value"], "ms_per_step": v["ms_per_step"]})
+                             for k, v in d["launches"].items()}
+        for f, v in d.get("forms", {}).items():
+            e = v.get("error_vs_fp64", {})
+            o.setdefault("forms", {})[f] = {
+                "value": v["value"], "speedup_vs_fp64": v["speedup_vs_fp64"],
+                "error_vs_fp64": {q: e[q] for q in ("T", "mass", "dia") if q in e} or None,
+                "train_s": v.get("train", {}).get("seconds"), "tuples": v.get("train", {}).get("tuples"),
+                "fallback_frac": v["fallback_frac"]}
+        out[w] = o
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -539,6 +580,9 @@ def main():
                     help="config2 only: cells per side of a smaller cubic mesh (boxes of half that), "
                          "keeping droplets per cell at a given --droplets (profiling captures)")
     ap.add_argument("--e2e-steps", type=int, default=6)
+    ap.add_argument("--e2e-copy-source", action="store_true",
+                    help="e2e: copy the host source in and add the deposits to it (default: the "
+                         "source is zero on entry, as transferSource leaves it, and is overwritten)")
     ap.add_argument("--eager-steps", type=int, default=2,
                     help="eager steps timed beside the graph replays (the droplets' drift over all "
                          "steps must stay inside the ghost cells)")
@@ -557,6 +601,10 @@ def main():
     ap.add_argument("--learn-gens", type=int, default=12, help="states along the trajectory labelled")
     ap.add_argument("--learn-gap", type=int, default=2, help="FP64 steps between labelled states")
     ap.add_argument("--learn-epochs", type=int, default=4)
+    ap.add_argument("--also", default="config3,config4,config5",
+                    help="after the config-2 line (N=1, default sizes), the other workloads' figures, each "
+                         "run in its own process; 'none' skips them")
+    ap.add_argument("--also-steps", type=int, default=5)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -744,14 +792,20 @@ def main():
         st_hv = views(st_h, [prob.grown(b, prob.state_ghosts)[0] for b in range(nboxes)])
         src_hv = views(src_h, [prob.grown(b, prob.source_ghosts)[0] for b in range(nboxes)])
         # the state components the update reads (rho, velocity, T, species: all
-        # but rhoH) and every source component are copied, for MKD and MK
+        # but rhoH) are copied in for MKD and MK, the source components back;
+        # the source is zero on entry to each call, as the reference's
+        # transferSource leaves it, so it is not copied in unless asked
+        # (--e2e-copy-source: copied in and the deposits added to it)
+        sp.set_host_source_in(args.e2e_copy_source)
         used = (5 + prob.nspec) / prob.n_state_comp
-        h2d = 2 * used * sum(a.nbytes for a in st_h) + 2 * sum(a.nbytes for a in src_h)
+        h2d = 2 * used * sum(a.nbytes for a in st_h)
+        if args.e2e_copy_source:
+            h2d += 2 * sum(a.nbytes for a in src_h)
         d2h = 2 * sum(a.nbytes for a in src_h)
 
-        # the deposits accumulate in the host source arrays over the timed
-        # steps (zeroing them is the caller's host work, and the droplets do
-        # not read them); every call still copies them in and back
+        # with --e2e-copy-source the deposits accumulate in the host source
+        # arrays over the timed steps (zeroing them is the caller's host
+        # work, and the droplets do not read them)
         def host_step():
             for do_move in (1, 0):
                 sp.update_particles_host(st_hv, src_hv, prob.flow_dt, 0.0, prob.state_ghosts,
@@ -779,7 +833,9 @@ def main():
                "steps": args.e2e_steps, "form": head,
                "path": "pmp_spray_update_host: pinned host state/source, H2D+D2H inside, "
                        "copies overlapped with the update in box groups, calls stream-ordered "
-                       "(the host waits once, after the last step)"}
+                       "(the host waits once, after the last step); host source "
+                       + ("copied in, deposits added" if args.e2e_copy_source else
+                          "zero on entry (as transferSource leaves it): not copied in, overwritten")}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -833,10 +889,16 @@ def main():
             "clocks": clocks,
             "substeps_per_step": results[head]["substeps"] / args.steps,
         }
-        print(json.dumps(line), flush=True)
     graphs.clear()  # release the graphs before their containers
     for sp in containers.values():
         sp.close()
+    if rank == 0:
+        if (world == 1 and args.workload == "config2" and not args.mesh and not args.droplets
+                and args.also != "none"):
+            del st, src, st_v, src_v
+            torch.cuda.empty_cache()
+            line["other_workloads"] = other_workloads(args)
+        print(json.dumps(line), flush=True)
     if pg:
         pg.destroy_process_group()
 

@@ -291,6 +291,16 @@ int pmp_spray_update_host(
   int source_ghosts, int is_virt, int is_ghost, int do_move,
   double spray_cfl_lev, void* stream);
 
+/* What pmp_spray_update_host does with the host source arrays on entry.
+ * copy_in = 1 (default): they are copied to the device and the deposits are
+ * added to them.  copy_in = 0: they are taken to be zero, as the temporary
+ * source is in the reference's workflow (transferSource,
+ * SprayParticles.H:250-292, folds it into the flow's source and ends with
+ * tmpSource.setVal(0)); the device mirror is cleared instead of copied in
+ * and the call writes the deposits over the host arrays' source
+ * components, which saves one host-to-device copy of the source per call. */
+int pmp_spray_set_host_source_in(pmp_spray* h, int copy_in);
+
 /* moveKickDrift / moveKick (SprayParticles.cpp:37-87). */
 int pmp_spray_move_kick_drift(
   pmp_spray* h, const pmp_box_view* state, const pmp_box_view* source,

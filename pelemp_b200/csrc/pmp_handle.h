@@ -137,6 +137,9 @@ struct pmp_spray {
   // device mirrors of host views for pmp_spray_update_host
   std::vector<double*> stage_state, stage_src;
   std::vector<size_t> stage_state_n, stage_src_n;
+  // pmp_spray_set_host_source_in: 1 = the host source is copied in and the
+  // deposits added to it, 0 = it is taken as zero (device mirror cleared)
+  int host_src_in = 1;
   // streams and events of the overlapped host-view update (copy-in, copy-out;
   // per stage: copied in, updated; start; all copied out)
   static constexpr int kHostStages = 8;

@@ -585,6 +585,26 @@ cudaError_t copy_runs(double* dst, const double* src, const pmp_box_view& v,
   return cudaSuccess;
 }
 
+// The source mirror's components on entry to a host-view update: the host
+// arrays copied in (copy_in), or zeros (the host source is zero on entry).
+cudaError_t source_in(double* dst, const double* src, const pmp_box_view& v,
+                      const std::vector<std::pair<int, int>>& runs, int copy_in, cudaStream_t st)
+{
+  if (copy_in) {
+    return copy_runs(dst, src, v, runs, cudaMemcpyHostToDevice, st);
+  }
+  const size_t one = view_extent(v) - (size_t)(v.ncomp - 1) * v.nstride;
+  for (const auto& r : runs) {
+    const size_t off = (size_t)r.first * v.nstride;
+    const size_t n = (size_t)(r.second - 1 - r.first) * v.nstride + one;
+    const cudaError_t e = cudaMemsetAsync(dst + off, 0, sizeof(double) * n, st);
+    if (e != cudaSuccess) {
+      return e;
+    }
+  }
+  return cudaSuccess;
+}
+
 // tile_at_bndry (Source/PP_Spray/WallFunctions.H:8-35)
 int tile_at_bndry(const pmp_box& b, const pmp_geometry& g)
 {
@@ -1068,7 +1088,7 @@ int update_host_overlapped_impl(
   auto copy_in = [&](int g) -> int {
     for (int b = gfirst[g]; b < gfirst[g + 1]; ++b) {
       PMP_CUDA(h, copy_runs(dst[b].p, hst[b].p, hst[b], st_runs, cudaMemcpyHostToDevice, h->hs_in));
-      PMP_CUDA(h, copy_runs(dsr[b].p, hsr[b].p, hsr[b], sr_runs, cudaMemcpyHostToDevice, h->hs_in));
+      PMP_CUDA(h, source_in(dsr[b].p, hsr[b].p, hsr[b], sr_runs, h->host_src_in, h->hs_in));
     }
     PMP_CUDA(h, cudaEventRecord(h->hev_in[g], h->hs_in));
     return PMP_OK;
@@ -1931,7 +1951,7 @@ int pmp_spray_update_host(
   }
   for (int b = 0; b < nboxes; ++b) {
     PMP_CUDA(h, copy_runs(dst[b].p, state[b].p, state[b], st_runs, cudaMemcpyHostToDevice, st));
-    PMP_CUDA(h, copy_runs(dsr[b].p, source[b].p, source[b], sr_runs, cudaMemcpyHostToDevice, st));
+    PMP_CUDA(h, source_in(dsr[b].p, source[b].p, source[b], sr_runs, h->host_src_in, st));
   }
   const int rc = do_update(h, dst.data(), dsr.data(), nboxes, flow_dt, state_ghosts, source_ghosts,
                            is_virt, is_ghost, do_move, spray_cfl_lev, st);
@@ -1943,6 +1963,15 @@ int pmp_spray_update_host(
     PMP_CUDA(h, copy_runs(source[b].p, h->stage_src[b], source[b], sr_runs, cudaMemcpyDeviceToHost, st));
   }
   return mark_enqueued(h, st);
+}
+
+int pmp_spray_set_host_source_in(pmp_spray* h, int copy_in)
+{
+  if (!h || (copy_in != 0 && copy_in != 1)) {
+    return PMP_ERR_INVALID;
+  }
+  h->host_src_in = copy_in;
+  return PMP_OK;
 }
 
 int pmp_spray_move_kick_drift(

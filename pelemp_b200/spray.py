@@ -45,6 +45,7 @@ _SIGS = {
     "pmp_spray_move_kick": [C.c_void_p, C.POINTER(capi.BoxView), C.POINTER(capi.BoxView),
                             C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int,
                             C.c_double, C.c_void_p],
+    "pmp_spray_set_host_source_in": [C.c_void_p, C.c_int],
     "pmp_spray_set_mode": [C.c_void_p, C.c_int],
     "pmp_spray_set_coupling": [C.c_void_p, C.c_int],
     "pmp_spray_get_coupling": [C.c_void_p, C.POINTER(C.c_int)],
@@ -294,6 +295,12 @@ class SprayParticleContainer:
             int(is_virt), int(is_ghost), int(do_move), spray_cfl_lev, C.c_void_p(stream)))
         if sync:
             self.sync()
+
+    def set_host_source_in(self, copy_in):
+        """update_particles_host: add the deposits to the host source (True,
+        default) or take it as zero on entry and write the deposits over it
+        (False; saves its host-to-device copy)."""
+        self._check(lib().pmp_spray_set_host_source_in(self._h, int(bool(copy_in))))
 
     def move_kick_drift(self, state, source, dt, time, is_virt, is_ghost, state_ghosts,
                         source_ghosts, do_move=True, spray_cfl_lev=-1.0, stream=0, sync=True):

@@ -39,9 +39,10 @@ def gpu_run(prob, steps, mode=capi.PMP_MODE_FP64, is_ghost=0, keep=None, setup=N
     return parts, srcs, sp
 
 
-def host_run(prob, steps, mode=capi.PMP_MODE_FP64, setup=None, pinned=True):
+def host_run(prob, steps, mode=capi.PMP_MODE_FP64, setup=None, pinned=True, src_fill=0.0):
     """gpu_run through pmp_spray_update_host: state and sources in host memory
-    (page-locked when pinned)."""
+    (page-locked when pinned), the host sources filled with src_fill before
+    each call."""
     import torch
     sp = from_problem(prob, mode=mode)
     if setup is not None:
@@ -56,7 +57,7 @@ def host_run(prob, steps, mode=capi.PMP_MODE_FP64, setup=None, pinned=True):
     srcs = []
     for _step in range(steps):
         for do_move in (1, 0):
-            src = [host(s) for s in prob.new_sources()]
+            src = [host(np.full_like(s, src_fill)) for s in prob.new_sources()]
             src_v = views(src, [prob.grown(b, prob.source_ghosts)[0] for b in range(len(prob.boxes))])
             sp.update_particles_host(st_v, src_v, prob.flow_dt, 0.0, prob.state_ghosts,
                                      prob.source_ghosts, 0, 0, do_move, prob.spray_cfl_lev,

@@ -54,6 +54,7 @@ def test_invalid_arguments_rejected_without_gpu():
     from pelemp_b200 import spray
     L = spray.lib()
     assert L.pmp_spray_create(None, None) == capi.PMP_ERR_INVALID
+    assert L.pmp_spray_set_host_source_in(None, 0) == capi.PMP_ERR_INVALID
     cfg = capi.SprayConfig()
     cfg.nfuel = 0
     cfg.nspec = 3

@@ -4,8 +4,9 @@ of boxes) against pmp_spray_update (device views) on a B200.
 Each droplet bit-identical after every call; deposits equal up to the order
 of the atomic additions (1e-12 of the component's largest).  Cases: the FP64
 form (several box groups, uneven and empty boxes), the mixed form, the PeleC
-coupling, page-locked and pageable host memory, and the FP64 form with a
-non-default launch shape (copies, update and copy-back in sequence).
+coupling, page-locked and pageable host memory, the FP64 form with a
+non-default launch shape (copies, update and copy-back in sequence), and a
+host source taken as zero on entry (not copied in, overwritten).
 """
 import numpy as np
 import pytest
@@ -28,9 +29,10 @@ def uneven(total=120_000):
     return prob
 
 
-def compare(prob, mode=capi.PMP_MODE_FP64, setup=None, pinned=True):
+def compare(prob, mode=capi.PMP_MODE_FP64, setup=None, pinned=True, host_setup=None, src_fill=0.0):
     pd, sd, _ = gpu_run(prob, prob.steps, mode=mode, setup=setup)
-    ph, sh, sp = host_run(prob, prob.steps, mode=mode, setup=setup, pinned=pinned)
+    ph, sh, sp = host_run(prob, prob.steps, mode=mode, setup=host_setup or setup, pinned=pinned,
+                          src_fill=src_fill)
     assert_bitwise(pd, ph)
     for a, b in zip(sd, sh):
         assert source_errors(b, a) <= 1e-12
@@ -58,6 +60,16 @@ def test_host_views_sequential_launch_shape():
     def persistent(sp):
         sp.set_launch(kind=capi.PMP_LAUNCH_PERSISTENT, block=128, regs=96, chunk=512)
     compare(uneven(60_000), setup=persistent)
+
+
+@pytest.mark.parametrize("mode", [capi.PMP_MODE_FP64, capi.PMP_MODE_MIXED])
+def test_host_source_taken_as_zero(mode):
+    """set_host_source_in(False): the host source is not copied in, the call
+    writes the deposits over it.  Host sources pre-filled with 3.0 end equal
+    to the device-view update's deposits into zeroed sources."""
+    def no_copy_in(sp):
+        sp.set_host_source_in(False)
+    compare(uneven(60_000), mode, host_setup=no_copy_in, src_fill=3.0)
 
 
 def test_host_views_copy_only_the_components_used():
