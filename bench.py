@@ -560,7 +560,7 @@ def other_workloads(args):
                 "value": v["value"], "speedup_vs_fp64": v["speedup_vs_fp64"],
                 "error_vs_fp64": {q: e[q] for q in ("T", "mass", "dia") if q in e} or None,
                 "train_s": v.get("train", {}).get("seconds"), "tuples": v.get("train", {}).get("tuples"),
-                "fallback_frac": v["fallback_frac"]}
+                "fallback_frac": v["fallback_frac"], "inner_per_substep": v.get("inner_per_substep")}
         out[w] = o
     return out
 
@@ -676,7 +676,7 @@ def main():
         sp.sync()
         st_ = sp.stats()
         t_max, sub_total = reduce_over_ranks(pg, ev0.elapsed_time(ev1), st_.substeps)
-        return t_max, sub_total, st_.substeps, st_.fallback
+        return t_max, sub_total, st_.substeps, st_.fallback, st_.inner_steps
 
     results = {}
     containers = {}
@@ -706,7 +706,7 @@ def main():
                 if do_move and w > 0:
                     mkd_ms.append(sp.stats().kernel_ms)
         # eager steps (a launch per kernel, the host never waits inside)
-        t_eager, _, _, _ = timed_steps(sp, lambda: step(sp, stream.cuda_stream), args.eager_steps)
+        t_eager, _, _, _, _ = timed_steps(sp, lambda: step(sp, stream.cuda_stream), args.eager_steps)
         graph = None
         sampler = ClockSampler(local)
         if not args.no_graph:
@@ -717,11 +717,11 @@ def main():
                 step(sp, torch.cuda.current_stream().cuda_stream)
             sampler.start()
             time.sleep(0.3)
-            t_max, sub_total, sub_local, fb = timed_steps(sp, graph.replay, args.steps)
+            t_max, sub_total, sub_local, fb, inner = timed_steps(sp, graph.replay, args.steps)
         else:
             sampler.start()
             time.sleep(0.3)
-            t_max, sub_total, sub_local, fb = timed_steps(sp, lambda: step(sp, stream.cuda_stream),
+            t_max, sub_total, sub_local, fb, inner = timed_steps(sp, lambda: step(sp, stream.cuda_stream),
                                                           args.steps)
         c = sampler.stop()
         graphs[form] = graph
@@ -737,7 +737,8 @@ def main():
                      "ms_per_step_eager": t_eager / args.eager_steps,
                      "timed": "whole-step CUDA graph replays" if graph is not None else "eager steps",
                      "mkd_launch_ms": float(np.mean(mkd_ms)), "substeps": sub_total,
-                     "fallback_frac": fb / max(sub_local, 1), "clocks": c})
+                     "fallback_frac": fb / max(sub_local, 1), "clocks": c,
+                     "inner_per_substep": inner / max(sub_local, 1)})
         results[form] = info
 
     fast = [f for f in forms if f != "fp64"]
@@ -848,6 +849,7 @@ def main():
             forms_out[f] = {"value": r["value"], "ms_per_step": r["ms_per_step"],
                             "ms_per_step_eager": r["ms_per_step_eager"], "timed": r["timed"],
                             "mkd_launch_ms": r["mkd_launch_ms"], "fallback_frac": r["fallback_frac"],
+                            "inner_per_substep": r["inner_per_substep"],
                             "speedup_vs_fp64": (r["value"] / results["fp64"]["value"]
                                                 if "fp64" in results else None)}
             if "train" in r:
