@@ -223,19 +223,44 @@ __device__ __forceinline__ void load_gas_rec(const BoxEntry& B, int i, int j, in
 // counters accumulate over every call since the host last read and cleared
 // the block (pmp_spray_sync); fb_count alone is per call (the length of the
 // call's FP64 fallback list, reset by each call before its kernels).
+// The update kernels' counters (droplet-substeps, kills, inner sub-steps),
+// spread over PMP_CTR_SLOTS 32-byte slots: each warp adds its sums to the
+// slot of its CTA, so that the ~3 adds per warp of a 16M-droplet launch do
+// not all queue at one L2 address; the host adds the slots up.
+#ifndef PMP_CTR_SLOTS
+#define PMP_CTR_SLOTS 64
+#endif
+struct alignas(32) CtrSlot {
+  unsigned long long substeps;
+  unsigned long long killed;
+  unsigned long long inner;
+  unsigned long long pad;
+};
+
 struct DevStatus {
   int code;
   int box;
   long long slot;
-  unsigned long long substeps;
-  unsigned long long killed;
-  unsigned long long inner;
   unsigned long long fallback;
   unsigned long long fb_count;
   // learned form: droplets its gate rejects, listed from the end of the
   // fallback list (per call, reset with fb_count)
   unsigned long long fb_gate;
+  // the counters start on a cache line of their own: every CTA reads `code`
+  // when it starts, which must not queue behind the warps' adds
+  alignas(128) CtrSlot ctr[PMP_CTR_SLOTS];
 };
+
+// The counters of a status read back to the host, summed over the slots.
+inline void status_counters(const DevStatus& st, long long& substeps, long long& killed, long long& inner)
+{
+  substeps = killed = inner = 0;
+  for (int i = 0; i < PMP_CTR_SLOTS; ++i) {
+    substeps += (long long)st.ctr[i].substeps;
+    killed += (long long)st.ctr[i].killed;
+    inner += (long long)st.ctr[i].inner;
+  }
+}
 
 // SoA droplet store: ncomp double arrays of length cap, then ids.
 struct DevParts {

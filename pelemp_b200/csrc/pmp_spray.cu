@@ -1207,9 +1207,7 @@ int pmp::sync_status(pmp_spray* h)
     h->stats.kernel_ms = -1.;
     cudaGetLastError();  // not sticky: clear it so that the next call does not report it
   }
-  h->stats.substeps = (long long)h->h_status->substeps;
-  h->stats.killed = (long long)h->h_status->killed;
-  h->stats.inner_steps = (long long)h->h_status->inner;
+  pmp::status_counters(*h->h_status, h->stats.substeps, h->stats.killed, h->stats.inner_steps);
   h->stats.fallback = (long long)h->h_status->fallback;
   if (h->h_status->code != 0) {
     const int b = h->h_status->box;

@@ -575,9 +575,12 @@ __device__ __forceinline__ void flush_counters(const KParams& P, Counters& c)
     c.inner += __shfl_down_sync(mask, c.inner, o);
   }
   if ((threadIdx.x & 31) == 0 && (c.sub | c.killed | c.inner)) {
-    atomicAdd(&P.status->substeps, (unsigned long long)c.sub);
-    atomicAdd(&P.status->killed, (unsigned long long)c.killed);
-    atomicAdd(&P.status->inner, (unsigned long long)c.inner);
+    CtrSlot& k = P.status->ctr[blockIdx.x % PMP_CTR_SLOTS];
+    atomicAdd(&k.substeps, (unsigned long long)c.sub);
+    if (c.killed) {
+      atomicAdd(&k.killed, (unsigned long long)c.killed);
+    }
+    atomicAdd(&k.inner, (unsigned long long)c.inner);
   }
 }
 
