@@ -241,7 +241,9 @@ struct DevStatus {
   int code;
   int box;
   long long slot;
-  unsigned long long fallback;
+  // the fallback lists' counters (adds from the gate and the selection of
+  // small droplets) on a line apart from the error word as well
+  alignas(128) unsigned long long fallback;
   unsigned long long fb_count;
   // learned form: droplets its gate rejects, listed from the end of the
   // fallback list (per call, reset with fb_count)
