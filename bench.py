@@ -275,19 +275,19 @@ KERNEL = {"fp64": "spray_update_fp64<5,2,128>", "mixed": "spray_update_mixed<5,2
 # x this.  The mixed and learned kernels move less than the 184 algorithmic
 # bytes per droplet: their gathers read the FP32 gas records (written by a
 # separate pass) instead of the FP64 state.
-DRAM_BYTES_PER_DROPLET = {"fp64": 184.6, "mixed": 160.1, "learned": 153.4}
+DRAM_BYTES_PER_DROPLET = {"fp64": 184.2, "mixed": 159.9, "learned": 152.9}
 # Pipe utilisation of each form's update kernel in the same captures (% of
 # the pipe's peak while the SM is active: sm__inst_executed_pipe_*; issue:
 # smsp__issue_active), and its measured pipe peaks: the compute side of the
 # roofline.  The kernels are bound by instruction issue and latency, not by
 # one pipe.
 PIPE_PCT = {
-    "mixed": {"issue": 58.97, "xu": 39.06, "fma": 22.14, "alu": 25.42, "fp64": 11.97, "lsu": 15.89,
+    "mixed": {"issue": 59.34, "xu": 39.73, "fma": 22.96, "alu": 23.05, "fp64": 11.87, "lsu": 15.60,
               "tensor": 0.0},
-    "fp64": {"issue": 46.61, "xu": 13.34, "fma": 6.21, "alu": 15.90, "fp64": 32.02, "lsu": 9.69,
+    "fp64": {"issue": 47.04, "xu": 13.46, "fma": 6.25, "alu": 16.06, "fp64": 32.31, "lsu": 9.77,
              "tensor": 0.0},
-    "learned": {"issue": 45.55, "xu": 41.07, "fma": 13.91, "alu": 22.27, "fp64": 8.65, "lsu": 12.16,
-                "tensor": 5.84},
+    "learned": {"issue": 44.79, "xu": 40.63, "fma": 14.27, "alu": 20.49, "fp64": 8.48, "lsu": 11.24,
+                "tensor": 5.85},
 }
 
 
