@@ -287,6 +287,7 @@ struct KParams {
   // call settings
   double flow_dt, sub_dt;
   int num_iter, do_move, is_ghost, nboxes;
+  long long nslots;  // droplet slots in the store (bound of the start-of-CTA prefetch; 0: none)
   const BoxEntry* boxes;
   const int* cta_box;
   const long long* cta_start;

@@ -891,6 +891,7 @@ int prepare_update_impl(
   P.box_begin = h->d_box_begin;
   P.fb_list = h->fb_list;
   P.fb_cap = h->total > 0 ? h->total : 1;
+  P.nslots = h->total;
   return PMP_OK;
 }
 

@@ -611,6 +611,40 @@ __device__ __forceinline__ bool stage_box(const KParams& P, int b, BoxEntry& sB)
   return s_failed != 0;
 }
 
+// Ask for the lines of slot s's droplet (L1) before the CTA waits for its
+// box entry: their DRAM latency then overlaps the start of the CTA, whose
+// droplet loads come after the barrier.
+#ifndef PMP_PREFETCH_DROPLETS
+#define PMP_PREFETCH_DROPLETS 1
+#endif
+__device__ __forceinline__ void prefetch_l1(const void* p)
+{
+  asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
+template <int NF>
+__device__ __forceinline__ void prefetch_droplet(const KParams& P, long long s)
+{
+#if PMP_PREFETCH_DROPLETS
+  if (s < P.nslots) {
+    const DevParts& D = P.parts;
+    prefetch_l1(D.id + s);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      prefetch_l1(D.pos[d] + s);
+      prefetch_l1(D.rd[PMP_PSTATE_VEL + d] + s);
+    }
+    prefetch_l1(D.rd[PMP_PSTATE_T] + s);
+    prefetch_l1(D.rd[PMP_PSTATE_DIA] + s);
+#pragma unroll
+    for (int spf = 0; spf < NF; ++spf) {
+      prefetch_l1(D.rd[PMP_PSTATE_Y + spf] + s);
+    }
+    prefetch_l1(D.rd[PMP_PSTATE_NUMDENS(NF)] + s);
+    prefetch_l1(D.rd[PMP_PSTATE_FILMHGHT(NF)] + s);
+  }
+#endif
+}
+
 // capacities of the gather tiles, in cells: FP64 records (the FP64 forms,
 // 5 CTAs per SM) and FP32 records (the mixed form, 7 CTAs per SM)
 #ifndef PMP_TILE64_CELLS
@@ -625,10 +659,11 @@ __device__ __forceinline__ void fp64_cta(const KParams& P)
 {
   __shared__ BoxEntry sB;
   const int b = P.cta_box[blockIdx.x];
+  const long long s = P.cta_start[blockIdx.x] + threadIdx.x;
+  prefetch_droplet<NF>(P, s);
   if (stage_box(P, b, sB)) {
     return;
   }
-  const long long s = P.cta_start[blockIdx.x] + threadIdx.x;
   Counters c;
   // per thread: position, parcel count, start mass, composition, across the
   // droplet physics (update_one, spray_source_fp64)
@@ -671,10 +706,11 @@ __global__ void __launch_bounds__(BLOCK, PMP_MIXED_MIN_BLOCKS) spray_update_mixe
 {
   __shared__ BoxEntry sB;
   const int b = P.cta_box[blockIdx.x];
+  const long long s = P.cta_start[blockIdx.x] + threadIdx.x;
+  prefetch_droplet<NF>(P, s);
   if (stage_box(P, b, sB)) {
     return;
   }
-  const long long s = P.cta_start[blockIdx.x] + threadIdx.x;
   Counters c;
   // per thread: position, parcel count, start mass, composition (update_one,
   // spray_source_mixed)
