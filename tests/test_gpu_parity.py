@@ -231,3 +231,39 @@ def test_fp64_energy_identity(name, oracle):
     gas = sum(float(np.sum(s[prob.comps().rhoSrcIndx])) for call in sg for s in call) * vol * fdat.dtmod * prob.flow_dt
     assert abs(gas + (m1 - m0)) <= 1e-10 * abs(m1 - m0)
     sp.close()
+
+
+@pytest.mark.parametrize("mode", [capi.PMP_MODE_FP64, capi.PMP_MODE_MIXED])
+def test_counters_exact_per_call(mode, oracle):
+    """The update counters, summed by the host over their device slots: every
+    call's droplet-substeps equal the oracle's count, and its kills equal
+    the droplets the call removed (a fifth of box 0's droplets start at
+    0.75 um and evaporate within the call; the mixed form hands them to its
+    FP64 kernel, so its kills match the oracle's too)."""
+    import torch
+    prob = W.config1(n=20_000, steps=2)
+    prob.parts[0]["rdata"][capi.PSTATE_DIA, ::5] = 0.75e-6
+    mech = oracle.mech(prob.species)
+    rc, fdat = oracle.setup(prob, mech)
+    assert rc == 0
+    parts = prob.copy_parts()
+    sp = from_problem(prob, mode=mode)
+    st_keep, st_v = device_state(prob)
+    killed_total = 0
+    for _step in range(prob.steps):
+        for do_move in (1, 0):
+            alive0 = sum(int(np.sum(p["id"] > 0)) for p in parts)
+            rc, err, n_or = oracle.update(prob, mech, fdat, parts, prob.new_sources(), do_move)
+            assert rc == 0, err.message
+            alive1 = sum(int(np.sum(p["id"] > 0)) for p in parts)
+            _src, src_v = device_sources(prob)
+            sp.update_particles(st_v, src_v, prob.flow_dt, 0.0, prob.state_ghosts, prob.source_ghosts,
+                                0, 0, do_move, prob.spray_cfl_lev, torch.cuda.current_stream().cuda_stream)
+            s = sp.stats()
+            assert s.substeps == n_or
+            assert s.killed == alive0 - alive1
+            assert s.inner_steps >= s.substeps
+            killed_total += s.killed
+    assert killed_total > 0
+    del st_keep
+    sp.close()
