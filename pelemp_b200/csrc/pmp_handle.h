@@ -129,7 +129,7 @@ struct pmp_spray {
   bool pending = false;
   // the mixed form's FP64 list kernel runs on `side` beside the mixed kernel
   cudaStream_t side = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_sel = nullptr;
   pmp_error_info last_err;
   pmp_stats stats;
   // view pointers already checked to be device-accessible

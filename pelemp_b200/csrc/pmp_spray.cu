@@ -949,25 +949,37 @@ int do_update(
   return mark_enqueued(h, st);
 }
 
-// The mixed form over CTA-map items [c0, c0 + n) (Q's map already offset) and
-// droplet slots [s0, s1): the droplets it leaves to the FP64 kernel (d < 2 um)
-// are listed first, then the FP64 list kernel runs on the handle's
-// high-priority side stream beside the mixed kernel (which skips them), and
-// the caller's stream waits for both.  The list kernel is one thread per
-// listed droplet, so it costs the latency of one droplet's FP64 sub-cycles;
-// beside the mixed kernel that latency is hidden.
-int enqueue_mixed(pmp_spray* h, const KParams& Q, int n, long long s0, long long s1, cudaStream_t st)
+// The mixed form over CTA-map items [c0, c0 + n) (Q's map already offset),
+// droplet slots [s0, s1) and boxes [b0, b0 + nb): the droplets it leaves to
+// the FP64 kernel (d < 2 um at the call's start) are listed on the handle's
+// high-priority side stream while the FP32 gas records are built on the
+// caller's stream; the mixed kernel (which skips those droplets itself)
+// starts once both are done, and the FP64 list kernel runs beside it on the
+// side stream (it gathers the FP64 state, not the records).  The list kernel
+// is one thread per listed droplet, so it costs the latency of one droplet's
+// FP64 sub-cycles; beside the mixed kernel that latency is hidden.  The
+// caller's stream waits for both.
+int enqueue_mixed(pmp_spray* h, const KParams& Q, int n, long long s0, long long s1, int b0, int nb,
+                  cudaStream_t st)
 {
   KParams R = Q;
   R.fb_pre = 1;
-  int rc = pmp::launch_select_small(R, s0, s1, st);
-  if (rc != PMP_OK) {
-    return rc;
-  }
   PMP_CUDA(h, cudaEventRecord(h->ev_fork, st));
   PMP_CUDA(h, cudaStreamWaitEvent(h->side, h->ev_fork, 0));
-  rc = dispatch_fp64_list(h->nspec, h->nfuel, R, h->total, h->side);
-  if (rc == PMP_OK) {
+  int rc = pmp::launch_select_small(R, s0, s1, h->side);
+  // the selection must read the droplets before the mixed kernel changes them
+  const cudaError_t es = rc == PMP_OK ? cudaEventRecord(h->ev_sel, h->side) : cudaSuccess;
+  if (rc == PMP_OK && es == cudaSuccess) {
+    rc = dispatch_fp64_list(h->nspec, h->nfuel, R, h->total, h->side);
+  }
+  if (rc == PMP_OK && es == cudaSuccess) {
+    rc = pmp::launch_gas_records(h->nspec, Q, b0, nb, h->gas_rec_max_cells, st);
+    if (rc != PMP_OK) {
+      rc = set_err(h, rc, "no gas-record kernel for this species count");
+    }
+  }
+  const cudaError_t ew = rc == PMP_OK && es == cudaSuccess ? cudaStreamWaitEvent(st, h->ev_sel, 0) : cudaSuccess;
+  if (rc == PMP_OK && es == cudaSuccess && ew == cudaSuccess) {
     rc = pmp::launch_mixed(h->nspec, h->nfuel, R, n, kBlock, st);
   }
   // join the side stream whatever happened (a capture must not end with
@@ -977,6 +989,8 @@ int enqueue_mixed(pmp_spray* h, const KParams& Q, int n, long long s0, long long
   if (rc != PMP_OK) {
     return rc;
   }
+  PMP_CUDA(h, es);
+  PMP_CUDA(h, ew);
   PMP_CUDA(h, e1);
   PMP_CUDA(h, e2);
   return PMP_OK;
@@ -1108,10 +1122,13 @@ int update_host_overlapped_impl(
     Q.list_box0 = b0;
     Q.list_nbox = b1 - b0;
     if (n > 0) {
-      rc = h->mode != PMP_MODE_FP64 ? pmp::launch_gas_records(NS, P, b0, b1 - b0, h->gas_rec_max_cells, st)
-                                    : pmp::launch_gas_records64(h, P, b0, b1 - b0, st);
-      if (rc != PMP_OK) {
-        return set_err(h, rc, "no gas-record kernel for this species count");
+      // the mixed form builds its gas records inside enqueue_mixed
+      if (h->mode != PMP_MODE_MIXED) {
+        rc = h->mode == PMP_MODE_LEARNED ? pmp::launch_gas_records(NS, P, b0, b1 - b0, h->gas_rec_max_cells, st)
+                                         : pmp::launch_gas_records64(h, P, b0, b1 - b0, st);
+        if (rc != PMP_OK) {
+          return set_err(h, rc, "no gas-record kernel for this species count");
+        }
       }
       if (h->mode == PMP_MODE_LEARNED) {
         // the learned kernel takes the whole map and an item range; the
@@ -1121,7 +1138,7 @@ int update_host_overlapped_impl(
         Lq.list_nbox = b1 - b0;
         rc = enqueue_learned(h, Lq, c0, n, h->box_begin[b0], h->box_begin[b1], st);
       } else if (h->mode == PMP_MODE_MIXED) {
-        rc = enqueue_mixed(h, Q, n, h->box_begin[b0], h->box_begin[b1], st);
+        rc = enqueue_mixed(h, Q, n, h->box_begin[b0], h->box_begin[b1], b0, b1 - b0, st);
       } else if (P.pelec) {
         rc = dispatch_fp64_pelec(NS, NF, Q, n, st);
       } else {
@@ -1305,10 +1322,7 @@ int pmp::enqueue_update(pmp_spray* h, const KParams& P, int nboxes, cudaStream_t
         rc = enqueue_learned(h, P, 0, h->ncta, 0, h->total, st);
       }
     } else if (h->mode == PMP_MODE_MIXED) {
-      rc = pmp::launch_gas_records(NS, P, 0, nboxes, h->gas_rec_max_cells, st);
-      if (rc == PMP_OK) {
-        rc = enqueue_mixed(h, P, h->ncta, 0, h->total, st);
-      }
+      rc = enqueue_mixed(h, P, h->ncta, 0, h->total, 0, nboxes, st);
     } else if (P.pelec) {
       rc = pmp::launch_gas_records64(h, P, 0, nboxes, st);
       if (rc == PMP_OK) {
@@ -1437,7 +1451,8 @@ int pmp_spray_create(const pmp_spray_config* cfg, pmp_spray** out)
     if (cudaDeviceGetStreamPriorityRange(&lo, &hi) != cudaSuccess ||
         cudaStreamCreateWithPriority(&h->side, cudaStreamNonBlocking, hi) != cudaSuccess ||
         cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+        cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_sel, cudaEventDisableTiming) != cudaSuccess) {
       pmp_spray_destroy(h);
       return PMP_ERR_CUDA;
     }
@@ -1495,6 +1510,9 @@ int pmp_spray_destroy(pmp_spray* h)
   }
   if (h->ev_join) {
     cudaEventDestroy(h->ev_join);
+  }
+  if (h->ev_sel) {
+    cudaEventDestroy(h->ev_sel);
   }
   if (h->hs_in) {
     cudaStreamDestroy(h->hs_in);
