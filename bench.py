@@ -19,7 +19,10 @@ Arms
   pmp_spray_update_host with the mesh state and source in pinned host memory
   (copies inside the timed region).  ``other_workloads`` (N=1, default
   sizes): the figures of configs 3, 4 and 5, each from a run of this script
-  in its own process.
+  in its own process.  ``operations``: the time-step estimate, derived
+  fields, source transfer and re-binning on the config-2 workload (device
+  time, algorithmic bytes, HBM fraction; their numpy oracle on one core
+  beside them).
 * --impl reference: PeleMP's own spray physics headers (oracle/_ref, built
   from the reference sources) on the host cores, OpenMP over droplets, on a
   bounded random sample of the same workload.
@@ -526,6 +529,114 @@ def bench_batched(args, world, rank, local, pg):
         pg.destroy_process_group()
 
 
+def bench_operations(prob, sp, stream, peak, calls=5, cpu_sample=1_000_000):
+    """The operations around the update on the config-2 workload, each timed
+    with CUDA events on the stream over `calls` calls after two (the entry
+    points that return a value -- the time-step estimate and the re-binning's
+    removed count -- include their read-back): algorithmic bytes, GB/s and
+    the fraction of the HBM peak; beside each, the numpy oracle of the same
+    operation on one host core (the reference's versions are AMReX code that
+    does not build here) on a bounded sample, scaled to the workload."""
+    import torch
+    from pelemp_b200 import workloads as W
+    from pelemp_b200.spray import views
+    from oracle import mesh_oracle as MO
+    nb = len(prob.boxes)
+    nf = prob.nfuel
+    n = prob.n_droplets
+
+    def timed(fn):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(calls):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / calls
+
+    def cpu_timed(fn, scale):
+        t0 = time.perf_counter()
+        fn()
+        return (time.perf_counter() - t0) * 1e3 * scale
+
+    def grown_cells(g):
+        tot = 0
+        for b in range(nb):
+            lo, hi = prob.grown(b, g)
+            tot += int(np.prod([hi[d] - lo[d] + 1 for d in range(3)]))
+        return tot
+
+    out = {}
+    cs = stream.cuda_stream
+    # est_timestep (SprayParticles.cpp:89-140): velocity and id of every droplet
+    ms = timed(lambda: sp.est_timestep(0.5, stream=cs))
+    nbytes = n * (3 * 8 + 4)
+    sub = [{k: v[..., :cpu_sample // nb] for k, v in p.items()} for p in prob.parts]
+    cpu = cpu_timed(lambda: MO.est_timestep(sub, prob.dx, 0.5), n / sum(p["id"].size for p in sub))
+    out["est_timestep"] = {"ms": ms, "bytes": nbytes, "cpu_ms": cpu}
+    # computeDerivedVars (SprayDerive.cpp:9-155): droplets in, 15 + F fields per cell
+    g = 1
+    nvar = 15 + nf
+    dshapes = []
+    for b in range(nb):
+        lo, hi = prob.grown(b, g)
+        dshapes.append((nvar,) + tuple(hi[d] - lo[d] + 1 for d in (2, 1, 0)))
+    dvars = [torch.zeros(s, dtype=torch.float64, device="cuda") for s in dshapes]
+    dv = views(dvars, [prob.grown(b, g)[0] for b in range(nb)])
+    ms = timed(lambda: sp.compute_derived_vars(dv, 0, True, stream=cs))
+    nbytes = n * ((3 + 3 + 1 + 1 + nf + 1 + 1) * 8 + 4) + 2 * grown_cells(g) * nvar * 8
+    rho_coef = np.zeros(16)
+    for f, name in enumerate(prob.fuels):
+        rho_coef[4 * f] = W.LIQUIDS[name]["rho"]
+    want = [np.zeros(s) for s in dshapes]
+    cpu = cpu_timed(lambda: MO.derive(sub, want, [prob.grown(b, g)[0] for b in range(nb)], 0, nf, True,
+                                      rho_coef, prob.plo, prob.dx), n / sum(p["id"].size for p in sub))
+    out["derive"] = {"ms": ms, "bytes": nbytes, "cpu_ms": cpu}
+    del dvars, dv
+    # transferSource + addSpraySrc (SprayParticles.H:250-319): fold the
+    # temporary source's ghosts, add it into the flow's source, zero it
+    gs, ga = prob.source_ghosts, 1
+    tmp = [torch.zeros(s.shape, dtype=torch.float64, device="cuda") for s in prob.new_sources()]
+    tv = views(tmp, [prob.grown(b, gs)[0] for b in range(nb)])
+    act = []
+    for b in range(nb):
+        lo, hi = prob.grown(b, ga)
+        act.append(torch.zeros((prob.n_state_comp,) + tuple(hi[d] - lo[d] + 1 for d in (2, 1, 0)),
+                               dtype=torch.float64, device="cuda"))
+    av = views(act, [prob.grown(b, ga)[0] for b in range(nb)])
+    ms = timed(lambda: sp.transfer_source(tv, av, gs, ga, stream=cs))
+    nsrc = prob.n_src_comp
+    nbytes = 2 * grown_cells(gs) * nsrc * 8 + 2 * grown_cells(ga) * nsrc * 8
+    periodic = [prob.bndry_lo[d] == 0 for d in range(3)]
+    tmp_h = [np.zeros(s.shape) for s in prob.new_sources()]
+    act_h = [a.cpu().numpy() for a in act]
+    dep = list(sp.spray_data().dep_indx)[:nf]
+    cpu = cpu_timed(lambda: MO.transfer_source(tmp_h, [prob.grown(b, gs)[0] for b in range(nb)], act_h,
+                                               [prob.grown(b, ga)[0] for b in range(nb)], prob.boxes,
+                                               prob.domain_lo, prob.domain_hi, periodic, gs, ga,
+                                               comps=prob.comps(), nfuel=nf, dep_indx=dep), 1.0)
+    out["transfer_source"] = {"ms": ms, "bytes": nbytes, "cpu_ms": cpu}
+    del tmp, act, tv, av
+    # re-binning (AMReX Redistribute for this container): every droplet read
+    # and written once in its new order
+    ms = timed(lambda: sp.redistribute(stream=cs))
+    nbytes = 2 * n * ((3 + 10 + nf) * 8 + 4)
+    cpu = cpu_timed(lambda: MO.redistribute(sub, prob.boxes, prob.plo, prob.phi, prob.dx, prob.domain_lo,
+                                            prob.domain_hi, periodic), n / sum(p["id"].size for p in sub))
+    out["redistribute"] = {"ms": ms, "bytes": nbytes, "cpu_ms": cpu}
+    for v in out.values():
+        v["gbs"] = v["bytes"] / (v["ms"] * 1e-3) / 1e9
+        v["frac_hbm"] = v["gbs"] / peak
+    out["what"] = ("device time per call (CUDA events on the stream, mean of %d calls after 2); bytes: "
+                   "algorithmic (droplet fields read or written once, mesh arrays read / written once); "
+                   "cpu_ms: the numpy oracle on one host core, %d droplets (the transfer on the whole "
+                   "mesh), scaled to the workload" % (calls, cpu_sample))
+    return out
+
+
 def other_workloads(args):
     """The other workloads' lines, each from its own process (`--workload W
     --steps S --no-cpu --no-e2e`), reduced to their figures: config 3 the
@@ -594,6 +705,8 @@ def main():
                          "whole step -- source zeroing, MKD and MK -- and eager steps are timed beside)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-ops", action="store_true",
+                    help="skip the timing of the operations around the update (config 2)")
     ap.add_argument("--forms", default="fp64,mixed,learned",
                     help="forms to time; the fastest non-FP64 one is the headline value")
     ap.add_argument("--learn-stride", type=int, default=16,
@@ -838,6 +951,10 @@ def main():
                        + ("copied in, deposits added" if args.e2e_copy_source else
                           "zero on entry (as transferSource leaves it): not copied in, overwritten")}
 
+    ops = None
+    if rank == 0 and world == 1 and args.workload == "config2" and not args.no_ops:
+        ops = bench_operations(prob, containers[head], stream, peak)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(args)
@@ -886,6 +1003,7 @@ def main():
                          if peak_src == "measured" else "fallback 6650 GB/s",
                          "compute": compute_roofline(head, peaks_c)},
             "e2e": e2e,
+            "operations": ops,
             "cpu_baseline": cpu,
             "gpu_launches": 2 * args.steps * KERNELS_PER_CALL[head],
             "clocks": clocks,

@@ -155,6 +155,15 @@ struct pmp_spray {
   int* d_box_map = nullptr;
   void* mesh_scratch = nullptr;
   size_t mesh_scratch_bytes = 0;
+  // re-binning (pmp_spray_redistribute): its working arrays (sort keys and
+  // values, CUB's temporary storage), kept between calls, and a spare
+  // droplet store that the re-binned droplets are gathered into (the old
+  // store then becomes the spare); spare_cap droplets
+  void* rebin_scratch = nullptr;
+  size_t rebin_scratch_bytes = 0;
+  double* soa_spare = nullptr;
+  int* ids_spare = nullptr;
+  long long spare_cap = 0;
   // gas records of the grown boxes (BoxEntry::gr, FP32, mixed and learned
   // forms; BoxEntry::gr64, FP64 form): capacity in bytes, and the largest
   // grown box (cells) of the last prepared update
@@ -196,10 +205,9 @@ int run_update(
   double spray_cfl_lev, cudaStream_t st);
 // pack the staged droplets if needed
 int ensure_packed(pmp_spray* h);
-// replace the packed droplets by soa/ids (device, ncomp arrays of stride
-// box_begin.back(), taken over by the handle), sorted by box and cell; the
-// caller order of every box becomes the stored order
-int install_packed(pmp_spray* h, double* soa, int* ids, const std::vector<long long>& box_begin);
+// after re-binning: the store (soa, ids, perm) already holds the droplets in
+// their new order; install the new box bounds and rebuild the CTA map
+int install_rebinned(pmp_spray* h, const std::vector<long long>& box_begin);
 // pmp_mesh.cu
 void mesh_free(pmp_spray* h);
 // pmp_batch.cu

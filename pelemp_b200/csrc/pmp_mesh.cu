@@ -527,6 +527,28 @@ __global__ void k_gather_soa(const double* src, long long stride_src, const int*
   did[s] = sid[j];
 }
 
+// perm[s] = s - begin[b] for the slots s of box b (the re-binned order is
+// each box's caller order)
+__global__ void k_rebin_perm(long long* perm, const long long* begin, int nb, long long n)
+{
+  const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (s >= n) {
+    return;
+  }
+  int lo = 0, hi = nb;  // the box b with begin[b] <= s < begin[b + 1]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) / 2;
+    if (begin[mid] <= s) {
+      lo = mid;
+    } else {
+      hi = mid;
+    }
+  }
+  perm[s] = s - begin[lo];
+}
+
+size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
 }  // namespace
 
 void mesh_free(pmp_spray* h)
@@ -537,6 +559,9 @@ void mesh_free(pmp_spray* h)
   cudaFree(h->mesh_scratch);
   h->mesh_scratch = nullptr;
   h->mesh_scratch_bytes = 0;
+  cudaFree(h->rebin_scratch);
+  h->rebin_scratch = nullptr;
+  h->rebin_scratch_bytes = 0;
 }
 
 }  // namespace pmp
@@ -820,85 +845,89 @@ extern "C" int pmp_spray_redistribute(pmp_spray* h, long long* removed, void* st
       return set_err(h, PMP_ERR_INVALID, "box too large for the re-binning key");
     }
   }
-  unsigned long long *keys = nullptr, *keys2 = nullptr;
-  long long *idx = nullptr, *perm = nullptr, *d_begin = nullptr;
-  void* tmp = nullptr;
-  double* soa = nullptr;
-  int* ids = nullptr;
+  // working arrays, kept in the handle between calls: keys, sorted keys,
+  // slot indices, sorted indices, box bounds, the box list, CUB's storage
   const long long cap = std::max(n, 1LL);
-  auto cleanup = [&]() {
-    cudaFree(keys);
-    cudaFree(keys2);
-    cudaFree(idx);
-    cudaFree(perm);
-    cudaFree(d_begin);
-    cudaFree(tmp);
-  };
-  if (cudaMalloc(&keys, sizeof(unsigned long long) * cap) != cudaSuccess ||
-      cudaMalloc(&keys2, sizeof(unsigned long long) * cap) != cudaSuccess ||
-      cudaMalloc(&idx, sizeof(long long) * cap) != cudaSuccess ||
-      cudaMalloc(&perm, sizeof(long long) * cap) != cudaSuccess ||
-      cudaMalloc(&d_begin, sizeof(long long) * (nb + 1)) != cudaSuccess) {
-    cleanup();
-    return set_err(h, PMP_ERR_CUDA, "redistribute: allocation failed");
+  int end_bit = kKeyShift;
+  while ((1LL << (end_bit - kKeyShift)) <= nb) {
+    ++end_bit;
   }
+  size_t tbytes = 0;
+  if (n > 0) {
+    cub::DeviceRadixSort::SortPairs(nullptr, tbytes, (const unsigned long long*)nullptr,
+                                    (unsigned long long*)nullptr, (const long long*)nullptr, (long long*)nullptr,
+                                    (int)n, 0, end_bit, st);
+  }
+  const size_t o_keys2 = align256(sizeof(unsigned long long) * cap);
+  const size_t o_idx = o_keys2 + align256(sizeof(unsigned long long) * cap);
+  const size_t o_perm = o_idx + align256(sizeof(long long) * cap);
+  const size_t o_begin = o_perm + align256(sizeof(long long) * cap);
+  const size_t o_boxes = o_begin + align256(sizeof(long long) * (nb + 1));
+  const size_t o_tmp = o_boxes + align256(sizeof(pmp_box) * std::max(nb, 1));
+  const size_t need = o_tmp + align256(std::max(tbytes, (size_t)1));
+  if (h->rebin_scratch_bytes < need) {
+    cudaFree(h->rebin_scratch);
+    h->rebin_scratch = nullptr;
+    h->rebin_scratch_bytes = 0;
+    if (cudaMalloc(&h->rebin_scratch, need) != cudaSuccess) {
+      return set_err(h, PMP_ERR_CUDA, "redistribute: allocation failed");
+    }
+    h->rebin_scratch_bytes = need;
+  }
+  char* base = static_cast<char*>(h->rebin_scratch);
+  unsigned long long* keys = reinterpret_cast<unsigned long long*>(base);
+  unsigned long long* keys2 = reinterpret_cast<unsigned long long*>(base + o_keys2);
+  long long* idx = reinterpret_cast<long long*>(base + o_idx);
+  long long* perm = reinterpret_cast<long long*>(base + o_perm);
+  long long* d_begin = reinterpret_cast<long long*>(base + o_begin);
+  pmp_box* d_boxes = reinterpret_cast<pmp_box*>(base + o_boxes);
+  void* tmp = base + o_tmp;
   const pmp_geometry& g = h->geom;
-  std::vector<pmp_box> hb(h->boxes);
-  pmp_box* d_boxes = nullptr;
-  if (cudaMalloc(&d_boxes, sizeof(pmp_box) * std::max(nb, 1)) != cudaSuccess) {
-    cleanup();
-    return set_err(h, PMP_ERR_CUDA, "redistribute: allocation failed");
-  }
-  cudaMemcpyAsync(d_boxes, hb.data(), sizeof(pmp_box) * nb, cudaMemcpyHostToDevice, st);
+  PMP_TRY(h, cudaMemcpyAsync(d_boxes, h->boxes.data(), sizeof(pmp_box) * nb, cudaMemcpyHostToDevice, st));
   const Domain D = domain_of(h);
   if (n > 0) {
     k_rebin_keys<<<nblk(n), 256, 0, st>>>(h->soa, h->soa + n, h->soa + 2 * n, h->ids, n, h->d_box_map, D, g.plo[0],
                                           g.plo[1], g.plo[2], g.phi[0], g.phi[1], g.phi[2], 1. / g.dx[0], 1. / g.dx[1],
                                           1. / g.dx[2], d_boxes, nb, keys, idx);
-    int end_bit = kKeyShift;
-    while ((1LL << (end_bit - kKeyShift)) <= nb) {
-      ++end_bit;
-    }
-    size_t tbytes = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, tbytes, keys, keys2, idx, perm, (int)n, 0, end_bit, st);
-    if (cudaMalloc(&tmp, tbytes) != cudaSuccess) {
-      cudaFree(d_boxes);
-      cleanup();
-      return set_err(h, PMP_ERR_CUDA, "redistribute: allocation failed");
-    }
     cub::DeviceRadixSort::SortPairs(tmp, tbytes, keys, keys2, idx, perm, (int)n, 0, end_bit, st);
     k_box_bounds<<<nblk(nb + 1, 64), 64, 0, st>>>(keys2, n, nb, d_begin);
   } else {
-    cudaMemsetAsync(d_begin, 0, sizeof(long long) * (nb + 1), st);
+    PMP_TRY(h, cudaMemsetAsync(d_begin, 0, sizeof(long long) * (nb + 1), st));
   }
   std::vector<long long> begin(nb + 1, 0);
-  cudaMemcpyAsync(begin.data(), d_begin, sizeof(long long) * (nb + 1), cudaMemcpyDeviceToHost, st);
-  const cudaError_t e = cudaStreamSynchronize(st);
-  cudaFree(d_boxes);
-  if (e != cudaSuccess || cudaGetLastError() != cudaSuccess) {
-    cleanup();
+  PMP_TRY(h, cudaMemcpyAsync(begin.data(), d_begin, sizeof(long long) * (nb + 1), cudaMemcpyDeviceToHost, st));
+  if (cudaStreamSynchronize(st) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
     return set_err(h, PMP_ERR_CUDA, "redistribute: kernel failed");
   }
   const long long live = begin[nb];
-  const long long lcap = std::max(live, 1LL);
-  if (cudaMalloc(&soa, sizeof(double) * nc * lcap) != cudaSuccess || cudaMalloc(&ids, sizeof(int) * lcap) != cudaSuccess) {
-    cudaFree(soa);
-    cudaFree(ids);
-    cleanup();
-    return set_err(h, PMP_ERR_CUDA, "redistribute: allocation failed");
+  // gather into the spare store (grown when too small), which then becomes
+  // the store; the old store becomes the spare
+  if (h->spare_cap < live || !h->soa_spare) {
+    cudaFree(h->soa_spare);
+    cudaFree(h->ids_spare);
+    h->soa_spare = nullptr;
+    h->ids_spare = nullptr;
+    h->spare_cap = 0;
+    const long long lcap = std::max(live, 1LL);
+    if (cudaMalloc(&h->soa_spare, sizeof(double) * nc * lcap) != cudaSuccess ||
+        cudaMalloc(&h->ids_spare, sizeof(int) * lcap) != cudaSuccess) {
+      return set_err(h, PMP_ERR_CUDA, "redistribute: allocation failed");
+    }
+    h->spare_cap = lcap;
   }
   if (live > 0) {
-    k_gather_soa<<<nblk(live), 256, 0, st>>>(h->soa, n, h->ids, perm, live, nc, soa, ids);
+    k_gather_soa<<<nblk(live), 256, 0, st>>>(h->soa, n, h->ids, perm, live, nc, h->soa_spare, h->ids_spare);
+    // each box's new order is its caller order (h->perm holds >= n >= live slots)
+    k_rebin_perm<<<nblk(live), 256, 0, st>>>(h->perm, d_begin, nb, live);
   }
-  if (cudaStreamSynchronize(st) != cudaSuccess) {
-    cudaFree(soa);
-    cudaFree(ids);
-    cleanup();
+  if (cudaStreamSynchronize(st) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
     return set_err(h, PMP_ERR_CUDA, "redistribute: gather failed");
   }
-  cleanup();
+  std::swap(h->soa, h->soa_spare);
+  std::swap(h->ids, h->ids_spare);
+  h->spare_cap = cap;  // the old store
   if (removed) {
     *removed = n - live;
   }
-  return install_packed(h, soa, ids, begin);
+  return install_rebinned(h, begin);
 }

@@ -178,6 +178,11 @@ void free_packed(pmp_spray* h)
   cudaFree(h->d_cta_start);
   cudaFree(h->d_box_begin);
   cudaFree(h->fb_list);
+  cudaFree(h->soa_spare);
+  cudaFree(h->ids_spare);
+  h->soa_spare = nullptr;
+  h->ids_spare = nullptr;
+  h->spare_cap = 0;
   h->soa = nullptr;
   h->ids = nullptr;
   h->perm = nullptr;
@@ -476,7 +481,9 @@ int build_cta_map(pmp_spray* h)
   PMP_CUDA(h, cudaMalloc(&h->d_box_begin, sizeof(long long) * (nb + 1)));
   PMP_CUDA(h, cudaMemcpy(h->d_box_begin, h->box_begin.data(), sizeof(long long) * (nb + 1),
                          cudaMemcpyHostToDevice));
-  PMP_CUDA(h, cudaMalloc(&h->fb_list, sizeof(long long) * cap));
+  if (!h->fb_list) {  // kept by a re-binning, whose droplet count only falls
+    PMP_CUDA(h, cudaMalloc(&h->fb_list, sizeof(long long) * cap));
+  }
   h->packed = true;
   return PMP_OK;
 }
@@ -1274,33 +1281,26 @@ int pmp::prepare_update(
 
 int pmp::ensure_packed(pmp_spray* h) { return pack(h); }
 
-int pmp::install_packed(pmp_spray* h, double* soa, int* ids, const std::vector<long long>& box_begin)
+int pmp::install_rebinned(pmp_spray* h, const std::vector<long long>& box_begin)
 {
   const int nb = (int)h->boxes.size();
-  free_packed(h);
   h->box_begin = box_begin;
-  const long long total = box_begin[nb];
-  h->total = total;
-  h->soa = soa;
-  h->ids = ids;
-  const long long cap = total > 0 ? total : 1;
-  PMP_CUDA(h, cudaMalloc(&h->perm, sizeof(long long) * cap));
-  {
-    std::vector<long long> perm(total);
-    for (int b = 0; b < nb; ++b) {
-      for (long long o = box_begin[b]; o < box_begin[b + 1]; ++o) {
-        perm[o] = o - box_begin[b];
-      }
-    }
-    if (total > 0) {
-      PMP_CUDA(h, cudaMemcpy(h->perm, perm.data(), sizeof(long long) * total, cudaMemcpyHostToDevice));
-    }
-  }
+  h->total = box_begin[nb];
   for (int b = 0; b < nb; ++b) {
     free_store(h->staged[b]);
     h->staged[b].n = box_begin[b + 1] - box_begin[b];
     h->box_set[b] = true;
   }
+  // the CTA map and the box bounds of the new counts (perm and the fallback
+  // list keep their capacity: the droplet count only falls)
+  cudaFree(h->d_cta_box);
+  cudaFree(h->d_cta_start);
+  cudaFree(h->d_box_begin);
+  h->d_cta_box = nullptr;
+  h->d_cta_start = nullptr;
+  h->d_box_begin = nullptr;
+  h->ncta = 0;
+  pmp::batch_reset(h);
   return build_cta_map(h);
 }
 

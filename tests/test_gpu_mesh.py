@@ -149,3 +149,38 @@ def test_redistribute_then_update():
     assert sp.stats().substeps > 0
     assert sp.est_timestep(0.5) > 0.0
     del st_keep
+
+
+def test_redistribute_repeated():
+    """Re-binning several times in a row: the second call gathers into the
+    store the first one left as its spare, the third runs after an update
+    moved the droplets; every time the boxes hold what the oracle's
+    re-binning of the droplets before the call gives."""
+    import torch
+    prob = W.config2(**SMALL2)
+    rng = np.random.default_rng(11)
+    L = prob.phi - prob.plo
+    for p in prob.parts:
+        n = p["id"].shape[0]
+        move = rng.random(n) < 0.2
+        p["pos"][:, move] += (rng.random((3, int(move.sum()))) - 0.5) * L[:, None]
+        p["id"][rng.random(n) < 0.03] = -1
+    sp = from_problem(prob)
+    periodic = [prob.bndry_lo[d] == 0 for d in range(3)]
+    st_keep, st_v = device_state(prob)
+    for it in range(3):
+        if it == 2:
+            _src, src_v = device_sources(prob)
+            sp.update_particles(st_v, src_v, prob.flow_dt, 0.0, prob.state_ghosts, prob.source_ghosts, 0, 0, 1,
+                                prob.spray_cfl_lev, torch.cuda.current_stream().cuda_stream)
+        cur = [sp.get_particles(b) for b in range(len(prob.boxes))]
+        want = MO.redistribute(cur, prob.boxes, prob.plo, prob.phi, prob.dx, prob.domain_lo, prob.domain_hi,
+                               periodic)
+        removed = sp.redistribute()
+        assert removed == sum(int(np.sum(p["id"] <= 0)) for p in cur)
+        for b in range(len(prob.boxes)):
+            got = sp.get_particles(b)
+            order = np.argsort(got["id"], kind="stable")
+            for k in ("pos", "rdata", "id"):
+                assert np.array_equal(got[k][..., order], want[b][k]), (it, b, k)
+    del st_keep
