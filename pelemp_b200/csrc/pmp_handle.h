@@ -106,6 +106,7 @@ struct pmp_spray {
   long long* perm = nullptr;
   std::vector<long long> box_begin;
   int ncta = 0;
+  int cta_cap = 0;  // allocated entries of d_cta_box / d_cta_start
   int* d_cta_box = nullptr;
   long long* d_cta_start = nullptr;
   long long* d_box_begin = nullptr;

@@ -445,19 +445,21 @@ __global__ void k_zero_views(const View32* v, const long long* prefix, int nb, l
 // --------------------------------------------------------------------------
 // redistribute
 
-constexpr int kKeyShift = 40;
-
+// Sort key of a droplet: its new box o above `shift` bits of its cell's
+// place in the box's sort order (pmp::brick_key); dead droplets and droplets
+// in no box get box nb, so that they sort last.  K / V: 32-bit keys and slot
+// indices when the key fits 32 bits and the count 2^31, else 64-bit.
+template <typename K, typename V>
 __global__ void k_rebin_keys(double* px, double* py, double* pz, const int* id, long long n, const int* map, Domain D,
                              double plo0, double plo1, double plo2, double phi0, double phi1, double phi2, double dxi0,
-                             double dxi1, double dxi2, const pmp_box* boxes, int nb, unsigned long long* keys,
-                             long long* idx)
+                             double dxi1, double dxi2, const pmp_box* boxes, int nb, int shift, K* keys, V* idx)
 {
   const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (s >= n) {
     return;
   }
-  idx[s] = s;
-  const unsigned long long dead = (unsigned long long)nb << kKeyShift;
+  idx[s] = (V)s;
+  const K dead = (K)nb << shift;
   if (!(id[s] > 0)) {
     keys[s] = dead;
     return;
@@ -491,16 +493,18 @@ __global__ void k_rebin_keys(double* px, double* py, double* pz, const int* id, 
   const pmp_box& bx = boxes[o];
   const int ex = bx.hi[0] - bx.lo[0] + 1, ey = bx.hi[1] - bx.lo[1] + 1;
   const unsigned long long local = pmp::brick_key(c[0] - bx.lo[0], c[1] - bx.lo[1], c[2] - bx.lo[2], ex, ey);
-  keys[s] = ((unsigned long long)o << kKeyShift) | local;
+  keys[s] = ((K)o << shift) | (K)local;
 }
 
-__global__ void k_box_bounds(const unsigned long long* keys, long long n, int nb, long long* begin)
+// begin[b]: the first sorted position of box b (b = nb: the dead)
+template <typename K>
+__global__ void k_box_bounds(const K* keys, long long n, int nb, int shift, long long* begin)
 {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b > nb) {
     return;
   }
-  const unsigned long long key = (unsigned long long)b << kKeyShift;
+  const K key = (K)b << shift;
   long long lo = 0, hi = n;  // first index with keys[i] >= key
   while (lo < hi) {
     const long long mid = (lo + hi) / 2;
@@ -513,14 +517,15 @@ __global__ void k_box_bounds(const unsigned long long* keys, long long n, int nb
   begin[b] = lo;
 }
 
-__global__ void k_gather_soa(const double* src, long long stride_src, const int* sid, const long long* perm, long long n,
+template <typename V>
+__global__ void k_gather_soa(const double* src, long long stride_src, const int* sid, const V* perm, long long n,
                              int ncomp, double* dst, int* did)
 {
   const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (s >= n) {
     return;
   }
-  const long long j = perm[s];
+  const long long j = (long long)perm[s];
   for (int c = 0; c < ncomp; ++c) {
     dst[c * n + s] = src[c * stride_src + j];
   }
@@ -548,6 +553,26 @@ __global__ void k_rebin_perm(long long* perm, const long long* begin, int nb, lo
 }
 
 size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+// Offsets of the re-binning's working arrays in the handle's rebin_scratch:
+// keys, sorted keys, slot indices, sorted indices (the gather order), box
+// bounds, the box list, CUB's temporary storage.
+struct RebinLayout {
+  size_t keys2, idx, perm, begin, boxes, tmp, total;
+};
+RebinLayout rebin_layout(long long n, int nb, size_t kbytes, size_t vbytes, size_t tbytes)
+{
+  const size_t cap = (size_t)std::max(n, 1LL);
+  RebinLayout L;
+  L.keys2 = align256(kbytes * cap);
+  L.idx = L.keys2 + align256(kbytes * cap);
+  L.perm = L.idx + align256(vbytes * cap);
+  L.begin = L.perm + align256(vbytes * cap);
+  L.boxes = L.begin + align256(sizeof(long long) * (nb + 1));
+  L.tmp = L.boxes + align256(sizeof(pmp_box) * std::max(nb, 1));
+  L.total = L.tmp + align256(std::max(tbytes, (size_t)1));
+  return L;
+}
 
 }  // namespace
 
@@ -817,6 +842,55 @@ extern "C" int pmp_spray_transfer_source(pmp_spray* h, const pmp_box_view* tmp_s
   return PMP_OK;
 }
 
+// The re-binning's keys, their sort and the box bounds (begin, host copy),
+// with K-bit keys over bits [0, end_bit) and V-bit slot indices; the sorted
+// indices (the gather order) stay in rebin_scratch at RebinLayout::perm.
+template <typename K, typename V>
+static int rebin_sort(pmp_spray* h, cudaStream_t st, long long n, int nb, int shift, int end_bit,
+                      std::vector<long long>& begin)
+{
+  size_t tbytes = 0;
+  if (n > 0) {
+    cub::DeviceRadixSort::SortPairs(nullptr, tbytes, (const K*)nullptr, (K*)nullptr, (const V*)nullptr, (V*)nullptr,
+                                    (int)n, 0, end_bit, st);
+  }
+  const RebinLayout L = rebin_layout(n, nb, sizeof(K), sizeof(V), tbytes);
+  if (h->rebin_scratch_bytes < L.total) {
+    cudaFree(h->rebin_scratch);
+    h->rebin_scratch = nullptr;
+    h->rebin_scratch_bytes = 0;
+    if (cudaMalloc(&h->rebin_scratch, L.total) != cudaSuccess) {
+      return set_err(h, PMP_ERR_CUDA, "redistribute: allocation failed");
+    }
+    h->rebin_scratch_bytes = L.total;
+  }
+  char* base = static_cast<char*>(h->rebin_scratch);
+  K* keys = reinterpret_cast<K*>(base);
+  K* keys2 = reinterpret_cast<K*>(base + L.keys2);
+  V* idx = reinterpret_cast<V*>(base + L.idx);
+  V* perm = reinterpret_cast<V*>(base + L.perm);
+  long long* d_begin = reinterpret_cast<long long*>(base + L.begin);
+  pmp_box* d_boxes = reinterpret_cast<pmp_box*>(base + L.boxes);
+  const pmp_geometry& g = h->geom;
+  PMP_TRY(h, cudaMemcpyAsync(d_boxes, h->boxes.data(), sizeof(pmp_box) * nb, cudaMemcpyHostToDevice, st));
+  const Domain D = domain_of(h);
+  if (n > 0) {
+    k_rebin_keys<K, V><<<nblk(n), 256, 0, st>>>(h->soa, h->soa + n, h->soa + 2 * n, h->ids, n, h->d_box_map, D,
+                                                g.plo[0], g.plo[1], g.plo[2], g.phi[0], g.phi[1], g.phi[2],
+                                                1. / g.dx[0], 1. / g.dx[1], 1. / g.dx[2], d_boxes, nb, shift, keys,
+                                                idx);
+    cub::DeviceRadixSort::SortPairs(base + L.tmp, tbytes, keys, keys2, idx, perm, (int)n, 0, end_bit, st);
+    k_box_bounds<K><<<nblk(nb + 1, 64), 64, 0, st>>>(keys2, n, nb, shift, d_begin);
+  } else {
+    PMP_TRY(h, cudaMemsetAsync(d_begin, 0, sizeof(long long) * (nb + 1), st));
+  }
+  PMP_TRY(h, cudaMemcpyAsync(begin.data(), d_begin, sizeof(long long) * (nb + 1), cudaMemcpyDeviceToHost, st));
+  if (cudaStreamSynchronize(st) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+    return set_err(h, PMP_ERR_CUDA, "redistribute: kernel failed");
+  }
+  return PMP_OK;
+}
+
 extern "C" int pmp_spray_redistribute(pmp_spray* h, long long* removed, void* stream)
 {
   if (!h) {
@@ -838,66 +912,28 @@ extern "C" int pmp_spray_redistribute(pmp_spray* h, long long* removed, void* st
   const int nb = (int)h->boxes.size();
   const long long n = h->total;
   const int nc = h->ncomp();
+  // key bits: the largest box's cell count, then the box index (nb: dead)
+  int shift = 0;
   for (const pmp_box& bx : h->boxes) {
     const unsigned long long cells =
       pmp::brick_key_count(bx.hi[0] - bx.lo[0] + 1, bx.hi[1] - bx.lo[1] + 1, bx.hi[2] - bx.lo[2] + 1);
-    if (cells >= (1ULL << kKeyShift) || nb >= (1 << 22)) {
-      return set_err(h, PMP_ERR_INVALID, "box too large for the re-binning key");
+    while (shift < 63 && (1ULL << shift) < cells) {
+      ++shift;
     }
   }
-  // working arrays, kept in the handle between calls: keys, sorted keys,
-  // slot indices, sorted indices, box bounds, the box list, CUB's storage
-  const long long cap = std::max(n, 1LL);
-  int end_bit = kKeyShift;
-  while ((1LL << (end_bit - kKeyShift)) <= nb) {
+  int end_bit = shift + 1;
+  while (end_bit < 64 && (1LL << (end_bit - shift)) <= nb) {
     ++end_bit;
   }
-  size_t tbytes = 0;
-  if (n > 0) {
-    cub::DeviceRadixSort::SortPairs(nullptr, tbytes, (const unsigned long long*)nullptr,
-                                    (unsigned long long*)nullptr, (const long long*)nullptr, (long long*)nullptr,
-                                    (int)n, 0, end_bit, st);
-  }
-  const size_t o_keys2 = align256(sizeof(unsigned long long) * cap);
-  const size_t o_idx = o_keys2 + align256(sizeof(unsigned long long) * cap);
-  const size_t o_perm = o_idx + align256(sizeof(long long) * cap);
-  const size_t o_begin = o_perm + align256(sizeof(long long) * cap);
-  const size_t o_boxes = o_begin + align256(sizeof(long long) * (nb + 1));
-  const size_t o_tmp = o_boxes + align256(sizeof(pmp_box) * std::max(nb, 1));
-  const size_t need = o_tmp + align256(std::max(tbytes, (size_t)1));
-  if (h->rebin_scratch_bytes < need) {
-    cudaFree(h->rebin_scratch);
-    h->rebin_scratch = nullptr;
-    h->rebin_scratch_bytes = 0;
-    if (cudaMalloc(&h->rebin_scratch, need) != cudaSuccess) {
-      return set_err(h, PMP_ERR_CUDA, "redistribute: allocation failed");
-    }
-    h->rebin_scratch_bytes = need;
-  }
-  char* base = static_cast<char*>(h->rebin_scratch);
-  unsigned long long* keys = reinterpret_cast<unsigned long long*>(base);
-  unsigned long long* keys2 = reinterpret_cast<unsigned long long*>(base + o_keys2);
-  long long* idx = reinterpret_cast<long long*>(base + o_idx);
-  long long* perm = reinterpret_cast<long long*>(base + o_perm);
-  long long* d_begin = reinterpret_cast<long long*>(base + o_begin);
-  pmp_box* d_boxes = reinterpret_cast<pmp_box*>(base + o_boxes);
-  void* tmp = base + o_tmp;
-  const pmp_geometry& g = h->geom;
-  PMP_TRY(h, cudaMemcpyAsync(d_boxes, h->boxes.data(), sizeof(pmp_box) * nb, cudaMemcpyHostToDevice, st));
-  const Domain D = domain_of(h);
-  if (n > 0) {
-    k_rebin_keys<<<nblk(n), 256, 0, st>>>(h->soa, h->soa + n, h->soa + 2 * n, h->ids, n, h->d_box_map, D, g.plo[0],
-                                          g.plo[1], g.plo[2], g.phi[0], g.phi[1], g.phi[2], 1. / g.dx[0], 1. / g.dx[1],
-                                          1. / g.dx[2], d_boxes, nb, keys, idx);
-    cub::DeviceRadixSort::SortPairs(tmp, tbytes, keys, keys2, idx, perm, (int)n, 0, end_bit, st);
-    k_box_bounds<<<nblk(nb + 1, 64), 64, 0, st>>>(keys2, n, nb, d_begin);
-  } else {
-    PMP_TRY(h, cudaMemsetAsync(d_begin, 0, sizeof(long long) * (nb + 1), st));
+  if (end_bit > 62 || nb >= (1 << 22)) {
+    return set_err(h, PMP_ERR_INVALID, "box too large for the re-binning key");
   }
   std::vector<long long> begin(nb + 1, 0);
-  PMP_TRY(h, cudaMemcpyAsync(begin.data(), d_begin, sizeof(long long) * (nb + 1), cudaMemcpyDeviceToHost, st));
-  if (cudaStreamSynchronize(st) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
-    return set_err(h, PMP_ERR_CUDA, "redistribute: kernel failed");
+  const bool narrow = end_bit <= 32 && n < (1LL << 31);
+  const int rc2 = narrow ? rebin_sort<unsigned, int>(h, st, n, nb, shift, end_bit, begin)
+                         : rebin_sort<unsigned long long, long long>(h, st, n, nb, shift, end_bit, begin);
+  if (rc2 != PMP_OK) {
+    return rc2;
   }
   const long long live = begin[nb];
   // gather into the spare store (grown when too small), which then becomes
@@ -916,13 +952,23 @@ extern "C" int pmp_spray_redistribute(pmp_spray* h, long long* removed, void* st
     h->spare_cap = lcap;
   }
   if (live > 0) {
-    k_gather_soa<<<nblk(live), 256, 0, st>>>(h->soa, n, h->ids, perm, live, nc, h->soa_spare, h->ids_spare);
+    const RebinLayout Lr = rebin_layout(n, nb, narrow ? 4 : 8, narrow ? 4 : 8, 0);
+    const void* perm = static_cast<char*>(h->rebin_scratch) + Lr.perm;
+    const long long* d_begin = reinterpret_cast<const long long*>(static_cast<char*>(h->rebin_scratch) + Lr.begin);
+    if (narrow) {
+      k_gather_soa<<<nblk(live), 256, 0, st>>>(h->soa, n, h->ids, static_cast<const int*>(perm), live, nc,
+                                               h->soa_spare, h->ids_spare);
+    } else {
+      k_gather_soa<<<nblk(live), 256, 0, st>>>(h->soa, n, h->ids, static_cast<const long long*>(perm), live, nc,
+                                               h->soa_spare, h->ids_spare);
+    }
     // each box's new order is its caller order (h->perm holds >= n >= live slots)
     k_rebin_perm<<<nblk(live), 256, 0, st>>>(h->perm, d_begin, nb, live);
   }
   if (cudaStreamSynchronize(st) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
     return set_err(h, PMP_ERR_CUDA, "redistribute: gather failed");
   }
+  const long long cap = std::max(n, 1LL);
   std::swap(h->soa, h->soa_spare);
   std::swap(h->ids, h->ids_spare);
   h->spare_cap = cap;  // the old store

@@ -190,6 +190,7 @@ void free_packed(pmp_spray* h)
   h->d_cta_start = nullptr;
   h->d_box_begin = nullptr;
   h->fb_list = nullptr;
+  h->cta_cap = 0;
   h->packed = false;
   h->ncta = 0;
   pmp::batch_reset(h);
@@ -472,13 +473,23 @@ int build_cta_map(pmp_spray* h)
     }
   }
   h->ncta = (int)cb.size();
-  if (h->ncta > 0) {
+  if (h->ncta > h->cta_cap) {  // kept by a re-binning while large enough
+    cudaFree(h->d_cta_box);
+    cudaFree(h->d_cta_start);
+    h->d_cta_box = nullptr;
+    h->d_cta_start = nullptr;
+    h->cta_cap = 0;
     PMP_CUDA(h, cudaMalloc(&h->d_cta_box, sizeof(int) * h->ncta));
     PMP_CUDA(h, cudaMalloc(&h->d_cta_start, sizeof(long long) * h->ncta));
+    h->cta_cap = h->ncta;
+  }
+  if (h->ncta > 0) {
     PMP_CUDA(h, cudaMemcpy(h->d_cta_box, cb.data(), sizeof(int) * h->ncta, cudaMemcpyHostToDevice));
     PMP_CUDA(h, cudaMemcpy(h->d_cta_start, cs.data(), sizeof(long long) * h->ncta, cudaMemcpyHostToDevice));
   }
-  PMP_CUDA(h, cudaMalloc(&h->d_box_begin, sizeof(long long) * (nb + 1)));
+  if (!h->d_box_begin) {
+    PMP_CUDA(h, cudaMalloc(&h->d_box_begin, sizeof(long long) * (nb + 1)));
+  }
   PMP_CUDA(h, cudaMemcpy(h->d_box_begin, h->box_begin.data(), sizeof(long long) * (nb + 1),
                          cudaMemcpyHostToDevice));
   if (!h->fb_list) {  // kept by a re-binning, whose droplet count only falls
@@ -1291,14 +1302,8 @@ int pmp::install_rebinned(pmp_spray* h, const std::vector<long long>& box_begin)
     h->staged[b].n = box_begin[b + 1] - box_begin[b];
     h->box_set[b] = true;
   }
-  // the CTA map and the box bounds of the new counts (perm and the fallback
-  // list keep their capacity: the droplet count only falls)
-  cudaFree(h->d_cta_box);
-  cudaFree(h->d_cta_start);
-  cudaFree(h->d_box_begin);
-  h->d_cta_box = nullptr;
-  h->d_cta_start = nullptr;
-  h->d_box_begin = nullptr;
+  // the CTA map and the box bounds of the new counts (their arrays, perm and
+  // the fallback list keep their capacity: the droplet count only falls)
   h->ncta = 0;
   pmp::batch_reset(h);
   return build_cta_map(h);
