@@ -529,6 +529,47 @@ def bench_batched(args, world, rank, local, pg):
         pg.destroy_process_group()
 
 
+def pcie_rates(host_in, host_out, stream, reps=3):
+    """Host<->device copy rates of the e2e path's pinned arrays, copied with
+    no update beside them: host-to-device, device-to-host, and both at once
+    on two streams (GB/s per direction, from CUDA events)."""
+    import torch
+    din = [torch.empty(a.shape, dtype=torch.float64, device="cuda") for a in host_in]
+    dout = [torch.zeros(a.shape, dtype=torch.float64, device="cuda") for a in host_out]
+    tin = [torch.from_numpy(a) for a in host_in]
+    tout = [torch.from_numpy(a) for a in host_out]
+    b_in = sum(a.nbytes for a in host_in)
+    b_out = sum(a.nbytes for a in host_out)
+    s2 = torch.cuda.Stream()
+
+    def run(h2d, d2h):
+        torch.cuda.synchronize()
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        e[0].record(stream)
+        e[2].record(s2)
+        for _ in range(reps):
+            if h2d:
+                with torch.cuda.stream(stream):
+                    for d, h in zip(din, tin):
+                        d.copy_(h, non_blocking=True)
+            if d2h:
+                with torch.cuda.stream(s2):
+                    for h, d in zip(tout, dout):
+                        h.copy_(d, non_blocking=True)
+        e[1].record(stream)
+        e[3].record(s2)
+        torch.cuda.synchronize()
+        return e[0].elapsed_time(e[1]) * 1e-3, e[2].elapsed_time(e[3]) * 1e-3
+
+    t_in, _ = run(True, False)
+    _, t_out = run(False, True)
+    b1, b2 = run(True, True)
+    out = {"h2d": reps * b_in / t_in / 1e9, "d2h": reps * b_out / t_out / 1e9,
+           "both_h2d": reps * b_in / b1 / 1e9, "both_d2h": reps * b_out / b2 / 1e9}
+    del din, dout
+    return out
+
+
 def bench_operations(prob, sp, stream, peak, calls=5, cpu_sample=1_000_000):
     """The operations around the update on the config-2 workload, each timed
     with CUDA events on the stream over `calls` calls after two (the entry
@@ -950,6 +991,9 @@ def main():
                        "(the host waits once, after the last step); host source "
                        + ("copied in, deposits added" if args.e2e_copy_source else
                           "zero on entry (as transferSource leaves it): not copied in, overwritten")}
+        # the link the copies cross: the same pinned arrays copied alone, each
+        # direction alone and both at once (GB/s per direction)
+        e2e["pcie_gbs"] = pcie_rates(st_h, src_h, stream)
 
     ops = None
     if rank == 0 and world == 1 and args.workload == "config2" and not args.no_ops:

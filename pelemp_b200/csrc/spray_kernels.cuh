@@ -606,6 +606,14 @@ __device__ __forceinline__ void flush_counters(const KParams& P, Counters& c)
 #define PMP_MIXED_MIN_BLOCKS 7  /* 72 registers: 7 CTAs of 128 per SM (measured best against 6 and 8
                                    with the FP32 gas records and the shared-memory stash) */
 #endif
+#ifndef PMP_MIXED_MIN_BLOCKS_SMALL
+#define PMP_MIXED_MIN_BLOCKS_SMALL 8  /* one fuel, <= 3 species: 64 registers, 8 CTAs per SM (config 5:
+                                         +3 % against 7; the 5-species, 2-fuel kernel loses 7 % at 8) */
+#endif
+__host__ __device__ constexpr int mixed_min_blocks(int ns, int nf)
+{
+  return (nf == 1 && ns <= 3) ? PMP_MIXED_MIN_BLOCKS_SMALL : PMP_MIXED_MIN_BLOCKS;
+}
 
 // Copy box b's entry into shared memory (all threads of the CTA call it).
 // Returns true, for the whole CTA, when a call of the handle failed since the
@@ -717,7 +725,7 @@ __global__ void __launch_bounds__(BLOCK, PMP_FP64_MIN_BLOCKS) spray_update_fp64_
 }
 
 template <int NS, int NF, int BLOCK, bool FF, bool PELEC = false>
-__global__ void __launch_bounds__(BLOCK, PMP_MIXED_MIN_BLOCKS) spray_update_mixed(const __grid_constant__ KParams P)
+__global__ void __launch_bounds__(BLOCK, mixed_min_blocks(NS, NF)) spray_update_mixed(const __grid_constant__ KParams P)
 {
   __shared__ BoxEntry sB;
   const int b = P.cta_box[blockIdx.x];
