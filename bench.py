@@ -752,7 +752,8 @@ def main():
                     help="forms to time; the fastest non-FP64 one is the headline value")
     ap.add_argument("--learn-stride", type=int, default=16,
                     help="label every n-th droplet (x4 with the perturbed copies) at each state")
-    ap.add_argument("--learn-gens", type=int, default=12, help="states along the trajectory labelled")
+    ap.add_argument("--learn-gens", type=int, default=13,
+                    help="states along the trajectory labelled (13 x 16M / 16 x 4 = 52M tuples at 16M droplets)")
     ap.add_argument("--learn-gap", type=int, default=2, help="FP64 steps between labelled states")
     ap.add_argument("--learn-epochs", type=int, default=4)
     ap.add_argument("--also", default="config3,config4,config5",
