@@ -710,7 +710,11 @@ def other_workloads(args):
             e = v.get("error_vs_fp64", {})
             o.setdefault("forms", {})[f] = {
                 "value": v["value"], "speedup_vs_fp64": v["speedup_vs_fp64"],
-                "error_vs_fp64": {q: e[q] for q in ("T", "mass", "dia") if q in e} or None,
+                # per quantity (diameter, T_d, velocity, the last step's deposits
+                # of mass, energy and species) and the global balances
+                "error_vs_fp64": {q: e[q] for q in ("T", "mass", "dia", "vel", "deposits_last_step",
+                                                    "mass_balance_last_step", "energy_drift_vs_fp64")
+                                  if q in e} or None,
                 "train_s": v.get("train", {}).get("seconds"), "tuples": v.get("train", {}).get("tuples"),
                 "fallback_frac": v["fallback_frac"], "inner_per_substep": v.get("inner_per_substep")}
         out[w] = o
@@ -843,6 +847,7 @@ def main():
             t_train, rep, ntup = train_surrogate(sp, prob, st_v, src_v, stream.cuda_stream, args)
             info["train"] = {"seconds": t_train, "tuples": rep.tuples, "adam_steps": rep.steps,
                              "val_rel_rms": list(rep.val_rel_rms), "epochs": args.learn_epochs,
+                             "baseline_residual_spread": list(rep.base_resid_frac),
                              "sample_stride": args.learn_stride, "states": args.learn_gens,
                              "steps_between_states": args.learn_gap,
                              "what": "tuples labelled by the FP64 teacher along the workload's "

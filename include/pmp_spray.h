@@ -522,6 +522,10 @@ typedef struct pmp_learn_report {
                               film viscosity, film density), so this is
                               their relative error */
   double train_ms;         /* wall time of pmp_spray_learn_train */
+  double base_resid_frac[5]; /* spread (std) of each output's residual about
+                              the fitted quadratic baseline over the spread
+                              of the output: the network predicts the
+                              residual, so its error scales with this */
 } pmp_learn_report;
 
 /* Label droplets for training: every sample_stride-th droplet (offset from
@@ -540,11 +544,15 @@ int pmp_spray_learn_count(const pmp_spray* h, long long* n);
  * receives the number held. */
 int pmp_spray_learn_tuples(const pmp_spray* h, float* buf, long long* n);
 /* Train the network on the GPU (own forward / backward / Adam kernels; the
- * forward pass rounds weights and activations to bf16 as inference does). */
+ * forward pass rounds weights and activations to bf16 as inference does).
+ * The network learns each output's residual about a quadratic polynomial in
+ * the normalised inputs, fitted first by least squares (FP64) over the
+ * tuples; inference adds the polynomial (FP32) back. */
 int pmp_spray_learn_train(pmp_spray* h, const pmp_learn_config* cfg,
                           pmp_learn_report* report);
-/* get = 1: copy the trained parameters and normalisation to buf; get = 0:
- * install them from buf.  With buf NULL, *count receives the length. */
+/* get = 1: copy the trained parameters, normalisation and baseline
+ * coefficients to buf; get = 0: install them from buf.  With buf NULL,
+ * *count receives the length. */
 int pmp_spray_learn_weights(pmp_spray* h, int get, float* buf,
                             long long* count);
 /* Share of droplets audited by the teacher in each learned update. */

@@ -183,6 +183,7 @@ class LearnReport(C.Structure):
         ("tuples", C.c_longlong), ("steps", C.c_longlong),
         ("loss_first", C.c_double), ("loss_last", C.c_double),
         ("val_rel_rms", C.c_double * 5), ("train_ms", C.c_double),
+        ("base_resid_frac", C.c_double * 5),
     ]
 
 

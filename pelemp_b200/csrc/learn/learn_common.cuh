@@ -37,15 +37,95 @@ constexpr int kLearnIn = 10;
 constexpr int kLearnOut = 5;
 constexpr int kLearnHidden = 64;
 
+// Baseline of the targets.  The network predicts each target's residual
+// about a polynomial in the inputs, fitted by least squares over the
+// training tuples.  The network's error is set by its bf16 weights and
+// activations and is a near-constant fraction (a few 1e-3) of the spread of
+// what it predicts; the polynomial leaves the network a residual with 0.1-3 %
+// of each target's spread, so the same network error is that much smaller in
+// the target.  Terms: the inputs that vary in a spray (ln d, T_d, T_gas,
+// ln(Re mu), Y_liq, Y_fv x2) linear and quadratic, the gas pressure and fuel
+// vapour in the gas linear, and ln(1 + B_M) and its square (the transfer
+// rates' steep dependence near boiling, where Y_fv -> 1).
+constexpr int kBaseQ = 7;                                   // quadratic inputs
+constexpr int kBaseL = 3;                                   // linear-only inputs
+constexpr int kBaseTerms = 1 + kBaseQ + kBaseL + 2 + kBaseQ * (kBaseQ + 1) / 2;  // 41
+__host__ __device__ constexpr int base_q_input(int i)
+{
+  return i < 3 ? i : i + 3;  // 0 1 2 6 7 8 9
+}
+__host__ __device__ constexpr int base_l_input(int i) { return 3 + i; }  // 3 4 5
+
 // Normalisation and gate, FP32, in the kernel parameters of the learned form
 struct LearnNorm {
   float x_mean[kLearnIn];
   float x_inv_std[kLearnIn];
   float x_lo[kLearnIn];   // gate: accepted input range (training range widened by the margin)
   float x_hi[kLearnIn];
-  float y_mean[kLearnOut];
+  float y_mean[kLearnOut];  // of the residual about the baseline
   float y_std[kLearnOut];
+  // baseline coefficients per target: [0] constant, [1..7] linear in the
+  // quadratic inputs, [8..10] linear in the linear-only inputs, [11] ell,
+  // [12] ell^2, then the products z_i z_j (i <= j) row by row
+  float base[kLearnOut][kBaseTerms];
 };
+
+#ifdef __CUDACC__
+// ln(1 + B_M) of a droplet from its raw surrogate inputs: (1 + B_M) =
+// (1 - sum Y_gas,fuel) / (1 - sum Y_fv), B_M capped at 20 as in calcVaporState
+// (Drag.H:125-127); the same function in training and inference.
+__device__ __forceinline__ float base_ell(const float* x)
+{
+  const float num = fmaxf(1.f - x[4] - x[5], 1e-30f);
+  const float den = fmaxf(1.f - x[8] - x[9], 1e-6f);
+  return fminf(flog(num / den), 3.04452244f);  // ln 21
+}
+#endif
+
+// Features of the baseline (the polynomial's terms) of normalised inputs xn
+// and ell = ln(1 + B_M).
+template <typename R>
+__host__ __device__ __forceinline__ void base_features(const float* xn, float ell, R* f)
+{
+  f[0] = R(1);
+  for (int i = 0; i < kBaseQ; ++i) {
+    f[1 + i] = R(xn[base_q_input(i)]);
+  }
+  for (int i = 0; i < kBaseL; ++i) {
+    f[1 + kBaseQ + i] = R(xn[base_l_input(i)]);
+  }
+  f[1 + kBaseQ + kBaseL] = R(ell);
+  f[2 + kBaseQ + kBaseL] = R(ell) * R(ell);
+  int t = 3 + kBaseQ + kBaseL;
+  for (int i = 0; i < kBaseQ; ++i) {
+    for (int j = i; j < kBaseQ; ++j) {
+      f[t++] = R(xn[base_q_input(i)]) * R(xn[base_q_input(j)]);
+    }
+  }
+}
+
+// Baseline of target o, FP32, the quadratic part in nested form:
+// sum_i z_i (b_i + sum_{j >= i} c_ij z_j).
+__host__ __device__ __forceinline__ float learn_base(const LearnNorm& nrm, int o, const float* xn, float ell)
+{
+  const float* c = nrm.base[o];
+  float acc = fmaf(fmaf(c[2 + kBaseQ + kBaseL], ell, c[1 + kBaseQ + kBaseL]), ell, c[0]);
+#pragma unroll
+  for (int i = 0; i < kBaseL; ++i) {
+    acc = fmaf(c[1 + kBaseQ + i], xn[base_l_input(i)], acc);
+  }
+  int t = 3 + kBaseQ + kBaseL;
+#pragma unroll
+  for (int i = 0; i < kBaseQ; ++i) {
+    float s = c[1 + i];
+#pragma unroll
+    for (int j = i; j < kBaseQ; ++j) {
+      s = fmaf(c[t++], xn[base_q_input(j)], s);
+    }
+    acc = fmaf(s, xn[base_q_input(i)], acc);
+  }
+  return acc;
+}
 
 // Raw (un-normalised) surrogate inputs of a droplet.
 template <int NF>

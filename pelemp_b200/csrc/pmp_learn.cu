@@ -74,6 +74,7 @@ struct LearnState {
   double audit_fraction = 0.0;
   double* d_audit = nullptr;
   unsigned long long seed = 1;
+  double target_std[kLearnOut] = {1., 1., 1., 1., 1.};  // of the raw targets (report)
 };
 
 // ---------------------------------------------------------------------------
@@ -289,7 +290,121 @@ __global__ void k_tuple_stats(const float* t, long long n, double* st)
   }
 }
 
-// batch rows: normalised inputs (16 columns, 10 used) and targets (8, 5 used)
+// Normal equations of the baseline fit in FP64: the upper triangle of F^T F
+// (kBaseTerms x kBaseTerms) and F^T Y (kBaseTerms x kLearnOut) over every
+// stride-th tuple, F the baseline features of the normalised inputs and Y the
+// raw targets.  A block of 256 threads stages 256 tuples' features and
+// targets in shared memory; each thread sums fixed entries over them.
+constexpr int kBaseCols = kBaseTerms + kLearnOut;
+constexpr int kBaseTri = kBaseTerms * (kBaseTerms + 1) / 2;
+constexpr int kBaseEntries = kBaseTri + kBaseTerms * kLearnOut;
+__global__ void __launch_bounds__(256) k_base_normal(const float* t, long long n, long long stride,
+                                                     LearnNorm nrm, double* out)
+{
+  __shared__ float F[256][kBaseCols + 1];
+  constexpr int kPer = (kBaseEntries + 255) / 256;
+  int ea[kPer], eb[kPer];
+  double acc[kPer];
+#pragma unroll
+  for (int q = 0; q < kPer; ++q) {
+    const int e = threadIdx.x + 256 * q;
+    int a = -1, b = -1;
+    if (e < kBaseTri) {
+      int r = e;
+      a = 0;
+      while (r >= kBaseTerms - a) {
+        r -= kBaseTerms - a;
+        ++a;
+      }
+      b = a + r;
+    } else if (e < kBaseEntries) {
+      const int r = e - kBaseTri;
+      a = r / kLearnOut;
+      b = kBaseTerms + r % kLearnOut;
+    }
+    ea[q] = a;
+    eb[q] = b;
+    acc[q] = 0.;
+  }
+  const long long m = (n + stride - 1) / stride;
+  for (long long c0 = (long long)blockIdx.x * 256; c0 < m; c0 += (long long)gridDim.x * 256) {
+    const long long i = c0 + threadIdx.x;
+    float* row = F[threadIdx.x];
+    if (i < m) {
+      const float* o = t + (i * stride) * kTupleW;
+      float xn[kLearnIn];
+      for (int k = 0; k < kLearnIn; ++k) {
+        xn[k] = (o[k] - nrm.x_mean[k]) * nrm.x_inv_std[k];
+      }
+      base_features(xn, base_ell(o), row);
+      for (int k = 0; k < kLearnOut; ++k) {
+        row[kBaseTerms + k] = o[kLearnIn + k];
+      }
+    } else {
+      for (int k = 0; k < kBaseCols; ++k) {
+        row[k] = 0.f;
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < kPer; ++q) {
+      if (ea[q] >= 0) {
+        double s = 0.;
+        for (int r = 0; r < 256; ++r) {
+          s = fma((double)F[r][ea[q]], (double)F[r][eb[q]], s);
+        }
+        acc[q] += s;
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int q = 0; q < kPer; ++q) {
+    if (ea[q] >= 0) {
+      atomicAdd(&out[threadIdx.x + 256 * q], acc[q]);
+    }
+  }
+}
+
+// Sum and sum of squares of each target's residual about the baseline
+// (st[0..4], st[5..9]).
+__global__ void k_resid_stats(const float* t, long long n, LearnNorm nrm, double* st)
+{
+  __shared__ double ss[2 * kLearnOut];
+  if (threadIdx.x < 2 * kLearnOut) {
+    ss[threadIdx.x] = 0.;
+  }
+  __syncthreads();
+  double ls[kLearnOut], lq[kLearnOut];
+  for (int k = 0; k < kLearnOut; ++k) {
+    ls[k] = 0.;
+    lq[k] = 0.;
+  }
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float* o = t + i * kTupleW;
+    float xn[kLearnIn];
+    for (int k = 0; k < kLearnIn; ++k) {
+      xn[k] = (o[k] - nrm.x_mean[k]) * nrm.x_inv_std[k];
+    }
+    const float ell = base_ell(o);
+    for (int k = 0; k < kLearnOut; ++k) {
+      const double r = (double)o[kLearnIn + k] - (double)learn_base(nrm, k, xn, ell);
+      ls[k] += r;
+      lq[k] += r * r;
+    }
+  }
+  for (int k = 0; k < kLearnOut; ++k) {
+    atomicAdd(&ss[k], ls[k]);
+    atomicAdd(&ss[kLearnOut + k], lq[k]);
+  }
+  __syncthreads();
+  if (threadIdx.x < 2 * kLearnOut) {
+    atomicAdd(&st[threadIdx.x], ss[threadIdx.x]);
+  }
+}
+
+// batch rows: normalised inputs (16 columns, 10 used) and normalised
+// residual targets about the baseline (8, 5 used)
 __global__ void k_gather_batch(
   const float* t, long long ntrain, long long base, int B, unsigned long long seed, long long step, int random,
   LearnNorm nrm, float* X, float* Y)
@@ -305,11 +420,16 @@ __global__ void k_gather_batch(
     i = base + r;
   }
   const float* o = t + i * kTupleW;
-  for (int k = 0; k < 16; ++k) {
-    X[r * 16 + k] = k < kLearnIn ? (o[k] - nrm.x_mean[k]) * nrm.x_inv_std[k] : 0.f;
+  float xn[kLearnIn];
+  for (int k = 0; k < kLearnIn; ++k) {
+    xn[k] = (o[k] - nrm.x_mean[k]) * nrm.x_inv_std[k];
   }
+  for (int k = 0; k < 16; ++k) {
+    X[r * 16 + k] = k < kLearnIn ? xn[k] : 0.f;
+  }
+  const float ell = base_ell(o);
   for (int k = 0; k < 8; ++k) {
-    Y[r * 8 + k] = k < kLearnOut ? (o[kLearnIn + k] - nrm.y_mean[k]) / nrm.y_std[k] : 0.f;
+    Y[r * 8 + k] = k < kLearnOut ? (o[kLearnIn + k] - learn_base(nrm, k, xn, ell) - nrm.y_mean[k]) / nrm.y_std[k] : 0.f;
   }
 }
 
@@ -715,6 +835,13 @@ static void upload_mlp_tc(LearnState* L, const std::vector<float>& p)
 #ifndef PMP_LEARNED_THREADS
 #define PMP_LEARNED_THREADS 128  /* one M tile per CTA: 4 warps per barrier (measured against 256) */
 #endif
+#ifndef PMP_LEARNED_GRID_CAP
+/* > 0: at most this many CTAs per SM (the resident ones), each looping over
+   map items, so that a CTA allocates tensor memory and loads the weights
+   once; 0: one CTA per item.  4 measured against 0: config 5 (calls of one
+   sub-cycle) 4.88e9 vs 4.31e9 droplet-substeps/s, config 2 equal */
+#define PMP_LEARNED_GRID_CAP 4
+#endif
 #ifndef PMP_LEARNED_MIN_BLOCKS
 #define PMP_LEARNED_MIN_BLOCKS 4  /* 128 registers; 4 CTAs of 47 KB shared memory per SM */
 #endif
@@ -1001,6 +1128,16 @@ __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
             in_range = in_range && xin[k] >= L.norm.x_lo[k] && xin[k] <= L.norm.x_hi[k];
           }
         }
+        // the targets' baseline plus the residual mean; the network adds the
+        // residual (outputs 1 unused with one fuel)
+        float yb[kLearnOut];
+        {
+          const float ell = base_ell(xin);
+#pragma unroll
+          for (int k = 0; k < kLearnOut; ++k) {
+            yb[k] = (NF > 1 || k != 1) && pending ? learn_base(L.norm, k, xn, ell) + L.norm.y_mean[k] : 0.f;
+          }
+        }
         float yo[kLearnOut];
         if (!weights_in) {
           weights_in = true;
@@ -1035,7 +1172,7 @@ __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
           float yv[kLearnOut];
 #pragma unroll
           for (int k = 0; k < kLearnOut; ++k) {
-            yv[k] = fmaf(yo[k], L.norm.y_std[k], L.norm.y_mean[k]);
+            yv[k] = fmaf(yo[k], L.norm.y_std[k], yb[k]);
           }
           if (cur_iter == 0 && isub == 1) {
             // gate: some fuel evaporates, inputs inside the (widened)
@@ -1058,7 +1195,7 @@ __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
           float yv[kLearnOut];
 #pragma unroll
           for (int k = 0; k < kLearnOut; ++k) {
-            yv[k] = fmaf(yo[k], L.norm.y_std[k], L.norm.y_mean[k]);
+            yv[k] = fmaf(yo[k], L.norm.y_std[k], yb[k]);
           }
           const float Tp_f = (float)T_part;
           T_h = Tp_f;
@@ -1388,7 +1525,7 @@ __global__ void k_learn_audit(const __grid_constant__ KParams P, const __grid_co
   mlp_simt(*L.mlp, xn, yp);
   atomicAdd(&L.audit[0], 1.);
   for (int k = 0; k < kLearnOut; ++k) {
-    const double yk = (double)fmaf(yp[k], L.norm.y_std[k], L.norm.y_mean[k]);
+    const double yk = (double)fmaf(yp[k], L.norm.y_std[k], L.norm.y_mean[k] + learn_base(L.norm, k, xn, base_ell(x)));
     const double e = yk - (double)yt[k];
     atomicAdd(&L.audit[1 + k], e * e);
     atomicAdd(&L.audit[6 + k], (double)yt[k] * (double)yt[k]);
@@ -1405,7 +1542,14 @@ static int launch_learned_t(pmp_spray* h, const KParams& P, const LearnParams& L
     }
   }
   constexpr int per = kLearnThreads / kBlock;
-  const int grid = (LP.ncta + per - 1) / per;
+  int grid = (LP.ncta + per - 1) / per;
+#if PMP_LEARNED_GRID_CAP > 0
+  {
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
+    grid = std::min(grid, sms * PMP_LEARNED_GRID_CAP);
+  }
+#endif
   constexpr size_t smem = sizeof(tc::TcMlp) + sizeof(tc::TcTileA) * (kLearnThreads / tc::kTile) +
                           sizeof(double) * learn_stash(NF) * kLearnThreads;
   auto kern = P.fuel_first ? spray_update_learned<NS, NF, kLearnThreads, true>
@@ -1416,9 +1560,8 @@ static int launch_learned_t(pmp_spray* h, const KParams& P, const LearnParams& L
       return PMP_ERR_CUDA;
     }
   }
-  // one CTA per TILES items (a grid capped at the resident CTAs, each looping
-  // over items, measured 2.8x slower: the CTA-wide steps of one item then
-  // leave the SM idle; nor does a shared-memory carveout preference help)
+  // the resident CTAs loop over the items (PMP_LEARNED_GRID_CAP); a
+  // shared-memory carveout preference measured no help
   kern<<<grid, kLearnThreads, smem, st>>>(P, LP);
   return PMP_OK;
 }
@@ -1640,6 +1783,90 @@ extern "C" int pmp_spray_learn_tuples(const pmp_spray* h, float* buf, long long*
   return PMP_OK;
 }
 
+// Least-squares fit of the targets' quadratic baseline (LearnNorm::base) on
+// the tuples, with the input normalisation already in nrm: FP64 normal
+// equations over at most 8M tuples (k_base_normal), a relative ridge of 1e-10
+// (features that never vary get no weight), Cholesky on the host.
+static bool fit_baseline(LearnState* L, long long n, LearnNorm& nrm)
+{
+  const long long stride = std::max(1LL, (n + 8000000LL - 1) / 8000000LL);
+  double* d_acc = nullptr;
+  if (cudaMalloc(&d_acc, sizeof(double) * kBaseEntries) != cudaSuccess) {
+    return false;
+  }
+  cudaMemset(d_acc, 0, sizeof(double) * kBaseEntries);
+  k_base_normal<<<592, 256>>>(L->tuples, n, stride, nrm, d_acc);
+  std::vector<double> acc(kBaseEntries);
+  const bool ok = cudaMemcpy(acc.data(), d_acc, sizeof(double) * kBaseEntries, cudaMemcpyDeviceToHost) == cudaSuccess;
+  cudaFree(d_acc);
+  if (!ok) {
+    return false;
+  }
+  constexpr int T = kBaseTerms;
+  std::vector<double> G(T * T), R(T * kLearnOut);
+  int e = 0;
+  for (int a = 0; a < T; ++a) {
+    for (int b = a; b < T; ++b, ++e) {
+      G[a * T + b] = G[b * T + a] = acc[e];
+    }
+  }
+  for (int a = 0; a < T; ++a) {
+    for (int k = 0; k < kLearnOut; ++k) {
+      R[a * kLearnOut + k] = acc[kBaseTri + a * kLearnOut + k];
+    }
+  }
+  double dmax = 0.;
+  for (int a = 0; a < T; ++a) {
+    dmax = std::max(dmax, G[a * T + a]);
+  }
+  if (!(dmax > 0.)) {
+    return false;
+  }
+  for (int a = 0; a < T; ++a) {
+    G[a * T + a] += 1e-10 * dmax;
+  }
+  // G = C C^T (lower C in place)
+  for (int j = 0; j < T; ++j) {
+    double d = G[j * T + j];
+    for (int k = 0; k < j; ++k) {
+      d -= G[j * T + k] * G[j * T + k];
+    }
+    if (!(d > 0.)) {
+      return false;
+    }
+    d = sqrt(d);
+    G[j * T + j] = d;
+    for (int i = j + 1; i < T; ++i) {
+      double v = G[i * T + j];
+      for (int k = 0; k < j; ++k) {
+        v -= G[i * T + k] * G[j * T + k];
+      }
+      G[i * T + j] = v / d;
+    }
+  }
+  for (int o = 0; o < kLearnOut; ++o) {
+    std::vector<double> y(T);
+    for (int i = 0; i < T; ++i) {  // C y = r
+      double v = R[i * kLearnOut + o];
+      for (int k = 0; k < i; ++k) {
+        v -= G[i * T + k] * y[k];
+      }
+      y[i] = v / G[i * T + i];
+    }
+    for (int i = T - 1; i >= 0; --i) {  // C^T c = y
+      double v = y[i];
+      for (int k = i + 1; k < T; ++k) {
+        v -= G[k * T + i] * y[k];
+      }
+      y[i] = v / G[i * T + i];
+    }
+    for (int i = 0; i < T; ++i) {
+      nrm.base[o][i] = (float)y[i];
+    }
+  }
+  return true;
+}
+
 extern "C" int pmp_spray_learn_train(pmp_spray* h, const pmp_learn_config* cfg, pmp_learn_report* rep)
 {
   if (!h || !cfg) {
@@ -1688,9 +1915,23 @@ extern "C" int pmp_spray_learn_train(pmp_spray* h, const pmp_learn_config* cfg, 
     nrm.x_lo[k] = (float)(lo - w);
     nrm.x_hi[k] = (float)(hi + w);
   }
+  // the baseline of the targets, then the statistics of the residuals
+  if (!fit_baseline(L, n, nrm)) {
+    return set_err(h, PMP_ERR_CUDA, "baseline fit failed");
+  }
   for (int k = 0; k < kLearnOut; ++k) {
     const double mean = stt[kLearnIn + k] / n;
     const double var = std::max(0., stt[15 + kLearnIn + k] / n - mean * mean);
+    L->target_std[k] = var > 0. ? sqrt(var) : 1.;
+  }
+  cudaMemset(L->d_stats, 0, sizeof(double) * 64);
+  k_resid_stats<<<592, 256>>>(L->tuples, n, nrm, L->d_stats);
+  if (cudaMemcpy(stt, L->d_stats, sizeof(double) * 2 * kLearnOut, cudaMemcpyDeviceToHost) != cudaSuccess) {
+    return set_err(h, PMP_ERR_CUDA, "statistics failed");
+  }
+  for (int k = 0; k < kLearnOut; ++k) {
+    const double mean = stt[k] / n;
+    const double var = std::max(0., stt[kLearnOut + k] / n - mean * mean);
     nrm.y_mean[k] = (float)mean;
     nrm.y_std[k] = (float)(var > 0. ? sqrt(var) : 1.);
   }
@@ -1779,6 +2020,9 @@ extern "C" int pmp_spray_learn_train(pmp_spray* h, const pmp_learn_config* cfg, 
       rep->val_rel_rms[k] = sqrt(se[k] / (double)nval);
     }
     rep->train_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    for (int k = 0; k < kLearnOut; ++k) {
+      rep->base_resid_frac[k] = (double)nrm.y_std[k] / L->target_std[k];
+    }
   }
   return PMP_OK;
 }
@@ -1786,7 +2030,8 @@ extern "C" int pmp_spray_learn_train(pmp_spray* h, const pmp_learn_config* cfg, 
 extern "C" int pmp_spray_learn_weights(pmp_spray* h, int get, float* buf, long long* count)
 {
   // layout: kP_N parameters, then x_mean[10] x_inv_std[10] x_lo[10] x_hi[10] y_mean[5] y_std[5]
-  const long long total = kP_N + 4 * kLearnIn + 2 * kLearnOut;
+  // base[5][kBaseTerms]
+  const long long total = kP_N + 4 * kLearnIn + 2 * kLearnOut + kLearnOut * kBaseTerms;
   if (!h || !count) {
     return PMP_ERR_INVALID;
   }
@@ -1816,6 +2061,7 @@ extern "C" int pmp_spray_learn_weights(pmp_spray* h, int get, float* buf, long l
     memcpy(tail + 30, nrm.x_hi, sizeof(float) * kLearnIn);
     memcpy(tail + 40, nrm.y_mean, sizeof(float) * kLearnOut);
     memcpy(tail + 45, nrm.y_std, sizeof(float) * kLearnOut);
+    memcpy(tail + 50, nrm.base, sizeof(float) * kLearnOut * kBaseTerms);
   } else {
     cudaMemcpy(L->params, buf, sizeof(float) * kP_N, cudaMemcpyHostToDevice);
     memcpy(nrm.x_mean, tail, sizeof(float) * kLearnIn);
@@ -1824,6 +2070,7 @@ extern "C" int pmp_spray_learn_weights(pmp_spray* h, int get, float* buf, long l
     memcpy(nrm.x_hi, tail + 30, sizeof(float) * kLearnIn);
     memcpy(nrm.y_mean, tail + 40, sizeof(float) * kLearnOut);
     memcpy(nrm.y_std, tail + 45, sizeof(float) * kLearnOut);
+    memcpy(nrm.base, tail + 50, sizeof(float) * kLearnOut * kBaseTerms);
     std::vector<float> pw(buf, buf + kP_N);
     MlpSmem S;
     build_mlp(pw, S);

@@ -6,15 +6,19 @@ update against the FP64 oracle.
   (relative 2-norm) of the FP64 oracle; bf16-rounded network: 1e-3 / 1e-2
   (a rounding tie may resolve differently after FP32 accumulation);
 * inference (bf16 mma.sync): RMS within 1e-2 of the output scale;
-* update after several MKD+MK steps with a surrogate trained on another
-  sample of the same workload: droplet temperature, diameter and mass within
-  1e-4 relative of the FP64 oracle in RMS over the droplets (99.9% of the
-  droplets within 1e-3; the tail is the surrogate's own error on the
-  transfer rates, largest for small droplets that heat and evaporate fast --
-  every droplet-substep of these workloads takes one inner sub-step, so no
-  sub-step count flips), total liquid mass within 1e-6, liquid + gas mass
-  balance closed to FP64 round-off, deposits within 5e-2 of the component's
-  largest deposit;
+* the network learns each output's residual about a fitted polynomial
+  baseline (its bf16 error scales with the spread of what it predicts);
+* update on the learned form's own workload (config-1 distributions, one
+  fuel, 10 MKD+MK steps) with a surrogate trained on another sample: EVERY
+  droplet's temperature, mass and diameter within 1e-4 relative of the FP64
+  oracle, the fallback share below 1 %;
+* update of the two-fuel config-2 workload (4 steps): droplet temperature,
+  diameter and mass within 1e-5 relative of the FP64 oracle in RMS, 99.9 %
+  of the droplets within 1e-4 and every droplet within 2e-4 (the tail:
+  droplets near the balance of convective heating and latent heat, where
+  the net heating is a small difference of the two modelled fluxes), total
+  liquid mass within 1e-6, liquid + gas mass balance closed to FP64
+  round-off, deposits within 5e-2 of the component's largest deposit;
 * droplets outside the training range go to the FP64 kernel: bit-identical
   to the oracle;
 * the learned update against the plain FP64 update and against the method
@@ -135,7 +139,8 @@ def trained():
         _advance(sp, prob, st_v, stream)
     rep = sp.learn_train(epochs=60, batch=2048, audit_fraction=0.05)
     print("training: tuples", rep.tuples, "steps", rep.steps, "loss", rep.loss_first, "->",
-          rep.loss_last, "val", list(rep.val_rel_rms), "ms", rep.train_ms)
+          rep.loss_last, "val", list(rep.val_rel_rms), "ms", rep.train_ms,
+          "residual spread about the baseline", list(rep.base_resid_frac))
     w = sp.learn_weights()
     del st_keep
     sp.close()
@@ -143,9 +148,14 @@ def trained():
 
 
 def test_training_converges(trained):
+    """The network learns the residuals about the fitted baseline: the
+    baseline leaves a few percent of each output's spread or less, the
+    normalised loss falls 100x, and the held-out relative error of every
+    output is below 2e-3."""
     _, rep = trained
-    assert rep.loss_last < 1e-3 * rep.loss_first
-    assert max(rep.val_rel_rms) < 5e-3
+    assert max(rep.base_resid_frac) < 0.1
+    assert rep.loss_last < 1e-2 * rep.loss_first
+    assert max(rep.val_rel_rms) < 2e-3
 
 
 def rel_errors(pg, po, nfuel, rho_l):
@@ -190,9 +200,10 @@ def test_learned_vs_fp64_oracle(trained, oracle):
         print("learned vs FP64 %-4s rms %.3g p99.9 %.3g max %.3g" % (
             k, np.sqrt(np.mean(v ** 2)), np.quantile(v, 0.999), v.max()))
     for k in ("T", "dia", "mass"):
-        assert np.sqrt(np.mean(e[k] ** 2)) <= 1e-4, k
-        assert np.quantile(e[k], 0.999) <= 1e-3, k
-    assert np.sqrt(np.mean(e["vel"] ** 2)) <= 1e-3
+        assert np.sqrt(np.mean(e[k] ** 2)) <= 1e-5, k
+        assert np.quantile(e[k], 0.999) <= 1e-4, k
+        assert e[k].max() <= 2e-4, k
+    assert np.sqrt(np.mean(e["vel"] ** 2)) <= 1e-4
     m_g = sum(float(np.sum(m)) for m in droplet_mass(prob, pg, rho_l))
     m_o = sum(float(np.sum(m)) for m in droplet_mass(prob, po, rho_l))
     print("total liquid mass rel error", m_g / m_o - 1)
@@ -206,6 +217,50 @@ def test_learned_vs_fp64_oracle(trained, oracle):
                     worst = max(worst, float(np.max(np.abs(x[c] - y[c])) / scale))
     print("learned vs FP64 deposit error:", worst)
     assert worst <= 5e-2
+
+
+@pytest.fixture(scope="module")
+def trained_c1():
+    """Surrogate trained on another sample (seed 1) of the learned form's own
+    workload: config-1 distributions (n-heptane droplets, 3 gas species),
+    labelled along its 10 steps."""
+    import torch
+    prob = W.config1(n=40_000, seed=1, steps=10)
+    sp = from_problem(prob)
+    st_keep, st_v = device_state(prob)
+    stream = torch.cuda.current_stream().cuda_stream
+    for step in range(prob.steps):
+        sp.learn_generate(st_v, prob.flow_dt, prob.state_ghosts, True, prob.spray_cfl_lev,
+                          sample_stride=1, augment=3, seed=step + 1, stream=stream)
+        _advance(sp, prob, st_v, stream)
+    rep = sp.learn_train(epochs=30, batch=2048)
+    print("training (config 1): tuples", rep.tuples, "val", list(rep.val_rel_rms),
+          "residual spread about the baseline", list(rep.base_resid_frac))
+    w = sp.learn_weights()
+    del st_keep
+    sp.close()
+    return w
+
+
+def test_learned_max_error_on_its_workload(trained_c1, oracle):
+    """Every droplet's temperature and mass within 1e-4 relative of the FP64
+    oracle after config 1's 10 MKD+MK steps (40k droplets, config-1
+    distributions, the surrogate trained on another sample); the share of
+    droplet-substeps handed to the FP64 kernel is reported and stays below 1 %."""
+    prob = W.config1(n=40_000, seed=0, steps=10)
+    pg, _sg, sp = gpu_run(prob, prob.steps, mode=capi.PMP_MODE_LEARNED,
+                          setup=lambda s: s.set_learn_weights(trained_c1))
+    st = sp.stats()
+    po, _so = oracle_run(oracle, prob, prob.steps)
+    e = rel_errors(pg, po, prob.nfuel, [W.LIQUIDS[f]["rho"] for f in prob.fuels])
+    print("learned (config 1): fallback share %.3g of %d droplet-substeps" % (st.fallback / st.substeps, st.substeps))
+    for k, v in e.items():
+        print("learned vs FP64 (config 1) %-4s rms %.3g p99.9 %.3g max %.3g" % (
+            k, np.sqrt(np.mean(v ** 2)), np.quantile(v, 0.999), v.max()))
+    assert st.fallback < 0.01 * st.substeps
+    assert e["T"].max() <= 1e-4
+    assert e["mass"].max() <= 1e-4
+    assert e["dia"].max() <= 1e-4
 
 
 def test_learned_mass_balance_closes(trained):
