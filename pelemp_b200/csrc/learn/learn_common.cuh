@@ -73,7 +73,7 @@ struct LearnNorm {
 #ifdef __CUDACC__
 // ln(1 + B_M) of a droplet from its raw surrogate inputs: (1 + B_M) =
 // (1 - sum Y_gas,fuel) / (1 - sum Y_fv), B_M capped at 20 as in calcVaporState
-// (Drag.H:125-127); the same function in training and inference.
+// (Drag.H:134); the same function in training and inference.
 __device__ __forceinline__ float base_ell(const float* x)
 {
   const float num = fmaxf(1.f - x[4] - x[5], 1e-30f);
