@@ -45,11 +45,17 @@ constexpr int kLearnHidden = 64;
 // of each target's spread, so the same network error is that much smaller in
 // the target.  Terms: the inputs that vary in a spray (ln d, T_d, T_gas,
 // ln(Re mu), Y_liq, Y_fv x2) linear and quadratic, the gas pressure and fuel
-// vapour in the gas linear, and ln(1 + B_M) and its square (the transfer
-// rates' steep dependence near boiling, where Y_fv -> 1).
+// vapour in the gas linear, ell = ln(1 + B_M) and its square (the transfer
+// rates' steep dependence near boiling, where Y_fv -> 1), and the
+// Frossling-shaped g = (1 + c Re)^(1/3) with its square and its products
+// with the quadratic inputs (the Sherwood and Nusselt numbers' dependence on
+// the Reynolds number).
 constexpr int kBaseQ = 7;                                   // quadratic inputs
 constexpr int kBaseL = 3;                                   // linear-only inputs
-constexpr int kBaseTerms = 1 + kBaseQ + kBaseL + 2 + kBaseQ * (kBaseQ + 1) / 2;  // 41
+constexpr int kBaseEll = 1 + kBaseQ + kBaseL;               // first ell term
+constexpr int kBaseG = kBaseEll + 2;                        // first g term
+constexpr int kBaseQuad = kBaseG + 2 + kBaseQ;              // first product z_i z_j
+constexpr int kBaseTerms = kBaseQuad + kBaseQ * (kBaseQ + 1) / 2;  // 50
 __host__ __device__ constexpr int base_q_input(int i)
 {
   return i < 3 ? i : i + 3;  // 0 1 2 6 7 8 9
@@ -65,27 +71,39 @@ struct LearnNorm {
   float y_mean[kLearnOut];  // of the residual about the baseline
   float y_std[kLearnOut];
   // baseline coefficients per target: [0] constant, [1..7] linear in the
-  // quadratic inputs, [8..10] linear in the linear-only inputs, [11] ell,
-  // [12] ell^2, then the products z_i z_j (i <= j) row by row
+  // quadratic inputs z, [8..10] linear in the linear-only inputs, [11] ell,
+  // [12] ell^2, [13] g, [14] g^2, [15..21] g z_i, then the products z_i z_j
+  // (i <= j) row by row
   float base[kLearnOut][kBaseTerms];
 };
 
+// The baseline's two derived variables of a droplet.
+struct BaseVars {
+  float ell;  // ln(1 + B_M)
+  float g;    // (1 + c Re)^(1/3) - 2
+};
+
 #ifdef __CUDACC__
-// ln(1 + B_M) of a droplet from its raw surrogate inputs: (1 + B_M) =
-// (1 - sum Y_gas,fuel) / (1 - sum Y_fv), B_M capped at 20 as in calcVaporState
-// (Drag.H:134); the same function in training and inference.
-__device__ __forceinline__ float base_ell(const float* x)
+// From the raw surrogate inputs, the same function in training and
+// inference.  (1 + B_M) = (1 - sum Y_gas,fuel) / (1 - sum Y_fv), B_M capped at
+// 20 as in calcVaporState (Drag.H:134).  c Re = exp(x6 - mean(x6) + 2),
+// input 6 being ln(Re mu_gas): the cube root's knee sits at e^-2 of the
+// training set's typical Re mu (chosen on labelled config-2 tuples, where
+// moving the knee 8x changed the fitted residual by under 15 %).
+__device__ __forceinline__ BaseVars base_vars(const float* x, const LearnNorm& nrm)
 {
   const float num = fmaxf(1.f - x[4] - x[5], 1e-30f);
   const float den = fmaxf(1.f - x[8] - x[9], 1e-6f);
-  return fminf(flog(num / den), 3.04452244f);  // ln 21
+  BaseVars v;
+  v.ell = fminf(flog(num / den), 3.04452244f);  // ln 21
+  v.g = fcbrt(1.f + fexp(fminf(x[6] - nrm.x_mean[6] + 2.f, 60.f))) - 2.f;  // centred near its mean
+  return v;
 }
 #endif
 
-// Features of the baseline (the polynomial's terms) of normalised inputs xn
-// and ell = ln(1 + B_M).
+// Features of the baseline (the polynomial's terms) of normalised inputs xn.
 template <typename R>
-__host__ __device__ __forceinline__ void base_features(const float* xn, float ell, R* f)
+__host__ __device__ __forceinline__ void base_features(const float* xn, BaseVars v, R* f)
 {
   f[0] = R(1);
   for (int i = 0; i < kBaseQ; ++i) {
@@ -94,9 +112,14 @@ __host__ __device__ __forceinline__ void base_features(const float* xn, float el
   for (int i = 0; i < kBaseL; ++i) {
     f[1 + kBaseQ + i] = R(xn[base_l_input(i)]);
   }
-  f[1 + kBaseQ + kBaseL] = R(ell);
-  f[2 + kBaseQ + kBaseL] = R(ell) * R(ell);
-  int t = 3 + kBaseQ + kBaseL;
+  f[kBaseEll] = R(v.ell);
+  f[kBaseEll + 1] = R(v.ell) * R(v.ell);
+  f[kBaseG] = R(v.g);
+  f[kBaseG + 1] = R(v.g) * R(v.g);
+  for (int i = 0; i < kBaseQ; ++i) {
+    f[kBaseG + 2 + i] = R(v.g) * R(xn[base_q_input(i)]);
+  }
+  int t = kBaseQuad;
   for (int i = 0; i < kBaseQ; ++i) {
     for (int j = i; j < kBaseQ; ++j) {
       f[t++] = R(xn[base_q_input(i)]) * R(xn[base_q_input(j)]);
@@ -104,17 +127,24 @@ __host__ __device__ __forceinline__ void base_features(const float* xn, float el
   }
 }
 
-// Baseline of target o, FP32, the quadratic part in nested form:
+// Baseline of target o, FP32, in nested form: the g terms as
+// g (c_g + c_gg g + sum_i c_gi z_i), the quadratic part as
 // sum_i z_i (b_i + sum_{j >= i} c_ij z_j).
-__host__ __device__ __forceinline__ float learn_base(const LearnNorm& nrm, int o, const float* xn, float ell)
+__host__ __device__ __forceinline__ float learn_base(const LearnNorm& nrm, int o, const float* xn, BaseVars v)
 {
   const float* c = nrm.base[o];
-  float acc = fmaf(fmaf(c[2 + kBaseQ + kBaseL], ell, c[1 + kBaseQ + kBaseL]), ell, c[0]);
+  float acc = fmaf(fmaf(c[kBaseEll + 1], v.ell, c[kBaseEll]), v.ell, c[0]);
 #pragma unroll
   for (int i = 0; i < kBaseL; ++i) {
     acc = fmaf(c[1 + kBaseQ + i], xn[base_l_input(i)], acc);
   }
-  int t = 3 + kBaseQ + kBaseL;
+  float sg = fmaf(c[kBaseG + 1], v.g, c[kBaseG]);
+#pragma unroll
+  for (int i = 0; i < kBaseQ; ++i) {
+    sg = fmaf(c[kBaseG + 2 + i], xn[base_q_input(i)], sg);
+  }
+  acc = fmaf(sg, v.g, acc);
+  int t = kBaseQuad;
 #pragma unroll
   for (int i = 0; i < kBaseQ; ++i) {
     float s = c[1 + i];

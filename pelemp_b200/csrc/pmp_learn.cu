@@ -293,7 +293,7 @@ __global__ void k_tuple_stats(const float* t, long long n, double* st)
 // Normal equations of the baseline fit in FP64: the upper triangle of F^T F
 // (kBaseTerms x kBaseTerms) and F^T Y (kBaseTerms x kLearnOut) over every
 // stride-th tuple, F the baseline features of the normalised inputs and Y the
-// raw targets.  A block of 256 threads stages 256 tuples' features and
+// raw targets.  A block of 256 threads stages 128 tuples' features and
 // targets in shared memory; each thread sums fixed entries over them.
 constexpr int kBaseCols = kBaseTerms + kLearnOut;
 constexpr int kBaseTri = kBaseTerms * (kBaseTerms + 1) / 2;
@@ -301,7 +301,8 @@ constexpr int kBaseEntries = kBaseTri + kBaseTerms * kLearnOut;
 __global__ void __launch_bounds__(256) k_base_normal(const float* t, long long n, long long stride,
                                                      LearnNorm nrm, double* out)
 {
-  __shared__ float F[256][kBaseCols + 1];
+  constexpr int kChunk = 128;  // tuples staged per pass (shared memory)
+  __shared__ float F[kChunk][kBaseCols + 1];
   constexpr int kPer = (kBaseEntries + 255) / 256;
   int ea[kPer], eb[kPer];
   double acc[kPer];
@@ -327,16 +328,18 @@ __global__ void __launch_bounds__(256) k_base_normal(const float* t, long long n
     acc[q] = 0.;
   }
   const long long m = (n + stride - 1) / stride;
-  for (long long c0 = (long long)blockIdx.x * 256; c0 < m; c0 += (long long)gridDim.x * 256) {
+  for (long long c0 = (long long)blockIdx.x * kChunk; c0 < m; c0 += (long long)gridDim.x * kChunk) {
     const long long i = c0 + threadIdx.x;
-    float* row = F[threadIdx.x];
-    if (i < m) {
+    float* row = F[threadIdx.x % kChunk];
+    if (threadIdx.x >= kChunk) {
+      // the second half of the block only sums
+    } else if (i < m) {
       const float* o = t + (i * stride) * kTupleW;
       float xn[kLearnIn];
       for (int k = 0; k < kLearnIn; ++k) {
         xn[k] = (o[k] - nrm.x_mean[k]) * nrm.x_inv_std[k];
       }
-      base_features(xn, base_ell(o), row);
+      base_features(xn, base_vars(o, nrm), row);
       for (int k = 0; k < kLearnOut; ++k) {
         row[kBaseTerms + k] = o[kLearnIn + k];
       }
@@ -350,7 +353,7 @@ __global__ void __launch_bounds__(256) k_base_normal(const float* t, long long n
     for (int q = 0; q < kPer; ++q) {
       if (ea[q] >= 0) {
         double s = 0.;
-        for (int r = 0; r < 256; ++r) {
+        for (int r = 0; r < kChunk; ++r) {
           s = fma((double)F[r][ea[q]], (double)F[r][eb[q]], s);
         }
         acc[q] += s;
@@ -386,9 +389,9 @@ __global__ void k_resid_stats(const float* t, long long n, LearnNorm nrm, double
     for (int k = 0; k < kLearnIn; ++k) {
       xn[k] = (o[k] - nrm.x_mean[k]) * nrm.x_inv_std[k];
     }
-    const float ell = base_ell(o);
+    const BaseVars bv = base_vars(o, nrm);
     for (int k = 0; k < kLearnOut; ++k) {
-      const double r = (double)o[kLearnIn + k] - (double)learn_base(nrm, k, xn, ell);
+      const double r = (double)o[kLearnIn + k] - (double)learn_base(nrm, k, xn, bv);
       ls[k] += r;
       lq[k] += r * r;
     }
@@ -427,9 +430,9 @@ __global__ void k_gather_batch(
   for (int k = 0; k < 16; ++k) {
     X[r * 16 + k] = k < kLearnIn ? xn[k] : 0.f;
   }
-  const float ell = base_ell(o);
+  const BaseVars bv = base_vars(o, nrm);
   for (int k = 0; k < 8; ++k) {
-    Y[r * 8 + k] = k < kLearnOut ? (o[kLearnIn + k] - learn_base(nrm, k, xn, ell) - nrm.y_mean[k]) / nrm.y_std[k] : 0.f;
+    Y[r * 8 + k] = k < kLearnOut ? (o[kLearnIn + k] - learn_base(nrm, k, xn, bv) - nrm.y_mean[k]) / nrm.y_std[k] : 0.f;
   }
 }
 
@@ -1132,10 +1135,10 @@ __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
         // residual (outputs 1 unused with one fuel)
         float yb[kLearnOut];
         {
-          const float ell = base_ell(xin);
+          const BaseVars bv = base_vars(xin, L.norm);
 #pragma unroll
           for (int k = 0; k < kLearnOut; ++k) {
-            yb[k] = (NF > 1 || k != 1) && pending ? learn_base(L.norm, k, xn, ell) + L.norm.y_mean[k] : 0.f;
+            yb[k] = (NF > 1 || k != 1) && pending ? learn_base(L.norm, k, xn, bv) + L.norm.y_mean[k] : 0.f;
           }
         }
         float yo[kLearnOut];
@@ -1525,7 +1528,7 @@ __global__ void k_learn_audit(const __grid_constant__ KParams P, const __grid_co
   mlp_simt(*L.mlp, xn, yp);
   atomicAdd(&L.audit[0], 1.);
   for (int k = 0; k < kLearnOut; ++k) {
-    const double yk = (double)fmaf(yp[k], L.norm.y_std[k], L.norm.y_mean[k] + learn_base(L.norm, k, xn, base_ell(x)));
+    const double yk = (double)fmaf(yp[k], L.norm.y_std[k], L.norm.y_mean[k] + learn_base(L.norm, k, xn, base_vars(x, L.norm)));
     const double e = yk - (double)yt[k];
     atomicAdd(&L.audit[1 + k], e * e);
     atomicAdd(&L.audit[6 + k], (double)yt[k] * (double)yt[k]);
@@ -1785,8 +1788,9 @@ extern "C" int pmp_spray_learn_tuples(const pmp_spray* h, float* buf, long long*
 
 // Least-squares fit of the targets' quadratic baseline (LearnNorm::base) on
 // the tuples, with the input normalisation already in nrm: FP64 normal
-// equations over at most 8M tuples (k_base_normal), a relative ridge of 1e-10
-// (features that never vary get no weight), Cholesky on the host.
+// equations over at most 8M tuples (k_base_normal), a ridge of 1e-10 of each
+// feature's diagonal (features that never vary get no weight), Cholesky on
+// the host.
 static bool fit_baseline(LearnState* L, long long n, LearnNorm& nrm)
 {
   const long long stride = std::max(1LL, (n + 8000000LL - 1) / 8000000LL);
@@ -1822,8 +1826,11 @@ static bool fit_baseline(LearnState* L, long long n, LearnNorm& nrm)
   if (!(dmax > 0.)) {
     return false;
   }
+  // ridge relative to each feature's own scale (a ridge scaled by the
+  // largest diagonal over-damped the small features: the viscosity
+  // residual doubled), plus a floor for features that never vary
   for (int a = 0; a < T; ++a) {
-    G[a * T + a] += 1e-10 * dmax;
+    G[a * T + a] += 1e-10 * G[a * T + a] + 1e-14 * dmax;
   }
   // G = C C^T (lower C in place)
   for (int j = 0; j < T; ++j) {
