@@ -278,19 +278,19 @@ KERNEL = {"fp64": "spray_update_fp64<5,2,128>", "mixed": "spray_update_mixed<5,2
 # x this.  The mixed and learned kernels move less than the 184 algorithmic
 # bytes per droplet: their gathers read the FP32 gas records (written by a
 # separate pass) instead of the FP64 state.
-DRAM_BYTES_PER_DROPLET = {"fp64": 184.2, "mixed": 159.9, "learned": 152.9}
+DRAM_BYTES_PER_DROPLET = {"fp64": 175.6, "mixed": 158.3, "learned": 153.6}
 # Pipe utilisation of each form's update kernel in the same captures (% of
 # the pipe's peak while the SM is active: sm__inst_executed_pipe_*; issue:
 # smsp__issue_active), and its measured pipe peaks: the compute side of the
 # roofline.  The kernels are bound by instruction issue and latency, not by
 # one pipe.
 PIPE_PCT = {
-    "mixed": {"issue": 59.34, "xu": 39.73, "fma": 22.96, "alu": 23.05, "fp64": 11.87, "lsu": 15.60,
+    "mixed": {"issue": 60.23, "xu": 39.97, "fma": 23.11, "alu": 23.52, "fp64": 11.94, "lsu": 16.02,
               "tensor": 0.0},
-    "fp64": {"issue": 47.04, "xu": 13.46, "fma": 6.25, "alu": 16.06, "fp64": 32.31, "lsu": 9.77,
+    "fp64": {"issue": 47.17, "xu": 13.48, "fma": 6.19, "alu": 16.31, "fp64": 32.35, "lsu": 9.86,
              "tensor": 0.0},
-    "learned": {"issue": 44.79, "xu": 40.63, "fma": 14.27, "alu": 20.49, "fp64": 8.48, "lsu": 11.24,
-                "tensor": 5.85},
+    "learned": {"issue": 47.10, "xu": 38.67, "fma": 16.86, "alu": 19.74, "fp64": 7.84, "lsu": 10.02,
+                "tensor": 5.41},
 }
 
 
