@@ -75,6 +75,10 @@ struct LearnNorm {
   // [12] ell^2, [13] g, [14] g^2, [15..21] g z_i, then the products z_i z_j
   // (i <= j) row by row
   float base[kLearnOut][kBaseTerms];
+  // residual gate: the accepted range of each normalised network output
+  // (the training residuals' range widened by the gate margin)
+  float r_lo[kLearnOut];
+  float r_hi[kLearnOut];
 };
 
 // The baseline's two derived variables of a droplet.

@@ -406,6 +406,54 @@ __global__ void k_resid_stats(const float* t, long long n, LearnNorm nrm, double
   }
 }
 
+// float min / max through the ordered integer view (mn, mx start at +/-3.4e38)
+__device__ __forceinline__ void atomic_min_max_f(float* mn, float* mx, float lo, float hi)
+{
+  if (lo >= 0.f) {
+    atomicMin(reinterpret_cast<int*>(mn), __float_as_int(lo));
+  } else {
+    atomicMax(reinterpret_cast<unsigned*>(mn), __float_as_uint(lo));
+  }
+  if (hi >= 0.f) {
+    atomicMax(reinterpret_cast<int*>(mx), __float_as_int(hi));
+  } else {
+    atomicMin(reinterpret_cast<unsigned*>(mx), __float_as_uint(hi));
+  }
+}
+
+// Range of each target's normalised residual about the baseline over the
+// tuples (mm[0..4] min, mm[5..9] max): the residual gate's bounds.
+__global__ void k_resid_range(const float* t, long long n, LearnNorm nrm, float* mm)
+{
+  float lo[kLearnOut], hi[kLearnOut];
+  for (int k = 0; k < kLearnOut; ++k) {
+    lo[k] = 3.4e38f;
+    hi[k] = -3.4e38f;
+  }
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float* o = t + i * kTupleW;
+    float xn[kLearnIn];
+    for (int k = 0; k < kLearnIn; ++k) {
+      xn[k] = (o[k] - nrm.x_mean[k]) * nrm.x_inv_std[k];
+    }
+    const BaseVars bv = base_vars(o, nrm);
+    for (int k = 0; k < kLearnOut; ++k) {
+      const float r = (o[kLearnIn + k] - learn_base(nrm, k, xn, bv) - nrm.y_mean[k]) / nrm.y_std[k];
+      lo[k] = fminf(lo[k], r);
+      hi[k] = fmaxf(hi[k], r);
+    }
+  }
+  for (int k = 0; k < kLearnOut; ++k) {
+    for (int off = 16; off > 0; off >>= 1) {
+      lo[k] = fminf(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], off));
+      hi[k] = fmaxf(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], off));
+    }
+    if ((threadIdx.x & 31) == 0) {
+      atomic_min_max_f(&mm[k], &mm[kLearnOut + k], lo[k], hi[k]);
+    }
+  }
+}
+
 // batch rows: normalised inputs (16 columns, 10 used) and normalised
 // residual targets about the baseline (8, 5 used)
 __global__ void k_gather_batch(
@@ -1179,11 +1227,13 @@ __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
           }
           if (cur_iter == 0 && isub == 1) {
             // gate: some fuel evaporates, inputs inside the (widened)
-            // training range, outputs finite
+            // training range, outputs finite, and the predicted residuals
+            // about the baseline inside the (widened) training range
             bool in = sumXVap > 0.f && in_range;
 #pragma unroll
             for (int k = 0; k < kLearnOut; ++k) {
-              in = in && isfinite(yv[k]);
+              in = in && isfinite(yv[k]) &&
+                   ((k == 1 && NF == 1) || (yo[k] >= L.norm.r_lo[k] && yo[k] <= L.norm.r_hi[k]));
             }
             if (!in) {
               push_fallback_back(P, s);
@@ -1942,6 +1992,25 @@ extern "C" int pmp_spray_learn_train(pmp_spray* h, const pmp_learn_config* cfg, 
     nrm.y_mean[k] = (float)mean;
     nrm.y_std[k] = (float)(var > 0. ? sqrt(var) : 1.);
   }
+  // the residual gate's range: the training residuals', widened by the margin
+  {
+    float mm[2 * kLearnOut];
+    for (int k = 0; k < kLearnOut; ++k) {
+      mm[k] = 3.4e38f;
+      mm[kLearnOut + k] = -3.4e38f;
+    }
+    float* d_mm = reinterpret_cast<float*>(L->d_stats);
+    cudaMemcpy(d_mm, mm, sizeof(mm), cudaMemcpyHostToDevice);
+    k_resid_range<<<592, 256>>>(L->tuples, n, nrm, d_mm);
+    if (cudaMemcpy(mm, d_mm, sizeof(mm), cudaMemcpyDeviceToHost) != cudaSuccess) {
+      return set_err(h, PMP_ERR_CUDA, "statistics failed");
+    }
+    for (int k = 0; k < kLearnOut; ++k) {
+      const double span = std::max(0., (double)mm[kLearnOut + k] - (double)mm[k]);
+      nrm.r_lo[k] = (float)(mm[k] - margin * span);
+      nrm.r_hi[k] = (float)(mm[kLearnOut + k] + margin * span);
+    }
+  }
   L->gate_margin = margin;
   L->audit_fraction = cfg->audit_fraction;
   L->seed = cfg->seed ? cfg->seed : 1;
@@ -2037,8 +2106,8 @@ extern "C" int pmp_spray_learn_train(pmp_spray* h, const pmp_learn_config* cfg, 
 extern "C" int pmp_spray_learn_weights(pmp_spray* h, int get, float* buf, long long* count)
 {
   // layout: kP_N parameters, then x_mean[10] x_inv_std[10] x_lo[10] x_hi[10] y_mean[5] y_std[5]
-  // base[5][kBaseTerms]
-  const long long total = kP_N + 4 * kLearnIn + 2 * kLearnOut + kLearnOut * kBaseTerms;
+  // base[5][kBaseTerms] r_lo[5] r_hi[5]
+  const long long total = kP_N + 4 * kLearnIn + 4 * kLearnOut + kLearnOut * kBaseTerms;
   if (!h || !count) {
     return PMP_ERR_INVALID;
   }
@@ -2069,6 +2138,8 @@ extern "C" int pmp_spray_learn_weights(pmp_spray* h, int get, float* buf, long l
     memcpy(tail + 40, nrm.y_mean, sizeof(float) * kLearnOut);
     memcpy(tail + 45, nrm.y_std, sizeof(float) * kLearnOut);
     memcpy(tail + 50, nrm.base, sizeof(float) * kLearnOut * kBaseTerms);
+    memcpy(tail + 50 + kLearnOut * kBaseTerms, nrm.r_lo, sizeof(float) * kLearnOut);
+    memcpy(tail + 55 + kLearnOut * kBaseTerms, nrm.r_hi, sizeof(float) * kLearnOut);
   } else {
     cudaMemcpy(L->params, buf, sizeof(float) * kP_N, cudaMemcpyHostToDevice);
     memcpy(nrm.x_mean, tail, sizeof(float) * kLearnIn);
@@ -2078,6 +2149,8 @@ extern "C" int pmp_spray_learn_weights(pmp_spray* h, int get, float* buf, long l
     memcpy(nrm.y_mean, tail + 40, sizeof(float) * kLearnOut);
     memcpy(nrm.y_std, tail + 45, sizeof(float) * kLearnOut);
     memcpy(nrm.base, tail + 50, sizeof(float) * kLearnOut * kBaseTerms);
+    memcpy(nrm.r_lo, tail + 50 + kLearnOut * kBaseTerms, sizeof(float) * kLearnOut);
+    memcpy(nrm.r_hi, tail + 55 + kLearnOut * kBaseTerms, sizeof(float) * kLearnOut);
     std::vector<float> pw(buf, buf + kP_N);
     MlpSmem S;
     build_mlp(pw, S);

@@ -19,8 +19,9 @@ update against the FP64 oracle.
   the net heating is a small difference of the two modelled fluxes), total
   liquid mass within 1e-6, liquid + gas mass balance closed to FP64
   round-off, deposits within 5e-2 of the component's largest deposit;
-* droplets outside the training range go to the FP64 kernel: bit-identical
-  to the oracle;
+* droplets outside the training range (input gate), or whose predicted
+  residual about the baseline lies outside the training residuals' range
+  (residual gate), go to the FP64 kernel: bit-identical to the oracle;
 * the learned update against the plain FP64 update and against the method
   without the network (the mixed form, the same FP32 physics with the
   transport, B_T fixed point and Nusselt/Sherwood numbers evaluated
@@ -307,6 +308,28 @@ def test_gate_sends_out_of_range_droplets_to_fp64(trained, oracle):
     for b, idx in enumerate(planted):
         for k in ("pos", "rdata", "id"):
             assert np.array_equal(pg[b][k][..., idx], po[b][k][..., idx]), (b, k)
+
+
+def test_residual_gate_sends_droplets_to_fp64(trained, oracle):
+    """The residual gate: a network whose predicted residual about the
+    baseline lies outside the training residuals' (widened) range sends the
+    droplet to the FP64 kernel before any of its deposits.  Here the output
+    bias of the first output is moved 1000 training spreads away, so every
+    droplet in range of the input gate trips the residual gate: every droplet
+    is bit-identical to the FP64 oracle."""
+    w, _ = trained
+    w = w.copy()
+    off, _size = M.OFF["b4"]
+    w[off] += 1000.0
+    prob = W.config2(n=20_000, seed=0, **dict(SMALL, steps=1))
+    pg, _, sp = gpu_run(prob, 1, mode=capi.PMP_MODE_LEARNED, setup=lambda s: s.set_learn_weights(w))
+    live = sum(int(np.sum(p["id"] > 0)) for p in prob.parts)
+    print("residual gate: fallback", sp.stats().fallback, "live droplets", live)
+    assert sp.stats().fallback >= live
+    po, _ = oracle_run(oracle, prob, 1)
+    for b in range(len(prob.parts)):
+        for k in ("pos", "rdata", "id"):
+            assert np.array_equal(pg[b][k], po[b][k]), (b, k)
 
 
 def test_learned_gain_over_fp64_and_over_the_method_without_it():
