@@ -1126,13 +1126,12 @@ __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
       if (fdat.fixed_parts) {
         vel_part[0] = vel_part[1] = vel_part[2] = 0.;
       }
-      double T_part = T, dia_part = dia, rho_part = 0.;
+      double T_part = T, dia_part = dia;
 #pragma unroll
       for (int spf = 0; spf < NF; ++spf) {
         Y_part[spf] = Y[spf];
-        rho_part += Y_part[spf] / rhoL(fdat, dmin(T_part, (double)cBoilT[spf]), spf);
       }
-      rho_part = 1. / rho_part;
+      double rho_part = mixed_rho_liquid<NF>(fdat, Y_part, T_part, cBoilT);
       double dt = P.sub_dt;
       const double flow_dt = P.sub_dt;
       int isub = 1, nsub = 1;
@@ -1289,7 +1288,7 @@ __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
           const float diff_vel_mag =
             sqrtf(diff_vel[0] * diff_vel[0] + diff_vel[1] * diff_vel[1] + diff_vel[2] * diff_vel[2]);
           const float Reyn = fdiv(rho_skin * diff_vel_mag * dia_f, mu_skin);
-          const float inv_pmass = (float)(1. / pmass);
+          const float inv_pmass = __frcp_rn((float)pmass);  // consumed in FP32
           float drag_coef = 0.f;
           if (Reyn > 1000.f) {
             drag_coef = 0.424f;
@@ -1338,22 +1337,23 @@ __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
           if (new_mass > 1.E-13 * kMassConv && newT < Tboil) {
             T_part = newT;
             if (NF > 1) {
-              rho_part = 0.;
+              // one reciprocal of the new mass and one of the composition sum
+              const double inv_nm = 1. / new_mass;
               double sumY = 0.;
 #pragma unroll
               for (int spf = 0; spf < NF; ++spf) {
-                Y_part[spf] = dmin(1., dmax(0., (Y_part[spf] * pmass + (double)mi_dot[spf] * part_dt) / new_mass));
+                Y_part[spf] = dmin(1., dmax(0., (Y_part[spf] * pmass + (double)mi_dot[spf] * part_dt) * inv_nm));
                 if (Y_part[spf] <= 1.E-12) {
                   Y_part[spf] = 0.;
                 }
                 sumY += Y_part[spf];
               }
+              const double inv_sum = 1. / sumY;
 #pragma unroll
               for (int spf = 0; spf < NF; ++spf) {
-                Y_part[spf] /= sumY;
-                rho_part += Y_part[spf] / rhoL(fdat, dmin(T_part, (double)cBoilT[spf]), spf);
+                Y_part[spf] *= inv_sum;
               }
-              rho_part = 1. / rho_part;
+              rho_part = mixed_rho_liquid<NF>(fdat, Y_part, T_part, cBoilT);
             } else {
               rho_part = rhoL(fdat, dmin(T_part, (double)cBoilT[0]), 0);
             }

@@ -263,6 +263,27 @@ struct SrcD {
   double eng;
 };
 
+// Liquid density of the droplet, 1 / sum_f Y_f / rhoL_f: with two fuels as
+// rhoL_0 rhoL_1 / (Y_0 rhoL_1 + Y_1 rhoL_0), one FP64 division instead of
+// three (the same value to FP64 round-off).
+template <int NF>
+__device__ __forceinline__ double mixed_rho_liquid(const DevFuel& fdat, const double* Y, double T,
+                                                   const float* cBoilT)
+{
+  if (NF == 2) {
+    constexpr int f1 = NF > 1 ? 1 : 0;
+    const double r0 = rhoL(fdat, dmin(T, (double)cBoilT[0]), 0);
+    const double r1 = rhoL(fdat, dmin(T, (double)cBoilT[f1]), f1);
+    return (r0 * r1) / (Y[0] * r1 + Y[f1] * r0);
+  }
+  double s = 0.;
+#pragma unroll
+  for (int spf = 0; spf < NF; ++spf) {
+    s += Y[spf] / rhoL(fdat, dmin(T, (double)cBoilT[spf]), spf);
+  }
+  return 1. / s;
+}
+
 // calculateSpraySource with FP32 physics and FP64 state (see the file header);
 // PELEC: CGS units and the drag-work and evaporated kinetic-energy terms of
 // the energy source (Drag.H:282-286, 418-421).
@@ -299,13 +320,11 @@ __device__ __forceinline__ int spray_source_mixed(
   }
   double T_part = T_io;
   double dia_part = dia_io;
-  double rho_part = 0.;
 #pragma unroll
   for (int spf = 0; spf < NF; ++spf) {
     Y_part[spf] = Y_io[spf];
-    rho_part += Y_part[spf] / rhoL(fdat, dmin(T_part, (double)cBoilT[spf]), spf);
   }
-  rho_part = 1. / rho_part;
+  double rho_part = mixed_rho_liquid<NF>(fdat, Y_part, T_part, cBoilT);
   double dt = flow_dt;
   int isub = 1;
   int nsub = 1;
@@ -475,7 +494,7 @@ __device__ __forceinline__ int spray_source_mixed(
     const float diff_vel_mag =
       sqrtf(diff_vel[0] * diff_vel[0] + diff_vel[1] * diff_vel[1] + diff_vel[2] * diff_vel[2]);
     const float Reyn = fdiv(rho_skin * diff_vel_mag * dia_f, mu_skin);
-    const float inv_pmass = (float)(1. / pmass);
+    const float inv_pmass = __frcp_rn((float)pmass);  // consumed in FP32
     float drag_coef = 0.f;
     if (Reyn > 1000.f) {
       drag_coef = 0.424f;
@@ -580,22 +599,23 @@ __device__ __forceinline__ int spray_source_mixed(
       if (new_mass > min_mass && newT < Tboil) {
         T_part = newT;
         if (NF > 1) {
-          rho_part = 0.;
+          // one reciprocal of the new mass and one of the composition sum
+          const double inv_nm = 1. / new_mass;
           double sumY = 0.;
 #pragma unroll
           for (int spf = 0; spf < NF; ++spf) {
-            Y_part[spf] = dmin(1., dmax(0., (Y_part[spf] * pmass + (double)mi_dot[spf] * part_dt) / new_mass));
+            Y_part[spf] = dmin(1., dmax(0., (Y_part[spf] * pmass + (double)mi_dot[spf] * part_dt) * inv_nm));
             if (Y_part[spf] <= 1.E-12) {
               Y_part[spf] = 0.;
             }
             sumY += Y_part[spf];
           }
+          const double inv_sum = 1. / sumY;
 #pragma unroll
           for (int spf = 0; spf < NF; ++spf) {
-            Y_part[spf] /= sumY;
-            rho_part += Y_part[spf] / rhoL(fdat, dmin(T_part, (double)cBoilT[spf]), spf);
+            Y_part[spf] *= inv_sum;
           }
-          rho_part = 1. / rho_part;
+          rho_part = mixed_rho_liquid<NF>(fdat, Y_part, T_part, cBoilT);
         } else {
           rho_part = rhoL(fdat, dmin(T_part, (double)cBoilT[0]), 0);
         }
