@@ -286,6 +286,8 @@ struct KParams {
   int s_rho, s_mom, s_eng, s_spec;
   // call settings
   double flow_dt, sub_dt;
+  double cur_coef;  // deposit factor -(1/V) sub_dt / flow_dt (SprayParticles.cpp:419-421), set on the host
+  double inv_dtf;   // 1 / (dtmod sub_dt): the FP32 forms' mass-source factor, set on the host
   int num_iter, do_move, is_ghost, nboxes;
   long long nslots;  // droplet slots in the store (bound of the start-of-CTA prefetch; 0: none)
   const BoxEntry* boxes;

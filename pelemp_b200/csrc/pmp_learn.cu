@@ -1323,7 +1323,7 @@ __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
                        100);
           }
           if (isub == 1) {
-            dt = flow_dt / static_cast<double>(nsub);
+            dt = nsub == 1 ? flow_dt : flow_dt / static_cast<double>(nsub);
           }
           const double part_dt = fdat.dtmod * dt;
           if (!fdat.fixed_parts) {
@@ -1399,7 +1399,7 @@ __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
             src.mom[d] /= static_cast<double>(nsub);
           }
         }
-        const double inv_dtf = 1. / (fdat.dtmod * flow_dt);
+        const double inv_dtf = P.inv_dtf;  // 1 / (dtmod sub_dt), computed on the host
         const double mdot_total = (pmass - startmass) * inv_dtf;
         src.mass = num_ppp * mdot_total;
         if (fdat.mom_trans) {
@@ -1424,7 +1424,7 @@ __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
         c.sub += 1;
         c.inner += static_cast<unsigned>(nsub);
         // deposit into the cell holding the droplet (SprayParticles.cpp:419-441)
-        const double cur_coef = __dmul_rn(-P.inv_vol, P.sub_dt) / P.flow_dt;
+        const double cur_coef = P.cur_coef;  // -(1/V) sub_dt / flow_dt, computed on the host
         bool src_ok = in_box(B.src_lo, B.src_hi, ijkc[0], ijkc[1], ijkc[2]) ||
                       (P.is_ghost && in_box(B.sr_alo, B.sr_ahi, ijkc[0], ijkc[1], ijkc[2]));
         if (!src_ok) {

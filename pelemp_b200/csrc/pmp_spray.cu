@@ -898,6 +898,12 @@ int prepare_update_impl(
     P.num_iter = static_cast<int>(std::ceil(spray_cfl_lev / sub_cfl));
     P.sub_dt = flow_dt / static_cast<double>(P.num_iter);
   }
+  {
+    // launch constants, the same IEEE operations the kernels did per droplet
+    const double t = -P.inv_vol * P.sub_dt;
+    P.cur_coef = t / P.flow_dt;
+    P.inv_dtf = 1. / (P.f.dtmod * P.sub_dt);
+  }
   P.do_move = do_move;
   P.is_ghost = is_ghost;
   P.nboxes = nboxes;

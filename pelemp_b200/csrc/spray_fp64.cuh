@@ -488,7 +488,7 @@ __device__ __forceinline__ int spray_source_fp64(
       }
     }
     if (isub == 1) {
-      dt = flow_dt / static_cast<double>(nsub);
+      dt = nsub == 1 ? flow_dt : flow_dt / static_cast<double>(nsub);  // the same value
     }
     const double part_dt = fdat.dtmod * dt;
     if (!fdat.fixed_parts) {

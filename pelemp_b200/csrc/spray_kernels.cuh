@@ -515,7 +515,7 @@ __device__ __forceinline__ void update_one(const KParams& P, const DevParts& D, 
     c.sub += 1;
     c.inner += static_cast<unsigned>(nsub);
     // source scatter into the cell holding the droplet (SprayParticles.cpp:419-441)
-    const double cur_coef = __dmul_rn(-P.inv_vol, P.sub_dt) / P.flow_dt;
+    const double cur_coef = P.cur_coef;  // -(1/V) sub_dt / flow_dt, computed on the host
     if (!in_box(B.src_lo, B.src_hi, ijkc[0], ijkc[1], ijkc[2])) {
       if (!P.is_ghost || !in_box(B.sr_alo, B.sr_ahi, ijkc[0], ijkc[1], ijkc[2])) {
         set_error(P, PMP_ERR_SOURCE_BOX, b, s);

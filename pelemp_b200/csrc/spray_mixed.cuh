@@ -584,7 +584,7 @@ __device__ __forceinline__ int spray_source_mixed(
       }
     }
     if (isub == 1) {
-      dt = flow_dt / static_cast<double>(nsub);
+      dt = nsub == 1 ? flow_dt : flow_dt / static_cast<double>(nsub);
     }
     const double part_dt = fdat.dtmod * dt;
     if (!fdat.fixed_parts) {
@@ -651,7 +651,8 @@ __device__ __forceinline__ int spray_source_mixed(
       src.mom[d] /= static_cast<double>(nsub);
     }
   }
-  const double inv_dtf = 1. / (fdat.dtmod * flow_dt);
+  // 1 / (dtmod flow_dt), computed on the host (every caller passes the sub-cycle dt)
+  const double inv_dtf = P.inv_dtf;
   const double mdot_total = (pmass - startmass_) * inv_dtf;
   src.mass = num_ppp * mdot_total;
   if (PELEC) {
