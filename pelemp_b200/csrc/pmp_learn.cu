@@ -1337,28 +1337,10 @@ __global__ void __launch_bounds__(BLOCK, PMP_LEARNED_MIN_BLOCKS)
           if (new_mass > 1.E-13 * kMassConv && newT < Tboil) {
             T_part = newT;
             if (NF > 1) {
-              // one reciprocal of the new mass and one of the composition sum
-              const double inv_nm = 1. / new_mass;
-              double sumY = 0.;
-#pragma unroll
-              for (int spf = 0; spf < NF; ++spf) {
-                Y_part[spf] = dmin(1., dmax(0., (Y_part[spf] * pmass + (double)mi_dot[spf] * part_dt) * inv_nm));
-                if (Y_part[spf] <= 1.E-12) {
-                  Y_part[spf] = 0.;
-                }
-                sumY += Y_part[spf];
-              }
-              const double inv_sum = 1. / sumY;
-#pragma unroll
-              for (int spf = 0; spf < NF; ++spf) {
-                Y_part[spf] *= inv_sum;
-              }
-              rho_part = mixed_rho_liquid<NF>(fdat, Y_part, T_part, cBoilT);
-            } else {
-              rho_part = rhoL(fdat, dmin(T_part, (double)cBoilT[0]), 0);
+              mixed_new_composition<NF>(Y_part, pmass, mi_dot, part_dt, new_mass);
             }
             pmass = new_mass;
-            dia_part = dcbrt_from_f(6. * pmass / (PMP_PI * rho_part));
+            mixed_rho_dia<NF>(fdat, Y_part, T_part, cBoilT, pmass, rho_part, dia_part);
           } else {
             pmass = 0.;
             id = -1;

@@ -284,6 +284,72 @@ __device__ __forceinline__ double mixed_rho_liquid(const DevFuel& fdat, const do
   return 1. / s;
 }
 
+// Liquid density and diameter after an inner sub-step (mass pmass): with
+// two fuels one FP64 division, r = 1 / (P S) with P = rhoL_0 rhoL_1 and
+// S = Y_0 rhoL_1 + Y_1 rhoL_0, giving rho = P^2 r and 1 / rho = S^2 r.
+template <int NF>
+__device__ __forceinline__ void mixed_rho_dia(const DevFuel& fdat, const double* Y, double T, const float* cBoilT,
+                                              double pmass, double& rho, double& dia)
+{
+  if (NF == 2) {
+    constexpr int f1 = NF > 1 ? 1 : 0;
+    const double r0 = rhoL(fdat, dmin(T, (double)cBoilT[0]), 0);
+    const double r1 = rhoL(fdat, dmin(T, (double)cBoilT[f1]), f1);
+    const double Pr = r0 * r1;
+    const double S = Y[0] * r1 + Y[f1] * r0;
+    const double r = 1. / (Pr * S);
+    rho = Pr * Pr * r;
+    dia = dcbrt_from_f((6. / PMP_PI) * pmass * (S * S * r));
+    return;
+  }
+  // one fuel: the density itself, as the reference's update takes it
+  // (Drag.H:396-398)
+  rho = NF == 1 ? rhoL(fdat, dmin(T, (double)cBoilT[0]), 0) : mixed_rho_liquid<NF>(fdat, Y, T, cBoilT);
+  dia = dcbrt_from_f(6. * pmass / (PMP_PI * rho));
+}
+
+// Composition after an inner sub-step (Drag.H:377-396): each fuel's mass
+// Y_f m + mdot_f dt over the new mass, clipped to [0, 1], zeroed below
+// 1e-12, renormalised.  When no clip or zeroing applies (nearly always) that
+// is a_f / sum a, one FP64 division.
+template <int NF>
+__device__ __forceinline__ void mixed_new_composition(double* Y, double pmass, const float* mi_dot, double part_dt,
+                                                      double new_mass)
+{
+  double a[NF];
+  double asum = 0.;
+  bool plain = true;
+#pragma unroll
+  for (int spf = 0; spf < NF; ++spf) {
+    a[spf] = Y[spf] * pmass + (double)mi_dot[spf] * part_dt;
+    asum += a[spf];
+    plain = plain && a[spf] > 1.E-12 * new_mass && a[spf] <= new_mass;
+  }
+  if (plain) {
+    const double inv = 1. / asum;
+#pragma unroll
+    for (int spf = 0; spf < NF; ++spf) {
+      Y[spf] = a[spf] * inv;
+    }
+    return;
+  }
+  const double inv_nm = 1. / new_mass;
+  double sumY = 0.;
+#pragma unroll
+  for (int spf = 0; spf < NF; ++spf) {
+    Y[spf] = dmin(1., dmax(0., a[spf] * inv_nm));
+    if (Y[spf] <= 1.E-12) {
+      Y[spf] = 0.;
+    }
+    sumY += Y[spf];
+  }
+  const double inv_sum = 1. / sumY;
+#pragma unroll
+  for (int spf = 0; spf < NF; ++spf) {
+    Y[spf] *= inv_sum;
+  }
+}
+
 // calculateSpraySource with FP32 physics and FP64 state (see the file header);
 // PELEC: CGS units and the drag-work and evaporated kinetic-energy terms of
 // the energy source (Drag.H:282-286, 418-421).
@@ -599,28 +665,10 @@ __device__ __forceinline__ int spray_source_mixed(
       if (new_mass > min_mass && newT < Tboil) {
         T_part = newT;
         if (NF > 1) {
-          // one reciprocal of the new mass and one of the composition sum
-          const double inv_nm = 1. / new_mass;
-          double sumY = 0.;
-#pragma unroll
-          for (int spf = 0; spf < NF; ++spf) {
-            Y_part[spf] = dmin(1., dmax(0., (Y_part[spf] * pmass + (double)mi_dot[spf] * part_dt) * inv_nm));
-            if (Y_part[spf] <= 1.E-12) {
-              Y_part[spf] = 0.;
-            }
-            sumY += Y_part[spf];
-          }
-          const double inv_sum = 1. / sumY;
-#pragma unroll
-          for (int spf = 0; spf < NF; ++spf) {
-            Y_part[spf] *= inv_sum;
-          }
-          rho_part = mixed_rho_liquid<NF>(fdat, Y_part, T_part, cBoilT);
-        } else {
-          rho_part = rhoL(fdat, dmin(T_part, (double)cBoilT[0]), 0);
+          mixed_new_composition<NF>(Y_part, pmass, mi_dot, part_dt, new_mass);
         }
         pmass = new_mass;
-        dia_part = dcbrt_from_f(6. * pmass / (PMP_PI * rho_part));
+        mixed_rho_dia<NF>(fdat, Y_part, T_part, cBoilT, pmass, rho_part, dia_part);
       } else {
         pmass = 0.;
         id = -1;
