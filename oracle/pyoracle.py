@@ -160,7 +160,7 @@ class Oracle(_Base):
         return mu[0], lam[0], Dd[:mech.nspec]
 
     def abi_sizes(self):
-        out = np.zeros(11, dtype=np.int64)
+        out = np.zeros(15, dtype=np.int64)
         self.lib.pmp_oracle_abi_sizes(out.ctypes.data)
         return out
 

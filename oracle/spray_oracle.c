@@ -1158,4 +1158,8 @@ void pmp_oracle_abi_sizes(long long* out)
   out[8] = (long long)sizeof(pmp_error_info);
   out[9] = (long long)sizeof(pmp_stats);
   out[10] = (long long)sizeof(pmp_mech);
+  out[11] = (long long)sizeof(pmp_launch_config);
+  out[12] = (long long)sizeof(pmp_tune_report);
+  out[13] = (long long)sizeof(pmp_learn_config);
+  out[14] = (long long)sizeof(pmp_learn_report);
 }

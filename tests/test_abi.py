@@ -35,7 +35,8 @@ def test_struct_sizes_match_c(oracle):
     sizes = oracle.abi_sizes()
     mirror = [capi.Geometry, capi.Box, capi.BoxView, capi.SprayComps, capi.SprayData,
               capi.SprayInputs, capi.Particles, capi.SprayConfig, capi.ErrorInfo, capi.Stats,
-              capi.Mech]
+              capi.Mech, capi.LaunchConfig, capi.TuneReport, capi.LearnConfig, capi.LearnReport]
+    assert len(sizes) == len(mirror)
     for s, m in zip(sizes, mirror):
         assert s == C.sizeof(m), m.__name__
 
