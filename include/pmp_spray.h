@@ -582,6 +582,19 @@ int pmp_learn_debug_infer_tc(const float* params, const float* xn, int n,
  * (as it must), with the cycles it waited; the device stays usable. */
 int pmp_learn_debug_wait_timeout(long long* cycles);
 int pmp_learn_param_count(void);
+/* Number of terms of the targets' baseline polynomial (per output). */
+int pmp_learn_base_terms(void);
+/* Host evaluation of the baseline (no GPU): its terms feats[base_terms] for
+ * normalised inputs xn[10] and the derived variables ell = ln(1 + B_M) and
+ * g = (1 + c Re)^(1/3) - 2, and the polynomial with coefficients
+ * coef[base_terms] in FP32 as the kernels evaluate it. */
+int pmp_learn_debug_base(const float* xn, float ell, float g, const float* coef,
+                         double* feats, float* value);
+/* Host solve of the baseline fit (no GPU): acc holds the normal equations
+ * (the upper triangle of F^T F row by row, then F^T Y row by row, F the
+ * terms, Y the 5 targets); coef[5][base_terms] receives the ridge least
+ * squares coefficients. */
+int pmp_learn_debug_solve_baseline(const double* acc, float* coef);
 
 /* ---------------------------------------------------------------------------
  * Measured compute peaks of a device (no counterpart in the reference): the

@@ -1,4 +1,5 @@
-"""CPU oracle of the learned form's network and its training gradient.
+"""CPU oracle of the learned form's network, its training gradient and the
+targets' baseline polynomial.
 
 Test infrastructure: only the tests use this module, to check the
 GPU training kernels (pmp_learn_debug_grad) and of the tensor-core inference.
@@ -143,3 +144,43 @@ def infer(p, xn):
     A = silu_bf16(A @ bf16_round(w["W3"]).T + w["b3"])
     Y = A @ bf16_round(w["W4"]).T + w["b4"]
     return Y[:, :N_OUT]
+
+
+# --- the targets' baseline (learn_common.cuh base_features / learn_base,
+# pmp_learn.cu solve_baseline): a polynomial in the normalised inputs whose
+# residual the network predicts.  Terms, in the library's order: 1; the
+# quadratic inputs z = xn[0, 1, 2, 6, 7, 8, 9]; the linear-only inputs
+# xn[3, 4, 5]; ell, ell^2; g, g^2; g z_i; z_i z_j (i <= j, row by row).
+BASE_Q = (0, 1, 2, 6, 7, 8, 9)
+BASE_L = (3, 4, 5)
+BASE_TERMS = 1 + len(BASE_Q) + len(BASE_L) + 2 + 2 + len(BASE_Q) + len(BASE_Q) * (len(BASE_Q) + 1) // 2
+
+
+def base_features(xn, ell, g):
+    """Terms of the baseline, float64 (rows of xn: droplets)."""
+    xn = np.atleast_2d(np.asarray(xn, np.float64))
+    ell = np.atleast_1d(np.asarray(ell, np.float64))
+    g = np.atleast_1d(np.asarray(g, np.float64))
+    z = xn[:, BASE_Q]
+    cols = [np.ones(len(xn))] + [z[:, i] for i in range(z.shape[1])] + [xn[:, i] for i in BASE_L]
+    cols += [ell, ell * ell, g, g * g] + [g * z[:, i] for i in range(z.shape[1])]
+    cols += [z[:, i] * z[:, j] for i in range(z.shape[1]) for j in range(i, z.shape[1])]
+    return np.array(cols).T
+
+
+def normal_equations(F, Y):
+    """The library's accumulator layout: the upper triangle of F^T F row by
+    row, then F^T Y row by row."""
+    G = F.T @ F
+    R = F.T @ Y
+    tri = np.concatenate([G[a, a:] for a in range(G.shape[0])])
+    return np.concatenate([tri, R.reshape(-1)])
+
+
+def solve_baseline(F, Y):
+    """Ridge least squares as the library solves it: 1e-10 of each feature's
+    diagonal plus 1e-14 of the largest diagonal."""
+    G = F.T @ F
+    d = np.diag(G).copy()
+    G = G + np.diag(1e-10 * d + 1e-14 * d.max())
+    return np.linalg.solve(G, F.T @ Y).T

@@ -1818,7 +1818,9 @@ extern "C" int pmp_spray_learn_tuples(const pmp_spray* h, float* buf, long long*
   return PMP_OK;
 }
 
-// Least-squares fit of the targets' quadratic baseline (LearnNorm::base) on
+static bool solve_baseline(const double* acc, LearnNorm& nrm);
+
+// Least-squares fit of the targets' polynomial baseline (LearnNorm::base) on
 // the tuples, with the input normalisation already in nrm: FP64 normal
 // equations over at most 8M tuples (k_base_normal), a ridge of 1e-10 of each
 // feature's diagonal (features that never vary get no weight), Cholesky on
@@ -1835,9 +1837,14 @@ static bool fit_baseline(LearnState* L, long long n, LearnNorm& nrm)
   std::vector<double> acc(kBaseEntries);
   const bool ok = cudaMemcpy(acc.data(), d_acc, sizeof(double) * kBaseEntries, cudaMemcpyDeviceToHost) == cudaSuccess;
   cudaFree(d_acc);
-  if (!ok) {
-    return false;
-  }
+  return ok && solve_baseline(acc.data(), nrm);
+}
+
+// The baseline's coefficients from the accumulated normal equations acc
+// (k_base_normal's layout: the upper triangle of F^T F row by row, then
+// F^T Y row by row): ridge and Cholesky in FP64 on the host.
+static bool solve_baseline(const double* acc, LearnNorm& nrm)
+{
   constexpr int T = kBaseTerms;
   std::vector<double> G(T * T), R(T * kLearnOut);
   int e = 0;
@@ -2200,6 +2207,46 @@ extern "C" int pmp_learn_debug_grad(
 }
 
 extern "C" int pmp_learn_param_count(void) { return kP_N; }
+
+extern "C" int pmp_learn_base_terms(void) { return kBaseTerms; }
+
+// Host instantiation of the baseline's term layout and its FP32 nested
+// evaluation (the code the kernels run): feats[kBaseTerms] for normalised
+// inputs xn[10] and the derived variables (ell, g); value = the polynomial
+// with coefficients coef[kBaseTerms].  No GPU needed.
+extern "C" int pmp_learn_debug_base(const float* xn, float ell, float g, const float* coef, double* feats,
+                                    float* value)
+{
+  if (!xn || !coef || !feats || !value) {
+    return PMP_ERR_INVALID;
+  }
+  BaseVars v;
+  v.ell = ell;
+  v.g = g;
+  base_features(xn, v, feats);
+  LearnNorm nrm;
+  memset(&nrm, 0, sizeof(nrm));
+  memcpy(nrm.base[0], coef, sizeof(float) * kBaseTerms);
+  *value = learn_base(nrm, 0, xn, v);
+  return PMP_OK;
+}
+
+// The host solve of the baseline fit: acc[kBaseTerms (kBaseTerms + 1) / 2 +
+// 5 kBaseTerms] in k_base_normal's layout (upper triangle of F^T F row by
+// row, then F^T Y row by row) -> coef[5][kBaseTerms].  No GPU needed.
+extern "C" int pmp_learn_debug_solve_baseline(const double* acc, float* coef)
+{
+  if (!acc || !coef) {
+    return PMP_ERR_INVALID;
+  }
+  LearnNorm nrm;
+  memset(&nrm, 0, sizeof(nrm));
+  if (!solve_baseline(acc, nrm)) {
+    return PMP_ERR_INVALID;
+  }
+  memcpy(coef, nrm.base, sizeof(float) * kLearnOut * kBaseTerms);
+  return PMP_OK;
+}
 
 namespace {
 

@@ -78,6 +78,9 @@ _SIGS = {
     "pmp_learn_debug_infer_tc": [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p],
     "pmp_learn_debug_wait_timeout": [C.POINTER(C.c_longlong)],
     "pmp_learn_param_count": [],
+    "pmp_learn_base_terms": [],
+    "pmp_learn_debug_base": [C.c_void_p, C.c_float, C.c_float, C.c_void_p, C.c_void_p, C.POINTER(C.c_float)],
+    "pmp_learn_debug_solve_baseline": [C.c_void_p, C.c_void_p],
     "pmp_measure_peaks": [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)],
 }
 
@@ -429,6 +432,39 @@ class SprayParticleContainer:
 
 def learn_param_count():
     return lib().pmp_learn_param_count()
+
+
+def learn_base_terms():
+    return lib().pmp_learn_base_terms()
+
+
+def learn_debug_base(xn, ell, g, coef):
+    """(terms, value): the baseline's terms for normalised inputs xn[10] and
+    derived variables ell, g, and the FP32 polynomial with coefficients coef,
+    from the library's host code (no GPU)."""
+    nt = learn_base_terms()
+    xn = np.ascontiguousarray(xn, np.float32)
+    coef = np.ascontiguousarray(coef, np.float32)
+    assert xn.size == capi.LEARN_IN and coef.size == nt
+    feats = np.zeros(nt)
+    val = C.c_float(0.0)
+    rc = lib().pmp_learn_debug_base(xn.ctypes.data, float(ell), float(g), coef.ctypes.data,
+                                    feats.ctypes.data, C.byref(val))
+    if rc != capi.PMP_OK:
+        raise SprayError(rc)
+    return feats, val.value
+
+
+def learn_debug_solve_baseline(acc):
+    """coef[5, terms] from the normal equations in k_base_normal's layout (no GPU)."""
+    nt = learn_base_terms()
+    acc = np.ascontiguousarray(acc, np.float64)
+    assert acc.size == nt * (nt + 1) // 2 + nt * capi.LEARN_OUT
+    coef = np.zeros((capi.LEARN_OUT, nt), np.float32)
+    rc = lib().pmp_learn_debug_solve_baseline(acc.ctypes.data, coef.ctypes.data)
+    if rc != capi.PMP_OK:
+        raise SprayError(rc)
+    return coef
 
 
 def learn_debug_grad(params, x, y, quant=True):

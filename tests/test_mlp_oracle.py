@@ -1,6 +1,8 @@
 """The learned form's CPU oracle (oracle/mlp_oracle.py): gradient against
-central differences, bf16 rounding against known values, and the parameter
-layout against the library's count (no GPU call)."""
+central differences, bf16 rounding against known values, the parameter
+layout against the library's count, and the library's host code of the
+targets' baseline (terms, nested evaluation, ridge solve) against the
+oracle's restatement (no GPU call)."""
 import numpy as np
 
 from oracle import mlp_oracle as M
@@ -67,3 +69,42 @@ def test_quantised_forward_is_close_to_fp64():
     scale = np.sqrt(np.mean(a * a))
     assert np.sqrt(np.mean((a - b) ** 2)) < 2e-2 * scale
     assert np.sqrt(np.mean((b - c) ** 2)) < 1e-2 * scale
+
+
+def test_baseline_terms_and_nested_evaluation():
+    """The library's host code of the targets' baseline (the code the kernels
+    run): its terms equal the oracle's restatement exactly, and its FP32
+    nested evaluation equals the dense polynomial within FP32 rounding."""
+    from pelemp_b200.spray import learn_base_terms, learn_debug_base
+    assert learn_base_terms() == M.BASE_TERMS
+    rng = np.random.default_rng(5)
+    for _ in range(20):
+        xn = rng.standard_normal(M.N_IN).astype(np.float32)
+        ell = np.float32(rng.uniform(0, 3))
+        g = np.float32(rng.uniform(-1, 3))
+        coef = rng.standard_normal(M.BASE_TERMS).astype(np.float32)
+        feats, value = learn_debug_base(xn, ell, g, coef)
+        want = M.base_features(xn.astype(np.float64), float(ell), float(g))[0]
+        assert np.array_equal(feats, want)
+        dense = float(want @ coef.astype(np.float64))
+        assert abs(value - dense) <= 1e-6 * float(np.abs(want * coef).sum())
+
+
+def test_baseline_solve_matches_numpy():
+    """The library's host solve of the baseline fit, from normal equations in
+    the accumulator layout of its GPU kernel, against numpy's ridge solve."""
+    from pelemp_b200.spray import learn_debug_solve_baseline
+    rng = np.random.default_rng(6)
+    n = 20000
+    xn = rng.standard_normal((n, M.N_IN))
+    xn[:, 5] = 0.0   # a feature that never varies (one fuel) gets no weight
+    ell = rng.uniform(0, 3, n)
+    g = rng.uniform(-1, 3, n)
+    F = M.base_features(xn, ell, g)
+    true = rng.standard_normal((M.N_OUT, M.BASE_TERMS))
+    true[:, 1 + len(M.BASE_Q) + 2] = 0.0
+    Y = F @ true.T + 1e-3 * rng.standard_normal((n, M.N_OUT))
+    coef = learn_debug_solve_baseline(M.normal_equations(F, Y))
+    want = M.solve_baseline(F, Y)
+    assert np.max(np.abs(coef - want)) <= 1e-5 * np.max(np.abs(want))
+    assert np.max(np.abs(coef - true)) <= 1e-3
