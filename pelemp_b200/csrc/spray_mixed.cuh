@@ -222,7 +222,14 @@ __device__ __forceinline__ float heat_coeff_f(float ratio, float B_M, float Nu_0
   float B_T = fexp(phi * lnBM1) - 1.f;
   float error = fabsf(B_T - B_T_old);
   int k = 0;
-  while (k < 100 && error > fmaxf(1e-7f, 8.f * 1.1920929e-7f * fabsf(B_T))) {
+  // B_T = exp(x) - 1 in FP32 lies on a grid of one ulp of 1 + B_T (1.2e-7
+  // below 1), coarser than the 1e-7 tolerance for small B_T: there the
+  // iterates can settle into a 1-ulp two-cycle that never meets it.  The
+  // loop also stops when the change stops shrinking (the FP32 noise floor
+  // of a contracting iteration) instead of running to 100 iterations.
+  float prev_error = 3.4e38f;
+  while (k < 100 && error > fmaxf(1e-7f, 8.f * 1.1920929e-7f * fabsf(B_T)) && error < prev_error) {
+    prev_error = error;
     B_T_old = B_T;
     flog1p_pow07(B_T, logB, p07);
     invFT = fdiv(B_T, logB * p07);
