@@ -301,8 +301,9 @@ def compute_roofline(form, peaks):
            "pipes_source": "ncu capture of the same kernel: one MKD launch of 2M droplets at config-2 density "
                            "(sm__inst_executed_pipe_*.avg.pct_of_peak_sustained_active, "
                            "smsp__issue_active, sm__pipe_tensor_cycles_active), taken before the FP64 "
-                           "divisions of the FP32 forms' state update were cut (their MKD launch is 7 % "
-                           "shorter since)"}
+                           "divisions of the FP32 forms' state update were cut and the mixed form's B_T "
+                           "fixed point stopped at its noise floor (the mixed MKD launch is 17 % shorter "
+                           "since)"}
     if peaks is not None:
         out["peaks"] = peaks
         out["peaks_source"] = ("pmp_measure_peaks on this GPU: loop kernels of independent DFMA, FFMA and "
